@@ -1,0 +1,323 @@
+"""Seeded synthetic ROMS-like grids and particle releases.
+
+No ROMS output is available offline, so every workload here runs on a
+synthetic grid with the construction below (the same one for every size):
+
+* rho grid ``nx x ny``, ``dx = dy = 2 km`` (constant static fields);
+* bathymetry ``h = 50 + 950 G`` with ``G`` a Gaussian-filtered random field
+  (sigma ~ 8 cells) normalised to [0, 1], clipped to [50, 1000] m;
+* land: one contiguous blob of ~10 % of the cells (a disc around a seeded
+  point, its edge perturbed by a smooth field); velocities are zero on masked
+  faces, as ROMS writes them;
+* ``zeta = 0.5 sin(2 pi t / 12.42 h)``, uniform in space;
+* ``C = Cs_r`` from the published ROMS ``Vstretching = 4`` formula with
+  ``theta_s = 5``, ``theta_b = 0.4``, ``hc = 20 m`` (``Vtransform = 2`` is what
+  the reference's vertical coordinate implements);
+* ``u, v`` from a streamfunction of 16 seeded Fourier modes plus a weak
+  potential-flow part, with a decaying vertical profile, scaled to 0.5 m/s rms
+  and modulated in time;
+* ``w`` from continuity on the sigma layers, zero at the bottom (~1e-4 m/s).
+
+Snapshots are produced lazily and deterministically from (seed, snapshot
+index), so an object of this module can stand in for a ``(t, z, y, x)`` array:
+it exposes ``shape``, ``ndim``, ``dtype`` and ``__getitem__(it)``.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import functools
+
+import numpy as np
+
+HOUR = 3600.0
+M2_PERIOD = 12.42 * HOUR
+
+
+def vstretching4(nz: int, theta_s: float = 5.0, theta_b: float = 0.4, *, w_levels: bool = False) -> np.ndarray:
+    """ROMS Vstretching = 4 stretching function at rho (or w) levels."""
+    if w_levels:
+        sc = (np.arange(nz + 1, dtype=np.float64) - nz) / nz
+    else:
+        sc = (np.arange(nz, dtype=np.float64) + 0.5) / nz - 1.0
+    if theta_s > 0:
+        csur = (1.0 - np.cosh(theta_s * sc)) / (np.cosh(theta_s) - 1.0)
+    else:
+        csur = -(sc**2)
+    if theta_b > 0:
+        return (np.exp(theta_b * csur) - 1.0) / (1.0 - np.exp(-theta_b))
+    return csur
+
+
+def _smooth_field(rng: np.random.Generator, ny: int, nx: int, sigma: float) -> np.ndarray:
+    """Gaussian-filtered white noise (periodic FFT filter), normalised to [0, 1]."""
+    noise = rng.standard_normal((ny, nx))
+    ky = np.fft.fftfreq(ny)[:, None]
+    kx = np.fft.rfftfreq(nx)[None, :]
+    filt = np.exp(-2.0 * (np.pi * sigma) ** 2 * (kx**2 + ky**2))
+    g = np.fft.irfft2(np.fft.rfft2(noise) * filt, s=(ny, nx))
+    g -= g.min()
+    g /= max(g.max(), 1e-300)
+    return g
+
+
+@dataclasses.dataclass(frozen=True)
+class GridSpec:
+    nx: int
+    ny: int
+    nz: int
+    nt: int
+    seed: int
+    dtype: str = "float64"
+    dx: float = 2000.0
+    hc: float = 20.0
+    theta_s: float = 5.0
+    theta_b: float = 0.4
+    land_fraction: float = 0.10
+    snapshot_interval: float = HOUR
+
+
+class _LazyField:
+    """(t, ...) array-like over the snapshots of one time-dependent field."""
+
+    def __init__(self, grid: "SyntheticROMS", name: str, spatial_shape: tuple[int, ...]) -> None:
+        self._grid = grid
+        self._name = name
+        self.shape = (grid.spec.nt,) + spatial_shape
+        self.ndim = len(self.shape)
+        self.dtype = grid.dtype
+
+    def __len__(self) -> int:
+        return self.shape[0]
+
+    def __getitem__(self, key):
+        if isinstance(key, tuple):
+            it, rest = key[0], key[1:]
+        else:
+            it, rest = key, ()
+        if isinstance(it, (int, np.integer)):
+            snap = self._grid.snapshot(int(it))[self._name]
+            return snap[rest] if rest and rest != (Ellipsis,) else snap
+        if isinstance(it, slice):
+            idx = range(*it.indices(self.shape[0]))
+            out = np.stack([self._grid.snapshot(i)[self._name] for i in idx])
+            return out[(slice(None),) + rest] if rest and rest != (Ellipsis,) else out
+        raise TypeError(f"unsupported index {key!r}")
+
+    def __array__(self, dtype=None, copy=None):
+        out = self[0 : self.shape[0]]
+        return out.astype(dtype) if dtype is not None else out
+
+
+class SyntheticROMS:
+    """A seeded synthetic ROMS grid; see the module docstring."""
+
+    def __init__(self, spec: GridSpec) -> None:
+        self.spec = spec
+        self.dtype = np.dtype(spec.dtype)
+        nx, ny, nz = spec.nx, spec.ny, spec.nz
+        rng = np.random.default_rng(spec.seed)
+        self.time_array = np.arange(spec.nt, dtype=np.float64) * spec.snapshot_interval
+
+        # bathymetry
+        g = _smooth_field(rng, ny, nx, sigma=8.0)
+        self.h64 = np.clip(50.0 + 950.0 * g, 50.0, 1000.0)
+
+        # land: perturbed disc around a seeded point covering ~land_fraction
+        cy, cx = rng.uniform(0.2, 0.8) * ny, rng.uniform(0.2, 0.8) * nx
+        yy, xx = np.meshgrid(np.arange(ny, dtype=np.float64), np.arange(nx, dtype=np.float64), indexing="ij")
+        d = np.hypot(yy - cy, xx - cx)
+        r0 = np.sqrt(spec.land_fraction * nx * ny / np.pi)
+        d = d + 0.35 * r0 * (_smooth_field(rng, ny, nx, sigma=12.0) - 0.5)
+        thresh = np.quantile(d, spec.land_fraction)
+        self.mask_rho = (d > thresh).astype(np.float64)  # 1 = wet
+
+        # vertical
+        self.C64 = vstretching4(nz, spec.theta_s, spec.theta_b)
+        self.Cw64 = vstretching4(nz, spec.theta_s, spec.theta_b, w_levels=True)
+        self.sigma_w = (np.arange(nz + 1, dtype=np.float64) - nz) / nz
+
+        # flow modes: 16 streamfunction modes + 4 weak potential modes
+        nm = 16
+        L = rng.uniform(25.0, 150.0, nm)  # wavelength in cells
+        ang = rng.uniform(0, 2 * np.pi, nm)
+        self._k = 2 * np.pi / L * np.cos(ang)
+        self._l = 2 * np.pi / L * np.sin(ang)
+        self._phi = rng.uniform(0, 2 * np.pi, nm)
+        self._omega = 2 * np.pi / (rng.uniform(1.0, 6.0, nm) * 86400.0) * rng.choice([-1.0, 1.0], nm)
+        self._amp = rng.uniform(0.5, 1.0, nm) / np.sqrt(nm)
+        npm = 4
+        Lp = rng.uniform(40.0, 120.0, npm)
+        angp = rng.uniform(0, 2 * np.pi, npm)
+        self._kp = 2 * np.pi / Lp * np.cos(angp)
+        self._lp = 2 * np.pi / Lp * np.sin(angp)
+        self._phip = rng.uniform(0, 2 * np.pi, npm)
+        self._ampp = rng.uniform(0.5, 1.0, npm) / np.sqrt(npm) * 0.02
+        self._prof = 0.4 + 0.6 * np.exp((np.arange(nz) + 0.5 - nz) / (0.4 * nz))  # surface-intensified
+        self._scale = None
+        self._cache: dict[int, dict[str, np.ndarray]] = {}
+        self._cache_order: list[int] = []
+        self.max_cached = 3
+
+    # ---------------------------------------------------------------- static
+    @functools.cached_property
+    def h(self) -> np.ndarray:
+        return self.h64.astype(self.dtype)
+
+    @functools.cached_property
+    def dx(self) -> np.ndarray:
+        return np.full((self.spec.ny, self.spec.nx), self.spec.dx, dtype=self.dtype)
+
+    @functools.cached_property
+    def dy(self) -> np.ndarray:
+        return np.full((self.spec.ny, self.spec.nx), self.spec.dx, dtype=self.dtype)
+
+    @property
+    def C(self) -> np.ndarray:
+        return self.C64.copy()
+
+    @property
+    def hc(self) -> float:
+        return self.spec.hc
+
+    # ------------------------------------------------------------- dynamics
+    def zeta_value(self, t: float) -> float:
+        return 0.5 * np.sin(2 * np.pi * t / M2_PERIOD)
+
+    @functools.cached_property
+    def _taper(self) -> tuple[np.ndarray, np.ndarray]:
+        """Smooth [0, 1] coastal taper at rho points and at cell corners (0 on land)."""
+        ny, nx = self.spec.ny, self.spec.nx
+        m = self.mask_rho
+        ky = np.fft.fftfreq(ny)[:, None]
+        kx = np.fft.rfftfreq(nx)[None, :]
+        filt = np.exp(-2.0 * (np.pi * 4.0) ** 2 * (kx**2 + ky**2))
+        blur = np.fft.irfft2(np.fft.rfft2(m) * filt, s=(ny, nx))
+        rho = np.clip((blur - 0.5) * 2.0, 0.0, 1.0) ** 2 * m
+        pad = np.pad(rho, 1, mode="edge")
+        corner = 0.25 * (pad[:-1, :-1] + pad[1:, :-1] + pad[:-1, 1:] + pad[1:, 1:])  # (ny+1, nx+1)
+        corner = np.minimum(corner, np.minimum.reduce([pad[:-1, :-1], pad[1:, :-1], pad[:-1, 1:], pad[1:, 1:]]) + 0.0)
+        return rho, corner
+
+    def _uv_full(self, t: float) -> tuple[np.ndarray, np.ndarray]:
+        """Depth-independent velocity on ALL faces (unscaled): u (ny, nx+1), v (ny+1, nx).
+
+        Face u[:, i] sits at x = i - 0.5 and v[j, :] at y = j - 0.5.  The
+        rotational part is the discrete curl of a corner streamfunction tapered
+        to zero at the coast, so it is exactly divergence-free on the C grid;
+        the weak potential part carries all of the divergence.
+        """
+        nx, ny = self.spec.nx, self.spec.ny
+        yc = np.arange(ny + 1, dtype=np.float64)[:, None] - 0.5
+        xc = np.arange(nx + 1, dtype=np.float64)[None, :] - 0.5
+        psi = np.zeros((ny + 1, nx + 1))
+        for m in range(self._k.size):
+            ph = self._phi[m] + self._omega[m] * t
+            psi += self._amp[m] * np.cos(self._k[m] * xc + self._l[m] * yc + ph)
+        rho_t, corner_t = self._taper
+        psi *= corner_t
+        u = -(psi[1:, :] - psi[:-1, :])  # (ny, nx+1)
+        v = psi[:, 1:] - psi[:, :-1]  # (ny+1, nx)
+        # potential part, tapered on faces
+        yu = np.arange(ny, dtype=np.float64)[:, None]
+        xu = np.arange(nx + 1, dtype=np.float64)[None, :] - 0.5
+        yv = np.arange(ny + 1, dtype=np.float64)[:, None] - 0.5
+        xv = np.arange(nx, dtype=np.float64)[None, :]
+        pad = np.pad(rho_t, ((0, 0), (1, 1)), mode="edge")
+        tu = np.minimum(pad[:, :-1], pad[:, 1:])
+        pad = np.pad(rho_t, ((1, 1), (0, 0)), mode="edge")
+        tv = np.minimum(pad[:-1, :], pad[1:, :])
+        for m in range(self._kp.size):
+            a = self._ampp[m]
+            u += -a * self._kp[m] * np.sin(self._kp[m] * xu + self._lp[m] * yu + self._phip[m]) * tu
+            v += -a * self._lp[m] * np.sin(self._kp[m] * xv + self._lp[m] * yv + self._phip[m]) * tv
+        mod = 1.0 + 0.2 * np.sin(2 * np.pi * t / 86400.0)
+        return u * mod, v * mod
+
+    def _velocity_scale(self) -> float:
+        if self._scale is None:
+            u, v = self._uv_full(0.0)
+            wet = self.mask_rho > 0
+            um = u[:, 1:-1][wet[:, :-1] & wet[:, 1:]]
+            vm = v[1:-1, :][wet[:-1, :] & wet[1:, :]]
+            rms = np.sqrt(0.5 * (np.mean(um**2) + np.mean(vm**2)))
+            self._scale = 0.5 / max(rms, 1e-300)
+        return self._scale
+
+    def snapshot(self, it: int) -> dict[str, np.ndarray]:
+        """u, v, w, zeta of snapshot ``it`` in the storage dtype."""
+        if it < 0 or it >= self.spec.nt:
+            raise IndexError(it)
+        if it in self._cache:
+            return self._cache[it]
+        t = float(self.time_array[it])
+        s = self._velocity_scale()
+        uf, vf = self._uv_full(t)
+        uf *= s
+        vf *= s
+        prof = self._prof
+        u = (prof[:, None, None] * uf[None, :, 1:-1]).astype(self.dtype)
+        v = (prof[:, None, None] * vf[None, 1:-1, :]).astype(self.dtype)
+
+        # continuity: w(k+1) = w(k) - div(k) Hz(k), w(0) = 0 (bottom)
+        ny, nx = self.spec.ny, self.spec.nx
+        div = ((uf[:, 1:] - uf[:, :-1]) + (vf[1:, :] - vf[:-1, :])) / self.spec.dx
+        zeta = self.zeta_value(t)
+        hc, h = self.spec.hc, self.h64
+        Sw = (hc * self.sigma_w[:, None, None] + h[None] * self.Cw64[:, None, None]) / (hc + h)[None]
+        Hz = (zeta + h)[None] * np.diff(Sw, axis=0)  # (nz, ny, nx)
+        cum = np.concatenate([np.zeros((1, ny, nx)), np.cumsum(prof[:, None, None] * Hz, axis=0)], axis=0)
+        w = (-div[None] * cum * self.mask_rho[None]).astype(self.dtype)
+        zeta_arr = np.full((ny, nx), zeta, dtype=self.dtype)
+        snap = {"u": u, "v": v, "w": w, "zeta": zeta_arr}
+        self._cache[it] = snap
+        self._cache_order.append(it)
+        while len(self._cache_order) > self.max_cached:
+            self._cache.pop(self._cache_order.pop(0), None)
+        return snap
+
+    # ------------------------------------------------------------ accessors
+    def field(self, name: str) -> _LazyField:
+        nz, ny, nx = self.spec.nz, self.spec.ny, self.spec.nx
+        shapes = {"u": (nz, ny, nx - 1), "v": (nz, ny - 1, nx), "w": (nz + 1, ny, nx), "zeta": (ny, nx)}
+        return _LazyField(self, name, shapes[name])
+
+    def dense(self, name: str) -> np.ndarray:
+        """All snapshots of a time-dependent field as one array (small grids only)."""
+        return np.asarray(self.field(name))
+
+    def release(self, n: int, seed: int | None = None) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """``n`` particles uniform in wet cells, at uniform random sigma levels.
+
+        Returns (zidx, yidx, xidx) float64 arrays in centred index space.
+        """
+        rng = np.random.default_rng(self.spec.seed * 7919 + 17 if seed is None else seed)
+        wet = np.flatnonzero(self.mask_rho.ravel() > 0)
+        cells = wet[rng.integers(0, wet.size, n)]
+        j, i = np.divmod(cells, self.spec.nx)
+        y = np.clip(j + rng.uniform(-0.5, 0.5, n), 0.0, self.spec.ny - 1.0)
+        x = np.clip(i + rng.uniform(-0.5, 0.5, n), 0.0, self.spec.nx - 1.0)
+        z = rng.uniform(0.0, self.spec.nz - 1.0, n)
+        return z, y, x
+
+    def oracle_fields(self) -> dict[str, np.ndarray]:
+        """Dense field dict (u, v, w, zeta with a time axis; h, dx, dy, C)."""
+        out = {name: self.dense(name) for name in ("u", "v", "w", "zeta")}
+        out.update(h=self.h, dx=self.dx, dy=self.dy, C=self.C)
+        return out
+
+
+# The workloads: grid, snapshots, particles, scheme, dt (seconds).
+CONFIGS = {
+    "config1": dict(grid=GridSpec(nx=128, ny=96, nz=20, nt=26, seed=1, dtype="float64"),
+                    particles=10_000, scheme="rk2", dt=300.0, steps=288),
+    "config2": dict(grid=GridSpec(nx=1024, ny=768, nz=50, nt=170, seed=2, dtype="float32"),
+                    particles=4_194_304, scheme="ab3", dt=120.0, steps=5040),
+}
+
+
+def make_grid(name: str, **overrides) -> SyntheticROMS:
+    spec = CONFIGS[name]["grid"]
+    if overrides:
+        spec = dataclasses.replace(spec, **overrides)
+    return SyntheticROMS(spec)
