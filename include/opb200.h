@@ -1,0 +1,190 @@
+/*
+ * opb200.h -- C ABI of liboffline_particles_b200.so, the B200 (sm_100a)
+ * implementation of offline_particles' ROMS particle-advection hot path.
+ *
+ * Reference interface.  In offline_particles every particle kernel is a
+ * ParticleKernel wrapping  fn(particles, scalars, fielddata) -> None  that
+ * mutates the particle arrays in place (kernels/_kernels.py:12,22-44,85-93);
+ * Launcher.launch_kernel builds `scalars` and `fielddata` and calls it
+ * (launcher.py:167-174).  Each entry point below is the device-side
+ * replacement of one such function, with the same three arguments as plain C
+ * structs:
+ *   particles -> opb_particles  (device SoA, Particles / particles.py:76-92)
+ *   scalars   -> opb_scalars    (hc, NZ, _dt, _RK2_alpha, *idx_min/max)
+ *   fielddata -> opb_roms_fields + opb_time (FieldData(array, offsets) of
+ *                fields.py:12 with the time blend of fields.py:394-430 left
+ *                unmaterialised: the kernels blend each gathered corner)
+ * All pointers in these structs are DEVICE pointers; `stream` is a
+ * cudaStream_t (NULL = legacy default stream).  Every call is asynchronous.
+ *
+ * Return value: 0 on success, otherwise an OPB_E* code; opb_last_error()
+ * then describes the failure.  Per-particle problems are not errors: as in
+ * the reference they become status codes (kernels/status.pxd:1-14).  A zero
+ * grid spacing in a velocity division -- ZeroDivisionError in the reference
+ * (Cython cdivision=False) -- sets OPB_ERRF_ZERO_DIVISION in *particles->err
+ * on the device; the host reads that word when it synchronises.
+ *
+ * Numerics: float64 arithmetic in the reference's operation order with no
+ * FMA contraction, so results are bit-identical to the reference's x86-64
+ * build on the same inputs.
+ */
+#ifndef OPB200_H
+#define OPB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OPB_ABI_VERSION 1
+#define OPB_MAX_SLOTS 8
+
+/* storage dtypes of time-dependent fields */
+#define OPB_F64 0
+#define OPB_F32 1
+
+/* return codes */
+#define OPB_OK 0
+#define OPB_EINVAL 1  /* bad argument (sizes, dtype, NULL pointer, slot index) */
+#define OPB_ECUDA 2   /* a CUDA runtime call failed */
+
+/* bits of the device error word (opb_particles.err) */
+#define OPB_ERRF_ZERO_DIVISION 1u
+
+/* particle status codes: kernels/status.pxd:1-14 */
+#define OPB_STATUS_INACTIVE 0x80
+#define OPB_STATUS_NORMAL 0x00
+#define OPB_STATUS_NONFINITE 0x81
+#define OPB_STATUS_OUT_OF_DOMAIN 0x82
+#define OPB_STATUS_MULTISTEP_1 10
+#define OPB_STATUS_MULTISTEP_2 11
+
+/* A field: FieldData(array, offsets) of fields.py:12.
+ * Time-dependent fields (is_static == 0) give the device snapshot buffers
+ * `data[0..nslots-1]` in storage dtype `dtype`; an opb_time picks the two
+ * snapshots and the blend weights.  Static fields (is_static == 1) give one
+ * float64 buffer in data[0] (the reference casts every field to float64,
+ * kernels/_core.pyx:5-24).  Arrays are C-contiguous over the `ndim` active
+ * dimensions (slowest first); `offset` is added to the particle index of each
+ * active dimension (spatial_arrays.py:29-41,224-225). */
+typedef struct {
+    const void *data[OPB_MAX_SLOTS];
+    int32_t dtype;
+    int32_t ndim;
+    int64_t shape[3];
+    double offset[3];
+    int32_t is_static;
+    int32_t nslots;
+} opb_field;
+
+/* The simulation fields of the ROMS w-advection kernels
+ * (kernels/roms/rk2_w_advection.pyx:386-395, ab3_w_advection.pyx:265-274). */
+typedef struct {
+    opb_field u, v, w, dx, dy, h, zeta, C;
+} opb_roms_fields;
+
+/* Time selection for one launch: It, ft = divmod(time_index, 1)
+ * (fields.py:409-424).  prev/next are slot indices of snapshots It and It+1;
+ * ft and gt = 1 - ft are already rounded to the storage dtype. */
+typedef struct {
+    int32_t prev, next;
+    double ft, gt;
+} opb_time;
+
+/* Particle SoA (kernels/_kernels.py:14-19 plus the kernels' own fields).
+ * RK2 uses k1 = (dxidx1, dyidx1, dz1) and k2 = (dxidx2, dyidx2, dz2)
+ * (rk2_w_advection.pyx:377-410); AB3 uses the 0/1/2 history
+ * (ab3_w_advection.pyx:250-258).  Unused pointers may be NULL. */
+typedef struct {
+    int64_t n;
+    uint8_t *status;
+    double *zidx, *yidx, *xidx, *z;
+    double *dxidx0, *dyidx0, *dz0;
+    double *dxidx1, *dyidx1, *dz1;
+    double *dxidx2, *dyidx2, *dz2;
+    uint32_t *err; /* device error word (OPB_ERRF_*), may be NULL */
+} opb_particles;
+
+/* Scalars the ROMS kernels declare (rk2_w_advection.pyx:382-385,412-417;
+ * validation.pyx:113-120): hc, NZ, _dt, _RK2_alpha, zidx/yidx/xidx min/max. */
+typedef struct {
+    double hc;
+    int32_t NZ;
+    int32_t _pad;
+    double dt;
+    double alpha;
+    double bounds[6]; /* zmin, zmax, ymin, ymax, xmin, xmax */
+} opb_scalars;
+
+/* ---- one entry point per reference kernel function ---------------------- */
+
+/* kernels/validation.pyx:21-43 (finite_indices) */
+int opb_finite_indices(const opb_particles *p, void *stream);
+/* kernels/validation.pyx:45-77 (domain_bounds) */
+int opb_domain_bounds(const opb_particles *p, const opb_scalars *s, void *stream);
+/* kernels/validation.pyx:124 (validation_kernel = finite_indices, domain_bounds) */
+int opb_validation(const opb_particles *p, const opb_scalars *s, void *stream);
+/* kernels/roms/_roms_core.pyx:17-73 (compute_z_kernel): z into `out` */
+int opb_compute_z(const opb_particles *p, double *out, const opb_scalars *s, const opb_roms_fields *f,
+                  const opb_time *t, void *stream);
+/* kernels/roms/rk2_w_advection.pyx:31-153 (rk2_w_advection_step_1) */
+int opb_rk2_w_advection_step_1(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                               const opb_time *t, void *stream);
+/* kernels/roms/rk2_w_advection.pyx:155-275 (rk2_w_advection_step_2) */
+int opb_rk2_w_advection_step_2(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                               const opb_time *t, void *stream);
+/* kernels/roms/rk2_w_advection.pyx:278-354 (rk2_w_advection_update) */
+int opb_rk2_w_advection_update(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                               const opb_time *t, void *stream);
+/* kernels/roms/ab3_w_advection.pyx:20-178 (ab3_w_advection) */
+int opb_ab3_w_advection(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                        const opb_time *t, void *stream);
+/* kernels/roms/ab3_w_advection.pyx:180-229 (ab3_post_w_advection) */
+int opb_ab3_post_w_advection(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                             const opb_time *t, void *stream);
+
+/* ---- output sampling (kernels/output/linear_interpolation.pyx:34-136) ----- */
+
+/* out[i] = linear interpolation of a 1-D field at idx[i] + offset, for active
+ * particles (linear_interpolation_kernel_function, :34-68) */
+int opb_linear_interpolation(const opb_particles *p, const double *idx, const opb_field *f, const opb_time *t,
+                             double *out, void *stream);
+/* out[i] = bilinear interpolation of a 2-D field at (idx0[i], idx1[i]) + offsets
+ * (bilinear_interpolation_kernel_function, :70-103) */
+int opb_bilinear_interpolation(const opb_particles *p, const double *idx0, const double *idx1, const opb_field *f,
+                               const opb_time *t, double *out, void *stream);
+/* out[i] = trilinear interpolation of a 3-D field at (zidx, yidx, xidx) + offsets
+ * (trilinear_interpolation_kernel_function, :105-136) */
+int opb_trilinear_interpolation(const opb_particles *p, const opb_field *f, const opb_time *t, double *out,
+                                void *stream);
+
+/* ---- fused steppers ------------------------------------------------------ */
+
+/* `nsteps` whole RK2 steps in one launch: per step, the preset's validation
+ * pre-step, step_1 at t, step_2 at t + alpha dt, update at t + dt
+ * (timesteppers.py:241-257; models/roms/__init__.py:37-62).  `table` is a
+ * DEVICE array of 3*nsteps opb_time entries (t, t + alpha dt, t + dt per
+ * step).  validate = 0 drops the pre-step.  Results equal `nsteps` rounds of
+ * the stage entry points; k1/k2 and z hold the last step's values. */
+int opb_rk2_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                              const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
+/* `nsteps` whole AB3 steps in one launch: validation pre-step, ab3 at t,
+ * ab3_post at t + dt (timesteppers.py:296-305; models/roms/__init__.py:65-96).
+ * `table`: DEVICE array of 2*nsteps opb_time entries (t, t + dt per step). */
+int opb_ab3_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                              const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
+
+/* ---- library ------------------------------------------------------------- */
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char *opb_last_error(void);
+/* OPB_ABI_VERSION of the loaded library. */
+int opb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPB200_H */

@@ -1,0 +1,456 @@
+"""Fields on the device: static fields in HBM, time-dependent fields as a snapshot ring.
+
+Mirrors offline_particles' ``fields.py`` (``Field``, ``StaticField``,
+``TimeDependentField``, ``FieldData``) with the same constructors, window
+semantics and errors.  Two things change, both B200-first:
+
+* The time blend ``prev * (1 - ft) + next * ft`` (fields.py:419-428 of the
+  reference) is not materialised over the whole grid at every launch.
+  ``get_field_data`` returns a ``FieldData`` whose ``array`` is a
+  ``BlendedArray``: the two device snapshots plus the weights, rounded to the
+  storage dtype exactly as the reference rounds them.  The kernels blend each
+  gathered corner with the same storage-dtype arithmetic, which gives the
+  reference's values bit for bit while reading two snapshots instead of
+  writing and re-reading a blended float64 grid.
+* Snapshots live in a device ring of ``ring_size`` slots.  A background thread
+  reads snapshot ``k`` from the host source (a numpy array, a CPU tensor, or
+  any object with ``shape``/``ndim``/``dtype``/``__getitem__(k)``), stages it in
+  pinned memory and copies it to its slot on a side CUDA stream; the compute
+  stream waits on that copy's event.  The next snapshots are prefetched while
+  the current interval runs.  A CUDA tensor source is used in place.
+"""
+
+from __future__ import annotations
+
+import abc
+import collections
+import concurrent.futures
+import threading
+
+import numpy as np
+import torch
+
+from ._device import cuda_device, torch_dtype
+from .spatial_arrays import BBox, DeviceArray, SpatialArray, Stagger
+
+FieldData = collections.namedtuple("FieldData", ["array", "offsets"])
+
+SUPPORTED_DTYPES = (np.dtype(np.float64), np.dtype(np.float32))
+
+
+class BlendedArray:
+    """``prev * gt + next * ft`` of one time-dependent field, left unmaterialised.
+
+    ``ft`` and ``gt`` are numpy scalars of the storage dtype, computed as
+    fields.py:409-424 of the reference computes them.
+    """
+
+    __slots__ = ("field", "It", "prev", "next", "ft", "gt")
+
+    def __init__(self, field: "TimeDependentField", It: int, prev: torch.Tensor, nxt: torch.Tensor, ft, gt) -> None:
+        self.field = field
+        self.It = It
+        self.prev = prev
+        self.next = nxt
+        self.ft = ft
+        self.gt = gt
+
+    @property
+    def dtype(self) -> np.dtype:
+        return self.field.dtype
+
+    @property
+    def shape(self) -> tuple[int, ...]:
+        return tuple(self.prev.shape)
+
+    def materialize(self) -> torch.Tensor:
+        """The blended float64 array (both products and the sum in the storage dtype)."""
+        td = self.prev.dtype
+        a = self.prev * torch.tensor(float(self.gt), dtype=td, device=self.prev.device)
+        b = self.next * torch.tensor(float(self.ft), dtype=td, device=self.prev.device)
+        return (a + b).to(torch.float64)
+
+    def __array__(self, dtype=None, copy=None):
+        out = self.materialize().cpu().numpy()
+        return out.astype(dtype) if dtype is not None else out
+
+
+class Field(abc.ABC):
+    """Abstract base class for fields used in particle tracking (fields.py:15-119)."""
+
+    def __init__(self, z_stagger: Stagger, y_stagger: Stagger, x_stagger: Stagger) -> None:
+        self._z_stagger = Stagger(z_stagger)
+        self._y_stagger = Stagger(y_stagger)
+        self._x_stagger = Stagger(x_stagger)
+        self._z_offset = self._z_stagger.offset
+        self._y_offset = self._y_stagger.offset
+        self._x_offset = self._x_stagger.offset
+
+    @property
+    def z_stagger(self) -> Stagger:
+        return self._z_stagger
+
+    @property
+    def y_stagger(self) -> Stagger:
+        return self._y_stagger
+
+    @property
+    def x_stagger(self) -> Stagger:
+        return self._x_stagger
+
+    @property
+    def stagger(self) -> tuple[Stagger, Stagger, Stagger]:
+        return (self._z_stagger, self._y_stagger, self._x_stagger)
+
+    @property
+    def z_offset(self) -> float | None:
+        return self._z_offset
+
+    @property
+    def y_offset(self) -> float | None:
+        return self._y_offset
+
+    @property
+    def x_offset(self) -> float | None:
+        return self._x_offset
+
+    @property
+    def all_offsets(self) -> tuple[float | None, float | None, float | None]:
+        return (self._z_offset, self._y_offset, self._x_offset)
+
+    @property
+    def active_offsets(self) -> tuple[float, ...]:
+        return tuple(o for o in self.all_offsets if o is not None)
+
+    @property
+    def dmask(self) -> tuple[bool, bool, bool]:
+        return (self._z_stagger.is_active, self._y_stagger.is_active, self._x_stagger.is_active)
+
+    @property
+    @abc.abstractmethod
+    def dtype(self) -> np.dtype: ...
+
+    @property
+    @abc.abstractmethod
+    def spatial_shape(self) -> tuple[int, ...]: ...
+
+    @property
+    def nspatial_dims(self) -> int:
+        return len(self.spatial_shape)
+
+    def _staggered_shape(self, simulation_shape: tuple[int, int, int, int]) -> tuple[int, ...]:
+        staggered = (
+            self.z_stagger.expected_size(simulation_shape[1]),
+            self.y_stagger.expected_size(simulation_shape[2]),
+            self.x_stagger.expected_size(simulation_shape[3]),
+        )
+        return tuple(s for s in staggered if s is not None)
+
+    @abc.abstractmethod
+    def validate_shape(self, simulation_shape: tuple[int, int, int, int]) -> None: ...
+
+    @abc.abstractmethod
+    def get_field_data(self, time_index: float, bbox: BBox | None = None) -> FieldData: ...
+
+
+class StaticField(Field):
+    """A time-invariant field, held on the device as float64.
+
+    The reference casts every field to contiguous float64 at each launch
+    (kernels/_core.pyx:5-24); a static field is cast once, at upload.
+    """
+
+    def __init__(self, data: SpatialArray) -> None:
+        super().__init__(data.z_stagger, data.y_stagger, data.x_stagger)
+        if not isinstance(data, DeviceArray):
+            raise TypeError("StaticField expects a DeviceArray / NumpyArray")
+        self._source_dtype = data.dtype
+        if data.data.dtype != torch.float64:
+            data = DeviceArray(data.data, data.z_stagger, data.y_stagger, data.x_stagger, dtype=torch.float64)
+        self._data = data
+
+    @property
+    def data(self) -> DeviceArray:
+        return self._data
+
+    def __repr__(self) -> str:
+        return (f"StaticField(shape={self._data.shape}, z_stagger={self.z_stagger}, "
+                f"y_stagger={self.y_stagger}, x_stagger={self.x_stagger})")
+
+    @property
+    def dtype(self) -> np.dtype:
+        return self._source_dtype
+
+    @property
+    def spatial_shape(self) -> tuple[int, ...]:
+        return self._data.shape
+
+    def validate_shape(self, simulation_shape: tuple[int, int, int, int]) -> None:
+        expected = self._staggered_shape(simulation_shape)
+        if self._data.shape != expected:
+            raise ValueError(f"Expected shape {expected} but data has shape {self._data.shape}")
+
+    def get_field_data(self, time_index: float, bbox: BBox | None = None) -> FieldData:
+        """The float64 device array and its offsets; ``time_index`` is ignored."""
+        array, offsets = self._data.get_data_subset(bbox)
+        return FieldData(array, offsets)
+
+    @classmethod
+    def from_numpy(cls, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
+                   *, device=None) -> "StaticField":
+        arr = np.asarray(data)
+        spatial = DeviceArray(arr.astype(np.float64, copy=False), Stagger(z_stagger), Stagger(y_stagger),
+                              Stagger(x_stagger), dtype=torch.float64, device=device)
+        f = cls(spatial)
+        f._source_dtype = arr.dtype
+        return f
+
+    @classmethod
+    def from_tensor(cls, data: torch.Tensor, z_stagger, y_stagger, x_stagger, *, device=None) -> "StaticField":
+        spatial = DeviceArray(data, Stagger(z_stagger), Stagger(y_stagger), Stagger(x_stagger), dtype=torch.float64,
+                              device=device)
+        return cls(spatial)
+
+
+class SnapshotRing:
+    """Device slots for the snapshots of one time-dependent field.
+
+    ``acquire(k)`` returns the device tensor of snapshot ``k`` and makes the
+    current stream wait for its upload.  Uploads run on a side stream from a
+    background thread: host read -> pinned staging buffer -> async H2D copy.
+    """
+
+    def __init__(self, source, spatial_shape: tuple[int, ...], np_dtype: np.dtype, nslots: int,
+                 device: torch.device) -> None:
+        self.source = source
+        self.np_dtype = np.dtype(np_dtype)
+        self.device = device
+        self.nslots = nslots
+        self.slots = torch.empty((nslots,) + tuple(spatial_shape), dtype=torch_dtype(np_dtype), device=device)
+        self.slot_of: dict[int, int] = {}
+        self.pending: dict[int, concurrent.futures.Future] = {}
+        self.ready: dict[int, torch.cuda.Event] = {}
+        self.lru: list[int] = []  # snapshots, least recently used first
+        self.copy_stream = torch.cuda.Stream(device=device)
+        self.staging = [torch.empty(tuple(spatial_shape), dtype=self.slots.dtype, pin_memory=True) for _ in range(2)]
+        self.staging_free = [None, None]  # events: staging buffer's last H2D copy done
+        self.staging_next = 0
+        self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=1, thread_name_prefix="opb-snapshots")
+        self.lock = threading.Lock()
+        self.h2d_bytes = 0
+
+    def _host_snapshot(self, k: int) -> np.ndarray:
+        src = self.source
+        if isinstance(src, torch.Tensor):
+            return src[k].numpy()
+        return np.ascontiguousarray(np.asarray(src[k]), dtype=self.np_dtype)
+
+    def _upload(self, k: int, slot: int, slot_free: torch.cuda.Event) -> None:
+        host = self._host_snapshot(k)
+        with torch.cuda.device(self.device):
+            b = self.staging_next
+            self.staging_next ^= 1
+            if self.staging_free[b] is not None:
+                self.staging_free[b].synchronize()
+            stage = self.staging[b]
+            stage.copy_(torch.from_numpy(host))
+            with torch.cuda.stream(self.copy_stream):
+                self.copy_stream.wait_event(slot_free)
+                self.slots[slot].copy_(stage, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.copy_stream)
+            self.staging_free[b] = ev
+            self.ready[k] = ev
+            self.h2d_bytes += stage.numel() * stage.element_size()
+
+    def _free_slot(self, keep: set[int]) -> int | None:
+        used = set(self.slot_of.values())
+        for s in range(self.nslots):
+            if s not in used:
+                return s
+        for k in self.lru:
+            if k not in keep:
+                slot = self.slot_of.pop(k)
+                self.lru.remove(k)
+                self.ready.pop(k, None)
+                return slot
+        return None
+
+    def _schedule(self, k: int, keep: set[int]) -> bool:
+        if k in self.slot_of:
+            return True
+        slot = self._free_slot(keep)
+        if slot is None:
+            return False
+        # the slot's previous contents may still be read by launches already queued
+        slot_free = torch.cuda.Event()
+        slot_free.record(torch.cuda.current_stream(self.device))
+        self.slot_of[k] = slot
+        self.lru.append(k)
+        self.pending[k] = self.pool.submit(self._upload, k, slot, slot_free)
+        return True
+
+    def acquire(self, k: int, keep: set[int] | frozenset = frozenset()) -> torch.Tensor:
+        with self.lock:
+            if not self._schedule(k, set(keep) | {k}):
+                raise RuntimeError(f"snapshot ring of {self.nslots} slots cannot hold snapshots {sorted(keep)}")
+            fut = self.pending.pop(k, None)
+            self.lru.remove(k)
+            self.lru.append(k)
+        if fut is not None:
+            fut.result()
+        ev = self.ready.get(k)
+        if ev is not None:
+            torch.cuda.current_stream(self.device).wait_event(ev)
+        return self.slots[self.slot_of[k]]
+
+    def prefetch(self, k: int, keep: set[int]) -> None:
+        with self.lock:
+            self._schedule(k, set(keep) | {k})
+
+    def resident(self) -> list[int]:
+        return sorted(self.slot_of)
+
+    def close(self) -> None:
+        self.pool.shutdown(wait=True)
+
+
+class TimeDependentField(Field):
+    """A field with a leading time axis, streamed to the device snapshot by snapshot.
+
+    Constructor and window semantics follow fields.py:237-392 of the reference:
+    at least 2 spatial+time dimensions, at least 2 snapshots, a window
+    ``[It, It + 1]`` moved by ``set_time_index`` / ``increment_time`` /
+    ``decrement_time`` with the same errors.
+    """
+
+    def __init__(self, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
+                 spatial_array_factory=None, output_dtype=np.float64, *, ring_size: int = 4, prefetch: int = 2,
+                 device=None) -> None:
+        super().__init__(Stagger(z_stagger), Stagger(y_stagger), Stagger(x_stagger))
+        if data.ndim < 2:
+            raise ValueError(
+                "TimeDependentField requires at least 2 dimensions (time + spatial). For spatially invariant fields,"
+                " use ConstantField or TemporalField."
+            )
+        if data.shape[0] < 2:
+            raise ValueError("TimeDependentField requires at least 2 time steps.")
+        self._data = data
+        self._data_dtype = np.dtype(data.dtype) if not isinstance(data, torch.Tensor) else np.dtype(
+            str(data.dtype).replace("torch.", ""))
+        if self._data_dtype not in SUPPORTED_DTYPES:
+            raise TypeError(f"storage dtype {self._data_dtype} is not supported (float32 or float64)")
+        self._output_dtype = output_dtype
+        self._num_timesteps = int(data.shape[0])
+        self._spatial_shape = tuple(int(s) for s in data.shape[1:])
+        self._device = cuda_device(device)
+        self._prefetch = max(0, int(prefetch))
+        self._resident_source = isinstance(data, torch.Tensor) and data.is_cuda
+        if self._resident_source:
+            self._ring = None
+        else:
+            if ring_size < 2 or ring_size > 8:
+                raise ValueError("ring_size must be between 2 and 8")
+            self._ring = SnapshotRing(data, self._spatial_shape, self._data_dtype, ring_size, self._device)
+        self._It = 0
+
+    # ------------------------------------------------------------ properties
+    @property
+    def data(self):
+        return self._data
+
+    def __repr__(self) -> str:
+        return (f"TimeDependentField(shape={tuple(self._data.shape)}, z_stagger={self.z_stagger}, "
+                f"y_stagger={self.y_stagger}, x_stagger={self.x_stagger})")
+
+    @property
+    def dtype(self) -> np.dtype:
+        return self._data_dtype
+
+    @property
+    def spatial_shape(self) -> tuple[int, ...]:
+        return self._spatial_shape
+
+    @property
+    def num_timesteps(self) -> int:
+        return self._num_timesteps
+
+    @property
+    def ring_size(self) -> int:
+        return self._ring.nslots if self._ring is not None else self._num_timesteps
+
+    @property
+    def time_index(self) -> int:
+        return self._It
+
+    def validate_shape(self, simulation_shape: tuple[int, int, int, int]) -> None:
+        expected = (simulation_shape[0],) + self._staggered_shape(simulation_shape)
+        if tuple(self._data.shape) != expected:
+            raise ValueError(f"Expected shape {expected} but data has shape {tuple(self._data.shape)}")
+
+    # ---------------------------------------------------------------- window
+    def increment_time(self) -> None:
+        if self._It == self._num_timesteps - 2:
+            raise IndexError("Cannot increment past the penultimate timestep.")
+        self._It += 1
+
+    def decrement_time(self) -> None:
+        if self._It == 0:
+            raise IndexError("Cannot decrement past the first timestep.")
+        self._It -= 1
+
+    def set_time_index(self, It: int) -> None:
+        if It == self._It:
+            return
+        if It == self._It + 1:
+            return self.increment_time()
+        if It == self._It - 1:
+            return self.decrement_time()
+        if It < 0 or It > self._num_timesteps - 2:
+            raise IndexError(f"Valid range of time indices is 0,...,{self._num_timesteps - 2}, got {It}.")
+        self._It = It
+
+    # -------------------------------------------------------------- snapshots
+    def snapshot(self, k: int, keep: set[int] | frozenset = frozenset()) -> torch.Tensor:
+        """Device tensor of snapshot ``k`` (uploaded if needed)."""
+        if k < 0 or k >= self._num_timesteps:
+            raise IndexError(k)
+        if self._ring is None:
+            return self._data[k]
+        return self._ring.acquire(k, keep)
+
+    def prefetch(self, k: int, keep: set[int]) -> None:
+        if self._ring is not None and 0 <= k < self._num_timesteps:
+            self._ring.prefetch(k, keep)
+
+    def blend_weights(self, time_index) -> tuple[int, object, object]:
+        """(It, ft, gt) with ft, gt in the storage dtype: fields.py:409-424."""
+        It, ft = divmod(time_index, 1)
+        ft = self._data_dtype.type(ft)
+        gt = self._data_dtype.type(1 - ft)
+        return int(It), ft, gt
+
+    def get_field_data(self, time_index: float, bbox: BBox | None = None) -> FieldData:
+        """FieldData whose array is the (unmaterialised) blend at ``time_index``."""
+        It, ft, gt = self.blend_weights(time_index)
+        self.set_time_index(It)
+        keep = {It, It + 1}
+        prev = self.snapshot(It, keep)
+        nxt = self.snapshot(It + 1, keep)
+        for j in range(2, 2 + self._prefetch):
+            self.prefetch(It + j, keep)
+        return FieldData(BlendedArray(self, It, prev, nxt, ft, gt), self.active_offsets)
+
+    @property
+    def h2d_bytes(self) -> int:
+        return self._ring.h2d_bytes if self._ring is not None else 0
+
+    @classmethod
+    def from_numpy(cls, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
+                   **kwargs) -> "TimeDependentField":
+        return cls(data, z_stagger, y_stagger, x_stagger, **kwargs)
+
+    @classmethod
+    def from_tensor(cls, data: torch.Tensor, z_stagger, y_stagger, x_stagger, **kwargs) -> "TimeDependentField":
+        """A CUDA tensor is used in place; a CPU tensor is streamed like a numpy array."""
+        return cls(data, z_stagger, y_stagger, x_stagger, **kwargs)

@@ -1,0 +1,217 @@
+"""Simulation and SimulationBuilder (simulation.py:1-367 of the reference).
+
+Same construction and stepping API.  Particle state lives on the device;
+``particles`` returns read-only host copies, ``run(n)`` advances many steps
+with fused multi-step launches between events, and ``synchronize()`` waits
+for the device and raises any error the kernels recorded (a zero grid
+spacing raises ``ZeroDivisionError``, as in the reference).
+"""
+
+from __future__ import annotations
+
+import itertools
+import types
+from typing import Mapping
+
+import numpy as np
+import torch
+
+from .events import Event, IterationScheduler, SimulationState, TimeScheduler
+from .fieldset import Fieldset
+from .kernels import merge_particle_fields
+from .launcher import Launcher
+from .particles import Particles, ParticlesView
+from .timesteppers import Timestepper
+
+
+class Simulation:
+    """A particle simulation on one CUDA device."""
+
+    def __init__(self, nparticles: int, timestepper: Timestepper, fieldset: Fieldset,
+                 iteration_scheduler: IterationScheduler, time_scheduler: TimeScheduler,
+                 output_writers: Mapping[str, object] | None = None, *, device=None) -> None:
+        self._timestepper = timestepper
+        self._fieldset = fieldset
+        self._iteration_scheduler = iteration_scheduler
+        self._time_scheduler = time_scheduler
+        self._output_writers = output_writers or {}
+        self._launcher = Launcher(fieldset)
+        self._launcher.maybe_increase_index_padding(timestepper.index_padding)
+        self._launcher.register_scalar_data_sources_from_object(self._timestepper)
+        for event in itertools.chain(self._iteration_scheduler.events, self._time_scheduler.events):
+            self._launcher.register_scalar_data_sources_from_object(event)
+        kernels = list(self._timestepper.kernels)
+        for event in itertools.chain(self._iteration_scheduler.events, self._time_scheduler.events):
+            kernels.extend(event.kernels)
+        particle_fields = merge_particle_fields(kernels)
+        self._particles = Particles(nparticles, device=device, **particle_fields)
+        self._particles_view = ParticlesView(self._particles)
+        self._invoke_events()
+
+    @property
+    def timestepper(self) -> Timestepper:
+        return self._timestepper
+
+    @property
+    def fieldset(self) -> Fieldset:
+        return self._fieldset
+
+    @property
+    def launcher(self) -> Launcher:
+        return self._launcher
+
+    @property
+    def time(self):
+        return self._timestepper.time
+
+    @property
+    def iteration(self) -> int:
+        return self._timestepper.iteration
+
+    @property
+    def dt(self):
+        return self._timestepper.dt
+
+    @property
+    def tidx(self) -> np.float64:
+        return self._timestepper.tidx
+
+    @property
+    def particles(self) -> ParticlesView:
+        return self._particles_view
+
+    @property
+    def device_particles(self) -> Particles:
+        """The device particle arrays (mutable; what the kernels write)."""
+        return self._particles
+
+    @property
+    def iteration_scheduler(self) -> IterationScheduler:
+        return self._iteration_scheduler
+
+    @property
+    def time_scheduler(self) -> TimeScheduler:
+        return self._time_scheduler
+
+    @property
+    def state(self) -> SimulationState:
+        return SimulationState(time=self.time, dt=self.dt, tidx=self.tidx, iteration=self.iteration,
+                               particles=self._particles_view)
+
+    def _invoke_events(self) -> None:
+        for event in itertools.chain(self._iteration_scheduler(self.iteration), self._time_scheduler(self.time)):
+            for kernel in event.kernels:
+                self._launcher.launch_kernel(kernel, self._particles, self.tidx)
+            event(self.state)
+
+    def set_indices(self, zidx=None, yidx=None, xidx=None) -> None:
+        """Set the particle indices (broadcast to the particle count; validated before any write)."""
+        vals = {}
+        for name, v in (("zidx", zidx), ("yidx", yidx), ("xidx", xidx)):
+            if v is not None:
+                vals[name] = self._as_device(v, self._particles[name])
+        for name, t in vals.items():
+            self._particles[name].copy_(t)
+
+    def set_particle_field(self, field_name: str, values) -> None:
+        """Set one particle field to ``values`` (cast to the field's dtype, broadcast)."""
+        target = self._particles[field_name]
+        target.copy_(self._as_device(values, target))
+
+    @staticmethod
+    def _as_device(values, target: torch.Tensor) -> torch.Tensor:
+        if isinstance(values, torch.Tensor):
+            t = values.to(device=target.device, dtype=target.dtype)
+        else:
+            from ._device import numpy_dtype
+
+            arr = np.asarray(values, dtype=numpy_dtype(target.dtype))
+            arr = np.broadcast_to(arr, tuple(target.shape))
+            t = torch.from_numpy(np.array(arr, copy=True, order="C")).to(target.device)
+        return t.expand(target.shape)
+
+    def step(self) -> None:
+        """Advance the simulation by one timestep, then run any scheduled events."""
+        self._timestepper.timestep_particles(self._particles, self._launcher)
+        self._invoke_events()
+
+    def steps_to_next_event(self, limit: int) -> int:
+        """How many steps can run before an event may fire (at most ``limit``)."""
+        n = limit
+        nxt = self._iteration_scheduler.next
+        if nxt is not None:
+            n = min(n, max(1, nxt - self.iteration))
+        nt = self._time_scheduler.next_time
+        if nt is not None:
+            t = self.time
+            k = 0
+            while k < n:
+                t = t + self.dt
+                k += 1
+                if t >= nt:
+                    break
+            n = min(n, max(1, k))
+        return n
+
+    def run(self, nsteps: int) -> None:
+        """Advance ``nsteps`` steps: fused multi-step launches between event firings."""
+        done = 0
+        while done < nsteps:
+            k = self.steps_to_next_event(nsteps - done)
+            self._timestepper.timestep_particles_many(self._particles, self._launcher, k)
+            done += k
+            self._invoke_events()
+
+    def synchronize(self) -> None:
+        """Wait for queued device work and raise any error it recorded."""
+        torch.cuda.synchronize(self._particles.device)
+        self._particles.check_errors()
+
+
+class SimulationBuilder:
+    """Builds a Simulation from a timestepper, a fieldset and events."""
+
+    def __init__(self, timestepper: Timestepper, fieldset: Fieldset) -> None:
+        self._timestepper = timestepper
+        self._fieldset = fieldset
+        self._iteration_scheduler = IterationScheduler()
+        self._time_scheduler = TimeScheduler()
+        self._output_writers: dict[str, tuple] = {}
+
+    def every_n(self, n: int, event: Event, *, first: int | None = None) -> None:
+        if n <= 0:
+            raise ValueError("n must be a positive integer.")
+        self._iteration_scheduler.register_event(0 if first is None else first, n, event)
+
+    def every_dt(self, dt, event: Event, *, first=None) -> None:
+        tt = self._timestepper.time
+        if first is None:
+            first = tt
+        try:
+            _ = tt + dt
+        except TypeError as e:
+            raise TypeError(f"Incompatible dt type {type(dt)} for timestepper time type {type(tt)}") from e
+        try:
+            _ = first + dt
+        except TypeError as e:
+            raise TypeError(f"Incompatible first type {type(first)} for timestepper time type {type(tt)}") from e
+        self._time_scheduler.register_event(first, dt, event)
+
+    def add_event(self, event: Event, *, n=None, dt=None, first=None) -> None:
+        if n is not None and dt is not None:
+            raise ValueError("Cannot specify both n and dt.")
+        elif n is not None:
+            self.every_n(n, event, first=first)
+        elif dt is not None:
+            self.every_dt(dt, event, first=first)
+        else:
+            raise ValueError("Either n or dt must be specified.")
+
+    def add_output_writer(self, builder, *, n=None, dt=None, first=None) -> None:
+        """Output writers (zarr) are outside this package's scope."""
+        raise NotImplementedError("output writers are not part of offline_particles_b200")
+
+    def build_simulation(self, nparticles: int, *, device=None) -> Simulation:
+        return Simulation(nparticles=nparticles, timestepper=self._timestepper, fieldset=self._fieldset,
+                          iteration_scheduler=self._iteration_scheduler, time_scheduler=self._time_scheduler,
+                          output_writers=types.MappingProxyType({}), device=device)

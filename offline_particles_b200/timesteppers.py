@@ -1,0 +1,406 @@
+"""Timesteppers: time bookkeeping and the launch order of one step (timesteppers.py:1-305 of the reference).
+
+The time arithmetic (``get_time_index``, ``advance_time``, ``set_dt``) is the
+reference's, in numpy float64, so every launch sees the same time index.
+
+B200 path: when a stepper is built from the stock ROMS kernels (the presets of
+``models.roms``), a step runs as ONE fused CUDA launch (validation + all
+stages) instead of three or four, and ``timestep_particles_many`` runs many
+steps per launch with the particle state held in registers.  Both give results
+identical to the stage-by-stage sequence.
+"""
+
+from __future__ import annotations
+
+import abc
+import ctypes
+
+import numpy as np
+import numpy.typing as npt
+import torch
+
+from . import _lib
+from .fields import TimeDependentField
+from .kernels import ParticleKernel
+from .kernels import _abi
+from .launcher import Launcher, ScalarSource
+
+type T = np.float64 | np.datetime64
+type D = np.float64 | np.timedelta64
+
+MAX_FUSED_STEPS = 240
+
+
+class Timestepper(abc.ABC):
+    """Particle advection time stepping."""
+
+    _dt_scalar = ScalarSource("_dt", lambda self, tidx: self._normalised_dt)
+    _time_scalar = ScalarSource("_time", lambda self, tidx: self.time)
+    _tidx_scalar = ScalarSource("_tidx", lambda self, tidx: self._tidx)
+
+    def __init__(self, time_array: npt.NDArray, dt: D, *, time_unit: D | None = None, time: T | None = None,
+                 iteration: int = 0, index_padding: int = 0) -> None:
+        if np.any(time_array[1:] <= time_array[:-1]):
+            raise ValueError("time_array must be strictly increasing.")
+        self._time_array = time_array
+        if time_unit is None:
+            if isinstance(dt, np.floating):
+                time_unit = np.float64(1.0)
+            else:
+                raise ValueError("time_unit must be specified for dimensional time.")
+        self._time_unit = time_unit
+        self.set_dt(dt)
+        if time is None:
+            time = self._time_array[0]
+        self.set_time(time)
+        self.set_iteration(iteration)
+        self._index_padding = 0
+        self.set_index_padding(index_padding)
+
+    def get_time_index(self, time: T) -> np.float64:
+        """timesteppers.py:64-85: searchsorted plus the fraction within the interval."""
+        time_array = self._time_array
+        if time < time_array[0] or time > time_array[-1]:
+            raise ValueError("Time is out of bounds of the time array.")
+        idx = np.searchsorted(time_array, time, side="right") - 1
+        t0 = time_array[idx]
+        t1 = time_array[idx + 1]
+        fraction = (time - t0) / (t1 - t0)
+        return idx + fraction
+
+    def set_dt(self, dt: D) -> None:
+        try:
+            self._normalised_dt = np.float64(dt / self._time_unit)
+        except Exception as e:
+            raise TypeError(f"dt must be of the same type as time_unit={self._time_unit!r}") from e
+
+    def set_time(self, time: T) -> None:
+        try:
+            _ = time + self.dt
+        except Exception as e:
+            raise TypeError(f"time must be compatible with dt={self.dt!r}") from e
+        self._tidx = self.get_time_index(time)
+        self._time = time
+
+    def set_iteration(self, iteration: int) -> None:
+        if iteration < 0:
+            raise ValueError("Iteration must be non-negative.")
+        self._iteration = iteration
+
+    def set_index_padding(self, index_padding: int, force: bool = False) -> None:
+        if index_padding < 0:
+            raise ValueError("Index padding must be non-negative.")
+        if force or index_padding > self._index_padding:
+            self._index_padding = index_padding
+
+    @property
+    def time_unit(self) -> D:
+        return self._time_unit
+
+    @property
+    def dt(self) -> D:
+        return self._normalised_dt * self._time_unit
+
+    @property
+    def time(self) -> T:
+        return self._time
+
+    @property
+    def time_array(self) -> npt.NDArray:
+        return self._time_array
+
+    @property
+    def iteration(self) -> int:
+        return self._iteration
+
+    @property
+    def tidx(self) -> np.float64:
+        return self._tidx
+
+    @property
+    def index_padding(self) -> int:
+        return self._index_padding
+
+    def advance_time(self) -> None:
+        """timesteppers.py:157-161."""
+        self._time += self.dt
+        self._tidx = self.get_time_index(self._time)
+        self._iteration += 1
+
+    @property
+    @abc.abstractmethod
+    def kernels(self) -> tuple[ParticleKernel, ...]: ...
+
+    @abc.abstractmethod
+    def timestep_particles(self, particles, launcher: Launcher) -> None: ...
+
+    # ------------------------------------------------------------ fused path
+    def _stage_times(self, time) -> tuple[list, object]:
+        """Time indices of the field lookups of one step starting at ``time``, and the next time."""
+        raise NotImplementedError
+
+    def fused(self) -> bool:
+        """True when the kernels are the stock ROMS ones and steps can run fused."""
+        return False
+
+    def timestep_particles_many(self, particles, launcher: Launcher, nsteps: int) -> None:
+        """Advance ``nsteps`` steps; fused launches where possible, else step by step."""
+        if not self.fused():
+            for _ in range(nsteps):
+                self.timestep_particles(particles, launcher)
+            return
+        done = 0
+        while done < nsteps:
+            done += self._fused_chunk(particles, launcher, nsteps - done)
+
+    def _fused_chunk(self, particles, launcher: Launcher, max_steps: int) -> int:
+        """Plan and launch as many steps as fit in one fused launch; return the number taken."""
+        td = _time_dependent_fields(launcher)
+        capacity = min([_lib.MAX_SLOTS] + [f.ring_size for f in td.values()])
+        time = self._time
+        steps: list[list] = []
+        needed: set[int] = set()
+        end_times = []
+        while len(steps) < min(max_steps, MAX_FUSED_STEPS):
+            try:
+                tidxs, nxt = self._stage_times(time)
+            except (ValueError, IndexError):
+                break
+            its = {int(divmod(t, 1)[0]) for t in tidxs}
+            more = needed | its | {i + 1 for i in its}
+            if len(more) > capacity or any(i + 1 >= f.num_timesteps for f in td.values() for i in its):
+                break
+            needed = more
+            steps.append(tidxs)
+            end_times.append(nxt)
+            time = nxt
+        if not steps:
+            # the next step raises or cannot be fused: run it the reference way (raises where it raises)
+            self._unfused_step(particles, launcher)
+            return 1
+        self._launch_fused(particles, launcher, steps, sorted(needed), td)
+        # bookkeeping exactly as advance_time would have left it after each step
+        self._time = end_times[-1]
+        self._tidx = steps[-1][-1]
+        self._iteration += len(steps)
+        return len(steps)
+
+    def _unfused_step(self, particles, launcher: Launcher) -> None:
+        raise NotImplementedError
+
+    def _launch_fused(self, particles, launcher: Launcher, steps: list[list], needed: list[int],
+                      td: dict[str, TimeDependentField]) -> None:
+        raise NotImplementedError
+
+
+def _time_dependent_fields(launcher: Launcher) -> dict[str, TimeDependentField]:
+    fs = launcher.fieldset
+    return {n: fs[n] for n in _abi.ROMS_FIELDS if n in fs and isinstance(fs[n], TimeDependentField)}
+
+
+def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: dict[str, TimeDependentField]):
+    """opb_roms_fields over the snapshots ``needed`` plus the per-stage opb_time table."""
+    fs = launcher.fieldset
+    for name in _abi.ROMS_FIELDS:
+        if name not in fs:
+            raise KeyError(f"Field '{name}' does not exist in Fieldset.")
+    dtypes = {np.dtype(f.dtype) for f in td.values()}
+    if len(dtypes) > 1:
+        raise ValueError("time-dependent fields of one launch must share one storage dtype")
+    dtype = dtypes.pop() if dtypes else np.dtype(np.float64)
+    slot = {k: j for j, k in enumerate(needed)}
+    keep = set(needed)
+    rf = _lib.opb_roms_fields()
+    for name in _abi.ROMS_FIELDS:
+        field = fs[name]
+        if name in td:
+            f = _lib.opb_field()
+            f.is_static = 0
+            f.dtype = _abi._dtype_code(field.dtype)
+            for k in needed:
+                f.data[slot[k]] = _abi._ptr(field.snapshot(k, keep))
+            f.nslots = len(needed)
+            shape = field.spatial_shape
+            offsets = field.active_offsets
+            nd = _abi.ROMS_NDIM[name]
+            if len(shape) != nd:
+                raise ValueError(f"field '{name}' must have {nd} active dimensions")
+            f.ndim = nd
+            for d in range(nd):
+                f.shape[d] = shape[d]
+                f.offset[d] = offsets[d]
+        else:
+            f = _abi.field_struct(field.get_field_data(0.0), _abi.ROMS_NDIM[name], name)
+        setattr(rf, name, f)
+    entries = [t for step in steps for t in step]
+    table = (_lib.opb_time * len(entries))()
+    for j, tidx in enumerate(entries):
+        It, ft = divmod(tidx, 1)
+        It = int(It)
+        ft = dtype.type(ft)
+        gt = dtype.type(1 - ft)
+        table[j] = _lib.opb_time(slot[It], slot[It + 1], float(ft), float(gt))
+    # move the field windows the way the stage launches would have
+    for field in td.values():
+        for tidx in entries:
+            field.set_time_index(int(divmod(tidx, 1)[0]))
+    return rf, table
+
+
+def _upload_table(table, device) -> torch.Tensor:
+    raw = torch.frombuffer(bytearray(bytes(table)), dtype=torch.uint8).pin_memory()
+    return raw.to(device, non_blocking=True)
+
+
+def _prefetch_after(td: dict[str, TimeDependentField], needed: list[int]) -> None:
+    if not needed:
+        return
+    last = needed[-1]
+    for f in td.values():
+        keep = {needed[-2], last} if len(needed) > 1 else {last}
+        f.prefetch(last + 1, keep)
+
+
+class RK2Timestepper(Timestepper):
+    """Two-stage explicit Runge-Kutta (timesteppers.py:164-257).
+
+    Butcher tableau  0 | ; alpha | alpha ; | 1 - 1/(2 alpha), 1/(2 alpha).  The
+    ROMS update kernel applies b1 = 1/(2 alpha) to k1 (rk2_w_advection.pyx:
+    317-318), the reference's own convention, which is kept.
+    """
+
+    _alpha_scalar = ScalarSource("_RK2_alpha", lambda self, tidx: self._alpha)
+
+    def __init__(self, time_array, dt, rk_step_1_kernel: ParticleKernel, rk_step_2_kernel: ParticleKernel,
+                 rk_update_kernel: ParticleKernel, *, alpha: float = 2 / 3, time_unit=None, time=None,
+                 iteration: int = 0, index_padding: int = 0, pre_step_kernel: ParticleKernel | None = None,
+                 post_step_kernel: ParticleKernel | None = None) -> None:
+        super().__init__(time_array, dt, time_unit=time_unit, time=time, index_padding=index_padding,
+                         iteration=iteration)
+        self._rk_step_1_kernel = rk_step_1_kernel
+        self._rk_step_2_kernel = rk_step_2_kernel
+        self._rk_update_kernel = rk_update_kernel
+        self._pre_step_kernel = pre_step_kernel
+        self._post_step_kernel = post_step_kernel
+        self._alpha = alpha
+
+    @property
+    def alpha(self) -> float:
+        return self._alpha
+
+    @property
+    def kernels(self) -> tuple[ParticleKernel, ...]:
+        pre = (self._pre_step_kernel,) if self._pre_step_kernel is not None else ()
+        post = (self._post_step_kernel,) if self._post_step_kernel is not None else ()
+        return pre + (self._rk_step_1_kernel, self._rk_step_2_kernel, self._rk_update_kernel) + post
+
+    def fused(self) -> bool:
+        from .kernels.roms import rk2_w_advection as rk
+        from .kernels.validation import validation_kernel
+
+        return (self._rk_step_1_kernel is rk.rk2_w_advection_step_1_kernel
+                and self._rk_step_2_kernel is rk.rk2_w_advection_step_2_kernel
+                and self._rk_update_kernel is rk.rk2_w_advection_update_kernel
+                and self._pre_step_kernel in (None, validation_kernel)
+                and self._post_step_kernel is None)
+
+    def _stage_times(self, time):
+        tidx1 = self.get_time_index(time)
+        tidx2 = self.get_time_index(time + self._alpha * self.dt)
+        nxt = time + self.dt
+        tidx3 = self.get_time_index(nxt)
+        return [tidx1, tidx2, tidx3], nxt
+
+    def timestep_particles(self, particles, launcher: Launcher) -> None:
+        """One RK2 step: one fused launch for the ROMS presets, else the reference's sequence."""
+        if self.fused():
+            self._fused_chunk(particles, launcher, 1)
+        else:
+            self._unfused_step(particles, launcher)
+
+    def _unfused_step(self, particles, launcher: Launcher) -> None:
+        """timesteppers.py:241-257."""
+        if self._pre_step_kernel is not None:
+            launcher.launch_kernel(self._pre_step_kernel, particles, self._tidx)
+        launcher.launch_kernel(self._rk_step_1_kernel, particles, self._tidx)
+        intermediate_time = self.time + self._alpha * self.dt
+        intermediate_tidx = self.get_time_index(intermediate_time)
+        launcher.launch_kernel(self._rk_step_2_kernel, particles, intermediate_tidx)
+        self.advance_time()
+        launcher.launch_kernel(self._rk_update_kernel, particles, self._tidx)
+        if self._post_step_kernel is not None:
+            launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
+
+    def _launch_fused(self, particles, launcher, steps, needed, td) -> None:
+        rf, table = _fused_fields(launcher, steps, needed, td)
+        sc = _abi.scalars_struct({
+            "hc": launcher.scalar("hc", self._tidx), "NZ": launcher.scalar("NZ", self._tidx),
+            "_dt": self._normalised_dt, "_RK2_alpha": self._alpha,
+            **{n: launcher.scalar(n, self._tidx) for n in ("zidx_min", "zidx_max", "yidx_min", "yidx_max",
+                                                           "xidx_min", "xidx_max")}})
+        dev_table = _upload_table(table, particles.device)
+        _lib.call("opb_rk2_w_advection_steps", ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
+                  ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
+                  _abi.stream(particles))
+        _prefetch_after(td, needed)
+
+
+class ABTimestepper(Timestepper):
+    """Adams-Bashforth stepping (timesteppers.py:260-305): pre, ab at t, advance, post at t + dt."""
+
+    def __init__(self, time_array, dt, ab_kernel: ParticleKernel, *, time_unit=None, time=None, iteration: int = 0,
+                 index_padding: int = 0, pre_step_kernel: ParticleKernel | None = None,
+                 post_step_kernel: ParticleKernel | None = None) -> None:
+        super().__init__(time_array, dt, time_unit=time_unit, time=time, index_padding=index_padding,
+                         iteration=iteration)
+        self._ab_kernel = ab_kernel
+        self._pre_step_kernel = pre_step_kernel
+        self._post_step_kernel = post_step_kernel
+
+    @property
+    def kernels(self) -> tuple[ParticleKernel, ...]:
+        pre = (self._pre_step_kernel,) if self._pre_step_kernel is not None else ()
+        post = (self._post_step_kernel,) if self._post_step_kernel is not None else ()
+        return pre + (self._ab_kernel,) + post
+
+    def fused(self) -> bool:
+        from .kernels.roms import ab3_w_advection as ab
+        from .kernels.validation import validation_kernel
+
+        return (self._ab_kernel is ab.ab3_w_advection_kernel
+                and self._post_step_kernel is ab.ab3_post_w_advection_kernel
+                and self._pre_step_kernel in (None, validation_kernel))
+
+    def _stage_times(self, time):
+        tidx1 = self.get_time_index(time)
+        nxt = time + self.dt
+        tidx2 = self.get_time_index(nxt)
+        return [tidx1, tidx2], nxt
+
+    def timestep_particles(self, particles, launcher: Launcher) -> None:
+        if self.fused():
+            self._fused_chunk(particles, launcher, 1)
+        else:
+            self._unfused_step(particles, launcher)
+
+    def _unfused_step(self, particles, launcher: Launcher) -> None:
+        """timesteppers.py:296-305."""
+        if self._pre_step_kernel is not None:
+            launcher.launch_kernel(self._pre_step_kernel, particles, self._tidx)
+        launcher.launch_kernel(self._ab_kernel, particles, self._tidx)
+        self.advance_time()
+        if self._post_step_kernel is not None:
+            launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
+
+    def _launch_fused(self, particles, launcher, steps, needed, td) -> None:
+        rf, table = _fused_fields(launcher, steps, needed, td)
+        sc = _abi.scalars_struct({
+            "hc": launcher.scalar("hc", self._tidx), "NZ": launcher.scalar("NZ", self._tidx),
+            "_dt": self._normalised_dt,
+            **{n: launcher.scalar(n, self._tidx) for n in ("zidx_min", "zidx_max", "yidx_min", "yidx_max",
+                                                           "xidx_min", "xidx_max")}})
+        dev_table = _upload_table(table, particles.device)
+        _lib.call("opb_ab3_w_advection_steps", ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
+                  ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
+                  _abi.stream(particles))
+        _prefetch_after(td, needed)

@@ -1,0 +1,121 @@
+"""The C-ABI boundary without a GPU: exports, struct layouts, argument checks."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from offline_particles_b200 import _lib
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADERS = sorted((ROOT / "include").glob("*.h"))
+
+
+def declared_functions() -> list[str]:
+    names = []
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(opb_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 16
+    for name in names:
+        assert hasattr(lib, name), f"{name} declared in include/ but not exported"
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\sT\s(opb_\w+)", out))
+    assert set(names) == exported, f"exports differ from the header: {set(names) ^ exported}"
+
+
+def test_every_declared_symbol_is_bound():
+    assert set(declared_functions()) - {"opb_last_error", "opb_abi_version"} == set(_lib.SIGNATURES)
+
+
+LAYOUT_PROBE = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "opb200.h"
+#define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m))
+#define S(T) printf(#T " %zu\n", sizeof(T))
+int main(void) {
+    S(opb_field); F(opb_field, data); F(opb_field, dtype); F(opb_field, ndim); F(opb_field, shape);
+    F(opb_field, offset); F(opb_field, is_static); F(opb_field, nslots);
+    S(opb_roms_fields); F(opb_roms_fields, zeta); F(opb_roms_fields, C);
+    S(opb_time); F(opb_time, ft); F(opb_time, gt);
+    S(opb_particles); F(opb_particles, status); F(opb_particles, z); F(opb_particles, dz2); F(opb_particles, err);
+    S(opb_scalars); F(opb_scalars, NZ); F(opb_scalars, dt); F(opb_scalars, alpha); F(opb_scalars, bounds);
+    return 0;
+}
+"""
+
+
+def test_struct_layouts_match_ctypes(tmp_path):
+    src = tmp_path / "probe.c"
+    src.write_text(LAYOUT_PROBE)
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c99", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    lines = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    c = dict(line.rsplit(" ", 1) for line in lines if line)
+    types = {"opb_field": _lib.opb_field, "opb_roms_fields": _lib.opb_roms_fields, "opb_time": _lib.opb_time,
+             "opb_particles": _lib.opb_particles, "opb_scalars": _lib.opb_scalars}
+    for key, val in c.items():
+        if "." in key:
+            t, m = key.split(".")
+            assert getattr(types[t], m).offset == int(val), key
+        else:
+            assert ctypes.sizeof(types[key]) == int(val), key
+
+
+def test_argument_errors_need_no_gpu():
+    lib = _lib.load()
+    assert lib.opb_validation(None, None, None) == _lib.EINVAL
+    assert b"particles is NULL" in lib.opb_last_error()
+    p = _lib.opb_particles()
+    p.n = -1
+    assert lib.opb_finite_indices(ctypes.byref(p), None) == _lib.EINVAL
+    p.n = 0
+    assert lib.opb_finite_indices(ctypes.byref(p), None) == _lib.OK  # nothing to launch
+    p.n = 4
+    assert lib.opb_finite_indices(ctypes.byref(p), None) == _lib.EINVAL  # status NULL
+    # a field with one point along a dimension cannot be interpolated
+    f = _lib.opb_field()
+    f.ndim, f.is_static, f.dtype = 1, 1, _lib.F64
+    f.data[0] = 16
+    f.shape[0] = 1
+    p.status = p.zidx = p.yidx = p.xidx = 16
+    assert lib.opb_linear_interpolation(ctypes.byref(p), 16, ctypes.byref(f), None, 16, None) == _lib.EINVAL
+    assert b"size 1" in lib.opb_last_error()
+    # mixed storage dtypes across time-dependent fields are rejected
+    rf = _lib.opb_roms_fields()
+    for name, nd in (("u", 3), ("v", 3), ("w", 3), ("dx", 2), ("dy", 2), ("h", 2), ("zeta", 2), ("C", 1)):
+        g = getattr(rf, name)
+        g.ndim = nd
+        for d in range(nd):
+            g.shape[d] = 4
+        g.data[0] = g.data[1] = 16
+        if name in ("u", "v", "w", "zeta"):
+            g.nslots, g.dtype = 2, _lib.F32
+        else:
+            g.is_static, g.dtype = 1, _lib.F64
+    rf.v.dtype = _lib.F64
+    s = _lib.opb_scalars()
+    t = _lib.opb_time(0, 1, 0.0, 1.0)
+    p.z = p.dxidx1 = p.dyidx1 = p.dz1 = 16
+    rc = lib.opb_rk2_w_advection_step_1(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), ctypes.byref(t), None)
+    assert rc == _lib.EINVAL and b"share one storage dtype" in lib.opb_last_error()
+    rf.v.dtype = _lib.F32
+    t.next = 5
+    rc = lib.opb_rk2_w_advection_step_1(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), ctypes.byref(t), None)
+    assert rc == _lib.EINVAL and b"slot out of range" in lib.opb_last_error()
+
+
+def test_call_raises_value_error():
+    with pytest.raises(ValueError, match="NULL"):
+        _lib.call("opb_validation", None, None, None)
