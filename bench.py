@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the ROMS advection step on B200.
+
+Workload (the plain GPU drop-in at production size): synthetic ROMS-like
+grid 1024 x 768 x 50 (float32 fields, hourly snapshots), 4,194,304 particles
+uniform in wet cells, AB3 w-advection at dt = 120 s, as the ROMS preset
+``ab3_w_advection_timestepper`` runs it (validation pre-step, AB3, zidx
+post-step).  A "step" is one AB3 step of every particle.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One JSON line on rank 0.  ``value``: fields and particles resident in HBM,
+K steps through ``Simulation.run`` (fused multi-step launches), CUDA events
+on the launching stream, max over ranks.  ``e2e``: the same K steps through
+the public API from host buffers -- particle indices copied in from pinned
+memory, every snapshot streamed from pinned host memory through the device
+ring, results copied back -- all inside the timed region.  ``--impl
+reference`` times the CPU implementation of the path (the oracle restatement
+of the reference's Cython/OpenMP kernels and numpy time blend) on the host's
+cores.  Multi-GPU runs shard particles (weak scaling, no collective on the
+data path).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s (1 B200) vs plain GPU path"
+UNIT = "particle-steps/s"
+STAGGERS = {
+    "u": ("center", "center", "inner"),
+    "v": ("center", "inner", "center"),
+    "w": ("outer", "center", "center"),
+    "zeta": ("invariant", "center", "center"),
+    "h": ("invariant", "center", "center"),
+    "dx": ("invariant", "center", "center"),
+    "dy": ("invariant", "center", "center"),
+    "C": ("center", "invariant", "invariant"),
+}
+TD = ("u", "v", "w", "zeta")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--particles", type=int, default=4_194_304)
+    ap.add_argument("--nx", type=int, default=1024)
+    ap.add_argument("--ny", type=int, default=768)
+    ap.add_argument("--nz", type=int, default=50)
+    ap.add_argument("--dt", type=float, default=120.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=25.0)
+    return ap.parse_args()
+
+
+def workload_config(a, nt: int, pair_bytes: float | None = None) -> dict:
+    state = a.particles * (1 + 13 * 8)
+    pair = pair_bytes if pair_bytes is not None else 2 * 4 * (a.nz * a.ny * (a.nx - 1) + a.nz * (a.ny - 1) * a.nx
+                                                               + (a.nz + 1) * a.ny * a.nx + a.ny * a.nx)
+    return {
+        "workload": f"AB3 w-advection, {a.nx}x{a.ny}x{a.nz} float32 synthetic ROMS grid, {a.particles:,} particles "
+                    f"per GPU, dt={a.dt:g} s",
+        "grid": [a.nz, a.ny, a.nx],
+        "particles_per_gpu": a.particles,
+        "scheme": "ab3",
+        "dt_s": a.dt,
+        "field_dtype": "float32",
+        "state_dtype": "float64",
+        "snapshots_resident": nt,
+        "l2": f"inputs larger than L2 (snapshot pair {pair / 1e6:.0f} MB, particle state {state / 1e6:.0f} MB "
+              f"per GPU; L2 126 MB), no flush",
+        "parallelism": f"particle shards x{a.gpus}" if a.gpus > 1 else "single GPU",
+    }
+
+
+# --------------------------------------------------------------- inputs
+def make_inputs(a, rank: int):
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    span = (a.warmup + a.steps) * a.dt
+    nt = int(math.floor(span / 3600.0)) + 3
+    grid = SyntheticROMS(GridSpec(nx=a.nx, ny=a.ny, nz=a.nz, nt=nt, seed=2, dtype="float32"))
+    snaps = {name: np.stack([grid.snapshot(k)[name] for k in range(nt)]) for name in TD}
+    z, y, x = grid.release(a.particles, seed=1000 + rank)
+    return grid, snaps, (z, y, x), nt
+
+
+def field_bytes(grid, snaps) -> dict:
+    per_snap = sum(snaps[n][0].nbytes for n in TD)
+    static = grid.h.nbytes + grid.dx.nbytes + grid.dy.nbytes + grid.C.nbytes
+    return {"snapshot": per_snap, "pair": 2 * per_snap, "static": static}
+
+
+def build_sim(grid, sources: dict, n: int, a, *, ring_size: int = 4):
+    import offline_particles_b200 as opb
+
+    kw = {}
+    for name in TD:
+        kw[name] = opb.TimeDependentField.from_tensor(sources[name], *STAGGERS[name], ring_size=ring_size)
+    for name, arr in (("h", grid.h), ("dx", grid.dx), ("dy", grid.dy), ("C", grid.C)):
+        kw[name] = opb.StaticField.from_numpy(arr, *STAGGERS[name])
+    nt = sources["u"].shape[0]
+    fs = opb.Fieldset(nt, a.nz, a.ny, a.nx, constants={"hc": grid.hc, "NZ": a.nz}, **kw)
+    ts = opb.roms.ab3_w_advection_timestepper(grid.time_array[:nt], np.float64(a.dt))
+    return opb.SimulationBuilder(ts, fs).build_simulation(n), fs
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """NVML samples of the SM clock and clock-event reasons every 10 ms while running (reads only)."""
+
+    REASONS = (("nvmlClocksEventReasonHwSlowdown", "hw_slowdown"),
+               ("nvmlClocksEventReasonHwThermalSlowdown", "hw_thermal_slowdown"),
+               ("nvmlClocksEventReasonSwThermalSlowdown", "sw_thermal_slowdown"),
+               ("nvmlClocksEventReasonSwPowerCap", "sw_power_cap"),
+               ("nvmlClocksEventReasonHwPowerBrakeSlowdown", "hw_power_brake"))
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.samples: list[tuple[float, int]] = []
+        self.max_mhz = None
+        self.stop = threading.Event()
+        self.nv = None
+
+    def __enter__(self):
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        except Exception:  # no NVML: the summary says so
+            self.nv = None
+        return self
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+            except Exception:
+                pass
+            self.stop.wait(0.01)
+
+    def __exit__(self, *exc):
+        if self.nv is not None:
+            self.stop.set()
+            self.t.join(timeout=5)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"], "samples": 0}
+        reasons = set()
+        for _, bits in self.samples:
+            for attr, name in self.REASONS:
+                mask = getattr(self.nv, attr, 0)
+                if mask and bits & mask:
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(self.samples), "source": "NVML, 10 ms"}
+
+
+# --------------------------------------------------------------- timing helpers
+class LaunchTimer:
+    """CUDA events around every fused launch, on the stream the kernel runs on."""
+
+    def __init__(self) -> None:
+        import torch
+
+        self.torch = torch
+        self.pairs = []
+        self.steps = []
+
+    def before(self, nsteps: int) -> None:
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(self.torch.cuda.current_stream())
+        self.pairs.append([e, None])
+        self.steps.append(nsteps)
+
+    def after(self, nsteps: int) -> None:
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(self.torch.cuda.current_stream())
+        self.pairs[-1][1] = e
+
+    def durations_ms(self) -> list[float]:
+        return [a.elapsed_time(b) for a, b in self.pairs]
+
+
+def dist_max(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# --------------------------------------------------------------- CPU path
+def cpu_run(grid, snaps, zyx, a, budget_s: float) -> dict:
+    """The oracle (the reference's algorithm on the CPU: numpy blend + C/OpenMP loops) on this workload."""
+    from oracle import oracle as O
+
+    fields = dict(snaps)
+    fields.update(h=grid.h, dx=grid.dx, dy=grid.dy, C=grid.C)
+    orc = O.OracleROMS(grid.time_array[: snaps["u"].shape[0]], fields, hc=grid.hc, scheme="ab3",
+                       dt=np.float64(a.dt))
+    n = zyx[0].size
+    p = O.new_particles(n, "ab3")
+    p["zidx"][:], p["yidx"][:], p["xidx"][:] = zyx
+    p["status"][:] = O.MULTISTEP_1
+    t0 = time.perf_counter()
+    orc.step(p)  # untimed warm-up step
+    first = time.perf_counter() - t0
+    steps = max(1, min(30, int(budget_s / max(first, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        orc.step(p)
+    el = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": n * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} AB3 steps of all {n:,} particles on the same grid after 1 warm-up step "
+                      f"({el:.1f} s); numpy time blend + C/OpenMP kernels, {threads} threads of "
+                      f"{os.cpu_count()} host CPUs"}
+
+
+def reference_arm(a) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    grid, snaps, zyx, nt = make_inputs(a, 0)
+    budget = max(10.0, min(150.0, 3.0 * a.cpu_budget_s))
+    cb = cpu_run(grid, snaps, zyx, a, budget)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": a.particles / cb["value"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(a, nt), "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- B200 path
+def b200_arm(a) -> None:
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import offline_particles_b200 as opb
+    from offline_particles_b200 import timesteppers
+
+    grid, snaps, zyx, nt = make_inputs(a, rank)
+    n = a.particles
+    fb = field_bytes(grid, snaps)
+    dev = torch.device("cuda", local)
+
+    # ---- device-resident: fused multi-step launches ----------------------------------
+    dsrc = {k: torch.from_numpy(v).to(dev) for k, v in snaps.items()}
+    sim, _ = build_sim(grid, dsrc, n, a)
+    sim.set_indices(*zyx)
+    sim.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+    sim.run(a.warmup)
+    sim.synchronize()
+    timer = LaunchTimer()
+    timesteppers.launch_observers.append(timer)
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        sim.run(a.steps)
+        e.record()
+        torch.cuda.synchronize()
+    timesteppers.launch_observers.remove(timer)
+    sim.synchronize()
+    run_ms = dist_max(s.elapsed_time(e), world)
+    launch_ms = timer.durations_ms()
+    launch_steps = timer.steps
+    active = int((sim.particles.tensor("status") & 0x80).eq(0).sum().item())
+
+    # ---- plain path: Simulation.step(), one fused launch per step --------------------
+    sim2, _ = build_sim(grid, dsrc, n, a)
+    sim2.set_indices(*zyx)
+    sim2.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+    for _ in range(a.warmup):
+        sim2.step()
+    sim2.synchronize()
+    barrier(world)
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record()
+    for _ in range(a.steps):
+        sim2.step()
+    e2.record()
+    torch.cuda.synchronize()
+    step_ms = dist_max(s2.elapsed_time(e2), world)
+    del sim2
+    del sim, dsrc
+    torch.cuda.empty_cache()
+
+    # ---- end to end from host buffers --------------------------------------------------
+    psrc = {k: torch.from_numpy(v).pin_memory() for k, v in snaps.items()}
+    hz, hy, hx = (torch.from_numpy(v).pin_memory() for v in zyx)
+    outs = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in ("zidx", "yidx", "xidx")}
+    outs["status"] = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    # untimed warm-up of the same path (allocator, ring, copy stream)
+    simw, _ = build_sim(grid, psrc, n, a, ring_size=4)
+    simw.set_indices(hz, hy, hx)
+    simw.run(a.warmup)
+    simw.synchronize()
+    del simw
+    sim3, fs3 = build_sim(grid, psrc, n, a, ring_size=4)
+    barrier(world)
+    torch.cuda.synchronize()
+    s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    s3.record()
+    sim3.set_indices(hz, hy, hx)
+    sim3.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+    sim3.run(a.steps)
+    P = sim3.device_particles
+    for k in outs:
+        outs[k].copy_(P[k], non_blocking=True)
+    e3.record()
+    torch.cuda.synchronize()
+    wall_e2e = time.perf_counter() - w0
+    sim3.synchronize()
+    e2e_ms = dist_max(max(s3.elapsed_time(e3), wall_e2e * 1e3), world)
+    h2d = 3 * 8 * n + sum(fs3[k].h2d_bytes for k in TD)
+    d2h = sum(t.numel() * t.element_size() for t in outs.values())
+
+    # ---- CPU baseline (rank 0, one GPU) ------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_run(grid, snaps, zyx, a, a.cpu_budget_s)
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    # ---- roofline of the fused kernel -------------------------------------------------
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs") or 6650.0
+    state_bytes = 2 * (1 + 3 * 8 + 6 * 8)  # status + 3 indices + 6 AB3 history values, float64, read + written
+    b_step = n * state_bytes + fb["pair"] + fb["static"]
+    tot_steps = sum(launch_steps)
+    avg_launch_ms = sum(launch_ms) / max(1, len(launch_ms))
+    avg_launch_steps = tot_steps / max(1, len(launch_steps))
+    achieved = b_step * avg_launch_steps / (avg_launch_ms * 1e-3) / 1e9
+
+    total = world * n * a.steps
+    line = {
+        "metric": METRIC, "value": total / (run_ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": run_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ROMS-like grid; no ROMS output offline)",
+        "config": workload_config(a, nt),
+        "plain_step": {"value": total / (step_ms * 1e-3), "unit": UNIT, "ms_per_step": step_ms / a.steps,
+                       "path": "Simulation.step(): one fused launch (validation + AB3 + post) per step"},
+        "e2e": {"value": total / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d / a.steps),
+                "d2h_bytes_per_step": int(d2h / a.steps),
+                "path": "Simulation.set_indices from pinned host + run(K) streaming every snapshot from pinned "
+                        "host memory + D2H of zidx/yidx/xidx/status"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                     "algorithmic_bytes_per_step": b_step, "bytes_per_particle_step": b_step / n,
+                     "steps_per_launch": avg_launch_steps, "launch_ms": avg_launch_ms,
+                     "kernel": "k_ab3_steps<float>"},
+        "gpu_launches": len(launch_ms),
+        "active_particles_end": active,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    a = parse()
+    if a.impl == "reference":
+        reference_arm(a)
+    else:
+        b200_arm(a)
+
+
+if __name__ == "__main__":
+    main()

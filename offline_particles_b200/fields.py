@@ -246,6 +246,17 @@ class SnapshotRing:
         return np.ascontiguousarray(np.asarray(src[k]), dtype=self.np_dtype)
 
     def _upload(self, k: int, slot: int, slot_free: torch.cuda.Event) -> None:
+        src = self.source
+        if isinstance(src, torch.Tensor) and src.is_pinned():
+            # already in pinned host memory: one async copy, no staging
+            with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
+                self.copy_stream.wait_event(slot_free)
+                self.slots[slot].copy_(src[k], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.copy_stream)
+            self.ready[k] = ev
+            self.h2d_bytes += src[k].numel() * src.element_size()
+            return
         host = self._host_snapshot(k)
         with torch.cuda.device(self.device):
             b = self.staging_next

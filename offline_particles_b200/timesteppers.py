@@ -30,6 +30,15 @@ type D = np.float64 | np.timedelta64
 
 MAX_FUSED_STEPS = 240
 
+# Observers of fused launches: objects with before(nsteps) / after(nsteps),
+# called on the host around each fused kernel launch (used for timing).
+launch_observers: list = []
+
+
+def _notify(phase: str, nsteps: int) -> None:
+    for obs in launch_observers:
+        getattr(obs, phase)(nsteps)
+
 
 class Timestepper(abc.ABC):
     """Particle advection time stepping."""
@@ -339,9 +348,11 @@ class RK2Timestepper(Timestepper):
             **{n: launcher.scalar(n, self._tidx) for n in ("zidx_min", "zidx_max", "yidx_min", "yidx_max",
                                                            "xidx_min", "xidx_max")}})
         dev_table = _upload_table(table, particles.device)
+        _notify("before", len(steps))
         _lib.call("opb_rk2_w_advection_steps", ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
                   ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
+        _notify("after", len(steps))
         _prefetch_after(td, needed)
 
 
@@ -400,7 +411,9 @@ class ABTimestepper(Timestepper):
             **{n: launcher.scalar(n, self._tidx) for n in ("zidx_min", "zidx_max", "yidx_min", "yidx_max",
                                                            "xidx_min", "xidx_max")}})
         dev_table = _upload_table(table, particles.device)
+        _notify("before", len(steps))
         _lib.call("opb_ab3_w_advection_steps", ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
                   ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
+        _notify("after", len(steps))
         _prefetch_after(td, needed)

@@ -249,7 +249,8 @@ class OracleROMS:
         return self._dt * np.float64(1.0)
 
     # ---------------------------------------------------------------- fields
-    def fielddata(self, time_index) -> ORomsFields:
+    def fielddata(self, time_index, names=TIME_DEPENDENT) -> ORomsFields:
+        """Blend the time-dependent ``names`` a launch declares (launcher.py:172)."""
         It, ft = divmod(time_index, 1)
         It = int(It)
         nt = self.fields["u"].shape[0]
@@ -257,8 +258,11 @@ class OracleROMS:
             raise IndexError(f"Valid range of time indices is 0,...,{nt - 2}, got {It}.")
         td = {}
         for name in TIME_DEPENDENT:
-            data = self.fields[name]
-            td[name] = make_field(time_blend(data[It], data[It + 1], ft), active_offsets(self.staggers[name]))
+            if name in names:
+                data = self.fields[name]
+                td[name] = make_field(time_blend(data[It], data[It + 1], ft), active_offsets(self.staggers[name]))
+            else:
+                td[name] = OF3() if name != "zeta" else OF2()
         f = ORomsFields(td["u"], td["v"], td["w"], self._static["dx"], self._static["dy"], self._static["h"],
                         td["zeta"], self._static["C"])
         f._keep = td  # type: ignore[attr-defined]
@@ -303,17 +307,17 @@ class OracleROMS:
             tidx_int = get_time_index(self.time_array, t_int)
             self._check(L.oracle_rk2_step_2(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(tidx_int))))
             self.advance_time()
-            L.oracle_rk2_update(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(self.tidx)))
+            L.oracle_rk2_update(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(self.tidx, ("zeta",))))
         else:  # timesteppers.py:296-305
             self._check(L.oracle_ab3(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(self.tidx))))
             self.advance_time()
-            L.oracle_ab3_post(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(self.tidx)))
+            L.oracle_ab3_post(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(self.tidx, ("zeta",))))
 
     def compute_z(self, p: Mapping[str, np.ndarray], out: np.ndarray) -> None:
         """kernels/roms/_roms_core.pyx:17-73 at the current time index."""
         op = self._particles(p)
         self._lib.oracle_compute_z(ctypes.byref(op), _ptr(out), ctypes.byref(self._scalars()),
-                                   ctypes.byref(self.fielddata(self.tidx)))
+                                   ctypes.byref(self.fielddata(self.tidx, ("zeta",))))
 
 
 def particle_fields(scheme: str) -> tuple[str, ...]:
