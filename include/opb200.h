@@ -176,6 +176,27 @@ int opb_rk2_w_advection_steps(const opb_particles *p, const opb_scalars *s, cons
 int opb_ab3_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                               const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
 
+/* ---- spatial ordering ------------------------------------------------------
+ * No counterpart in the reference, which keeps particles in release order and
+ * splits them statically over OpenMP threads (rk2_w_advection.pyx:85-91).
+ * Every kernel is per particle, so storage order changes no result; a
+ * Morton order by cell makes neighbouring threads gather neighbouring field
+ * corners, which is what lets the fused kernels reuse L1/L2. */
+
+/* Bytes of device workspace opb_sort_particles needs for n particles. */
+size_t opb_sort_workspace_bytes(int64_t n);
+/* perm[j] = index of the particle that belongs at position j: active particles
+ * in Morton order of their cell on the centred (z, y, x) grid of `shape`,
+ * inactive particles last, ties in index order.  `workspace` is a device buffer
+ * of at least opb_sort_workspace_bytes(n) bytes, used as scratch. */
+int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *perm, void *workspace,
+                       size_t workspace_bytes, void *stream);
+/* dst.f[j] = src.f[perm[j]] for status and every float64 field present in
+ * both (src and dst must not alias), and dst_ids[j] = src_ids[perm[j]] when
+ * id arrays are given. */
+int opb_gather_particles(const opb_particles *src, const opb_particles *dst, const int32_t *perm,
+                         const int64_t *src_ids, int64_t *dst_ids, void *stream);
+
 /* ---- library ------------------------------------------------------------- */
 
 /* Message of the last failed call on this host thread ("" if none). */

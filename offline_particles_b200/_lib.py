@@ -81,6 +81,12 @@ SIGNATURES = {
                                   ctypes.c_int32, _VP],
 }
 
+SIGNATURES_OTHER = {
+    "opb_sort_particles": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
+    "opb_gather_particles": ([_P(opb_particles), _P(opb_particles), _VP, _VP, _VP, _VP], ctypes.c_int),
+    "opb_sort_workspace_bytes": ([ctypes.c_int64], ctypes.c_size_t),
+}
+
 _lock = threading.Lock()
 _lib: ctypes.CDLL | None = None
 
@@ -100,6 +106,10 @@ def load(build: bool = True) -> ctypes.CDLL:
             fn = getattr(lib, name)
             fn.argtypes = argtypes
             fn.restype = ctypes.c_int
+        for name, (argtypes, restype) in SIGNATURES_OTHER.items():
+            fn = getattr(lib, name)
+            fn.argtypes = argtypes
+            fn.restype = restype
         lib.opb_last_error.argtypes = []
         lib.opb_last_error.restype = ctypes.c_char_p
         lib.opb_abi_version.argtypes = []

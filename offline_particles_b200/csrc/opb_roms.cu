@@ -7,7 +7,6 @@
 // -fmad=false: see opb_device.cuh.
 #include <cuda_runtime.h>
 
-#include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <initializer_list>
@@ -16,6 +15,7 @@
 
 #include "opb200.h"
 #include "opb_device.cuh"
+#include "opb_errors.h"
 
 namespace opb {
 namespace {
@@ -448,22 +448,10 @@ __global__ void __launch_bounds__(kBlock) k_interpolate(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------- host side
-thread_local std::string g_last_error;
-
-int fail(int code, const char *fmt, ...) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    g_last_error = buf;
-    return code;
-}
-
 int check_launch(const char *what) {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
-    g_last_error.clear();
+    clear_error();
     return OPB_OK;
 }
 
@@ -591,8 +579,6 @@ using namespace opb;
 
 // ====================================================================== C ABI
 extern "C" {
-
-const char *opb_last_error(void) { return g_last_error.c_str(); }
 
 int opb_abi_version(void) { return OPB_ABI_VERSION; }
 

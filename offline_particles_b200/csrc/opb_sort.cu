@@ -1,0 +1,194 @@
+// Spatial ordering of particles: Morton cell keys, radix sort, SoA gather.
+//
+// The advection kernels gather 8-corner stencils from fields far larger than
+// L2.  Consecutive threads that hold spatially close particles share DRAM
+// sectors and keep the in-flight working set in L2 across fused steps; this
+// file produces that order.  Particles are independent, so the order changes
+// no result -- only where each particle's state is stored.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include "opb200.h"
+#include "opb_errors.h"
+
+namespace opb_sort {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr uint32_t kInactiveKey = 0xFFFFFFFFu;
+
+// spread the low 10 bits of v to every third bit
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t cell(double idx, int n, int shift) {
+    // the particle's cell, clamped into the grid (non-finite -> 0), quantised by 2^shift
+    long long c = (idx >= 0.0 && idx < 9.0e18) ? (long long)idx : 0LL;
+    if (c > n - 1) c = n - 1;
+    return (uint32_t)(c >> shift);
+}
+
+struct KeyArgs {
+    const uint8_t *status;
+    const double *zidx, *yidx, *xidx;
+    long long n;
+    int nz, ny, nx;
+    int sz, sy, sx;  // right shifts that bring each dimension under 2^10 (x additionally by 2)
+};
+
+__global__ void __launch_bounds__(kBlock) k_cell_keys(KeyArgs a, uint32_t *keys, int32_t *ids) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    uint32_t key = kInactiveKey;
+    if (!(a.status[i] & OPB_STATUS_INACTIVE)) {
+        const uint32_t z = cell(a.zidx[i], a.nz, a.sz);
+        const uint32_t y = cell(a.yidx[i], a.ny, a.sy);
+        const uint32_t x = cell(a.xidx[i], a.nx, a.sx);
+        // x in the lowest bit of each triple: boxes of a Morton range are elongated along x,
+        // the contiguous dimension of every field
+        key = (spread3(z) << 2) | (spread3(y) << 1) | spread3(x);
+    }
+    keys[i] = key;
+    ids[i] = (int32_t)i;
+}
+
+struct GatherArgs {
+    const uint8_t *s_status;
+    uint8_t *d_status;
+    const double *s[13];
+    double *d[13];
+    const int64_t *s_ids;
+    int64_t *d_ids;
+    int nf;
+    long long n;
+};
+
+__global__ void __launch_bounds__(kBlock) k_gather(const __grid_constant__ GatherArgs a, const int32_t *perm) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= a.n) return;
+    const int32_t i = perm[j];
+    a.d_status[j] = a.s_status[i];
+    for (int f = 0; f < a.nf; ++f) a.d[f][j] = a.s[f][i];
+    if (a.d_ids) a.d_ids[j] = a.s_ids[i];
+}
+
+int shift_for(int n, int extra) {
+    int bits = 0;
+    while ((1 << bits) < n) ++bits;
+    int s = extra;
+    while (bits - s > 10) ++s;
+    return s;
+}
+
+size_t cub_temp_bytes(long long n) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, 32);
+    return bytes;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+}  // namespace opb_sort
+
+using namespace opb_sort;
+using opb::fail;
+
+extern "C" {
+
+size_t opb_sort_workspace_bytes(int64_t n) {
+    if (n <= 0) return 0;
+    return 3 * align256((size_t)n * 4) + align256(cub_temp_bytes(n));
+}
+
+int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *perm, void *workspace,
+                       size_t workspace_bytes, void *stream) {
+    if (!p) return fail(OPB_EINVAL, "opb_sort_particles: particles is NULL");
+    if (p->n < 0 || p->n > 0x7fffffffLL) return fail(OPB_EINVAL, "opb_sort_particles: particle count out of range");
+    if (p->n == 0) return OPB_OK;
+    if (!p->status || !p->zidx || !p->yidx || !p->xidx || !perm || !shape)
+        return fail(OPB_EINVAL, "opb_sort_particles: NULL argument");
+    if (shape[0] < 1 || shape[1] < 1 || shape[2] < 1 || shape[0] > (1 << 30) || shape[1] > (1 << 30) ||
+        shape[2] > (1 << 30))
+        return fail(OPB_EINVAL, "opb_sort_particles: bad grid shape");
+    const size_t need = opb_sort_workspace_bytes(p->n);
+    if (!workspace || workspace_bytes < need)
+        return fail(OPB_EINVAL, "opb_sort_particles: workspace of %zu bytes is smaller than the %zu needed",
+                    workspace_bytes, need);
+    const size_t a = align256((size_t)p->n * 4);
+    char *ws = (char *)workspace;
+    uint32_t *keys_in = (uint32_t *)ws;
+    uint32_t *keys_out = (uint32_t *)(ws + a);
+    int32_t *ids_in = (int32_t *)(ws + 2 * a);
+    void *temp = ws + 3 * a;
+    size_t temp_bytes = workspace_bytes - 3 * a;
+    KeyArgs k;
+    k.status = p->status;
+    k.zidx = p->zidx;
+    k.yidx = p->yidx;
+    k.xidx = p->xidx;
+    k.n = p->n;
+    k.nz = (int)shape[0];
+    k.ny = (int)shape[1];
+    k.nx = (int)shape[2];
+    k.sz = shift_for(k.nz, 0);
+    k.sy = shift_for(k.ny, 0);
+    k.sx = shift_for(k.nx, 2);
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned grid = (unsigned)((p->n + kBlock - 1) / kBlock);
+    k_cell_keys<<<grid, kBlock, 0, st>>>(k, keys_in, ids_in);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles: %s", cudaGetErrorString(e));
+    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, ids_in, perm, (int)p->n, 0, 32, st);
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles: radix sort: %s", cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+int opb_gather_particles(const opb_particles *src, const opb_particles *dst, const int32_t *perm,
+                         const int64_t *src_ids, int64_t *dst_ids, void *stream) {
+    if (!src || !dst || !perm) return fail(OPB_EINVAL, "opb_gather_particles: NULL argument");
+    if (src->n != dst->n) return fail(OPB_EINVAL, "opb_gather_particles: particle counts differ");
+    if (src->n < 0 || src->n > 0x7fffffffLL) return fail(OPB_EINVAL, "opb_gather_particles: bad particle count");
+    if (src->n == 0) return OPB_OK;
+    if (!src->status || !dst->status) return fail(OPB_EINVAL, "opb_gather_particles: status is NULL");
+    if ((src_ids == nullptr) != (dst_ids == nullptr))
+        return fail(OPB_EINVAL, "opb_gather_particles: give both id arrays or neither");
+    GatherArgs g{};
+    g.s_status = src->status;
+    g.d_status = dst->status;
+    const double *s[13] = {src->zidx, src->yidx, src->xidx, src->z, src->dxidx0, src->dyidx0, src->dz0,
+                           src->dxidx1, src->dyidx1, src->dz1, src->dxidx2, src->dyidx2, src->dz2};
+    double *d[13] = {dst->zidx, dst->yidx, dst->xidx, dst->z, dst->dxidx0, dst->dyidx0, dst->dz0,
+                     dst->dxidx1, dst->dyidx1, dst->dz1, dst->dxidx2, dst->dyidx2, dst->dz2};
+    int nf = 0;
+    for (int f = 0; f < 13; ++f) {
+        if ((s[f] == nullptr) != (d[f] == nullptr))
+            return fail(OPB_EINVAL, "opb_gather_particles: source and destination fields differ");
+        if (s[f]) {
+            g.s[nf] = s[f];
+            g.d[nf] = d[f];
+            ++nf;
+        }
+    }
+    g.nf = nf;
+    g.n = src->n;
+    g.s_ids = src_ids;
+    g.d_ids = dst_ids;
+    const unsigned grid = (unsigned)((src->n + kBlock - 1) / kBlock);
+    k_gather<<<grid, kBlock, 0, (cudaStream_t)stream>>>(g, perm);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_gather_particles: %s", cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+}  // extern "C"

@@ -26,12 +26,9 @@ def _ptr(t: torch.Tensor | None) -> int | None:
     return t.data_ptr()
 
 
-def particles_struct(particles) -> _lib.opb_particles:
-    """opb_particles for a Particles object (pointers are fixed for its lifetime)."""
-    cache = object.__getattribute__(particles, "_abi_cache") if hasattr(type(particles), "_abi_cache") else None
-    if cache is not None:
-        return cache
-    arrays = particles.arrays
+def particles_struct_for(arrays: Mapping[str, torch.Tensor], n: int, err: torch.Tensor | None = None
+                         ) -> _lib.opb_particles:
+    """opb_particles over a dict of particle-field tensors."""
     kw = {}
     for name in _lib.PARTICLE_POINTERS:
         t = arrays.get(name)
@@ -41,9 +38,21 @@ def particles_struct(particles) -> _lib.opb_particles:
     status = arrays["status"]
     if status.dtype != torch.uint8:
         raise TypeError("particle field status must be uint8")
-    err = getattr(particles, "error_word", None)
-    s = _lib.opb_particles(n=status.shape[0], status=_ptr(status), err=_ptr(err), **kw)
-    if hasattr(type(particles), "_abi_cache"):
+    if status.shape[0] != n:
+        raise ValueError("particle arrays do not match the particle count")
+    return _lib.opb_particles(n=n, status=_ptr(status), err=_ptr(err), **kw)
+
+
+def particles_struct(particles) -> _lib.opb_particles:
+    """opb_particles for a Particles object (cached until its storage is reordered)."""
+    cached = hasattr(type(particles), "_abi_cache")
+    if cached:
+        cache = object.__getattribute__(particles, "_abi_cache")
+        if cache is not None:
+            return cache
+    s = particles_struct_for(particles.arrays, particles.arrays["status"].shape[0],
+                             getattr(particles, "error_word", None))
+    if cached:
         object.__setattr__(particles, "_abi_cache", s)
     return s
 

@@ -1,20 +1,28 @@
 """Particles: a structure of arrays in device memory (particles.py:1-122 of the reference).
 
 Each particle field is a 1-D CUDA tensor; the kernels mutate them in place.
-``ParticlesView`` keeps the reference's read-only semantics: indexing it
-returns a read-only host numpy copy (which synchronises); ``tensor(name)``
-gives the device tensor itself without a copy.
+The device arrays may be kept in a spatial (Morton) storage order that differs
+from the particles' original order: ``sort`` reorders every field together
+and remembers each slot's original particle id.  Everything facing the user
+-- ``ParticlesView`` items, ``Simulation.set_indices`` / ``set_particle_field``
+-- speaks the original order; only the kernels see storage order, and they
+are per particle, so the order changes no result.
 """
 
 from __future__ import annotations
 
+import ctypes
 import types
 from typing import Mapping
 
 import numpy as np
 import torch
 
-from ._device import cuda_device, numpy_dtype, torch_dtype
+from ._device import cuda_device, numpy_dtype, stream_handle, torch_dtype
+
+
+# Observers of storage sorts: callables run after each Particles.sort (used for counting launches).
+sort_observers: list = []
 
 
 class _FrozenArrayMapping:
@@ -64,9 +72,9 @@ class _FrozenArrayMapping:
         return f"{self.__class__.__name__}(shape={self.shape}, fields={{ {fields} }})"
 
     def __str__(self) -> str:
-        arrays = object.__getattribute__(self, "_arrays")
-        public = [name for name in arrays if not name.startswith("_")]
-        hidden = sum(1 for name in arrays if name.startswith("_"))
+        names = list(self.dtypes)
+        public = [name for name in names if not name.startswith("_")]
+        hidden = sum(1 for name in names if name.startswith("_"))
         hidden_str = f", +{hidden} hidden fields" if hidden > 1 else (", +1 hidden field" if hidden == 1 else "")
         return f"{self.__class__.__name__} (shape={self.shape}, fields=[{', '.join(public)}]{hidden_str})"
 
@@ -74,7 +82,7 @@ class _FrozenArrayMapping:
 class Particles(_FrozenArrayMapping):
     """``nparticles`` particles with the given ``field=dtype`` arrays, zero-initialised on the device."""
 
-    __slots__ = ("_length", "_device", "_err", "_abi_cache")
+    __slots__ = ("_length", "_device", "_err", "_abi_cache", "_order", "_spare", "_perm", "_workspace")
 
     def __init__(self, nparticles: int, *, device=None, **fields) -> None:
         dev = cuda_device(device)
@@ -85,6 +93,10 @@ class Particles(_FrozenArrayMapping):
         # device error word written by the kernels (OPB_ERRF_*)
         object.__setattr__(self, "_err", torch.zeros((1,), dtype=torch.int32, device=dev))
         object.__setattr__(self, "_abi_cache", None)
+        object.__setattr__(self, "_order", None)  # original id of each storage slot (None: identity)
+        object.__setattr__(self, "_spare", None)
+        object.__setattr__(self, "_perm", None)
+        object.__setattr__(self, "_workspace", None)
 
     def __len__(self) -> int:
         return object.__getattribute__(self, "_length")
@@ -96,6 +108,11 @@ class Particles(_FrozenArrayMapping):
     @property
     def error_word(self) -> torch.Tensor:
         return object.__getattribute__(self, "_err")
+
+    @property
+    def order(self) -> torch.Tensor | None:
+        """Original particle id of every storage slot, or None while storage order is the original order."""
+        return object.__getattribute__(self, "_order")
 
     def check_errors(self) -> None:
         """Raise what the kernels recorded since the last check (synchronises)."""
@@ -109,28 +126,115 @@ class Particles(_FrozenArrayMapping):
                 raise ZeroDivisionError("float division")
             raise RuntimeError(f"device error word 0x{value:x}")
 
+    # ---------------------------------------------------------- original order
+    def original(self, name: str) -> torch.Tensor:
+        """A device copy of field ``name`` in the particles' original order."""
+        t = self.arrays[name]
+        order = self.order
+        if order is None:
+            return t.clone()
+        out = torch.empty_like(t)
+        out.index_copy_(0, order, t)
+        return out
 
-class ParticlesView(_FrozenArrayMapping):
-    """A read-only view of particle arrays; items are host numpy copies."""
+    def assign(self, name: str, values: torch.Tensor) -> None:
+        """Set field ``name`` from ``values`` given in the particles' original order."""
+        t = self.arrays[name]
+        order = self.order
+        values = values.to(device=t.device, dtype=t.dtype).expand(t.shape)
+        t.copy_(values if order is None else values.index_select(0, order))
 
-    __slots__ = ("_length", "_parent")
+    # ------------------------------------------------------------- reordering
+    def sort(self, shape: tuple[int, int, int]) -> None:
+        """Reorder storage by the Morton code of each particle's cell on the centred ``(z, y, x)`` grid."""
+        from . import _lib
+        from .kernels import _abi
+
+        n = len(self)
+        if n == 0:
+            return
+        lib = _lib.load()
+        if object.__getattribute__(self, "_workspace") is None:
+            ws = torch.empty(int(lib.opb_sort_workspace_bytes(n)), dtype=torch.uint8, device=self.device)
+            object.__setattr__(self, "_workspace", ws)
+            object.__setattr__(self, "_perm", torch.empty(n, dtype=torch.int32, device=self.device))
+            object.__setattr__(self, "_spare", {k: torch.empty_like(v) for k, v in self.arrays.items()})
+        ws = object.__getattribute__(self, "_workspace")
+        perm = object.__getattribute__(self, "_perm")
+        spare = object.__getattribute__(self, "_spare")
+        src = _abi.particles_struct(self)
+        dims = (ctypes.c_int64 * 3)(*[int(s) for s in shape])
+        stream = stream_handle(self.device)
+        _lib.call("opb_sort_particles", ctypes.byref(src), ctypes.byref(dims), perm.data_ptr(), ws.data_ptr(),
+                  ws.numel(), stream)
+        order = self.order
+        if order is None:
+            order = torch.arange(n, dtype=torch.int64, device=self.device)
+        new_order = torch.empty_like(order)
+        dst = _abi.particles_struct_for(spare, n)
+        _lib.call("opb_gather_particles", ctypes.byref(src), ctypes.byref(dst), perm.data_ptr(), order.data_ptr(),
+                  new_order.data_ptr(), stream)
+        # fields the kernels do not know about (e.g. output fields) are gathered by torch
+        known = {"status", *_lib.PARTICLE_POINTERS}
+        perm64 = None
+        for k, t in self.arrays.items():
+            if k not in known:
+                if perm64 is None:
+                    perm64 = perm.to(torch.int64)
+                torch.index_select(t, 0, perm64, out=spare[k])
+        old = dict(self.arrays)
+        object.__setattr__(self, "_arrays", types.MappingProxyType(dict(spare)))
+        object.__setattr__(self, "_spare", old)
+        object.__setattr__(self, "_order", new_order)
+        object.__setattr__(self, "_abi_cache", None)
+        for obs in sort_observers:
+            obs()
+
+
+class ParticlesView:
+    """A read-only view of particle arrays; items are host numpy copies in original order."""
+
+    __slots__ = ("_parent",)
 
     def __init__(self, parent: Particles) -> None:
-        object.__setattr__(self, "_length", len(parent))
         object.__setattr__(self, "_parent", parent)
-        super().__init__(**dict(parent.arrays))
+
+    def __setattr__(self, name, value):
+        raise AttributeError("ParticlesView is immutable")
 
     def __getitem__(self, name: str) -> np.ndarray:
         parent = object.__getattribute__(self, "_parent")
-        t = parent.arrays[name]
+        if name not in parent:
+            raise KeyError(name)
         parent.check_errors()
-        arr = t.cpu().numpy()
+        arr = parent.original(name).cpu().numpy()
         arr.setflags(write=False)
         return arr
 
+    def __getattr__(self, name: str) -> np.ndarray:
+        try:
+            return self[name]
+        except KeyError:
+            raise AttributeError(f"'ParticlesView' object has no attribute '{name}'")
+
+    def __contains__(self, name: str) -> bool:
+        return name in object.__getattribute__(self, "_parent")
+
     def tensor(self, name: str) -> torch.Tensor:
-        """The device tensor of a particle field (no copy; do not modify)."""
+        """The device tensor of a particle field in STORAGE order (no copy; do not modify)."""
         return object.__getattribute__(self, "_parent").arrays[name]
+
+    @property
+    def arrays(self) -> Mapping:
+        return object.__getattribute__(self, "_parent").arrays
+
+    @property
+    def dtypes(self) -> Mapping[str, np.dtype]:
+        return object.__getattribute__(self, "_parent").dtypes
+
+    @property
+    def shape(self) -> tuple[int, ...]:
+        return object.__getattribute__(self, "_parent").shape
 
     @staticmethod
     def readonly_view(array) -> np.ndarray:
@@ -139,4 +243,8 @@ class ParticlesView(_FrozenArrayMapping):
         return view
 
     def __len__(self) -> int:
-        return object.__getattribute__(self, "_length")
+        return len(object.__getattribute__(self, "_parent"))
+
+    def __repr__(self) -> str:
+        fields = ", ".join(f"{name}:{dtype}" for name, dtype in self.dtypes.items())
+        return f"ParticlesView(shape={self.shape}, fields={{ {fields} }})"

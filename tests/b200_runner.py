@@ -30,7 +30,8 @@ def b200_fieldset(fields: dict, hc: float, nz: int, ring_size: int = 4):
     return opb.Fieldset(nt, nz, ny, nxu + 1, constants={"hc": hc, "NZ": nz}, **kw)
 
 
-def build_sim(fields, *, hc, nz, scheme, dt, z, y, x, status=None, unfused=False, ring_size=4, time=None):
+def build_sim(fields, *, hc, nz, scheme, dt, z, y, x, status=None, unfused=False, ring_size=4, time=None,
+              sort_interval=None):
     import offline_particles_b200 as opb
     from offline_particles_b200.kernels import ParticleKernel
     from offline_particles_b200.kernels.validation import domain_bounds_kernel, finite_indices_kernel
@@ -47,7 +48,8 @@ def build_sim(fields, *, hc, nz, scheme, dt, z, y, x, status=None, unfused=False
         assert not ts.fused()
     else:
         assert ts.fused()
-    sim = opb.SimulationBuilder(ts, fs).build_simulation(len(z))
+    kw = {} if sort_interval is None else {"sort_interval": sort_interval}
+    sim = opb.SimulationBuilder(ts, fs).build_simulation(len(z), **kw)
     sim.set_indices(z, y, x)
     if status is not None:
         sim.set_particle_field("status", status)
@@ -57,10 +59,10 @@ def build_sim(fields, *, hc, nz, scheme, dt, z, y, x, status=None, unfused=False
 
 
 def run_b200(fields, *, hc, nz, scheme, dt, steps, z, y, x, status=None, mode="step", record_every=0,
-             record_idx=None, ring_size=4):
+             record_idx=None, ring_size=4, sort_interval=None):
     """mode: 'step' (one fused launch per step), 'run' (multi-step launches) or 'stages' (stage kernels)."""
     sim = build_sim(fields, hc=hc, nz=nz, scheme=scheme, dt=dt, z=z, y=y, x=x, status=status,
-                    unfused=(mode == "stages"), ring_size=ring_size)
+                    unfused=(mode == "stages"), ring_size=ring_size, sort_interval=sort_interval)
     rec = []
     if mode == "run" and record_every:
         for _ in range(steps // record_every):
