@@ -52,30 +52,39 @@ struct DScalars {
 // ------------------------------------------------------------------ fields
 // A field bound to one time selection: FieldData(array, offsets) of
 // fields.py:12 whose array is the blend prev*gt + next*ft (fields.py:426-428),
-// evaluated per gathered element instead of over the whole grid.
-template <typename T>
+// evaluated per gathered element instead of over the whole grid.  `I` is the
+// index type: int when every field has fewer than 2^31 elements (cheaper
+// address arithmetic, fewer registers), else long long.
+// Field kinds: KIND_ANY decides per access (static or time-dependent, known
+// only at run time); KIND_STATIC / KIND_TD fix it at compile time, which lets
+// the compiler drop the per-corner test (the ROMS layout: u, v, w, zeta
+// time-dependent; h, dx, dy, C static).
+constexpr int KIND_ANY = 0, KIND_STATIC = 1, KIND_TD = 2;
+
+template <typename T, typename I, int KIND = KIND_ANY>
 struct View {
+    using index_type = I;
     const T *prev;
     const T *next;
     const double *stat;  // non-null: static float64 field
     T ft, gt;
-    long long n0, n1, n2;
+    I n0, n1, n2;
     double o0, o1, o2;
 
     // fields.py:423-428: both products and their sum in the storage dtype,
     // then widened to float64 (np.add(..., out=float64, casting="unsafe")
     // adds in the inputs' dtype).
-    __device__ __forceinline__ double at(long long i) const {
-        if (stat) return __ldg(stat + i);
+    __device__ __forceinline__ double at(I i) const {
+        if (KIND == KIND_STATIC || (KIND == KIND_ANY && stat)) return __ldg(stat + i);
         const T a = __ldg(prev + i) * gt;
         const T b = __ldg(next + i) * ft;
         return (double)(a + b);
     }
 };
 
-template <typename T>
-__device__ __forceinline__ View<T> bind(const DField &f, const opb_time &t) {
-    View<T> v;
+template <typename T, typename I, int KIND = KIND_ANY>
+__device__ __forceinline__ View<T, I, KIND> bind(const DField &f, const opb_time &t) {
+    View<T, I, KIND> v;
     if (f.is_static) {
         v.stat = (const double *)f.data[0];
         v.prev = v.next = nullptr;
@@ -87,9 +96,9 @@ __device__ __forceinline__ View<T> bind(const DField &f, const opb_time &t) {
         v.ft = (T)t.ft;  // exact: the host rounded ft, gt to the storage dtype
         v.gt = (T)t.gt;
     }
-    v.n0 = f.n0;
-    v.n1 = f.n1;
-    v.n2 = f.n2;
+    v.n0 = (I)f.n0;
+    v.n1 = (I)f.n1;
+    v.n2 = (I)f.n2;
     v.o0 = f.o0;
     v.o1 = f.o1;
     v.o2 = f.o2;
@@ -108,10 +117,20 @@ __device__ __forceinline__ long long trunc_index(double idx, long long max_idx) 
     return i;
 }
 
+// The same map in 32-bit arithmetic, for max_idx < 2^31: anything that is not
+// in [1, 2^63) (NaN, negatives, -inf, +huge) gives 0, [max_idx, 2^63) gives
+// max_idx, and the rest truncates exactly as the 64-bit conversion does.
+__device__ __forceinline__ int trunc_index(double idx, int max_idx) {
+    if (!(idx >= 1.0 && idx < 9.223372036854775808e18)) return 0;
+    if (idx >= (double)max_idx) return max_idx;
+    return (int)idx;
+}
+
 // linear.pxd:11-17
 template <typename F>
 __device__ __forceinline__ double linear(const F &f, double idx) {
-    const long long I0 = trunc_index(idx, f.n0 - 2);
+    using I = typename F::index_type;
+    const I I0 = trunc_index(idx, (I)(f.n0 - 2));
     const double f0 = idx - (double)I0;
     const double g0 = 1.0 - f0;
     return g0 * f.at(I0) + f0 * f.at(I0 + 1);
@@ -120,13 +139,14 @@ __device__ __forceinline__ double linear(const F &f, double idx) {
 // linear.pxd:19-33
 template <typename F>
 __device__ __forceinline__ double bilinear(const F &f, double idx0, double idx1) {
-    const long long I0 = trunc_index(idx0, f.n0 - 2);
-    const long long I1 = trunc_index(idx1, f.n1 - 2);
+    using I = typename F::index_type;
+    const I I0 = trunc_index(idx0, (I)(f.n0 - 2));
+    const I I1 = trunc_index(idx1, (I)(f.n1 - 2));
     const double f0 = idx0 - (double)I0;
     const double f1 = idx1 - (double)I1;
     const double g0 = 1.0 - f0;
     const double g1 = 1.0 - f1;
-    const long long b = I0 * f.n1 + I1;
+    const I b = I0 * f.n1 + I1;
     const double v00 = f.at(b);
     const double v01 = f.at(b + 1);
     const double v10 = f.at(b + f.n1);
@@ -137,18 +157,19 @@ __device__ __forceinline__ double bilinear(const F &f, double idx0, double idx1)
 // linear.pxd:35-65
 template <typename F>
 __device__ __forceinline__ double trilinear(const F &f, double idx0, double idx1, double idx2) {
-    const long long I0 = trunc_index(idx0, f.n0 - 2);
-    const long long I1 = trunc_index(idx1, f.n1 - 2);
-    const long long I2 = trunc_index(idx2, f.n2 - 2);
+    using I = typename F::index_type;
+    const I I0 = trunc_index(idx0, (I)(f.n0 - 2));
+    const I I1 = trunc_index(idx1, (I)(f.n1 - 2));
+    const I I2 = trunc_index(idx2, (I)(f.n2 - 2));
     const double f0 = idx0 - (double)I0;
     const double f1 = idx1 - (double)I1;
     const double f2 = idx2 - (double)I2;
     const double g0 = 1.0 - f0;
     const double g1 = 1.0 - f1;
     const double g2 = 1.0 - f2;
-    const long long s1 = f.n2;
-    const long long s0 = f.n1 * f.n2;
-    const long long b = I0 * s0 + I1 * s1 + I2;
+    const I s1 = f.n2;
+    const I s0 = f.n1 * f.n2;
+    const I b = I0 * s0 + I1 * s1 + I2;
     const double v000 = f.at(b);
     const double v001 = f.at(b + 1);
     const double v010 = f.at(b + s1);
@@ -209,37 +230,84 @@ __device__ __forceinline__ double sigma_from_Cidx(long long Cidx, double C_offse
     return sigma_coordinate(zidx, Nz);
 }
 
-// S(k) of sigma level k of the C table
-__device__ __forceinline__ double S_level(long long k, const double *C, double C_offset, int NZ, double hc, double h) {
-    return S_coordinate(hc, sigma_from_Cidx(k, C_offset, NZ), h, __ldg(C + k));
+// The C levels the vertical search probes.  sigma_from_Cidx depends on the
+// level only, so each block tabulates it (with C) in shared memory once:
+// every probe then reads the same value the reference computes, minus one
+// float64 division.  sigma == nullptr: compute on the fly from global C.
+constexpr int kMaxLevels = 128;
+
+struct Levels {
+    const double *sigma;  // sigma_from_Cidx(k) for k < size, or nullptr
+    const double *C;      // C[k]
+    int size;             // C.shape[0]
+    double C_offset;
+    int Nz;
+    bool monotone;        // sigma and C non-decreasing (checked on the device)
+};
+
+__device__ __forceinline__ double level_sigma(const Levels &L, int k) {
+    return L.sigma ? L.sigma[k] : sigma_from_Cidx(k, L.C_offset, L.Nz);
 }
 
-// _vertical_coordinate.pxd:50-103: compute_zidx.  The binary search visits
-// the same levels and makes the same comparisons as the reference; S(lo) and
-// S(hi) are carried through the search so that the final interpolation reuses
-// them (identical values: S_level is a pure function of the level).
-__device__ __forceinline__ double compute_zidx(double z, double h, double zeta, double hc, int NZ, const double *C,
-                                               long long C_size, double C_offset) {
-    const double S = S_from_z(z, h, zeta);
-    long long lo = 0, hi = C_size - 2;
-    const double S0 = S_level(0, C, C_offset, NZ, hc, h);
-    long long Cidx;
+// S(k) of sigma level k
+__device__ __forceinline__ double S_level(const Levels &L, int k, double hc, double h) {
+    return S_coordinate(hc, level_sigma(L, k), h, L.C[k]);
+}
+
+// Fill the shared tables and test monotonicity.  Every thread of the block
+// must call this before any thread returns (it synchronises the block).
+__device__ __forceinline__ Levels load_levels(const double *C_global, long long C_size, double C_offset, int Nz,
+                                              double *s_sigma, double *s_C) {
+    Levels L;
+    L.size = (int)C_size;
+    L.C_offset = C_offset;
+    L.Nz = Nz;
+    const bool fits = C_size <= kMaxLevels;
+    if (fits) {
+        for (int k = threadIdx.x; k < C_size; k += blockDim.x) {
+            s_sigma[k] = sigma_from_Cidx(k, C_offset, Nz);
+            s_C[k] = __ldg(C_global + k);
+        }
+        L.sigma = s_sigma;
+        L.C = s_C;
+    } else {
+        L.sigma = nullptr;
+        L.C = C_global;
+    }
+    __syncthreads();
+    bool ok = fits && Nz > 0;
+    if (fits)
+        for (int k = threadIdx.x; k + 1 < C_size; k += blockDim.x)
+            ok = ok && (s_sigma[k] <= s_sigma[k + 1]) && (s_C[k] <= s_C[k + 1]);
+    L.monotone = __syncthreads_and(ok) != 0;
+    return L;
+}
+
+// _vertical_coordinate.pxd:50-96 for a given S: the reference's binary
+// search, visiting the same levels and making the same comparisons.  S(lo)
+// and S(hi) are carried through the search so that the final interpolation
+// reuses them (identical values: S_level is a pure function of the level).
+__device__ __forceinline__ double zidx_from_S_search(double S, double h, double hc, const Levels &L) {
+    const int C_size = L.size;
+    int lo = 0, hi = C_size - 2;
+    const double S0 = S_level(L, 0, hc, h);
+    int Cidx;
     double S_low, S_high;
     if (S <= S0) {
         Cidx = 0;
         S_low = S0;
-        S_high = S_level(1, C, C_offset, NZ, hc, h);
+        S_high = S_level(L, 1, hc, h);
     } else {
-        const double Sn = S_level(C_size - 2, C, C_offset, NZ, hc, h);
+        const double Sn = S_level(L, C_size - 2, hc, h);
         if (S >= Sn) {
             Cidx = C_size - 2;
             S_low = Sn;
-            S_high = S_level(C_size - 1, C, C_offset, NZ, hc, h);
+            S_high = S_level(L, C_size - 1, hc, h);
         } else {
             double S_lo = S0, S_hi = Sn;
             while (lo < hi - 1) {
-                const long long mid = (lo + hi) / 2;
-                const double S_mid = S_level(mid, C, C_offset, NZ, hc, h);
+                const int mid = (lo + hi) / 2;
+                const double S_mid = S_level(L, mid, hc, h);
                 if (S_mid <= S) {
                     lo = mid;
                     S_lo = S_mid;
@@ -252,7 +320,7 @@ __device__ __forceinline__ double compute_zidx(double z, double h, double zeta, 
             S_low = S_lo;
             // after the loop hi == lo + 1 unless the search never ran (hi <= lo + 1
             // from the start, i.e. C_size <= 3); recompute in that case
-            S_high = (hi == lo + 1) ? S_hi : S_level(lo + 1, C, C_offset, NZ, hc, h);
+            S_high = (hi == lo + 1) ? S_hi : S_level(L, lo + 1, hc, h);
         }
     }
     // _vertical_coordinate.pxd:86-96
@@ -260,7 +328,88 @@ __device__ __forceinline__ double compute_zidx(double z, double h, double zeta, 
     const double den = S_high - S_low;
     if (den == 0.0) return 0.0;
     const double f = num / den;
-    return ((double)Cidx - C_offset) + f;
+    return ((double)Cidx - L.C_offset) + f;
+}
+
+// _vertical_coordinate.pxd:98-103: compute_zidx, as the reference computes it.
+__device__ __forceinline__ double compute_zidx(double z, double h, double zeta, double hc, const Levels &L) {
+    return zidx_from_S_search(S_from_z(z, h, zeta), h, hc, L);
+}
+
+// compute_zidx starting from a level hint (the particle's previous zidx).
+//
+// Same result as the reference's binary search, bit for bit.  When sigma and
+// C are non-decreasing and hc, h >= 0 with hc + h > 0, every rounded S(k) =
+// RN(RN(RN(hc sigma_k) + RN(h C_k)) / (hc + h)) is non-decreasing in k, and
+// for S strictly between S(0) and S(C_size - 2) the binary search ends on the
+// unique k with S(k) <= S < S(k + 1); at the ends it returns 0 for S <= S(0)
+// (tested first) and C_size - 2 for S >= S(C_size - 2).  This function finds
+// that same k by walking from the hint, which is almost always the right
+// level already (particles move ~0.001 levels per step), so a call costs two
+// S(k) evaluations instead of a whole search.  Anything outside those
+// conditions -- a non-finite S or h, negative depths, a non-monotone table, a
+// hint more than a few levels off -- runs the reference's search instead.
+__device__ __forceinline__ double compute_zidx_hint(double z, double h, double zeta, double hc, const Levels &L,
+                                                    double zidx_hint) {
+    const double S = S_from_z(z, h, zeta);
+    const int top = L.size - 2;
+    if (!(L.monotone && top >= 1 && h >= 0.0 && hc >= 0.0 && hc + h > 0.0 && isfinite(S) && isfinite(h) &&
+          isfinite(hc)))
+        return zidx_from_S_search(S, h, hc, L);
+    const double hk = zidx_hint + L.C_offset;
+    int k = (hk >= 1.0 && hk < (double)top) ? (int)hk : (hk >= (double)top ? top : 0);
+    constexpr int kMaxWalk = 3;
+    int Cidx;
+    double S_low, S_high;
+    double lo_v = S_level(L, k, hc, h);
+    if (lo_v > S) {  // walk down
+        double hi_v = lo_v;
+        int walked = 0;
+        while (k > 0 && lo_v > S) {
+            if (++walked > kMaxWalk) return zidx_from_S_search(S, h, hc, L);
+            hi_v = lo_v;
+            --k;
+            lo_v = S_level(L, k, hc, h);
+        }
+        Cidx = k;
+        S_low = lo_v;
+        S_high = (walked > 0) ? hi_v : S_level(L, 1, hc, h);  // walked == 0 only when k == 0
+    } else {  // walk up
+        int walked = 0;
+        for (;;) {
+            if (k == top) {
+                Cidx = top;
+                S_low = lo_v;
+                S_high = S_level(L, top + 1, hc, h);
+                break;
+            }
+            const double hi_v = S_level(L, k + 1, hc, h);
+            if (hi_v > S) {
+                Cidx = k;
+                S_low = lo_v;
+                S_high = hi_v;
+                break;
+            }
+            if (++walked > kMaxWalk) return zidx_from_S_search(S, h, hc, L);
+            ++k;
+            lo_v = hi_v;
+        }
+    }
+    // the reference tests S <= S(0) first: on a plateau S(0) == ... == S(Cidx) == S it returns 0
+    if (Cidx > 0 && S_low == S) {
+        const double S0 = S_level(L, 0, hc, h);
+        if (S <= S0) {
+            Cidx = 0;
+            S_low = S0;
+            S_high = S_level(L, 1, hc, h);
+        }
+    }
+    // _vertical_coordinate.pxd:86-96
+    const double num = S - S_low;
+    const double den = S_high - S_low;
+    if (den == 0.0) return 0.0;
+    const double f = num / den;
+    return ((double)Cidx - L.C_offset) + f;
 }
 
 // ----------------------------------------------------------------- status

@@ -35,47 +35,47 @@ __device__ __forceinline__ void raise_zero_division(const DParticles &p) {
     if (p.err) atomicOr(p.err, (uint32_t)OPB_ERRF_ZERO_DIVISION);
 }
 
-template <typename T>
+// The fields of one stage.  FIXED: the ROMS layout (u, v, w, zeta
+// time-dependent; h, dx, dy, C static), known at compile time; otherwise each
+// field's kind is read at run time.
+template <typename T, typename I, bool FIXED = false>
 struct Bound {
-    View<T> u, v, w, dx, dy, h, zeta;
+    static constexpr int KT = FIXED ? KIND_TD : KIND_ANY;
+    static constexpr int KS = FIXED ? KIND_STATIC : KIND_ANY;
+    View<T, I, KT> u, v, w, zeta;
+    View<T, I, KS> dx, dy, h, C;
 };
 
-template <typename T>
-__device__ __forceinline__ Bound<T> bind_all(const DRoms &r, const opb_time &t) {
-    Bound<T> b;
-    b.u = bind<T>(r.u, t);
-    b.v = bind<T>(r.v, t);
-    b.w = bind<T>(r.w, t);
-    b.dx = bind<T>(r.dx, t);
-    b.dy = bind<T>(r.dy, t);
-    b.h = bind<T>(r.h, t);
-    b.zeta = bind<T>(r.zeta, t);
+template <typename T, typename I, bool FIXED = false>
+__device__ __forceinline__ Bound<T, I, FIXED> bind_all(const DRoms &r, const opb_time &t) {
+    using B = Bound<T, I, FIXED>;
+    B b;
+    b.u = bind<T, I, B::KT>(r.u, t);
+    b.v = bind<T, I, B::KT>(r.v, t);
+    b.w = bind<T, I, B::KT>(r.w, t);
+    b.zeta = bind<T, I, B::KT>(r.zeta, t);
+    b.dx = bind<T, I, B::KS>(r.dx, t);
+    b.dy = bind<T, I, B::KS>(r.dy, t);
+    b.h = bind<T, I, B::KS>(r.h, t);
+    b.C = bind<T, I, B::KS>(r.C, t);  // static float64 (kernels/_core.pyx:5-9)
     return b;
 }
 
-// View over the static float64 C table (kernels/_core.pyx:5-9)
-struct CView {
-    const double *a;
-    long long n0;
-    double o0;
-    __device__ __forceinline__ double at(long long i) const { return __ldg(a + i); }
-};
-
-__device__ __forceinline__ CView c_view(const DRoms &r) {
-    CView c;
-    c.a = (const double *)r.C.data[0];
-    c.n0 = r.C.n0;
-    c.o0 = r.C.o0;
-    return c;
-}
+// Every kernel starts here, before any thread can return: the block's shared
+// tables of the sigma levels (used by compute_zidx).
+#define OPB_LEVELS(r, sc)                                                                            \
+    __shared__ double s_sigma[kMaxLevels];                                                           \
+    __shared__ double s_C[kMaxLevels];                                                               \
+    const Levels L = load_levels((const double *)(r).C.data[0], (r).C.n0, (r).C.o0, (sc).NZ, s_sigma, s_C); \
+    __syncthreads()
 
 // rk2_w_advection.pyx:97-153 (stage 1 for one particle).  Returns false on a
 // zero grid spacing (the reference raises ZeroDivisionError).
-template <typename T>
-__device__ __forceinline__ bool rk2_stage1(PState &s, const Bound<T> &f, const CView &C, const DScalars &sc) {
+template <typename B>
+__device__ __forceinline__ bool rk2_stage1(PState &s, const B &f, const DScalars &sc) {
     const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
     const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
-    const double Cv = linear(C, s.zidx + C.o0);
+    const double Cv = linear(f.C, s.zidx + f.C.o0);
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
     const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
@@ -89,15 +89,15 @@ __device__ __forceinline__ bool rk2_stage1(PState &s, const Bound<T> &f, const C
 }
 
 // rk2_w_advection.pyx:225-275 (stage 2 for one particle)
-template <typename T>
-__device__ __forceinline__ bool rk2_stage2(PState &s, const Bound<T> &f, const CView &C, const DScalars &sc) {
+template <typename B>
+__device__ __forceinline__ bool rk2_stage2(PState &s, const B &f, const Levels &L, const DScalars &sc) {
     const double adt = sc.alpha * sc.dt;
     const double z_int = s.z + adt * s.k1z;
     const double y_int = s.yidx + adt * s.k1y;
     const double x_int = s.xidx + adt * s.k1x;
     const double h = bilinear(f.h, y_int + f.h.o0, x_int + f.h.o1);
     const double zeta = bilinear(f.zeta, y_int + f.zeta.o0, x_int + f.zeta.o1);
-    const double z_idx = compute_zidx(z_int, h, zeta, sc.hc, sc.NZ, C.a, C.n0, C.o0);
+    const double z_idx = compute_zidx_hint(z_int, h, zeta, sc.hc, L, s.zidx);
     const double u = trilinear(f.u, z_idx + f.u.o0, y_int + f.u.o1, x_int + f.u.o2);
     const double v = trilinear(f.v, z_idx + f.v.o0, y_int + f.v.o1, x_int + f.v.o2);
     const double dx = bilinear(f.dx, y_int + f.dx.o0, x_int + f.dx.o1);
@@ -111,8 +111,8 @@ __device__ __forceinline__ bool rk2_stage2(PState &s, const Bound<T> &f, const C
 
 // rk2_w_advection.pyx:316-354 (update for one particle); b1 = 1/(2 alpha)
 // weights k1, the reference's own convention (rk2_w_advection.pyx:317-318).
-template <typename T>
-__device__ __forceinline__ void rk2_update(PState &s, const Bound<T> &f, const CView &C, const DScalars &sc) {
+template <typename B>
+__device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &L, const DScalars &sc) {
     const double b1 = 1.0 / (2.0 * sc.alpha);
     const double b2 = 1.0 - b1;
     const double b1dt = b1 * sc.dt;
@@ -122,12 +122,12 @@ __device__ __forceinline__ void rk2_update(PState &s, const Bound<T> &f, const C
     s.xidx = s.xidx + b1dt * s.k1x + b2dt * s.k2x;
     const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
     const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
-    s.zidx = compute_zidx(s.z, h, zeta, sc.hc, sc.NZ, C.a, C.n0, C.o0);
+    s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
 }
 
 // ab3_w_advection.pyx:84-178 (AB3 step for one particle)
-template <typename T>
-__device__ __forceinline__ bool ab3_step(PState &s, const Bound<T> &f, const CView &C, const DScalars &sc) {
+template <typename B>
+__device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &sc) {
     const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
     const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
     if (dx == 0.0) return false;
@@ -153,7 +153,7 @@ __device__ __forceinline__ bool ab3_step(PState &s, const Bound<T> &f, const CVi
     }
     const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
     const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
-    const double Cv = linear(C, s.zidx + C.o0);
+    const double Cv = linear(f.C, s.zidx + f.C.o0);
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double dt = sc.dt;
     s.z = s.z + dt * (23.0 * s.k0z - 16.0 * s.k1z + 5.0 * s.k2z) / 12.0;
@@ -169,11 +169,11 @@ __device__ __forceinline__ bool ab3_step(PState &s, const Bound<T> &f, const CVi
 }
 
 // ab3_w_advection.pyx:214-229 (post step for one particle)
-template <typename T>
-__device__ __forceinline__ void ab3_post(PState &s, const Bound<T> &f, const CView &C, const DScalars &sc) {
+template <typename B>
+__device__ __forceinline__ void ab3_post(PState &s, const B &f, const Levels &L, const DScalars &sc) {
     const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
     const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
-    s.zidx = compute_zidx(s.z, h, zeta, sc.hc, sc.NZ, C.a, C.n0, C.o0);
+    s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
 }
 
 __device__ __forceinline__ long long gtid() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
@@ -192,22 +192,21 @@ __global__ void __launch_bounds__(kBlock) k_validation(const __grid_constant__ D
     if (out != st) p.status[i] = out;
 }
 
-template <typename T>
+template <typename T, typename I>
 __global__ void __launch_bounds__(kBlock) k_compute_z(const __grid_constant__ DParticles p, double *out,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r, opb_time t) {
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
-    const Bound<T> f = bind_all<T>(r, t);
-    const CView C = c_view(r);
+    const Bound<T, I> f = bind_all<T, I>(r, t);
     const double yi = p.yidx[i], xi = p.xidx[i], zi = p.zidx[i];
     const double h = bilinear(f.h, yi + f.h.o0, xi + f.h.o1);
     const double zeta = bilinear(f.zeta, yi + f.zeta.o0, xi + f.zeta.o1);
-    const double Cv = linear(C, zi + C.o0);
+    const double Cv = linear(f.C, zi + f.C.o0);
     out[i] = compute_z(zi, sc.NZ, sc.hc, h, Cv, zeta);
 }
 
-template <typename T>
+template <typename T, typename I>
 __global__ void __launch_bounds__(kBlock) k_rk2_step_1(const __grid_constant__ DParticles p,
                                                        const __grid_constant__ DScalars sc,
                                                        const __grid_constant__ DRoms r, opb_time t) {
@@ -217,8 +216,7 @@ __global__ void __launch_bounds__(kBlock) k_rk2_step_1(const __grid_constant__ D
     s.zidx = p.zidx[i];
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
-    const Bound<T> f = bind_all<T>(r, t);
-    const bool ok = rk2_stage1<T>(s, f, c_view(r), sc);
+    const bool ok = rk2_stage1(s, bind_all<T, I>(r, t), sc);
     p.z[i] = s.z;
     if (!ok) {
         raise_zero_division(p);
@@ -229,21 +227,22 @@ __global__ void __launch_bounds__(kBlock) k_rk2_step_1(const __grid_constant__ D
     p.dz1[i] = s.k1z;
 }
 
-template <typename T>
+template <typename T, typename I>
 __global__ void __launch_bounds__(kBlock) k_rk2_step_2(const __grid_constant__ DParticles p,
                                                        const __grid_constant__ DScalars sc,
                                                        const __grid_constant__ DRoms r, opb_time t) {
+    OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
     PState s;
+    s.zidx = p.zidx[i];  // hint for the vertical search
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
     s.z = p.z[i];
     s.k1x = p.dxidx1[i];
     s.k1y = p.dyidx1[i];
     s.k1z = p.dz1[i];
-    const Bound<T> f = bind_all<T>(r, t);
-    if (!rk2_stage2<T>(s, f, c_view(r), sc)) {
+    if (!rk2_stage2(s, bind_all<T, I>(r, t), L, sc)) {
         raise_zero_division(p);
         return;
     }
@@ -252,10 +251,11 @@ __global__ void __launch_bounds__(kBlock) k_rk2_step_2(const __grid_constant__ D
     p.dz2[i] = s.k2z;
 }
 
-template <typename T>
+template <typename T, typename I>
 __global__ void __launch_bounds__(kBlock) k_rk2_update(const __grid_constant__ DParticles p,
                                                        const __grid_constant__ DScalars sc,
                                                        const __grid_constant__ DRoms r, opb_time t) {
+    OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
     PState s;
@@ -269,15 +269,14 @@ __global__ void __launch_bounds__(kBlock) k_rk2_update(const __grid_constant__ D
     s.k2x = p.dxidx2[i];
     s.k2y = p.dyidx2[i];
     s.k2z = p.dz2[i];
-    const Bound<T> f = bind_all<T>(r, t);
-    rk2_update<T>(s, f, c_view(r), sc);
+    rk2_update(s, bind_all<T, I>(r, t), L, sc);
     p.z[i] = s.z;
     p.yidx[i] = s.yidx;
     p.xidx[i] = s.xidx;
     p.zidx[i] = s.zidx;
 }
 
-template <typename T>
+template <typename T, typename I>
 __global__ void __launch_bounds__(kBlock) k_ab3(const __grid_constant__ DParticles p,
                                                 const __grid_constant__ DScalars sc,
                                                 const __grid_constant__ DRoms r, opb_time t) {
@@ -295,8 +294,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3(const __grid_constant__ DParticl
     s.k2x = p.dxidx2[i];
     s.k2y = p.dyidx2[i];
     s.k2z = p.dz2[i];
-    const Bound<T> f = bind_all<T>(r, t);
-    if (!ab3_step<T>(s, f, c_view(r), sc)) {
+    if (!ab3_step(s, bind_all<T, I>(r, t), sc)) {
         raise_zero_division(p);
         return;
     }
@@ -315,29 +313,31 @@ __global__ void __launch_bounds__(kBlock) k_ab3(const __grid_constant__ DParticl
     p.dz2[i] = s.k2z;
 }
 
-template <typename T>
+template <typename T, typename I>
 __global__ void __launch_bounds__(kBlock) k_ab3_post(const __grid_constant__ DParticles p,
                                                      const __grid_constant__ DScalars sc,
                                                      const __grid_constant__ DRoms r, opb_time t) {
+    OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
     PState s;
+    s.zidx = p.zidx[i];  // hint for the vertical search
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
     s.z = p.z[i];
-    const Bound<T> f = bind_all<T>(r, t);
-    ab3_post<T>(s, f, c_view(r), sc);
+    ab3_post(s, bind_all<T, I>(r, t), L, sc);
     p.zidx[i] = s.zidx;
 }
 
 // ------------------------------------------------------------ fused kernels
 // `nsteps` RK2 steps (timesteppers.py:241-257) per launch.  table[3*k + j]
 // selects the fields of step k, stage j (t, t + alpha dt, t + dt).
-template <typename T>
-__global__ void __launch_bounds__(kBlock) k_rk2_steps(const __grid_constant__ DParticles p,
+template <typename T, typename I, bool FIXED>
+__global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
                                                       const opb_time *__restrict__ table, int nsteps, int validate_pre) {
+    OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
     PState s;
@@ -347,22 +347,21 @@ __global__ void __launch_bounds__(kBlock) k_rk2_steps(const __grid_constant__ DP
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
     const uint8_t st0 = s.status;
-    const CView C = c_view(r);
     bool moved = false;
     for (int k = 0; k < nsteps; ++k) {
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table[3 * k], t2 = table[3 * k + 1], t3 = table[3 * k + 2];
-        if (!rk2_stage1<T>(s, bind_all<T>(r, t1), C, sc)) {
+        if (!rk2_stage1(s, bind_all<T, I, FIXED>(r, t1), sc)) {
             raise_zero_division(p);
             break;
         }
         moved = true;
-        if (!rk2_stage2<T>(s, bind_all<T>(r, t2), C, sc)) {
+        if (!rk2_stage2(s, bind_all<T, I, FIXED>(r, t2), L, sc)) {
             raise_zero_division(p);
             break;
         }
-        rk2_update<T>(s, bind_all<T>(r, t3), C, sc);
+        rk2_update(s, bind_all<T, I, FIXED>(r, t3), L, sc);
     }
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;
@@ -380,11 +379,12 @@ __global__ void __launch_bounds__(kBlock) k_rk2_steps(const __grid_constant__ DP
 
 // `nsteps` AB3 steps (timesteppers.py:296-305) per launch.  table[2*k + j]
 // selects the fields of step k at t (j = 0) and t + dt (j = 1).
-template <typename T>
-__global__ void __launch_bounds__(kBlock) k_ab3_steps(const __grid_constant__ DParticles p,
+template <typename T, typename I, bool FIXED>
+__global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
                                                       const opb_time *__restrict__ table, int nsteps, int validate_pre) {
+    OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
     PState s;
@@ -400,18 +400,17 @@ __global__ void __launch_bounds__(kBlock) k_ab3_steps(const __grid_constant__ DP
     s.k2y = p.dyidx2[i];
     s.k2z = p.dz2[i];
     const uint8_t st0 = s.status;
-    const CView C = c_view(r);
     bool moved = false;
     for (int k = 0; k < nsteps; ++k) {
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table[2 * k], t2 = table[2 * k + 1];
-        if (!ab3_step<T>(s, bind_all<T>(r, t1), C, sc)) {
+        if (!ab3_step(s, bind_all<T, I, FIXED>(r, t1), sc)) {
             raise_zero_division(p);
             break;
         }
         moved = true;
-        ab3_post<T>(s, bind_all<T>(r, t2), C, sc);
+        ab3_post(s, bind_all<T, I, FIXED>(r, t2), L, sc);
     }
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;
@@ -433,7 +432,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3_steps(const __grid_constant__ DP
 // ---------------------------------------------------------- output kernels
 // kernels/output/linear_interpolation.pyx:34-136: sample one field (static,
 // or blended in time like every other field) at the active particles.
-template <typename T, int ND>
+template <typename T, typename I, int ND>
 __global__ void __launch_bounds__(kBlock) k_interpolate(const __grid_constant__ DParticles p,
                                                         const double *__restrict__ i0,
                                                         const double *__restrict__ i1,
@@ -441,10 +440,38 @@ __global__ void __launch_bounds__(kBlock) k_interpolate(const __grid_constant__ 
                                                         const __grid_constant__ DField f, opb_time t, double *out) {
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
-    const View<T> v = bind<T>(f, t);
+    const View<T, I> v = bind<T, I>(f, t);
     if (ND == 1) out[i] = linear(v, i0[i] + v.o0);
     else if (ND == 2) out[i] = bilinear(v, i0[i] + v.o0, i1[i] + v.o1);
     else out[i] = trilinear(v, i0[i] + v.o0, i1[i] + v.o1, i2[i] + v.o2);
+}
+
+// -------------------------------------------------------------- dispatch
+// Call f(T{}, I{}) for the storage type and the index width of a launch.
+template <typename F>
+void dispatch(int dtype, bool small_index, F &&f) {
+    if (dtype == OPB_F32) {
+        if (small_index) f(float{}, int{});
+        else f(float{}, (long long){});
+    } else {
+        if (small_index) f(double{}, int{});
+        else f(double{}, (long long){});
+    }
+}
+
+// every field of the launch has fewer than 2^31 elements
+bool fits_int(const DField &f) { return f.n0 * f.n1 * f.n2 < 0x7fffffffLL; }
+
+// u, v, w, zeta time-dependent and h, dx, dy, C static: the layout the ROMS
+// presets use, compiled with the field kinds fixed
+bool roms_layout(const DRoms &r) {
+    return !r.u.is_static && !r.v.is_static && !r.w.is_static && !r.zeta.is_static && r.h.is_static &&
+           r.dx.is_static && r.dy.is_static && r.C.is_static;
+}
+
+bool fits_int(const DRoms &r) {
+    return fits_int(r.u) && fits_int(r.v) && fits_int(r.w) && fits_int(r.dx) && fits_int(r.dy) && fits_int(r.h) &&
+           fits_int(r.zeta) && fits_int(r.C);
 }
 
 // ---------------------------------------------------------------- host side
@@ -619,10 +646,10 @@ int opb_compute_z(const opb_particles *p, double *out, const opb_scalars *s, con
     if ((rc = stage_common(what, p, s, f, t, false, dp, ds, dr, dtype))) return rc;
     if (dp.n > 0 && !out) return fail(OPB_EINVAL, "%s: out is NULL", what);
     if (dp.n == 0) return OPB_OK;
-    if (dtype == OPB_F32)
-        k_compute_z<float><<<grid_for(dp.n), kBlock, 0, (cudaStream_t)stream>>>(dp, out, ds, dr, *t);
-    else
-        k_compute_z<double><<<grid_for(dp.n), kBlock, 0, (cudaStream_t)stream>>>(dp, out, ds, dr, *t);
+    dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {
+        k_compute_z<decltype(tv), decltype(iv)><<<grid_for(dp.n), kBlock, 0, (cudaStream_t)stream>>>(dp, out, ds,
+                                                                                                   dr, *t);
+    });
     return check_launch(what);
 }
 
@@ -659,14 +686,17 @@ static int stage_launch(const char *what, int which, const opb_particles *p, con
     if (dp.n == 0) return OPB_OK;
     const unsigned g = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
-    const bool f32 = dtype == OPB_F32;
-    switch (which) {
-        case 0: f32 ? k_rk2_step_1<float><<<g, kBlock, 0, st>>>(dp, ds, dr, *t) : k_rk2_step_1<double><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
-        case 1: f32 ? k_rk2_step_2<float><<<g, kBlock, 0, st>>>(dp, ds, dr, *t) : k_rk2_step_2<double><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
-        case 2: f32 ? k_rk2_update<float><<<g, kBlock, 0, st>>>(dp, ds, dr, *t) : k_rk2_update<double><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
-        case 3: f32 ? k_ab3<float><<<g, kBlock, 0, st>>>(dp, ds, dr, *t) : k_ab3<double><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
-        default: f32 ? k_ab3_post<float><<<g, kBlock, 0, st>>>(dp, ds, dr, *t) : k_ab3_post<double><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
-    }
+    dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {
+        using T = decltype(tv);
+        using I = decltype(iv);
+        switch (which) {
+            case 0: k_rk2_step_1<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
+            case 1: k_rk2_step_2<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
+            case 2: k_rk2_update<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
+            case 3: k_ab3<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
+            default: k_ab3_post<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
+        }
+    });
     return check_launch(what);
 }
 
@@ -719,13 +749,18 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     if (dp.n == 0 || nsteps == 0) return OPB_OK;
     const unsigned g = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
-    if (rk2) {
-        if (dtype == OPB_F32) k_rk2_steps<float><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-        else k_rk2_steps<double><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-    } else {
-        if (dtype == OPB_F32) k_ab3_steps<float><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-        else k_ab3_steps<double><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-    }
+    const bool fixed = roms_layout(dr);
+    dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {
+        using T = decltype(tv);
+        using I = decltype(iv);
+        if (rk2) {
+            if (fixed) k_rk2_steps<T, I, true><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            else k_rk2_steps<T, I, false><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        } else {
+            if (fixed) k_ab3_steps<T, I, true><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            else k_ab3_steps<T, I, false><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        }
+    });
     return check_launch(what);
 }
 
@@ -762,14 +797,13 @@ static int interpolate_impl(const char *what, int nd, const opb_particles *p, co
     if (!out) return fail(OPB_EINVAL, "%s: out is NULL", what);
     const unsigned g = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
-    const bool f32 = !f->is_static && dtype == OPB_F32;
-#define OPB_INTERP(ND)                                                                          \
-    (f32 ? k_interpolate<float, ND><<<g, kBlock, 0, st>>>(dp, i0, i1, i2, df, tt, out)           \
-         : k_interpolate<double, ND><<<g, kBlock, 0, st>>>(dp, i0, i1, i2, df, tt, out))
-    if (nd == 1) OPB_INTERP(1);
-    else if (nd == 2) OPB_INTERP(2);
-    else OPB_INTERP(3);
-#undef OPB_INTERP
+    dispatch(f->is_static ? OPB_F64 : dtype, fits_int(df), [&](auto tv, auto iv) {
+        using T = decltype(tv);
+        using I = decltype(iv);
+        if (nd == 1) k_interpolate<T, I, 1><<<g, kBlock, 0, st>>>(dp, i0, i1, i2, df, tt, out);
+        else if (nd == 2) k_interpolate<T, I, 2><<<g, kBlock, 0, st>>>(dp, i0, i1, i2, df, tt, out);
+        else k_interpolate<T, I, 3><<<g, kBlock, 0, st>>>(dp, i0, i1, i2, df, tt, out);
+    });
     return check_launch(what);
 }
 

@@ -231,6 +231,9 @@ class SnapshotRing:
         self.pending: dict[int, concurrent.futures.Future] = {}
         self.ready: dict[int, torch.cuda.Event] = {}
         self.lru: list[int] = []  # snapshots, least recently used first
+        # per slot: event recorded after the last launch known to read it (None: unknown -> wait for
+        # everything queued so far before overwriting the slot)
+        self.last_use: dict[int, torch.cuda.Event | None] = {}
         self.copy_stream = torch.cuda.Stream(device=device)
         self.staging = [torch.empty(tuple(spatial_shape), dtype=self.slots.dtype, pin_memory=True) for _ in range(2)]
         self.staging_free = [None, None]  # events: staging buffer's last H2D copy done
@@ -293,9 +296,13 @@ class SnapshotRing:
         slot = self._free_slot(keep)
         if slot is None:
             return False
-        # the slot's previous contents may still be read by launches already queued
-        slot_free = torch.cuda.Event()
-        slot_free.record(torch.cuda.current_stream(self.device))
+        # the slot's previous contents may still be read by queued launches: wait for the last launch
+        # known to read it, or for everything queued so far when that is unknown
+        slot_free = self.last_use.get(slot)
+        if slot_free is None:
+            slot_free = torch.cuda.Event()
+            slot_free.record(torch.cuda.current_stream(self.device))
+        self.last_use[slot] = None
         self.slot_of[k] = slot
         self.lru.append(k)
         self.pending[k] = self.pool.submit(self._upload, k, slot, slot_free)
@@ -308,6 +315,8 @@ class SnapshotRing:
             fut = self.pending.pop(k, None)
             self.lru.remove(k)
             self.lru.append(k)
+            # a launch that follows may read the slot and nobody may mark it: forget the last-use event
+            self.last_use[self.slot_of[k]] = None
         if fut is not None:
             fut.result()
         ev = self.ready.get(k)
@@ -318,6 +327,15 @@ class SnapshotRing:
     def prefetch(self, k: int, keep: set[int]) -> None:
         with self.lock:
             self._schedule(k, set(keep) | {k})
+
+    def mark_used(self, ks) -> None:
+        """Record that the launches queued so far are the last to read snapshots ``ks``."""
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.device))
+        with self.lock:
+            for k in ks:
+                if k in self.slot_of:
+                    self.last_use[self.slot_of[k]] = ev
 
     def resident(self) -> list[int]:
         return sorted(self.slot_of)
@@ -433,6 +451,16 @@ class TimeDependentField(Field):
     def prefetch(self, k: int, keep: set[int]) -> None:
         if self._ring is not None and 0 <= k < self._num_timesteps:
             self._ring.prefetch(k, keep)
+
+    def mark_used(self, ks) -> None:
+        """Tell the ring that the launches queued so far are the last readers of snapshots ``ks``."""
+        if self._ring is not None:
+            self._ring.mark_used(ks)
+
+    @property
+    def streamed(self) -> bool:
+        """True when snapshots stream through a device ring (False: the source is resident)."""
+        return self._ring is not None
 
     def blend_weights(self, time_index) -> tuple[int, object, object]:
         """(It, ft, gt) with ft, gt in the storage dtype: fields.py:409-424."""

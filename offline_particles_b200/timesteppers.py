@@ -165,7 +165,9 @@ class Timestepper(abc.ABC):
     def _fused_chunk(self, particles, launcher: Launcher, max_steps: int) -> int:
         """Plan and launch as many steps as fit in one fused launch; return the number taken."""
         td = _time_dependent_fields(launcher)
-        capacity = min([_lib.MAX_SLOTS] + [f.ring_size for f in td.values()])
+        # a streamed field keeps one ring slot free so the next snapshot uploads while this launch runs
+        capacity = min([_lib.MAX_SLOTS] + [max(2, f.ring_size - 1) if f.streamed else f.ring_size
+                                           for f in td.values()])
         time = self._time
         steps: list[list] = []
         needed: set[int] = set()
@@ -262,10 +264,12 @@ def _upload_table(table, device) -> torch.Tensor:
 
 
 def _prefetch_after(td: dict[str, TimeDependentField], needed: list[int]) -> None:
+    """After a launch: mark its snapshots' slots as read by it, then start uploading the next snapshot."""
     if not needed:
         return
     last = needed[-1]
     for f in td.values():
+        f.mark_used(needed)
         keep = {needed[-2], last} if len(needed) > 1 else {last}
         f.prefetch(last + 1, keep)
 

@@ -212,3 +212,56 @@ def test_c_abi_rejects_bad_arguments():
     p.n = 10
     assert lib.opb_validation(ctypes.byref(p), None, None) == _lib.EINVAL
     assert b"NULL" in lib.opb_last_error()
+
+
+@pytest.mark.parametrize("table", ["stretched", "plateaus", "nonmonotone", "hc0"])
+def test_vertical_search_with_hints_matches_oracle(table):
+    """compute_zidx with a level hint (ab3_post) equals the reference's binary search for any hint."""
+    import torch
+
+    from offline_particles_b200.fields import FieldData
+    from offline_particles_b200.kernels.roms import ab3_w_advection
+    from offline_particles_b200.particles import Particles
+    from offline_particles_b200.synth import vstretching4
+    from oracle import oracle as O
+
+    rng = np.random.default_rng({"stretched": 1, "plateaus": 2, "nonmonotone": 3, "hc0": 4}[table])
+    nz, hc = 24, 20.0
+    C = vstretching4(nz)
+    if table == "plateaus":
+        C[5:9] = C[5]
+        C[15:18] = C[17]
+    elif table == "nonmonotone":
+        C[10], C[11] = C[11], C[10]
+    elif table == "hc0":
+        hc = 0.0
+    n = 20000
+    h = np.concatenate([rng.uniform(5.0, 1000.0, n - 2000), rng.uniform(0.0, 2.0, 1000), np.full(1000, 50.0)])
+    zeta = rng.uniform(-1.0, 1.0, n)
+    # z: anywhere in (and a little outside) the column, plus exactly on computed level depths
+    z = zeta + (zeta + h) * rng.uniform(-1.05, 0.05, n)
+    lev = rng.integers(0, nz, 3000)
+    sig = ((lev + 0.5) / nz) - 1.0
+    S = (hc * sig + h[:3000] * C[lev]) / (hc + h[:3000])
+    z[:3000] = zeta[:3000] + (zeta[:3000] + h[:3000]) * S
+    # hints: exact, off by a few, far off, non-finite
+    hint = rng.uniform(-2, nz + 2, n)
+    hint[::7] = np.nan
+    L = O.lib()
+    Cf = O.make_field(C, (0.0,))
+    ref = np.array([L.oracle_compute_zidx_scalar(zz, hh, ze, hc, nz, ctypes.byref(Cf)) for zz, hh, ze in zip(z, h, zeta)])
+    near = ~np.isnan(hint)
+    hint[near][: n // 3] = ref[near][: n // 3]
+    P = Particles(n, status=np.uint8, zidx=np.float64, yidx=np.float64, xidx=np.float64, z=np.float64)
+    dev = P["z"].device
+    P["zidx"].copy_(torch.from_numpy(hint))
+    P["xidx"].copy_(torch.from_numpy(2.0 * np.arange(n)))
+    P["z"].copy_(torch.from_numpy(z))
+    hf = np.repeat(h, 2)[None, :].repeat(2, axis=0)
+    zf = np.repeat(zeta, 2)[None, :].repeat(2, axis=0)
+    fd = {"h": FieldData(torch.from_numpy(hf).to(dev), (0.0, 0.0)),
+          "zeta": FieldData(torch.from_numpy(zf).to(dev), (0.0, 0.0)),
+          "C": FieldData(torch.from_numpy(C).to(dev), (0.0,))}
+    ab3_w_advection.ab3_post_w_advection(P, {"hc": hc, "NZ": nz}, fd)
+    got = P["zidx"].cpu().numpy()
+    assert same_bits(got, ref), mismatch_report(got, ref)
