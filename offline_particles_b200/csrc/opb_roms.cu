@@ -28,8 +28,17 @@ struct PState {
     double k0x, k0y, k0z;  // AB3 k(n)
     double k1x, k1y, k1z;  // RK2 k1 / AB3 k(n-1)
     double k2x, k2y, k2z;  // RK2 k2 / AB3 k(n-2)
+    // h and zeta at (yidx, xidx) for the time selection `at`, left by the
+    // previous step's last stage; the next step's first stage needs exactly
+    // these values (same position, same time index) and reuses them
+    double h_at, zeta_at;
+    opb_time at;
     uint8_t status;
 };
+
+__device__ __forceinline__ bool same_time(const opb_time &a, const opb_time &b) {
+    return a.prev == b.prev && a.next == b.next && a.ft == b.ft && a.gt == b.gt;
+}
 
 __device__ __forceinline__ void raise_zero_division(const DParticles &p) {
     if (p.err) atomicOr(p.err, (uint32_t)OPB_ERRF_ZERO_DIVISION);
@@ -72,9 +81,9 @@ __device__ __forceinline__ Bound<T, I, FIXED> bind_all(const DRoms &r, const opb
 // rk2_w_advection.pyx:97-153 (stage 1 for one particle).  Returns false on a
 // zero grid spacing (the reference raises ZeroDivisionError).
 template <typename B>
-__device__ __forceinline__ bool rk2_stage1(PState &s, const B &f, const DScalars &sc) {
-    const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
-    const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+__device__ __forceinline__ bool rk2_stage1(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false) {
+    const double h = reuse_hz ? s.h_at : bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
+    const double zeta = reuse_hz ? s.zeta_at : bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
     const double Cv = linear(f.C, s.zidx + f.C.o0);
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
@@ -123,11 +132,13 @@ __device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &
     const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
     const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
+    s.h_at = h;
+    s.zeta_at = zeta;
 }
 
 // ab3_w_advection.pyx:84-178 (AB3 step for one particle)
 template <typename B>
-__device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &sc) {
+__device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false) {
     const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
     const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
     if (dx == 0.0) return false;
@@ -151,8 +162,8 @@ __device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &
         s.k2z = -s.k0z + 2.0 * s.k1z;
         s.status = ST_NORMAL;
     }
-    const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
-    const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    const double h = reuse_hz ? s.h_at : bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
+    const double zeta = reuse_hz ? s.zeta_at : bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
     const double Cv = linear(f.C, s.zidx + f.C.o0);
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double dt = sc.dt;
@@ -174,6 +185,8 @@ __device__ __forceinline__ void ab3_post(PState &s, const B &f, const Levels &L,
     const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
     const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
+    s.h_at = h;
+    s.zeta_at = zeta;
 }
 
 __device__ __forceinline__ long long gtid() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
@@ -352,7 +365,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table[3 * k], t2 = table[3 * k + 1], t3 = table[3 * k + 2];
-        if (!rk2_stage1(s, bind_all<T, I, FIXED>(r, t1), sc)) {
+        const bool reuse = k > 0 && same_time(t1, s.at);
+        if (!rk2_stage1(s, bind_all<T, I, FIXED>(r, t1), sc, reuse)) {
             raise_zero_division(p);
             break;
         }
@@ -362,6 +376,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
             break;
         }
         rk2_update(s, bind_all<T, I, FIXED>(r, t3), L, sc);
+        s.at = t3;
     }
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;
@@ -405,12 +420,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table[2 * k], t2 = table[2 * k + 1];
-        if (!ab3_step(s, bind_all<T, I, FIXED>(r, t1), sc)) {
+        const bool reuse = k > 0 && same_time(t1, s.at);
+        if (!ab3_step(s, bind_all<T, I, FIXED>(r, t1), sc, reuse)) {
             raise_zero_division(p);
             break;
         }
         moved = true;
         ab3_post(s, bind_all<T, I, FIXED>(r, t2), L, sc);
+        s.at = t2;
     }
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;
