@@ -197,6 +197,33 @@ int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *
 int opb_gather_particles(const opb_particles *src, const opb_particles *dst, const int32_t *perm,
                          const int64_t *src_ids, int64_t *dst_ids, void *stream);
 
+/* ---- sorting without device allocation ---------------------------------------
+ * No counterpart in the reference (which has no GPU and no device memory).
+ * Some callers cannot allocate device memory at the moment they sort: a host
+ * runtime that reserved all device memory up front for its own pool, or a
+ * latency-critical loop in which a cudaMalloc / cudaFree pair would
+ * synchronise the device and stall the work already queued.  For them,
+ * opb_sort_particles_noalloc gives the same permutation as
+ * opb_sort_particles but takes its scratch from a static device array inside
+ * this library instead of a caller workspace, and calls no allocating routine.
+ *
+ *   - The array is OPB_NOALLOC_SCRATCH_BYTES (17 MiB).  Every GPU that loads
+ *     the library holds it until the process exits.
+ *   - At most OPB_NOALLOC_MAX_PARTICLES particles per call; more is rejected
+ *     with OPB_EINVAL and a message (use opb_sort_particles then).
+ *   - The first call on a device looks up the array's device address (once per
+ *     device, with that device current); make that first call before any
+ *     stream capture.
+ *   - Every call on a device shares the one array, which keeps the last call's
+ *     contents (nothing in it has to start at zero: each call writes its keys
+ *     and ids in full before reading them).  Calls that overlap on the GPU
+ *     race on it: issue them on one stream, or wait for one before the next. */
+#define OPB_NOALLOC_MAX_PARTICLES (1 << 20)
+#define OPB_NOALLOC_CUB_TEMP_BYTES (1u << 20)
+#define OPB_NOALLOC_SCRATCH_BYTES ((size_t)16 * OPB_NOALLOC_MAX_PARTICLES + OPB_NOALLOC_CUB_TEMP_BYTES)
+
+int opb_sort_particles_noalloc(const opb_particles *p, const int64_t shape[3], int32_t *perm, void *stream);
+
 /* ---- library ------------------------------------------------------------- */
 
 /* Message of the last failed call on this host thread ("" if none). */

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <mutex>
 
 #include "opb200.h"
 #include "opb_errors.h"
@@ -192,3 +193,108 @@ int opb_gather_particles(const opb_particles *src, const opb_particles *dst, con
 }
 
 }  // extern "C"
+
+// ====================================================================== no-alloc
+// opb_sort_particles_noalloc: the same sort with its scratch in a static
+// device array, for callers that cannot allocate device memory when they
+// sort.  Sizes are stated in include/opb200.h (OPB_NOALLOC_*).
+//
+// Layout of the array: two key buffers and two id buffers of
+// OPB_NOALLOC_MAX_PARTICLES entries each (the double buffers of the radix
+// sort), then OPB_NOALLOC_CUB_TEMP_BYTES of CUB temporary storage.
+namespace opb_sort {
+namespace {
+
+constexpr size_t kNoAllocBuf = (size_t)OPB_NOALLOC_MAX_PARTICLES * 4;
+constexpr size_t kNoAllocCubOffset = 4 * kNoAllocBuf;
+static_assert(kNoAllocCubOffset + OPB_NOALLOC_CUB_TEMP_BYTES == OPB_NOALLOC_SCRATCH_BYTES, "scratch layout");
+
+// Every GPU that loads this library holds this array until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[OPB_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the array on the current device.  In host code the
+// array's name is only a host-side stand-in, never a device address; the
+// runtime maps it the first time, once per device (which may load the module).
+int noalloc_scratch(void **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return fail(OPB_EINVAL, "opb_sort_particles_noalloc: device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(OPB_ECUDA, "opb_sort_particles_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = ptr;
+    }
+    *out = g_noalloc_ptr[dev];
+    return OPB_OK;
+}
+
+}  // namespace
+}  // namespace opb_sort
+
+extern "C" int opb_sort_particles_noalloc(const opb_particles *p, const int64_t shape[3], int32_t *perm,
+                                          void *stream) {
+    if (!p) return fail(OPB_EINVAL, "opb_sort_particles_noalloc: particles is NULL");
+    if (p->n < 0) return fail(OPB_EINVAL, "opb_sort_particles_noalloc: negative particle count");
+    if (p->n > OPB_NOALLOC_MAX_PARTICLES)
+        return fail(OPB_EINVAL,
+                    "opb_sort_particles_noalloc: %lld particles exceed the static scratch limit of %d "
+                    "(OPB_NOALLOC_MAX_PARTICLES); use opb_sort_particles with a caller-allocated workspace",
+                    (long long)p->n, (int)OPB_NOALLOC_MAX_PARTICLES);
+    if (p->n == 0) return OPB_OK;
+    if (!p->status || !p->zidx || !p->yidx || !p->xidx || !perm || !shape)
+        return fail(OPB_EINVAL, "opb_sort_particles_noalloc: NULL argument");
+    if (shape[0] < 1 || shape[1] < 1 || shape[2] < 1 || shape[0] > (1 << 30) || shape[1] > (1 << 30) ||
+        shape[2] > (1 << 30))
+        return fail(OPB_EINVAL, "opb_sort_particles_noalloc: bad grid shape");
+    void *base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    char *ws = (char *)base;
+    uint32_t *keys0 = (uint32_t *)ws;
+    uint32_t *keys1 = (uint32_t *)(ws + kNoAllocBuf);
+    int32_t *ids0 = (int32_t *)(ws + 2 * kNoAllocBuf);
+    int32_t *ids1 = (int32_t *)(ws + 3 * kNoAllocBuf);
+    void *temp = ws + kNoAllocCubOffset;
+    const int n = (int)p->n;
+    cub::DoubleBuffer<uint32_t> keys(keys0, keys1);
+    cub::DoubleBuffer<int32_t> ids(ids0, ids1);
+    size_t temp_bytes = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys, ids, n, 0, 32);
+    if (e != cudaSuccess)
+        return fail(OPB_ECUDA, "opb_sort_particles_noalloc: radix sort sizing: %s", cudaGetErrorString(e));
+    if (temp_bytes > OPB_NOALLOC_CUB_TEMP_BYTES)
+        return fail(OPB_EINVAL, "opb_sort_particles_noalloc: radix sort needs %zu temporary bytes, the static "
+                    "scratch reserves %zu", temp_bytes, (size_t)OPB_NOALLOC_CUB_TEMP_BYTES);
+    KeyArgs k;
+    k.status = p->status;
+    k.zidx = p->zidx;
+    k.yidx = p->yidx;
+    k.xidx = p->xidx;
+    k.n = p->n;
+    k.nz = (int)shape[0];
+    k.ny = (int)shape[1];
+    k.nx = (int)shape[2];
+    k.sz = shift_for(k.nz, 0);
+    k.sy = shift_for(k.ny, 0);
+    k.sx = shift_for(k.nx, 2);
+    cudaStream_t st = (cudaStream_t)stream;
+    // keys0 and ids0 are written in full before the sort reads them; the sort
+    // itself needs no initial contents in the other buffers or in its temp storage
+    k_cell_keys<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(k, keys0, ids0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles_noalloc: %s", cudaGetErrorString(e));
+    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, ids, n, 0, 32, st);
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles_noalloc: radix sort: %s", cudaGetErrorString(e));
+    e = cudaMemcpyAsync(perm, ids.Current(), (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles_noalloc: copy: %s", cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
