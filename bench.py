@@ -341,6 +341,18 @@ def b200_arm(a) -> None:
     hz, hy, hx = (torch.from_numpy(v).pin_memory() for v in zyx)
     outs = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in ("zidx", "yidx", "xidx")}
     outs["status"] = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    # the box's pinned host -> device bandwidth, for reading e2e (one snapshot of u)
+    probe = torch.empty_like(psrc["u"][0], device=dev)
+    probe.copy_(psrc["u"][0], non_blocking=True)
+    torch.cuda.synchronize()
+    hs, he = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hs.record()
+    for k in range(3):
+        probe.copy_(psrc["u"][k % psrc["u"].shape[0]], non_blocking=True)
+    he.record()
+    torch.cuda.synchronize()
+    h2d_gbs = 3 * probe.numel() * probe.element_size() / (hs.elapsed_time(he) * 1e-3) / 1e9
+    del probe
     # untimed warm-up of the same path (allocator, ring, copy stream)
     simw, _ = build_sim(grid, psrc, n, a, ring_size=4)
     simw.set_indices(hz, hy, hx)
@@ -386,6 +398,10 @@ def b200_arm(a) -> None:
     except (OSError, ValueError):
         pass
     peak = peaks.get("hbm_gbs") or 6650.0
+    # physical DRAM bytes per fused step of this kernel on this workload, from one ncu capture of the
+    # full-size timed launches (profiles/k_ab3_steps_f32_config2_sorted.md: 2.615 GB / 61 steps and
+    # 2.585 GB / 59 steps); traffic per launch scales with the steps it runs
+    traffic_per_step = 43.4e6 if (a.nx, a.ny, a.nz, a.particles) == (1024, 768, 50, 4_194_304) else None
     state_bytes = 2 * (1 + 3 * 8 + 6 * 8)  # status + 3 indices + 6 AB3 history values, float64, read + written
     b_step = n * state_bytes + fb["pair"] + fb["static"]
     tot_steps = sum(launch_steps)
@@ -404,9 +420,13 @@ def b200_arm(a) -> None:
         "e2e": {"value": total / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d / a.steps),
                 "d2h_bytes_per_step": int(d2h / a.steps),
                 "path": "Simulation.set_indices from pinned host + run(K) streaming every snapshot from pinned "
-                        "host memory + D2H of zidx/yidx/xidx/status"},
+                        "host memory + D2H of zidx/yidx/xidx/status",
+                "h2d_gbs_measured": h2d_gbs,
+                "h2d_bound_value": total / ((h2d + d2h) / (h2d_gbs * 1e9)) if h2d_gbs else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                     "traffic": traffic_per_step * avg_launch_steps if traffic_per_step else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the full-size launches, "
+                                       "per launch", "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                      "algorithmic_bytes_per_step": b_step, "bytes_per_particle_step": b_step / n,
                      "steps_per_launch": avg_launch_steps, "launch_ms": avg_launch_ms,
                      "kernel": "k_ab3_steps<float>"},

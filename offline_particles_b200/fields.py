@@ -253,7 +253,8 @@ class SnapshotRing:
         if isinstance(src, torch.Tensor) and src.is_pinned():
             # already in pinned host memory: one async copy, no staging
             with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
-                self.copy_stream.wait_event(slot_free)
+                if slot_free is not None:
+                    self.copy_stream.wait_event(slot_free)
                 self.slots[slot].copy_(src[k], non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(self.copy_stream)
@@ -269,7 +270,8 @@ class SnapshotRing:
             stage = self.staging[b]
             stage.copy_(torch.from_numpy(host))
             with torch.cuda.stream(self.copy_stream):
-                self.copy_stream.wait_event(slot_free)
+                if slot_free is not None:
+                    self.copy_stream.wait_event(slot_free)
                 self.slots[slot].copy_(stage, non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(self.copy_stream)
@@ -298,10 +300,13 @@ class SnapshotRing:
             return False
         # the slot's previous contents may still be read by queued launches: wait for the last launch
         # known to read it, or for everything queued so far when that is unknown
-        slot_free = self.last_use.get(slot)
-        if slot_free is None:
-            slot_free = torch.cuda.Event()
-            slot_free.record(torch.cuda.current_stream(self.device))
+        if slot not in self.last_use:
+            slot_free = None  # never written or read: nothing to wait for
+        else:
+            slot_free = self.last_use[slot]
+            if slot_free is None:
+                slot_free = torch.cuda.Event()
+                slot_free.record(torch.cuda.current_stream(self.device))
         self.last_use[slot] = None
         self.slot_of[k] = slot
         self.lru.append(k)
