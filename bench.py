@@ -207,14 +207,9 @@ class LaunchTimer:
 
 
 def dist_max(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from offline_particles_b200.sharding import max_over_ranks
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return max_over_ranks(value) if world > 1 else value
 
 
 def barrier(world: int) -> None:
