@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--dt", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
+    ap.add_argument("--study", choices=("precision",), default=None,
+                    help="precision: float64 vs float32 arithmetic with float32/float16/bfloat16 storage, "
+                         "separation in metres after --days")
+    ap.add_argument("--days", type=str, default="1,3,7")
     return ap.parse_args()
 
 
@@ -434,9 +438,89 @@ def b200_arm(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------- precision study
+def precision_study(a) -> None:
+    """Trajectory separation of the float32 steppers against the float64 (bit-exact) path.
+
+    The config-2 workload for max(--days) simulated days; snapshots are
+    generated on the device (all resident), particles released as for the
+    headline.  Every arm starts from the same state; separations are taken at
+    each requested day over particles active in both arms: horizontal
+    hypot(dx*d_xidx, dy*d_yidx) and vertical |d z|, in metres.
+    """
+    import torch
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    torch.cuda.set_device(0)
+    days = [float(d) for d in a.days.split(",")]
+    steps_at = [int(round(d * 86400.0 / a.dt)) for d in days]
+    nt = int(math.ceil(max(days) * 24.0)) + 2
+    grid = SyntheticROMS(GridSpec(nx=a.nx, ny=a.ny, nz=a.nz, nt=nt, seed=2, dtype="float32"))
+    t0 = time.perf_counter()
+    snaps = grid.device_snapshots(nt)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    z0, y0, x0 = grid.release(a.particles, seed=1000)
+    dxm = grid.spec.dx
+    arms = (("float64", None), ("float32", None), ("float32", "float16"), ("float32", "bfloat16"))
+    results, positions = {}, {}
+    for arith, storage in arms:
+        name = arith if storage is None else f"{arith}+{storage}"
+        kw = {n: opb.TimeDependentField.from_tensor(snaps[n], *STAGGERS[n], storage=storage) for n in TD}
+        for n, arr in (("h", grid.h), ("dx", grid.dx), ("dy", grid.dy), ("C", grid.C)):
+            kw[n] = opb.StaticField.from_numpy(arr, *STAGGERS[n])
+        fs = opb.Fieldset(nt, a.nz, a.ny, a.nx, constants={"hc": grid.hc, "NZ": a.nz}, **kw)
+        ts = opb.roms.ab3_w_advection_timestepper(grid.time_array[:nt], np.float64(a.dt))
+        sim = opb.SimulationBuilder(ts, fs).build_simulation(a.particles, arithmetic=arith)
+        sim.set_indices(z0, y0, x0)
+        sim.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+        done, elapsed, pos = 0, 0.0, []
+        for target in steps_at:
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record()
+            sim.run(target - done)
+            e_.record()
+            torch.cuda.synchronize()
+            elapsed += s_.elapsed_time(e_) * 1e-3
+            done = target
+            P = sim.particles
+            pos.append({k: P[k] for k in ("status", "yidx", "xidx", "z")})
+        sim.synchronize()
+        field_pair = 2 * sum(fs[n].storage_bytes_per_snapshot for n in TD)
+        b_step = a.particles * 2 * (1 + 3 * 8 + 6 * 8) + field_pair + grid.h.nbytes * 3
+        results[name] = {"value": a.particles * done / elapsed, "unit": UNIT, "ms_per_step": elapsed / done * 1e3,
+                         "field_storage": storage or "float32", "arithmetic": arith,
+                         "algorithmic_bytes_per_step": b_step}
+        positions[name] = pos
+        del sim, fs, kw
+        torch.cuda.empty_cache()
+    ref = positions["float64"]
+    for name, pos in positions.items():
+        if name == "float64":
+            continue
+        sep = {}
+        for d, p, r in zip(days, pos, ref):
+            both = ((p["status"] & 0x80) == 0) & ((r["status"] & 0x80) == 0)
+            hz = np.hypot((p["xidx"][both] - r["xidx"][both]) * dxm, (p["yidx"][both] - r["yidx"][both]) * dxm)
+            vt = np.abs(p["z"][both] - r["z"][both])
+            sep[f"day{d:g}"] = {"horizontal_mean_m": float(hz.mean()), "horizontal_p99_m": float(np.percentile(hz, 99)),
+                                "vertical_mean_m": float(vt.mean()), "vertical_p99_m": float(np.percentile(vt, 99)),
+                                "active_in_both": int(both.sum()),
+                                "status_agreement": float(np.mean(p["status"] == r["status"]))}
+        results[name]["separation_vs_float64"] = sep
+    line = {"study": "precision", "metric": "trajectory separation vs the float64 path (m); particle-steps/s",
+            "workload": workload_config(a, nt), "days": days, "steps": steps_at, "snapshot_generation_s": gen_s,
+            "arms": results, "data": "synthetic, snapshots generated on the device"}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     a = parse()
-    if a.impl == "reference":
+    if a.study == "precision":
+        precision_study(a)
+    elif a.impl == "reference":
         reference_arm(a)
     else:
         b200_arm(a)

@@ -38,12 +38,16 @@
 extern "C" {
 #endif
 
-#define OPB_ABI_VERSION 1
+#define OPB_ABI_VERSION 2
 #define OPB_MAX_SLOTS 8
 
-/* storage dtypes of time-dependent fields */
+/* storage dtypes of time-dependent fields (the float64-exact entry points take
+ * OPB_F64 and OPB_F32; the *_fp32 entry points also take OPB_BF16 / OPB_F16
+ * with per-level scales) */
 #define OPB_F64 0
 #define OPB_F32 1
+#define OPB_BF16 2
+#define OPB_F16 3
 
 /* return codes */
 #define OPB_OK 0
@@ -77,6 +81,10 @@ typedef struct {
     double offset[3];
     int32_t is_static;
     int32_t nslots;
+    /* OPB_BF16 / OPB_F16 storage: scale[k][l] multiplies the stored values of
+     * slot k at level l (the first active dimension; 2-D fields use l = 0);
+     * NULL for unscaled storage */
+    const float *scale[OPB_MAX_SLOTS];
 } opb_field;
 
 /* The simulation fields of the ROMS w-advection kernels
@@ -144,6 +152,25 @@ int opb_ab3_w_advection(const opb_particles *p, const opb_scalars *s, const opb_
 /* kernels/roms/ab3_w_advection.pyx:180-229 (ab3_post_w_advection) */
 int opb_ab3_post_w_advection(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                              const opb_time *t, void *stream);
+
+/* ---- reduced-precision steppers --------------------------------------------
+ * The precision variant of the fused steppers: float32 interpolation and
+ * updates, fractional x/y indices kept as compensated float32 pairs, float64
+ * only for z = zeta + (zeta + h) S and its inverse in columns with h < 100 m.
+ * Time-dependent fields may be stored as float32, or as bfloat16 / float16
+ * with per-level scales (opb_field.scale).  Not bit-identical to the
+ * reference: its error is measured as trajectory separation in metres against
+ * the float64 entry points. */
+int opb_rk2_w_advection_steps_fp32(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                   const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
+int opb_ab3_w_advection_steps_fp32(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                   const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
+/* Quantise `nsnap` float32 snapshots of `nlev` levels x `per_level` values each
+ * (C order) into `dtype` (OPB_BF16 or OPB_F16) at `dst`, writing one scale per
+ * (snapshot, level) to `scales` (nsnap x nlev): value ~= stored * scale,
+ * scale = max |value| of the level / 32768 (1 for an all-zero level). */
+int opb_quantize_levels(const float *src, int64_t nsnap, int64_t nlev, int64_t per_level, int32_t dtype, void *dst,
+                        float *scales, void *stream);
 
 /* ---- output sampling (kernels/output/linear_interpolation.pyx:34-136) ----- */
 

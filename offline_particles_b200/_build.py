@@ -21,8 +21,9 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 
 GENCODE = "-gencode=arch=compute_100a,code=sm_100a"
-# float64 path: no multiply-add contraction (bit parity with the reference)
-EXACT_SOURCES = ("opb_roms.cu",)
+# per-file flags, as CMakeLists.txt sets them: the float64 path contracts no
+# multiply-add (bit parity with the reference); the float32 path may
+SOURCE_FLAGS = {"opb_roms.cu": ["-fmad=false"], "opb_fast.cu": ["-prec-div=false", "-ftz=true"]}
 
 
 def _sources() -> list[Path]:
@@ -53,8 +54,7 @@ def _build_nvcc(build_dir: Path) -> None:
         obj = build_dir / (src.stem + ".o")
         flags = [GENCODE, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
                  f"-I{INCLUDE}", f"-I{CSRC}"]
-        if src.name in EXACT_SOURCES:
-            flags.append("-fmad=false")
+        flags += SOURCE_FLAGS.get(src.name, [])
         subprocess.run([_nvcc(), *flags, "-c", str(src), "-o", str(obj)], check=True)
         objs.append(str(obj))
     LIB_DIR.mkdir(parents=True, exist_ok=True)

@@ -12,7 +12,8 @@ import threading
 from ._build import LIB_PATH, build_library
 
 MAX_SLOTS = 8
-F64, F32 = 0, 1
+F64, F32, BF16, F16 = 0, 1, 2, 3
+ABI_VERSION = 2
 OK, EINVAL, ECUDA = 0, 1, 2
 ERRF_ZERO_DIVISION = 1
 
@@ -26,6 +27,7 @@ class opb_field(ctypes.Structure):
         ("offset", ctypes.c_double * 3),
         ("is_static", ctypes.c_int32),
         ("nslots", ctypes.c_int32),
+        ("scale", ctypes.c_void_p * MAX_SLOTS),
     ]
 
 
@@ -79,6 +81,11 @@ SIGNATURES = {
                                   ctypes.c_int32, _VP],
     "opb_ab3_w_advection_steps": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP, ctypes.c_int32,
                                   ctypes.c_int32, _VP],
+    "opb_rk2_w_advection_steps_fp32": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP,
+                                       ctypes.c_int32, ctypes.c_int32, _VP],
+    "opb_ab3_w_advection_steps_fp32": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP,
+                                       ctypes.c_int32, ctypes.c_int32, _VP],
+    "opb_quantize_levels": [_VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP, _VP],
 }
 
 SIGNATURES_OTHER = {
@@ -116,7 +123,7 @@ def load(build: bool = True) -> ctypes.CDLL:
         lib.opb_last_error.restype = ctypes.c_char_p
         lib.opb_abi_version.argtypes = []
         lib.opb_abi_version.restype = ctypes.c_int
-        if lib.opb_abi_version() != 1:
+        if lib.opb_abi_version() != ABI_VERSION:
             raise RuntimeError("offline_particles_b200: ABI version mismatch")
         _lib = lib
         return lib

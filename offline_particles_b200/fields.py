@@ -212,6 +212,23 @@ class StaticField(Field):
         return cls(spatial)
 
 
+STORAGE = {None: None, "float32": None, "float64": None, "bfloat16": torch.bfloat16, "float16": torch.float16}
+
+
+def quantize_levels(src: torch.Tensor, dst: torch.Tensor, scales: torch.Tensor, nlev: int) -> None:
+    """dst (bfloat16/float16) = src (float32) / scale, one scale per level (per leading index of src / nlev)."""
+    from . import _lib
+    from ._device import stream_handle
+
+    if src.dtype != torch.float32 or not src.is_contiguous() or not dst.is_contiguous():
+        raise TypeError("quantisation needs a contiguous float32 source")
+    code = {torch.bfloat16: _lib.BF16, torch.float16: _lib.F16}[dst.dtype]
+    groups = scales.numel()
+    per_level = src.numel() // groups
+    _lib.call("opb_quantize_levels", src.data_ptr(), 1, groups, per_level, code, dst.data_ptr(), scales.data_ptr(),
+              stream_handle(src.device))
+
+
 class SnapshotRing:
     """Device slots for the snapshots of one time-dependent field.
 
@@ -221,12 +238,19 @@ class SnapshotRing:
     """
 
     def __init__(self, source, spatial_shape: tuple[int, ...], np_dtype: np.dtype, nslots: int,
-                 device: torch.device) -> None:
+                 device: torch.device, storage: torch.dtype | None = None) -> None:
         self.source = source
         self.np_dtype = np.dtype(np_dtype)
         self.device = device
         self.nslots = nslots
-        self.slots = torch.empty((nslots,) + tuple(spatial_shape), dtype=torch_dtype(np_dtype), device=device)
+        # reduced-precision storage: slots hold bfloat16/float16 values, one scale per level
+        self.storage = storage
+        slot_dtype = storage if storage is not None else torch_dtype(np_dtype)
+        self.slots = torch.empty((nslots,) + tuple(spatial_shape), dtype=slot_dtype, device=device)
+        self.nlev = spatial_shape[0] if len(spatial_shape) == 3 else 1
+        if storage is not None:
+            self.slot_scales = torch.ones((nslots, self.nlev), dtype=torch.float32, device=device)
+            self.device_staging = torch.empty(tuple(spatial_shape), dtype=torch.float32, device=device)
         self.slot_of: dict[int, int] = {}
         self.pending: dict[int, concurrent.futures.Future] = {}
         self.ready: dict[int, torch.cuda.Event] = {}
@@ -235,7 +259,8 @@ class SnapshotRing:
         # everything queued so far before overwriting the slot)
         self.last_use: dict[int, torch.cuda.Event | None] = {}
         self.copy_stream = torch.cuda.Stream(device=device)
-        self.staging = [torch.empty(tuple(spatial_shape), dtype=self.slots.dtype, pin_memory=True) for _ in range(2)]
+        self.staging = [torch.empty(tuple(spatial_shape), dtype=torch_dtype(np_dtype), pin_memory=True)
+                        for _ in range(2)]
         self.staging_free = [None, None]  # events: staging buffer's last H2D copy done
         self.staging_next = 0
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=1, thread_name_prefix="opb-snapshots")
@@ -248,6 +273,17 @@ class SnapshotRing:
             return src[k].numpy()
         return np.ascontiguousarray(np.asarray(src[k]), dtype=self.np_dtype)
 
+    def _to_slot(self, slot: int, src: torch.Tensor) -> None:
+        """Copy (or quantise) one snapshot into its slot; runs on the copy stream."""
+        if self.storage is None:
+            self.slots[slot].copy_(src, non_blocking=True)
+            return
+        self.device_staging.copy_(src, non_blocking=True)
+        quantize_levels(self.device_staging, self.slots[slot], self.slot_scales[slot], self.nlev)
+
+    def scales(self, k: int) -> torch.Tensor | None:
+        return None if self.storage is None else self.slot_scales[self.slot_of[k]]
+
     def _upload(self, k: int, slot: int, slot_free: torch.cuda.Event) -> None:
         src = self.source
         if isinstance(src, torch.Tensor) and src.is_pinned():
@@ -255,7 +291,7 @@ class SnapshotRing:
             with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
                 if slot_free is not None:
                     self.copy_stream.wait_event(slot_free)
-                self.slots[slot].copy_(src[k], non_blocking=True)
+                self._to_slot(slot, src[k])
                 ev = torch.cuda.Event()
                 ev.record(self.copy_stream)
             self.ready[k] = ev
@@ -272,7 +308,7 @@ class SnapshotRing:
             with torch.cuda.stream(self.copy_stream):
                 if slot_free is not None:
                     self.copy_stream.wait_event(slot_free)
-                self.slots[slot].copy_(stage, non_blocking=True)
+                self._to_slot(slot, stage)
                 ev = torch.cuda.Event()
                 ev.record(self.copy_stream)
             self.staging_free[b] = ev
@@ -360,7 +396,9 @@ class TimeDependentField(Field):
 
     def __init__(self, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
                  spatial_array_factory=None, output_dtype=np.float64, *, ring_size: int = 4, prefetch: int = 2,
-                 device=None) -> None:
+                 device=None, storage: str | None = None) -> None:
+        """``storage``: keep the snapshots on the device as "bfloat16" or "float16" with one scale
+        per level (the float32 steppers only); default: the source dtype."""
         super().__init__(Stagger(z_stagger), Stagger(y_stagger), Stagger(x_stagger))
         if data.ndim < 2:
             raise ValueError(
@@ -379,13 +417,28 @@ class TimeDependentField(Field):
         self._spatial_shape = tuple(int(s) for s in data.shape[1:])
         self._device = cuda_device(device)
         self._prefetch = max(0, int(prefetch))
+        if storage not in STORAGE:
+            raise ValueError(f"storage must be one of {sorted(k for k in STORAGE if k)}")
+        self._storage = STORAGE[storage]
+        if self._storage is not None and self._data_dtype != np.float32:
+            raise TypeError("bfloat16/float16 storage quantises float32 snapshots")
+        self._nlev = self._spatial_shape[0] if len(self._spatial_shape) == 3 else 1
         self._resident_source = isinstance(data, torch.Tensor) and data.is_cuda
+        self._q = self._q_scales = None
         if self._resident_source:
             self._ring = None
+            if self._storage is not None:
+                self._q = torch.empty(tuple(data.shape), dtype=self._storage, device=data.device)
+                self._q_scales = torch.ones((self._num_timesteps, self._nlev), dtype=torch.float32,
+                                            device=data.device)
+                src = data.contiguous()
+                for k in range(self._num_timesteps):
+                    quantize_levels(src[k], self._q[k], self._q_scales[k], self._nlev)
         else:
             if ring_size < 2 or ring_size > 8:
                 raise ValueError("ring_size must be between 2 and 8")
-            self._ring = SnapshotRing(data, self._spatial_shape, self._data_dtype, ring_size, self._device)
+            self._ring = SnapshotRing(data, self._spatial_shape, self._data_dtype, ring_size, self._device,
+                                      storage=self._storage)
         self._It = 0
 
     # ------------------------------------------------------------ properties
@@ -446,12 +499,32 @@ class TimeDependentField(Field):
 
     # -------------------------------------------------------------- snapshots
     def snapshot(self, k: int, keep: set[int] | frozenset = frozenset()) -> torch.Tensor:
-        """Device tensor of snapshot ``k`` (uploaded if needed)."""
+        """Device tensor of snapshot ``k`` in the storage dtype (uploaded if needed)."""
         if k < 0 or k >= self._num_timesteps:
             raise IndexError(k)
         if self._ring is None:
-            return self._data[k]
+            return self._data[k] if self._q is None else self._q[k]
         return self._ring.acquire(k, keep)
+
+    def snapshot_scales(self, k: int) -> torch.Tensor | None:
+        """Per-level scales of resident snapshot ``k`` (None for unscaled storage)."""
+        if self._storage is None:
+            return None
+        if self._ring is None:
+            return self._q_scales[k]
+        return self._ring.scales(k)
+
+    @property
+    def storage(self) -> str:
+        """Device storage dtype of the snapshots: "float64", "float32", "bfloat16" or "float16"."""
+        if self._storage is None:
+            return str(self._data_dtype)
+        return {torch.bfloat16: "bfloat16", torch.float16: "float16"}[self._storage]
+
+    @property
+    def storage_bytes_per_snapshot(self) -> int:
+        n = int(np.prod(self._spatial_shape))
+        return n * (2 if self._storage is not None else self._data_dtype.itemsize)
 
     def prefetch(self, k: int, keep: set[int]) -> None:
         if self._ring is not None and 0 <= k < self._num_timesteps:
@@ -477,6 +550,9 @@ class TimeDependentField(Field):
     def get_field_data(self, time_index: float, bbox: BBox | None = None) -> FieldData:
         """FieldData whose array is the (unmaterialised) blend at ``time_index``."""
         It, ft, gt = self.blend_weights(time_index)
+        if self._storage is not None:
+            raise ValueError("bfloat16/float16 storage runs only in the fused float32 steppers "
+                             "(build_simulation(..., arithmetic='float32'))")
         self.set_time_index(It)
         keep = {It, It + 1}
         prev = self.snapshot(It, keep)

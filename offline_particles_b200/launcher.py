@@ -43,7 +43,12 @@ class Launcher:
     (launcher.py:122-148) has no use.  ``construct_bbox`` remains available.
     """
 
-    def __init__(self, fieldset: Fieldset, *, index_padding: int = 0) -> None:
+    def __init__(self, fieldset: Fieldset, *, index_padding: int = 0, arithmetic: str = "float64") -> None:
+        """``arithmetic``: "float64" (bit-identical to the reference) or "float32" (the reduced-precision
+        fused steppers; needed for bfloat16/float16 field storage)."""
+        if arithmetic not in ("float64", "float32"):
+            raise ValueError("arithmetic must be 'float64' or 'float32'")
+        self.arithmetic = arithmetic
         self._scalar_data_sources: dict[str, ScalarProvider] = {}
         self._fieldset = fieldset
         if index_padding < 0:

@@ -34,14 +34,16 @@ class Simulation:
     def __init__(self, nparticles: int, timestepper: Timestepper, fieldset: Fieldset,
                  iteration_scheduler: IterationScheduler, time_scheduler: TimeScheduler,
                  output_writers: Mapping[str, object] | None = None, *, device=None,
-                 sort_interval: int = DEFAULT_SORT_INTERVAL) -> None:
-        """``sort_interval``: reorder particle storage by cell every that many steps (0: never)."""
+                 sort_interval: int = DEFAULT_SORT_INTERVAL, arithmetic: str = "float64") -> None:
+        """``sort_interval``: reorder particle storage by cell every that many steps (0: never).
+        ``arithmetic``: "float64" (bit-identical to the reference) or "float32" (the reduced-precision
+        fused steppers, which also take bfloat16/float16 field storage)."""
         self._timestepper = timestepper
         self._fieldset = fieldset
         self._iteration_scheduler = iteration_scheduler
         self._time_scheduler = time_scheduler
         self._output_writers = output_writers or {}
-        self._launcher = Launcher(fieldset)
+        self._launcher = Launcher(fieldset, arithmetic=arithmetic)
         self._launcher.maybe_increase_index_padding(timestepper.index_padding)
         self._launcher.register_scalar_data_sources_from_object(self._timestepper)
         for event in itertools.chain(self._iteration_scheduler.events, self._time_scheduler.events):
@@ -243,8 +245,9 @@ class SimulationBuilder:
         """Output writers (zarr) are outside this package's scope."""
         raise NotImplementedError("output writers are not part of offline_particles_b200")
 
-    def build_simulation(self, nparticles: int, *, device=None, sort_interval: int = DEFAULT_SORT_INTERVAL
-                         ) -> Simulation:
+    def build_simulation(self, nparticles: int, *, device=None, sort_interval: int = DEFAULT_SORT_INTERVAL,
+                         arithmetic: str = "float64") -> Simulation:
         return Simulation(nparticles=nparticles, timestepper=self._timestepper, fieldset=self._fieldset,
                           iteration_scheduler=self._iteration_scheduler, time_scheduler=self._time_scheduler,
-                          output_writers=types.MappingProxyType({}), device=device, sort_interval=sort_interval)
+                          output_writers=types.MappingProxyType({}), device=device, sort_interval=sort_interval,
+                          arithmetic=arithmetic)

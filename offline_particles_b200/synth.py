@@ -276,6 +276,75 @@ class SyntheticROMS:
             self._cache.pop(self._cache_order.pop(0), None)
         return snap
 
+    # ------------------------------------------------------- device generation
+    def device_snapshots(self, nt: int, device=None, dtype=None) -> dict:
+        """Snapshots 0..nt-1 of u, v, w, zeta generated on a CUDA device.
+
+        The same construction as ``snapshot`` evaluated with torch in float64 on
+        the device (equal to the host arrays to rounding, not bit for bit), for
+        workloads whose snapshots would take minutes to build on the host.
+        Returns CUDA tensors of shape ``(nt, ...)`` in ``dtype`` (default: the
+        grid's storage dtype).
+        """
+        import torch
+
+        dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        td = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64}[
+            np.dtype(dtype) if dtype is not None else self.dtype]
+        nx, ny, nz = self.spec.nx, self.spec.ny, self.spec.nz
+        f64 = dict(dtype=torch.float64, device=dev)
+        rho_t, corner_t = self._taper
+        corner = torch.tensor(corner_t, **f64)
+        pad = np.pad(rho_t, ((0, 0), (1, 1)), mode="edge")
+        tu = torch.tensor(np.minimum(pad[:, :-1], pad[:, 1:]), **f64)
+        pad = np.pad(rho_t, ((1, 1), (0, 0)), mode="edge")
+        tv = torch.tensor(np.minimum(pad[:-1, :], pad[1:, :]), **f64)
+        h = torch.tensor(self.h64, **f64)
+        mask = torch.tensor(self.mask_rho, **f64)
+        prof = torch.tensor(self._prof, **f64)
+        hc = self.spec.hc
+        Sw = (hc * torch.tensor(self.sigma_w, **f64)[:, None, None]
+              + h[None] * torch.tensor(self.Cw64, **f64)[:, None, None]) / (hc + h)[None]
+        dSw = Sw[1:] - Sw[:-1]
+        yc = torch.arange(ny + 1, **f64)[:, None] - 0.5
+        xc = torch.arange(nx + 1, **f64)[None, :] - 0.5
+        yu = torch.arange(ny, **f64)[:, None]
+        xu = torch.arange(nx + 1, **f64)[None, :] - 0.5
+        yv = torch.arange(ny + 1, **f64)[:, None] - 0.5
+        xv = torch.arange(nx, **f64)[None, :]
+        scale = self._velocity_scale()
+        out = {
+            "u": torch.empty((nt, nz, ny, nx - 1), dtype=td, device=dev),
+            "v": torch.empty((nt, nz, ny - 1, nx), dtype=td, device=dev),
+            "w": torch.empty((nt, nz + 1, ny, nx), dtype=td, device=dev),
+            "zeta": torch.empty((nt, ny, nx), dtype=td, device=dev),
+        }
+        for it in range(nt):
+            t = float(self.time_array[it]) if it < len(self.time_array) else it * self.spec.snapshot_interval
+            psi = torch.zeros((ny + 1, nx + 1), **f64)
+            for m in range(self._k.size):
+                ph = self._phi[m] + self._omega[m] * t
+                psi += self._amp[m] * torch.cos(self._k[m] * xc + self._l[m] * yc + ph)
+            psi *= corner
+            uf = -(psi[1:, :] - psi[:-1, :])
+            vf = psi[:, 1:] - psi[:, :-1]
+            for m in range(self._kp.size):
+                a = self._ampp[m]
+                uf += -a * self._kp[m] * torch.sin(self._kp[m] * xu + self._lp[m] * yu + self._phip[m]) * tu
+                vf += -a * self._lp[m] * torch.sin(self._kp[m] * xv + self._lp[m] * yv + self._phip[m]) * tv
+            mod = (1.0 + 0.2 * np.sin(2 * np.pi * t / 86400.0)) * scale
+            uf *= mod
+            vf *= mod
+            out["u"][it] = (prof[:, None, None] * uf[None, :, 1:-1]).to(td)
+            out["v"][it] = (prof[:, None, None] * vf[None, 1:-1, :]).to(td)
+            div = ((uf[:, 1:] - uf[:, :-1]) + (vf[1:, :] - vf[:-1, :])) / self.spec.dx
+            zeta = self.zeta_value(t)
+            Hz = (zeta + h)[None] * dSw
+            cum = torch.cat([torch.zeros((1, ny, nx), **f64), torch.cumsum(prof[:, None, None] * Hz, dim=0)])
+            out["w"][it] = (-div[None] * cum * mask[None]).to(td)
+            out["zeta"][it].fill_(zeta)
+        return out
+
     # ------------------------------------------------------------ accessors
     def field(self, name: str) -> _LazyField:
         nz, ny, nx = self.spec.nz, self.spec.ny, self.spec.nx

@@ -204,6 +204,12 @@ class Timestepper(abc.ABC):
         raise NotImplementedError
 
 
+def _require_float64(launcher: Launcher) -> None:
+    if launcher.arithmetic != "float64":
+        raise ValueError("arithmetic='float32' runs only the fused ROMS steppers; this step needs the "
+                         "stage-by-stage float64 path")
+
+
 def _time_dependent_fields(launcher: Launcher) -> dict[str, TimeDependentField]:
     fs = launcher.fieldset
     return {n: fs[n] for n in _abi.ROMS_FIELDS if n in fs and isinstance(fs[n], TimeDependentField)}
@@ -219,6 +225,10 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
     if len(dtypes) > 1:
         raise ValueError("time-dependent fields of one launch must share one storage dtype")
     dtype = dtypes.pop() if dtypes else np.dtype(np.float64)
+    storages = {f.storage for f in td.values()}
+    if storages & {"bfloat16", "float16"} and launcher.arithmetic != "float32":
+        raise ValueError("bfloat16/float16 field storage needs the float32 steppers "
+                         "(build_simulation(..., arithmetic='float32'))")
     slot = {k: j for j, k in enumerate(needed)}
     keep = set(needed)
     rf = _lib.opb_roms_fields()
@@ -227,9 +237,12 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
         if name in td:
             f = _lib.opb_field()
             f.is_static = 0
-            f.dtype = _abi._dtype_code(field.dtype)
+            f.dtype = _STORAGE_CODE[field.storage]
             for k in needed:
                 f.data[slot[k]] = _abi._ptr(field.snapshot(k, keep))
+                sc = field.snapshot_scales(k)
+                if sc is not None:
+                    f.scale[slot[k]] = _abi._ptr(sc)
             f.nslots = len(needed)
             shape = field.spatial_shape
             offsets = field.active_offsets
@@ -256,6 +269,14 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
         for tidx in entries:
             field.set_time_index(int(divmod(tidx, 1)[0]))
     return rf, table
+
+
+_STORAGE_CODE = {"float64": _lib.F64, "float32": _lib.F32, "bfloat16": _lib.BF16, "float16": _lib.F16}
+
+
+def _entry(name: str, launcher: Launcher) -> str:
+    """The float64 (bit-exact) or float32 fused entry point."""
+    return name + ("_fp32" if launcher.arithmetic == "float32" else "")
 
 
 def _upload_table(table, device) -> torch.Tensor:
@@ -333,6 +354,7 @@ class RK2Timestepper(Timestepper):
 
     def _unfused_step(self, particles, launcher: Launcher) -> None:
         """timesteppers.py:241-257."""
+        _require_float64(launcher)
         if self._pre_step_kernel is not None:
             launcher.launch_kernel(self._pre_step_kernel, particles, self._tidx)
         launcher.launch_kernel(self._rk_step_1_kernel, particles, self._tidx)
@@ -353,7 +375,7 @@ class RK2Timestepper(Timestepper):
                                                            "xidx_min", "xidx_max")}})
         dev_table = _upload_table(table, particles.device)
         _notify("before", len(steps))
-        _lib.call("opb_rk2_w_advection_steps", ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
+        _lib.call(_entry("opb_rk2_w_advection_steps", launcher), ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
                   ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
         _notify("after", len(steps))
@@ -400,6 +422,7 @@ class ABTimestepper(Timestepper):
 
     def _unfused_step(self, particles, launcher: Launcher) -> None:
         """timesteppers.py:296-305."""
+        _require_float64(launcher)
         if self._pre_step_kernel is not None:
             launcher.launch_kernel(self._pre_step_kernel, particles, self._tidx)
         launcher.launch_kernel(self._ab_kernel, particles, self._tidx)
@@ -416,7 +439,7 @@ class ABTimestepper(Timestepper):
                                                            "xidx_min", "xidx_max")}})
         dev_table = _upload_table(table, particles.device)
         _notify("before", len(steps))
-        _lib.call("opb_ab3_w_advection_steps", ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
+        _lib.call(_entry("opb_ab3_w_advection_steps", launcher), ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
                   ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
         _notify("after", len(steps))

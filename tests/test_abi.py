@@ -47,7 +47,7 @@ LAYOUT_PROBE = r"""
 #define S(T) printf(#T " %zu\n", sizeof(T))
 int main(void) {
     S(opb_field); F(opb_field, data); F(opb_field, dtype); F(opb_field, ndim); F(opb_field, shape);
-    F(opb_field, offset); F(opb_field, is_static); F(opb_field, nslots);
+    F(opb_field, offset); F(opb_field, is_static); F(opb_field, nslots); F(opb_field, scale);
     S(opb_roms_fields); F(opb_roms_fields, zeta); F(opb_roms_fields, C);
     S(opb_time); F(opb_time, ft); F(opb_time, gt);
     S(opb_particles); F(opb_particles, status); F(opb_particles, z); F(opb_particles, dz2); F(opb_particles, err);
