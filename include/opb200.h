@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define OPB_ABI_VERSION 2
+#define OPB_ABI_VERSION 3
 #define OPB_MAX_SLOTS 8
 
 /* storage dtypes of time-dependent fields (the float64-exact entry points take
@@ -152,6 +152,63 @@ int opb_ab3_w_advection(const opb_particles *p, const opb_scalars *s, const opb_
 /* kernels/roms/ab3_w_advection.pyx:180-229 (ab3_post_w_advection) */
 int opb_ab3_post_w_advection(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                              const opb_time *t, void *stream);
+
+/* ---- batched release experiments ---------------------------------------------
+ * No single reference counterpart: the reference advances one release per
+ * Simulation (simulation.py:27-229).  Here many releases share one particle
+ * arena, each in its own contiguous segment, and advance in one launch; each
+ * release runs exactly the steps its own Simulation would run with the ROMS
+ * presets (timesteppers.py:241-257 / :296-305), so its results are the same. */
+#define OPB_SCHEME_RK2 1
+#define OPB_SCHEME_AB3 2
+#define OPB_BATCH_CHUNK 32 /* particles a warp claims at a time */
+
+/* One experiment's work in a launch.  Its steps read table[table_offset ...]:
+ * 3 opb_time entries per RK2 step (t, t + alpha dt, t + dt), 2 per AB3 step
+ * (t, t + dt).  Chunks: experiment e owns chunks [first_chunk, first_chunk +
+ * ceil(count / OPB_BATCH_CHUNK)); first_chunk ascends through the table. */
+typedef struct {
+    int64_t start;       /* first storage index of the experiment's segment */
+    int64_t count;       /* particles in the segment */
+    int64_t first_chunk; /* chunks of the experiments before this one */
+    int32_t scheme;      /* OPB_SCHEME_RK2 or OPB_SCHEME_AB3 */
+    int32_t nsteps;      /* steps in this launch (>= 1) */
+    int32_t table_offset;
+    int32_t validate;    /* 1: the validation kernel runs before every step */
+    double dt;
+    double alpha;        /* RK2 only */
+} opb_experiment;
+
+/* Per-launch header, in DEVICE memory next to the tables (so one captured
+ * CUDA graph serves every launch: only device contents change). */
+typedef struct {
+    int32_t nexp;        /* experiments in the table */
+    int32_t _pad;
+    int64_t nchunks;     /* total chunks */
+    uint64_t next_chunk; /* work counter: zeroed by opb_batched_steps before its kernel */
+} opb_batch_header;
+
+/* Advance the experiments of `header`/`experiments`/`table` (DEVICE arrays)
+ * over the particle arena p (all AB3 history pointers required).  A
+ * persistent grid (`ctas` CTAs of `block` threads; ctas = 0: as many as stay
+ * resident) in which each warp claims chunks until none are left.  block is
+ * 128, 256 or 512.  Fields must have the ROMS layout (u, v, w, zeta
+ * time-dependent; h, dx, dy, C static).  Results equal running each
+ * experiment alone with opb_rk2/ab3_w_advection_steps. */
+int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const opb_experiment *experiments,
+                      const opb_scalars *s, const opb_roms_fields *f, const opb_time *table, int32_t block,
+                      int32_t ctas, void *stream);
+
+/* Spatially sort particles WITHIN each of nseg segments [start, start+count)
+ * (host arrays; segments disjoint and ascending).  Each segment is reordered
+ * by the Morton key of opb_sort_particles (inactive last, stable); particles
+ * never leave their segment.  ids (int64, DEVICE, one per arena particle, or
+ * NULL) is permuted with the particles.  No reference counterpart (the
+ * reference never reorders particles). */
+size_t opb_sort_segments_workspace_bytes(int64_t total, int32_t nseg);
+int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int64_t *seg_start,
+                      const int64_t *seg_count, int32_t nseg, int64_t *ids, void *workspace, size_t workspace_bytes,
+                      void *stream);
 
 /* ---- reduced-precision steppers --------------------------------------------
  * The precision variant of the fused steppers: float32 interpolation and

@@ -1,0 +1,466 @@
+"""Batched release experiments: many releases advanced together on one device.
+
+The reference runs one release per ``Simulation`` (simulation.py:27-229); a
+study of many releases runs them one after another.  ``ReleaseBatch`` keeps
+every release's particles in one device arena, one contiguous segment per
+release, and advances all of them one snapshot interval at a time with ONE
+persistent launch (``opb_batched_steps``):
+
+* a per-experiment offset table (segment start and count, scheme, dt, alpha,
+  step count, offset into a shared stage-time table) is written to pinned host
+  memory and copied to the device with the launch;
+* the launch, its table upload and its work-counter reset are captured once
+  as a CUDA graph per ring phase and replayed every interval (the snapshots of
+  an interval sit in fixed ring slots, so only device contents change);
+* a release's segment is Morton-sorted when it starts and every
+  ``sort_interval`` intervals after that, in place (``opb_sort_segments``).
+
+Each release advances exactly as its own ``Simulation`` with the same stock
+ROMS stepper would have: its stage times come from the same float64 time
+arithmetic (``Timestepper.get_time_index`` / ``advance_time``,
+timesteppers.py:64-85,157-161), and the kernel runs the stage functions of
+the fused steppers.  The results are therefore identical to running each
+release alone.
+"""
+
+from __future__ import annotations
+
+import bisect
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .fields import TimeDependentField
+from .fieldset import Fieldset
+from .kernels import _abi
+from .kernels.status import ParticleStatus
+from .launcher import Launcher
+from .particles import Particles
+from .timesteppers import ABTimestepper, RK2Timestepper, Timestepper, _time_dependent_fields, window_fields
+
+TIME_DTYPE = np.dtype([("prev", "<i4"), ("next", "<i4"), ("ft", "<f8"), ("gt", "<f8")])
+EXPERIMENT_DTYPE = np.dtype([("start", "<i8"), ("count", "<i8"), ("first_chunk", "<i8"), ("scheme", "<i4"),
+                             ("nsteps", "<i4"), ("table_offset", "<i4"), ("validate", "<i4"), ("dt", "<f8"),
+                             ("alpha", "<f8")])
+HEADER_DTYPE = np.dtype([("nexp", "<i4"), ("_pad", "<i4"), ("nchunks", "<i8"), ("next_chunk", "<u8")])
+assert TIME_DTYPE.itemsize == ctypes.sizeof(_lib.opb_time)
+assert EXPERIMENT_DTYPE.itemsize == ctypes.sizeof(_lib.opb_experiment)
+assert HEADER_DTYPE.itemsize == ctypes.sizeof(_lib.opb_batch_header)
+
+ARENA_FIELDS = {"status": np.uint8, **{name: np.float64 for name in _lib.PARTICLE_POINTERS}}
+
+
+def _align(n: int, a: int = 256) -> int:
+    return (n + a - 1) // a * a
+
+
+class TimeIndex:
+    """``Timestepper.get_time_index`` (timesteppers.py:64-85) on Python floats.
+
+    numpy float64 scalars and Python floats are both IEEE binary64 with
+    round-to-nearest, and ``searchsorted(side="right")`` is ``bisect_right``,
+    so the results are bit-identical; this form costs a fraction of a
+    microsecond, which matters when thousands of stage times are planned per
+    snapshot interval.
+    """
+
+    def __init__(self, time_array) -> None:
+        self.times = [float(t) for t in np.asarray(time_array, dtype=np.float64)]
+
+    def __call__(self, t: float) -> float:
+        T = self.times
+        if t < T[0] or t > T[-1]:
+            raise ValueError("Time is out of bounds of the time array.")
+        idx = bisect.bisect_right(T, t) - 1
+        t0 = T[idx]
+        t1 = T[idx + 1]  # IndexError at the last time, as numpy indexing raises in the reference
+        return idx + (t - t0) / (t1 - t0)
+
+
+def stage_times(r: "Release", time_index: TimeIndex, t: float) -> tuple[list[float], float]:
+    """Stage time indices of one step of ``r`` from time ``t``, and the next time: ``_stage_times`` of
+    RK2Timestepper / ABTimestepper (timesteppers.py:241-257, 296-305) in float form."""
+    nxt = t + r.dt
+    if r.scheme == _lib.SCHEME_RK2:
+        return [time_index(t), time_index(t + r.adt), time_index(nxt)], nxt
+    return [time_index(t), time_index(nxt)], nxt
+
+
+class IntervalPlanner:
+    """Splits every release's steps into snapshot intervals.
+
+    Interval j holds the steps that START in [T_j, T_j+1); their stages read
+    snapshots j, j+1 and j+2 (a step may end past T_j+1).  A release whose
+    next step cannot be planned (past the last snapshot, or a dt longer than
+    the snapshot spacing) stops before that step with ``error`` set; where the
+    reference raises part-way through that step, the batch does not start it.
+    """
+
+    def __init__(self, time_array, num_snapshots: int) -> None:
+        self.time_index = TimeIndex(time_array)
+        self.T = self.time_index.times
+        self.num_snapshots = int(num_snapshots)
+
+    def plan(self, releases: list["Release"], j: int):
+        """[(release index, release, steps, first table entry)], flat stage time indices; advances the
+        releases' time and step count."""
+        T = self.T
+        Tn = T[j + 1]
+        last = min(j + 2, self.num_snapshots - 1)
+        ti = self.time_index
+        exps = []
+        tidx_all: list[float] = []
+        for e, r in enumerate(releases):
+            if r.finished or r.time >= Tn:
+                continue
+            if r.time < T[j]:
+                raise RuntimeError(f"release {e} is at time {r.time}, before interval {j}")
+            t = r.time
+            k = 0
+            first = len(tidx_all)
+            while r.done + k < r.nsteps and t < Tn:
+                try:
+                    tidxs, nxt = stage_times(r, ti, t)
+                except (ValueError, IndexError) as err:
+                    r.error = err
+                    break
+                if any(int(x) < j or int(x) + 1 > last for x in tidxs):
+                    r.error = IndexError(f"step at time {t} needs snapshots outside {j}..{last}: dt longer "
+                                         "than the snapshot spacing, or past the last snapshot")
+                    break
+                tidx_all.extend(tidxs)
+                t = nxt
+                k += 1
+            if k:
+                exps.append((e, r, k, first))
+                r.time = t
+                r.done += k
+        return exps, tidx_all
+
+
+@dataclass
+class Release:
+    """One release experiment.
+
+    ``timestepper``: a stock ROMS stepper (``models.roms`` presets), whose
+    scheme, dt, alpha, validation pre-step and current time (the release time)
+    the experiment uses.  ``nsteps``: steps to run.  ``zidx``/``yidx``/``xidx``:
+    initial particle indices.  ``status``: initial status (default: MULTISTEP_1
+    for AB3, NORMAL for RK2).
+    """
+
+    timestepper: Timestepper
+    nsteps: int
+    zidx: np.ndarray
+    yidx: np.ndarray
+    xidx: np.ndarray
+    status: int | np.ndarray | None = None
+    name: str | None = None
+    # filled in by the batch
+    start: int = field(default=-1, init=False)
+    done: int = field(default=0, init=False)
+    error: BaseException | None = field(default=None, init=False)
+
+    def __post_init__(self) -> None:
+        ts = self.timestepper
+        if not isinstance(ts, (RK2Timestepper, ABTimestepper)) or not ts.fused():
+            raise TypeError("a Release needs a stock ROMS RK2 or AB3 timestepper (models.roms presets)")
+        if not isinstance(ts.time, (float, np.floating)):
+            raise TypeError("batched releases use float64 times")
+        if self.nsteps < 0:
+            raise ValueError("nsteps must be non-negative")
+        self.zidx = np.ascontiguousarray(self.zidx, dtype=np.float64)
+        self.yidx = np.ascontiguousarray(self.yidx, dtype=np.float64)
+        self.xidx = np.ascontiguousarray(self.xidx, dtype=np.float64)
+        if not (self.zidx.shape == self.yidx.shape == self.xidx.shape) or self.zidx.ndim != 1:
+            raise ValueError("zidx, yidx and xidx must be 1-D arrays of one length")
+        self.scheme = _lib.SCHEME_AB3 if isinstance(ts, ABTimestepper) else _lib.SCHEME_RK2
+        self.dt = float(ts._normalised_dt * ts.time_unit)
+        self.alpha = float(ts.alpha) if self.scheme == _lib.SCHEME_RK2 else 0.0
+        self.adt = float(ts.alpha * ts.dt) if self.scheme == _lib.SCHEME_RK2 else 0.0
+        self.validate = int(ts._pre_step_kernel is not None)
+        self.time = float(ts.time)
+        if self.status is None:
+            self.status = ParticleStatus.MULTISTEP_1 if self.scheme == _lib.SCHEME_AB3 else ParticleStatus.NORMAL
+
+    def __len__(self) -> int:
+        return self.zidx.shape[0]
+
+    @property
+    def finished(self) -> bool:
+        return self.done >= self.nsteps or self.error is not None
+
+    @property
+    def particle_steps(self) -> int:
+        return len(self) * self.nsteps
+
+
+class ReleaseBatch:
+    """Advance many ``Release`` experiments together on one device.
+
+    ``fieldset``: the shared fields (u, v, w, zeta time-dependent; h, dx, dy, C
+    static).  ``block``: CTA size of the persistent launch (128, 256, 512).
+    ``ctas``: CTAs of the launch (0: as many as stay resident).
+    ``sort_interval``: snapshot intervals between re-sorts of a release's
+    segment (0: never; a release is always sorted when it starts).
+    ``graphs``: capture each interval's upload + launch as a CUDA graph (only
+    when every time-dependent field streams through a ring, whose slot
+    addresses repeat).
+    """
+
+    def __init__(self, fieldset: Fieldset, releases: list[Release], *, device=None, block: int = 256,
+                 ctas: int = 0, sort_interval: int = 4, graphs: bool = True) -> None:
+        if block not in _lib.BATCH_BLOCKS:
+            raise ValueError(f"block must be one of {_lib.BATCH_BLOCKS}")
+        self.fieldset = fieldset
+        self.releases = list(releases)
+        self.launcher = Launcher(fieldset)
+        self.block = int(block)
+        self.ctas = int(ctas)
+        self.sort_interval = int(sort_interval)
+        self._td = _time_dependent_fields(self.launcher)
+        if not self._td:
+            raise ValueError("the fieldset has no time-dependent fields")
+        nts = {f.num_timesteps for f in self._td.values()}
+        if len(nts) != 1:
+            raise ValueError("time-dependent fields must have the same number of snapshots")
+        self.num_snapshots = nts.pop()
+        times = None
+        for r in self.releases:
+            ta = np.asarray(r.timestepper.time_array, dtype=np.float64)
+            if times is None:
+                times = ta
+            elif ta.shape != times.shape or not np.array_equal(ta, times):
+                raise ValueError("every release must use the same time array")
+        if times is None:
+            raise ValueError("no releases")
+        if times.shape[0] > self.num_snapshots:
+            raise ValueError("the time array has more entries than the fields have snapshots")
+        self.time_array = times
+        self.planner = IntervalPlanner(times, self.num_snapshots)
+        self._T = self.planner.T
+        self.graphs = bool(graphs) and all(f.streamed for f in self._td.values())
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.interval = None  # index j of the next snapshot interval to run
+        self._init_arena()
+        self._init_tables()
+        self._graphs: dict = {}
+        self._sorted_at: dict[int, int] = {}
+        self._sort_ws = None
+        self.launches = 0
+        self.sorts = 0
+
+    # ------------------------------------------------------------------ arena
+    def _init_arena(self) -> None:
+        n = 0
+        for r in self.releases:
+            r.start = n
+            n += len(r)
+        self.arena = Particles(n, device=self.device, **ARENA_FIELDS)
+        A = self.arena.arrays
+        for r in self.releases:
+            sl = slice(r.start, r.start + len(r))
+            A["zidx"][sl].copy_(torch.from_numpy(r.zidx))
+            A["yidx"][sl].copy_(torch.from_numpy(r.yidx))
+            A["xidx"][sl].copy_(torch.from_numpy(r.xidx))
+            st = r.status
+            if isinstance(st, (int, np.integer)):
+                A["status"][sl].fill_(int(st))
+            else:
+                A["status"][sl].copy_(torch.from_numpy(np.ascontiguousarray(st, dtype=np.uint8)))
+        # original arena slot of each storage slot: segments keep their ranges, so the slot within a
+        # release is order - start
+        self.order = torch.arange(n, dtype=torch.int64, device=self.device)
+        self.n = n
+
+    def _init_tables(self) -> None:
+        # capacity: at most ceil(interval / dt) + 1 steps per release per interval
+        dT = float(np.min(np.diff(self.time_array))) if len(self.time_array) > 1 else 1.0
+        entries = 0
+        for r in self.releases:
+            per = (3 if r.scheme == _lib.SCHEME_RK2 else 2)
+            entries += per * (int(math.ceil(dT / r.dt)) + 2)
+        self.max_experiments = len(self.releases)
+        self.max_entries = max(entries, 1)
+        self._off_exp = _align(HEADER_DTYPE.itemsize)
+        self._off_tab = self._off_exp + _align(self.max_experiments * EXPERIMENT_DTYPE.itemsize)
+        self._nbytes = self._off_tab + _align(self.max_entries * TIME_DTYPE.itemsize)
+        # two pinned staging buffers and two device copies, used alternately
+        self._host = [torch.zeros(self._nbytes, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+        self._dev = [torch.zeros(self._nbytes, dtype=torch.uint8, device=self.device) for _ in range(2)]
+        self._host_free: list[torch.cuda.Event | None] = [None, None]
+        self._parity = 0
+        self._scalars = None
+
+    # --------------------------------------------------------------- planning
+    def _plan(self, j: int):
+        return self.planner.plan(self.releases, j)
+
+    def _write_tables(self, j: int, exps, tidx_all, dtype) -> tuple[int, int]:
+        """Fill a pinned staging buffer; return (parity, chunks)."""
+        b = self._parity
+        self._parity ^= 1
+        ev = self._host_free[b]
+        if ev is not None:
+            ev.synchronize()  # the upload that last read this staging buffer has finished
+        host = self._host[b].numpy()
+        hdr = host[:HEADER_DTYPE.itemsize].view(HEADER_DTYPE)
+        ex = host[self._off_exp:self._off_exp + len(exps) * EXPERIMENT_DTYPE.itemsize].view(EXPERIMENT_DTYPE)
+        chunk = _lib.BATCH_CHUNK
+        nchunks = 0
+        for q, (e, r, k, first) in enumerate(exps):
+            ex[q] = (r.start, len(r), nchunks, r.scheme, k, first, r.validate, r.dt, r.alpha)
+            nchunks += (len(r) + chunk - 1) // chunk
+        hdr[0] = (len(exps), 0, nchunks, 0)
+        if tidx_all:
+            tid = np.asarray(tidx_all, dtype=np.float64)
+            It, fr = np.divmod(tid, 1.0)
+            It = It.astype(np.int64)
+            ft = fr.astype(dtype)
+            gt = dtype.type(1) - ft
+            tab = host[self._off_tab:self._off_tab + len(tidx_all) * TIME_DTYPE.itemsize].view(TIME_DTYPE)
+            tab["prev"] = It - j
+            tab["next"] = It + 1 - j
+            tab["ft"] = ft.astype(np.float64)
+            tab["gt"] = gt.astype(np.float64)
+        return b, nchunks
+
+    # --------------------------------------------------------------- stepping
+    @property
+    def finished(self) -> bool:
+        return all(r.finished for r in self.releases)
+
+    def _first_interval(self) -> int:
+        t0 = min(r.time for r in self.releases if not r.finished)
+        return max(0, bisect.bisect_right(self._T, t0) - 1)
+
+    def _scalars_struct(self):
+        if self._scalars is None:
+            L = self.launcher
+            self._scalars = _abi.scalars_struct({
+                "hc": L.scalar("hc", 0.0), "NZ": L.scalar("NZ", 0.0), "_dt": 0.0, "_RK2_alpha": 0.0,
+                **{n: L.scalar(n, 0.0) for n in ("zidx_min", "zidx_max", "yidx_min", "yidx_max", "xidx_min",
+                                                 "xidx_max")}})
+        return self._scalars
+
+    def _sort_due(self, j: int, exps) -> None:
+        if not exps:
+            return
+        due = []
+        for e, r, k, first in exps:
+            last = self._sorted_at.get(e)
+            if last is None or (self.sort_interval > 0 and j - last >= self.sort_interval):
+                due.append(r)
+                self._sorted_at[e] = j
+        if not due:
+            return
+        due.sort(key=lambda r: r.start)
+        starts = (ctypes.c_int64 * len(due))(*[r.start for r in due])
+        counts = (ctypes.c_int64 * len(due))(*[len(r) for r in due])
+        total = sum(len(r) for r in due)
+        lib = _lib.load()
+        need = int(lib.opb_sort_segments_workspace_bytes(total, len(due)))
+        if self._sort_ws is None or self._sort_ws.numel() < need:
+            self._sort_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+        fs = self.fieldset
+        dims = (ctypes.c_int64 * 3)(fs.z_size, fs.y_size, fs.x_size)
+        _lib.call("opb_sort_segments", ctypes.byref(_abi.particles_struct(self.arena)), ctypes.byref(dims), starts,
+                  counts, len(due), self.order.data_ptr(), self._sort_ws.data_ptr(), self._sort_ws.numel(),
+                  _abi.stream(self.arena))
+        self.sorts += 1
+
+    def _launch(self, rf, b: int) -> None:
+        dev = self._dev[b]
+        host = self._host[b]
+        base = dev.data_ptr()
+        dev.copy_(host, non_blocking=True)
+        _lib.call("opb_batched_steps", ctypes.byref(_abi.particles_struct(self.arena)), base, base + self._off_exp,
+                  ctypes.byref(self._scalars_struct()), ctypes.byref(rf), base + self._off_tab, self.block,
+                  self.ctas, _abi.stream(self.arena))
+
+    def _run_launch(self, rf, b: int) -> None:
+        if not self.graphs:
+            self._launch(rf, b)
+            return
+        key = (bytes(rf), b)
+        g = self._graphs.get(key)
+        if g is None:
+            if len(self._graphs) >= 32:
+                self._graphs.clear()
+            # one eager launch first (loads the module, queries occupancy), then capture
+            self._launch(rf, b)
+            g = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream(device=self.device)
+            side.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(side):
+                g.capture_begin(capture_error_mode="thread_local")
+                self._launch(rf, b)
+                g.capture_end()
+            torch.cuda.current_stream(self.device).wait_stream(side)
+            self._graphs[key] = g
+            return  # the eager launch did this interval's work; the capture itself ran nothing
+        g.replay()
+
+    def step_interval(self) -> bool:
+        """Run one snapshot interval for every release that has steps in it; False when all are done."""
+        if self.finished:
+            return False
+        if self.interval is None:
+            self.interval = self._first_interval()
+        j = self.interval
+        if j + 1 >= len(self._T):
+            for r in self.releases:
+                if not r.finished:
+                    r.error = IndexError("no snapshot interval left")
+            return False
+        exps, tidx_all = self._plan(j)
+        self.interval = j + 1
+        if exps:
+            window = list(range(j, min(j + 3, self.num_snapshots)))
+            rf, dtype = window_fields(self.launcher, window, self._td)
+            b, nchunks = self._write_tables(j, exps, tidx_all, dtype)
+            self._sort_due(j, exps)
+            self._run_launch(rf, b)
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream(self.device))
+            self._host_free[b] = ev
+            self.launches += 1
+            for f in self._td.values():
+                f.mark_used(window)
+                f.prefetch(j + 3, set(window[1:]))
+        return not self.finished
+
+    def run(self) -> None:
+        """Run every release to its end."""
+        while self.step_interval():
+            pass
+
+    def synchronize(self) -> None:
+        torch.cuda.synchronize(self.device)
+        self.arena.check_errors()
+
+    # ---------------------------------------------------------------- results
+    def result(self, r: Release | int, names=("zidx", "yidx", "xidx", "status")) -> dict[str, np.ndarray]:
+        """Host copies of a release's particle fields in its original particle order."""
+        if isinstance(r, int):
+            r = self.releases[r]
+        self.synchronize()
+        sl = slice(r.start, r.start + len(r))
+        pos = (self.order[sl] - r.start)
+        out = {}
+        for name in names:
+            key = name if name in self.arena else "_" + name
+            t = self.arena.arrays[key][sl]
+            o = torch.empty_like(t)
+            o.index_copy_(0, pos, t)
+            out[name] = o.cpu().numpy()
+        return out
+
+    @property
+    def particle_steps(self) -> int:
+        """Particle-steps planned so far (particles x steps, over all releases)."""
+        return sum(len(r) * r.done for r in self.releases)

@@ -7,6 +7,9 @@
 // -fmad=false: see opb_device.cuh.
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+
 #include <cstdio>
 #include <cstring>
 #include <initializer_list>
@@ -446,6 +449,120 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
     p.dz2[i] = s.k2z;
 }
 
+// ------------------------------------------------------- batched experiments
+// Many release experiments in one persistent launch.  Every warp claims
+// chunks of OPB_BATCH_CHUNK consecutive particles from a counter in the
+// header; a chunk lies inside one experiment's segment, so the 32 lanes of a
+// warp share a scheme, a step count and a time table and never diverge on
+// them.  Each lane runs its particle through the same stage functions as
+// k_rk2_steps / k_ab3_steps with its experiment's dt and alpha.
+template <typename T, typename I>
+__device__ __forceinline__ void batched_particle(const DParticles &p, long long i, const opb_experiment &E,
+                                                 const DScalars &sc0, const DRoms &r, const opb_time *table,
+                                                 const Levels &L) {
+    PState s;
+    s.status = p.status[i];
+    if (s.status & ST_INACTIVE) return;
+    DScalars sc = sc0;
+    sc.dt = E.dt;
+    sc.alpha = E.alpha;
+    s.zidx = p.zidx[i];
+    s.yidx = p.yidx[i];
+    s.xidx = p.xidx[i];
+    const bool ab3 = E.scheme == OPB_SCHEME_AB3;
+    if (ab3) {
+        s.k1x = p.dxidx1[i];
+        s.k1y = p.dyidx1[i];
+        s.k1z = p.dz1[i];
+        s.k2x = p.dxidx2[i];
+        s.k2y = p.dyidx2[i];
+        s.k2z = p.dz2[i];
+    }
+    const uint8_t st0 = s.status;
+    bool moved = false;
+    const opb_time *tab = table + E.table_offset;
+    for (int k = 0; k < E.nsteps; ++k) {
+        if (E.validate) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
+        if (s.status & ST_INACTIVE) break;
+        if (ab3) {
+            const opb_time t1 = tab[2 * k], t2 = tab[2 * k + 1];
+            const bool reuse = k > 0 && same_time(t1, s.at);
+            if (!ab3_step(s, bind_all<T, I, true>(r, t1), sc, reuse)) {
+                raise_zero_division(p);
+                break;
+            }
+            moved = true;
+            ab3_post(s, bind_all<T, I, true>(r, t2), L, sc);
+            s.at = t2;
+        } else {
+            const opb_time t1 = tab[3 * k], t2 = tab[3 * k + 1], t3 = tab[3 * k + 2];
+            const bool reuse = k > 0 && same_time(t1, s.at);
+            if (!rk2_stage1(s, bind_all<T, I, true>(r, t1), sc, reuse)) {
+                raise_zero_division(p);
+                break;
+            }
+            moved = true;
+            if (!rk2_stage2(s, bind_all<T, I, true>(r, t2), L, sc)) {
+                raise_zero_division(p);
+                break;
+            }
+            rk2_update(s, bind_all<T, I, true>(r, t3), L, sc);
+            s.at = t3;
+        }
+    }
+    if (s.status != st0) p.status[i] = s.status;
+    if (!moved) return;
+    p.zidx[i] = s.zidx;
+    p.yidx[i] = s.yidx;
+    p.xidx[i] = s.xidx;
+    p.z[i] = s.z;
+    if (ab3) {
+        p.dxidx0[i] = s.k1x;
+        p.dyidx0[i] = s.k1y;
+        p.dz0[i] = s.k1z;
+    }
+    p.dxidx1[i] = s.k1x;
+    p.dyidx1[i] = s.k1y;
+    p.dz1[i] = s.k1z;
+    p.dxidx2[i] = s.k2x;
+    p.dyidx2[i] = s.k2y;
+    p.dz2[i] = s.k2z;
+}
+
+// 128 registers per thread at any block size: 16 warps per SM
+template <typename T, typename I, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_batched_steps(const __grid_constant__ DParticles p,
+                                                                   opb_batch_header *__restrict__ hdr,
+                                                                   const opb_experiment *__restrict__ exps,
+                                                                   const __grid_constant__ DScalars sc,
+                                                                   const __grid_constant__ DRoms r,
+                                                                   const opb_time *__restrict__ table) {
+    OPB_LEVELS(r, sc);
+    const int nexp = hdr->nexp;
+    const long long nchunks = hdr->nchunks;
+    const int lane = threadIdx.x & 31;
+    unsigned long long *counter = (unsigned long long *)&hdr->next_chunk;
+    for (;;) {
+        unsigned long long c = 0;
+        if (lane == 0) c = atomicAdd(counter, 1ULL);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if ((long long)c >= nchunks) break;
+        // the experiment owning chunk c: the last one whose first_chunk <= c
+        int lo = 0, hi = nexp - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (exps[mid].first_chunk <= (long long)c) lo = mid;
+            else hi = mid - 1;
+        }
+        const opb_experiment E = exps[lo];
+        const long long j = ((long long)c - E.first_chunk) * OPB_BATCH_CHUNK + lane;
+        if (j < 0 || j >= E.count || E.nsteps <= 0) continue;
+        const long long i = E.start + j;
+        if (i < 0 || i >= p.n) continue;
+        batched_particle<T, I>(p, i, E, sc, r, table, L);
+    }
+}
+
 // ---------------------------------------------------------- output kernels
 // kernels/output/linear_interpolation.pyx:34-136: sample one field (static,
 // or blended in time like every other field) at the active particles.
@@ -500,6 +617,24 @@ int check_launch(const char *what) {
 }
 
 unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+// CTAs of `kernel` that stay resident on the whole device (SMs x blocks per SM),
+// cached per (kernel, device)
+int resident_ctas(const void *kernel, int block) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find({kernel, dev});
+    if (it != cache.end()) return it->second;
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess) return 0;
+    const int g = sms * (per_sm > 0 ? per_sm : 1);
+    cache[{kernel, dev}] = g;
+    return g;
+}
 
 int convert_particles(const opb_particles *in, DParticles &out, const char *what, bool need_positions) {
     if (!in) return fail(OPB_EINVAL, "%s: particles is NULL", what);
@@ -838,6 +973,49 @@ int opb_trilinear_interpolation(const opb_particles *p, const opb_field *f, cons
                                 void *stream) {
     if (!p) return fail(OPB_EINVAL, "opb_trilinear_interpolation: particles is NULL");
     return interpolate_impl("opb_trilinear_interpolation", 3, p, p->zidx, p->yidx, p->xidx, f, t, out, stream);
+}
+
+int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const opb_experiment *experiments,
+                      const opb_scalars *s, const opb_roms_fields *f, const opb_time *table, int32_t block,
+                      int32_t ctas, void *stream) {
+    const char *what = "opb_batched_steps";
+    DParticles dp;
+    DScalars ds;
+    DRoms dr;
+    int dtype, rc;
+    if ((rc = convert_particles(p, dp, what, true))) return rc;
+    if (!s) return fail(OPB_EINVAL, "%s: scalars is NULL", what);
+    convert_scalars(s, ds);
+    if ((rc = convert_fields(f, dr, what, true, &dtype))) return rc;
+    if (!header || !experiments || !table) return fail(OPB_EINVAL, "%s: NULL device array", what);
+    if (block != 128 && block != 256 && block != 512) return fail(OPB_EINVAL, "%s: block must be 128, 256 or 512", what);
+    if (ctas < 0) return fail(OPB_EINVAL, "%s: negative CTA count", what);
+    if (!roms_layout(dr)) return fail(OPB_EINVAL, "%s: fields must have the ROMS layout (u, v, w, zeta "
+                                      "time-dependent; h, dx, dy, C static)", what);
+    rc = need_fields(p, what, {{"z", p->z}, {"_dxidx1", p->dxidx1}, {"_dyidx1", p->dyidx1}, {"_dz1", p->dz1},
+                               {"_dxidx2", p->dxidx2}, {"_dyidx2", p->dyidx2}, {"_dz2", p->dz2},
+                               {"_dxidx0", p->dxidx0}, {"_dyidx0", p->dyidx0}, {"_dz0", p->dz0}});
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(&header->next_chunk, 0, sizeof(header->next_chunk), st);
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    if (dp.n == 0) return OPB_OK;
+    int launched = 0;
+    dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {
+        using T = decltype(tv);
+        using I = decltype(iv);
+        auto go = [&](auto kernel, int B) {
+            const int g = ctas > 0 ? ctas : resident_ctas((const void *)kernel, B);
+            if (g <= 0) return;
+            kernel<<<g, B, 0, st>>>(dp, header, experiments, ds, dr, table);
+            launched = 1;
+        };
+        if (block == 128) go(k_batched_steps<T, I, 128>, 128);
+        else if (block == 256) go(k_batched_steps<T, I, 256>, 256);
+        else go(k_batched_steps<T, I, 512>, 512);
+    });
+    if (!launched) return fail(OPB_ECUDA, "%s: occupancy query failed", what);
+    return check_launch(what);
 }
 
 }  // extern "C"

@@ -9,6 +9,7 @@
 
 #include <cub/device/device_radix_sort.cuh>
 #include <mutex>
+#include <vector>
 
 #include "opb200.h"
 #include "opb_errors.h"
@@ -96,6 +97,105 @@ size_t cub_temp_bytes(long long n) {
 }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// ------------------------------------------------------------ segment sort
+// Compact position q enumerates the segments' particles in storage order;
+// seg_cstart[s] is the compact position of segment s's first particle.
+struct SegArgs {
+    KeyArgs k;
+    const int64_t *seg_start;
+    const int64_t *seg_cstart;
+    int nseg;
+    long long m;
+};
+
+__device__ __forceinline__ int segment_of(const int64_t *cstart, int nseg, long long q) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (cstart[mid] <= q) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kBlock) k_segment_keys(SegArgs a, uint64_t *keys, int32_t *ids, int32_t *slot) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.m) return;
+    const int s = segment_of(a.seg_cstart, a.nseg, q);
+    const long long i = a.seg_start[s] + (q - a.seg_cstart[s]);
+    uint32_t key = kInactiveKey;
+    if (!(a.k.status[i] & OPB_STATUS_INACTIVE)) {
+        const uint32_t z = cell(a.k.zidx[i], a.k.nz, a.k.sz);
+        const uint32_t y = cell(a.k.yidx[i], a.k.ny, a.k.sy);
+        const uint32_t x = cell(a.k.xidx[i], a.k.nx, a.k.sx);
+        key = (spread3(z) << 2) | (spread3(y) << 1) | spread3(x);
+    }
+    keys[q] = ((uint64_t)s << 32) | key;
+    ids[q] = (int32_t)q;
+    slot[q] = (int32_t)i;
+}
+
+// scratch[q] <- arena[slot[perm[q]]]  (sorted compact order)
+__global__ void __launch_bounds__(kBlock) k_segment_take(const __grid_constant__ GatherArgs a, const int32_t *perm,
+                                                         const int32_t *slot) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.n) return;
+    const int32_t i = slot[perm[q]];
+    a.d_status[q] = a.s_status[i];
+    for (int f = 0; f < a.nf; ++f) a.d[f][q] = a.s[f][i];
+    if (a.d_ids) a.d_ids[q] = a.s_ids[i];
+}
+
+// arena[slot[q]] <- scratch[q]
+__global__ void __launch_bounds__(kBlock) k_segment_put(const __grid_constant__ GatherArgs a, const int32_t *slot) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.n) return;
+    const int32_t i = slot[q];
+    a.d_status[i] = a.s_status[q];
+    for (int f = 0; f < a.nf; ++f) a.d[f][i] = a.s[f][q];
+    if (a.d_ids) a.d_ids[i] = a.s_ids[q];
+}
+
+size_t cub_temp_bytes64(long long n, int end_bit) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, end_bit);
+    return bytes;
+}
+
+int key_end_bit(int nseg) {
+    int bits = 0;
+    while ((1LL << bits) < (long long)nseg) ++bits;
+    return 32 + bits;
+}
+
+// the pieces of a segment-sort workspace, in order
+struct SegLayout {
+    size_t keys_in, keys_out, ids_in, perm, slot, seg, status, fields, ids, temp, total;
+};
+
+SegLayout seg_layout(long long m, int nseg) {
+    SegLayout L{};
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o += align256(bytes);
+        return at;
+    };
+    L.keys_in = take((size_t)m * 8);
+    L.keys_out = take((size_t)m * 8);
+    L.ids_in = take((size_t)m * 4);
+    L.perm = take((size_t)m * 4);
+    L.slot = take((size_t)m * 4);
+    L.seg = take((size_t)nseg * 16);
+    L.status = take((size_t)m);
+    L.fields = take((size_t)m * 8 * 13);
+    L.ids = take((size_t)m * 8);
+    L.temp = take(cub_temp_bytes64(m, key_end_bit(nseg)));
+    L.total = o;
+    return L;
+}
 
 }  // namespace
 }  // namespace opb_sort
@@ -188,6 +288,113 @@ int opb_gather_particles(const opb_particles *src, const opb_particles *dst, con
     k_gather<<<grid, kBlock, 0, (cudaStream_t)stream>>>(g, perm);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_gather_particles: %s", cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+size_t opb_sort_segments_workspace_bytes(int64_t total, int32_t nseg) {
+    if (total <= 0 || nseg <= 0) return 0;
+    return seg_layout(total, nseg).total;
+}
+
+int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int64_t *seg_start,
+                      const int64_t *seg_count, int32_t nseg, int64_t *ids, void *workspace, size_t workspace_bytes,
+                      void *stream) {
+    const char *what = "opb_sort_segments";
+    if (!p) return fail(OPB_EINVAL, "%s: particles is NULL", what);
+    if (p->n < 0 || p->n > 0x7fffffffLL) return fail(OPB_EINVAL, "%s: particle count out of range", what);
+    if (nseg < 0) return fail(OPB_EINVAL, "%s: negative segment count", what);
+    if (nseg == 0 || p->n == 0) return OPB_OK;
+    if (!seg_start || !seg_count || !shape) return fail(OPB_EINVAL, "%s: NULL argument", what);
+    if (!p->status || !p->zidx || !p->yidx || !p->xidx) return fail(OPB_EINVAL, "%s: NULL particle array", what);
+    if (shape[0] < 1 || shape[1] < 1 || shape[2] < 1 || shape[0] > (1 << 30) || shape[1] > (1 << 30) ||
+        shape[2] > (1 << 30))
+        return fail(OPB_EINVAL, "%s: bad grid shape", what);
+    // host-side checks: disjoint ascending in-range segments
+    long long m = 0, end = 0;
+    for (int s = 0; s < nseg; ++s) {
+        if (seg_count[s] < 0 || seg_start[s] < end || seg_start[s] + seg_count[s] > p->n)
+            return fail(OPB_EINVAL, "%s: segment %d [%lld, +%lld) is out of order or out of range", what, s,
+                        (long long)seg_start[s], (long long)seg_count[s]);
+        end = seg_start[s] + seg_count[s];
+        m += seg_count[s];
+    }
+    if (m == 0) return OPB_OK;
+    const SegLayout L = seg_layout(m, nseg);
+    if (!workspace || workspace_bytes < L.total)
+        return fail(OPB_EINVAL, "%s: workspace of %zu bytes is smaller than the %zu needed", what, workspace_bytes,
+                    L.total);
+    char *ws = (char *)workspace;
+    cudaStream_t st = (cudaStream_t)stream;
+    // segment table (start, compact start) -> device
+    std::vector<int64_t> seg(2 * (size_t)nseg);
+    long long c = 0;
+    for (int s = 0; s < nseg; ++s) {
+        seg[s] = seg_start[s];
+        seg[nseg + s] = c;
+        c += seg_count[s];
+    }
+    cudaError_t e = cudaMemcpyAsync(ws + L.seg, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    SegArgs a;
+    a.k.status = p->status;
+    a.k.zidx = p->zidx;
+    a.k.yidx = p->yidx;
+    a.k.xidx = p->xidx;
+    a.k.n = p->n;
+    a.k.nz = (int)shape[0];
+    a.k.ny = (int)shape[1];
+    a.k.nx = (int)shape[2];
+    a.k.sz = shift_for(a.k.nz, 0);
+    a.k.sy = shift_for(a.k.ny, 0);
+    a.k.sx = shift_for(a.k.nx, 2);
+    a.seg_start = (const int64_t *)(ws + L.seg);
+    a.seg_cstart = a.seg_start + nseg;
+    a.nseg = nseg;
+    a.m = m;
+    uint64_t *keys_in = (uint64_t *)(ws + L.keys_in);
+    uint64_t *keys_out = (uint64_t *)(ws + L.keys_out);
+    int32_t *ids_in = (int32_t *)(ws + L.ids_in);
+    int32_t *perm = (int32_t *)(ws + L.perm);
+    int32_t *slot = (int32_t *)(ws + L.slot);
+    const unsigned grid = (unsigned)((m + kBlock - 1) / kBlock);
+    k_segment_keys<<<grid, kBlock, 0, st>>>(a, keys_in, ids_in, slot);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    size_t temp_bytes = workspace_bytes - L.temp;
+    e = cub::DeviceRadixSort::SortPairs(ws + L.temp, temp_bytes, keys_in, keys_out, ids_in, perm, (int)m, 0,
+                                        key_end_bit(nseg), st);
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: radix sort: %s", what, cudaGetErrorString(e));
+    // arena -> scratch in sorted order -> arena
+    const double *arena[13] = {p->zidx, p->yidx, p->xidx, p->z, p->dxidx0, p->dyidx0, p->dz0,
+                               p->dxidx1, p->dyidx1, p->dz1, p->dxidx2, p->dyidx2, p->dz2};
+    GatherArgs take{}, put{};
+    take.s_status = p->status;
+    take.d_status = (uint8_t *)(ws + L.status);
+    put.s_status = take.d_status;
+    put.d_status = p->status;
+    int nf = 0;
+    for (int f = 0; f < 13; ++f) {
+        if (!arena[f]) continue;
+        double *buf = (double *)(ws + L.fields) + (size_t)nf * m;
+        take.s[nf] = arena[f];
+        take.d[nf] = buf;
+        put.s[nf] = buf;
+        put.d[nf] = (double *)arena[f];
+        ++nf;
+    }
+    take.nf = put.nf = nf;
+    take.n = put.n = m;
+    if (ids) {
+        take.s_ids = ids;
+        take.d_ids = (int64_t *)(ws + L.ids);
+        put.s_ids = take.d_ids;
+        put.d_ids = ids;
+    }
+    k_segment_take<<<grid, kBlock, 0, st>>>(take, perm, slot);
+    k_segment_put<<<grid, kBlock, 0, st>>>(put, slot);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     opb::clear_error();
     return OPB_OK;
 }

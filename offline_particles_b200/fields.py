@@ -259,8 +259,10 @@ class SnapshotRing:
         # everything queued so far before overwriting the slot)
         self.last_use: dict[int, torch.cuda.Event | None] = {}
         self.copy_stream = torch.cuda.Stream(device=device)
-        self.staging = [torch.empty(tuple(spatial_shape), dtype=torch_dtype(np_dtype), pin_memory=True)
-                        for _ in range(2)]
+        # a device-resident source is copied device to device: no host staging
+        on_device = isinstance(source, torch.Tensor) and source.is_cuda
+        self.staging = [] if on_device else [torch.empty(tuple(spatial_shape), dtype=torch_dtype(np_dtype),
+                                                         pin_memory=True) for _ in range(2)]
         self.staging_free = [None, None]  # events: staging buffer's last H2D copy done
         self.staging_next = 0
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=1, thread_name_prefix="opb-snapshots")
@@ -286,8 +288,8 @@ class SnapshotRing:
 
     def _upload(self, k: int, slot: int, slot_free: torch.cuda.Event) -> None:
         src = self.source
-        if isinstance(src, torch.Tensor) and src.is_pinned():
-            # already in pinned host memory: one async copy, no staging
+        if isinstance(src, torch.Tensor) and (src.is_pinned() or src.is_cuda):
+            # already in pinned host memory (or on the device): one async copy, no staging
             with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
                 if slot_free is not None:
                     self.copy_stream.wait_event(slot_free)
@@ -295,7 +297,8 @@ class SnapshotRing:
                 ev = torch.cuda.Event()
                 ev.record(self.copy_stream)
             self.ready[k] = ev
-            self.h2d_bytes += src[k].numel() * src.element_size()
+            if not src.is_cuda:
+                self.h2d_bytes += src[k].numel() * src.element_size()
             return
         host = self._host_snapshot(k)
         with torch.cuda.device(self.device):
@@ -396,9 +399,12 @@ class TimeDependentField(Field):
 
     def __init__(self, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
                  spatial_array_factory=None, output_dtype=np.float64, *, ring_size: int = 4, prefetch: int = 2,
-                 device=None, storage: str | None = None) -> None:
+                 device=None, storage: str | None = None, ring: bool | None = None) -> None:
         """``storage``: keep the snapshots on the device as "bfloat16" or "float16" with one scale
-        per level (the float32 steppers only); default: the source dtype."""
+        per level (the float32 steppers only); default: the source dtype.  ``ring``: stream the
+        snapshots through a ring of ``ring_size`` device slots (default: yes, unless ``data`` is
+        already a CUDA tensor, which is then read in place; ring=True copies such a source slot by
+        slot, so that every launch reads the same slot addresses)."""
         super().__init__(Stagger(z_stagger), Stagger(y_stagger), Stagger(x_stagger))
         if data.ndim < 2:
             raise ValueError(
@@ -423,7 +429,7 @@ class TimeDependentField(Field):
         if self._storage is not None and self._data_dtype != np.float32:
             raise TypeError("bfloat16/float16 storage quantises float32 snapshots")
         self._nlev = self._spatial_shape[0] if len(self._spatial_shape) == 3 else 1
-        self._resident_source = isinstance(data, torch.Tensor) and data.is_cuda
+        self._resident_source = isinstance(data, torch.Tensor) and data.is_cuda and not ring
         self._q = self._q_scales = None
         if self._resident_source:
             self._ring = None

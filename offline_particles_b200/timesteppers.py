@@ -217,6 +217,26 @@ def _time_dependent_fields(launcher: Launcher) -> dict[str, TimeDependentField]:
 
 def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: dict[str, TimeDependentField]):
     """opb_roms_fields over the snapshots ``needed`` plus the per-stage opb_time table."""
+    rf, dtype = window_fields(launcher, needed, td)
+    slot = {k: j for j, k in enumerate(needed)}
+    entries = [t for step in steps for t in step]
+    table = (_lib.opb_time * len(entries))()
+    for j, tidx in enumerate(entries):
+        It, ft = divmod(tidx, 1)
+        It = int(It)
+        ft = dtype.type(ft)
+        gt = dtype.type(1 - ft)
+        table[j] = _lib.opb_time(slot[It], slot[It + 1], float(ft), float(gt))
+    # move the field windows the way the stage launches would have
+    for field in td.values():
+        for tidx in entries:
+            field.set_time_index(int(divmod(tidx, 1)[0]))
+    return rf, table
+
+
+def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDependentField]):
+    """opb_roms_fields whose slot j of every time-dependent field holds snapshot ``needed[j]``, and the
+    storage dtype of the time-dependent fields (numpy float64 or float32)."""
     fs = launcher.fieldset
     for name in _abi.ROMS_FIELDS:
         if name not in fs:
@@ -256,19 +276,7 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
         else:
             f = _abi.field_struct(field.get_field_data(0.0), _abi.ROMS_NDIM[name], name)
         setattr(rf, name, f)
-    entries = [t for step in steps for t in step]
-    table = (_lib.opb_time * len(entries))()
-    for j, tidx in enumerate(entries):
-        It, ft = divmod(tidx, 1)
-        It = int(It)
-        ft = dtype.type(ft)
-        gt = dtype.type(1 - ft)
-        table[j] = _lib.opb_time(slot[It], slot[It + 1], float(ft), float(gt))
-    # move the field windows the way the stage launches would have
-    for field in td.values():
-        for tidx in entries:
-            field.set_time_index(int(divmod(tidx, 1)[0]))
-    return rf, table
+    return rf, dtype
 
 
 _STORAGE_CODE = {"float64": _lib.F64, "float32": _lib.F32, "bfloat16": _lib.BF16, "float16": _lib.F16}

@@ -52,6 +52,10 @@ int main(void) {
     S(opb_time); F(opb_time, ft); F(opb_time, gt);
     S(opb_particles); F(opb_particles, status); F(opb_particles, z); F(opb_particles, dz2); F(opb_particles, err);
     S(opb_scalars); F(opb_scalars, NZ); F(opb_scalars, dt); F(opb_scalars, alpha); F(opb_scalars, bounds);
+    S(opb_experiment); F(opb_experiment, count); F(opb_experiment, first_chunk); F(opb_experiment, scheme);
+    F(opb_experiment, nsteps); F(opb_experiment, table_offset); F(opb_experiment, validate);
+    F(opb_experiment, dt); F(opb_experiment, alpha);
+    S(opb_batch_header); F(opb_batch_header, nchunks); F(opb_batch_header, next_chunk);
     return 0;
 }
 """
@@ -65,7 +69,8 @@ def test_struct_layouts_match_ctypes(tmp_path):
     lines = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
     c = dict(line.rsplit(" ", 1) for line in lines if line)
     types = {"opb_field": _lib.opb_field, "opb_roms_fields": _lib.opb_roms_fields, "opb_time": _lib.opb_time,
-             "opb_particles": _lib.opb_particles, "opb_scalars": _lib.opb_scalars}
+             "opb_particles": _lib.opb_particles, "opb_scalars": _lib.opb_scalars,
+             "opb_experiment": _lib.opb_experiment, "opb_batch_header": _lib.opb_batch_header}
     for key, val in c.items():
         if "." in key:
             t, m = key.split(".")

@@ -1,0 +1,184 @@
+"""Batched release experiments (ReleaseBatch, opb_batched_steps, opb_sort_segments) on the GPU.
+
+The property: every release's particles end bit-identical to running that
+release alone through Simulation with the same stock ROMS stepper, whatever
+else shares the launch, and whatever the launch shape, sort schedule or graph
+use.  The alone runs are themselves bit-identical to the reference (the
+parity tests of the fused steppers).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import same_bits, mismatch_report
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("zidx", "yidx", "xidx", "status")
+
+
+@pytest.fixture(scope="module")
+def grid():
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    g = SyntheticROMS(GridSpec(nx=96, ny=80, nz=12, nt=12, seed=11, dtype="float32"))
+    return g, g.oracle_fields()
+
+
+def _stepper(scheme, t_arr, dt, t0):
+    from offline_particles_b200.models.roms import ab3_w_advection_timestepper, rk2_w_advection_timestepper
+
+    f = rk2_w_advection_timestepper if scheme == "rk2" else ab3_w_advection_timestepper
+    return f(t_arr, np.float64(dt), time=np.float64(t0))
+
+
+# (scheme, dt, release time, steps, particles): uneven sizes (one particle, a partial chunk, several
+# blocks), release times on and off the snapshot grid, steps that end mid-interval
+SPECS = [
+    ("ab3", 120.0, 0.0, 200, 5000),
+    ("rk2", 300.0, 1800.0, 60, 1),
+    ("rk2", 180.0, 3600.0 * 2 + 17.25, 100, 33),
+    ("ab3", 60.0, 3600.0 * 3.5, 150, 1000),
+    ("rk2", 120.0, 3600.0 * 1, 170, 2500),
+    ("ab3", 180.0, 3600.0 * 5 + 0.125, 80, 700),
+]
+
+
+def _releases(g, t_arr, specs):
+    from offline_particles_b200.batching import Release
+
+    out = []
+    for q, (scheme, dt, t0, nsteps, n) in enumerate(specs):
+        z, y, x = g.release(n, seed=100 + q)
+        out.append(Release(_stepper(scheme, t_arr, dt, t0), nsteps, z, y, x))
+    return out
+
+
+def _alone(g, fields, spec, seed):
+    from b200_runner import b200_fieldset
+
+    import offline_particles_b200 as opb
+
+    scheme, dt, t0, nsteps, n = spec
+    t_arr = g.time_array[:fields["u"].shape[0]]
+    fs = b200_fieldset(fields, g.hc, g.spec.nz)
+    ts = _stepper(scheme, t_arr, dt, t0)
+    sim = opb.SimulationBuilder(ts, fs).build_simulation(n)
+    z, y, x = g.release(n, seed=seed)
+    sim.set_indices(z, y, x)
+    sim.set_particle_field("status", 10 if scheme == "ab3" else 0)
+    sim.run(nsteps)
+    P = sim.particles
+    return {k: P[k] for k in NAMES}
+
+
+@pytest.fixture(scope="module")
+def alone(grid):
+    g, fields = grid
+    return [_alone(g, fields, spec, 100 + q) for q, spec in enumerate(SPECS)]
+
+
+def _batch(grid, **kw):
+    from b200_runner import b200_fieldset
+
+    from offline_particles_b200.batching import ReleaseBatch
+
+    g, fields = grid
+    t_arr = g.time_array[:fields["u"].shape[0]]
+    fs = b200_fieldset(fields, g.hc, g.spec.nz)
+    rels = _releases(g, t_arr, SPECS)
+    b = ReleaseBatch(fs, rels, **kw)
+    b.run()
+    b.synchronize()
+    return b
+
+
+def _check(b, alone):
+    for q, r in enumerate(b.releases):
+        assert r.error is None and r.done == r.nsteps, (q, r.error)
+        got = b.result(r)
+        for k in NAMES:
+            assert same_bits(got[k], alone[q][k]), f"release {q} {k}: " + mismatch_report(got[k], alone[q][k])
+
+
+@pytest.mark.parametrize("block", [128, 256, 512])
+def test_batch_equals_each_release_alone(grid, alone, block):
+    b = _batch(grid, block=block)
+    assert b.graphs  # ring-streamed fields: intervals replay captured graphs
+    _check(b, alone)
+
+
+@pytest.mark.parametrize("sort_interval,graphs,ctas", [(0, True, 0), (1, False, 0), (3, True, 7)])
+def test_batch_independent_of_sorting_graphs_and_grid(grid, alone, sort_interval, graphs, ctas):
+    b = _batch(grid, sort_interval=sort_interval, graphs=graphs, ctas=ctas)
+    _check(b, alone)
+    if sort_interval == 1:
+        assert b.sorts >= b.launches
+
+
+def test_release_past_the_last_snapshot_stops_with_an_error(grid):
+    from b200_runner import b200_fieldset
+
+    from offline_particles_b200.batching import Release, ReleaseBatch
+
+    g, fields = grid
+    nt = fields["u"].shape[0]
+    t_arr = g.time_array[:nt]
+    fs = b200_fieldset(fields, g.hc, g.spec.nz)
+    z, y, x = g.release(50, seed=5)
+    long = Release(_stepper("ab3", t_arr, 300.0, 3600.0 * (nt - 3)), 1000, z, y, x)
+    short = Release(_stepper("rk2", t_arr, 300.0, 0.0), 12, z, y, x)
+    b = ReleaseBatch(fs, [long, short])
+    b.run()
+    b.synchronize()
+    assert isinstance(long.error, (IndexError, ValueError)) and 0 < long.done < 1000
+    assert short.error is None and short.done == 12
+
+
+def test_segment_sort_keeps_segments_and_permutes_ids():
+    import ctypes
+
+    import torch
+
+    from offline_particles_b200 import _lib
+    from offline_particles_b200.batching import ARENA_FIELDS
+    from offline_particles_b200.kernels import _abi
+    from offline_particles_b200.particles import Particles
+
+    n = 50_000
+    rng = np.random.default_rng(3)
+    P = Particles(n, **ARENA_FIELDS)
+    for k, hi in (("zidx", 12), ("yidx", 80), ("xidx", 96)):
+        P[k].copy_(torch.from_numpy(rng.uniform(0, hi, n)))
+    P["z"].copy_(torch.arange(n, dtype=torch.float64))  # a payload that must travel with its particle
+    st = np.zeros(n, np.uint8)
+    st[rng.integers(0, n, 500)] = 0x82
+    P["status"].copy_(torch.from_numpy(st))
+    ids = torch.arange(n, dtype=torch.int64, device="cuda")
+    starts, counts = [100, 9000, 20000], [5000, 1, 30000]
+    lib = _lib.load()
+    ws = torch.empty(int(lib.opb_sort_segments_workspace_bytes(sum(counts), 3)), dtype=torch.uint8, device="cuda")
+    dims = (ctypes.c_int64 * 3)(12, 80, 96)
+    _lib.call("opb_sort_segments", ctypes.byref(_abi.particles_struct(P)), ctypes.byref(dims),
+              (ctypes.c_int64 * 3)(*starts), (ctypes.c_int64 * 3)(*counts), 3, ids.data_ptr(), ws.data_ptr(),
+              ws.numel(), None)
+    torch.cuda.synchronize()
+    idn = ids.cpu().numpy()
+    zn = P["z"].cpu().numpy()
+    assert np.array_equal(zn, idn.astype(np.float64))  # payload moved with the ids
+    inside = np.zeros(n, bool)
+    for s, c in zip(starts, counts):
+        seg = idn[s:s + c]
+        assert np.array_equal(np.sort(seg), np.arange(s, s + c))  # particles stay in their segment
+        inside[s:s + c] = True
+        # inactive particles last in each segment
+        stn = P["status"].cpu().numpy()[s:s + c]
+        act = (stn & 0x80) == 0
+        assert not np.any(act[np.argmax(~act):]) if (~act).any() else True
+    assert np.array_equal(idn[~inside], np.flatnonzero(~inside))  # outside the segments: untouched
+    with pytest.raises(ValueError, match="out of order"):
+        _lib.call("opb_sort_segments", ctypes.byref(_abi.particles_struct(P)), ctypes.byref(dims),
+                  (ctypes.c_int64 * 2)(5000, 100), (ctypes.c_int64 * 2)(10, 10), 2, None, ws.data_ptr(),
+                  ws.numel(), None)

@@ -62,7 +62,7 @@ def test_two_rank_shards_reassemble_the_single_process_run():
     from offline_particles_b200.synth import GridSpec, SyntheticROMS
     from oracle import oracle as O
 
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of a process that has threads
     out = mgr.dict()
     port = _free_port()
     mp.spawn(_rank_main, args=(2, port, out), nprocs=2, join=True)
