@@ -66,10 +66,24 @@ def parse():
     ap.add_argument("--dt", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
-    ap.add_argument("--study", choices=("precision",), default=None,
+    ap.add_argument("--study", choices=("precision", "batched"), default=None,
                     help="precision: float64 vs float32 arithmetic with float32/float16/bfloat16 storage, "
-                         "separation in metres after --days")
+                         "separation in metres after --days; batched: release experiments in one batch vs "
+                         "one after another through the plain path")
     ap.add_argument("--days", type=str, default="1,3,7")
+    # batched releases (--study batched)
+    ap.add_argument("--batch-grid", type=str, default="40,512,512", help="nz,ny,nx of the batched workload")
+    ap.add_argument("--experiments", type=int, default=256)
+    ap.add_argument("--count-range", type=str, default="1e3,1e6", help="log-uniform particle counts")
+    ap.add_argument("--count-scale", type=float, default=1.0, help="multiply every experiment's particle count")
+    ap.add_argument("--release-days", type=float, default=10.0)
+    ap.add_argument("--duration-days", type=str, default="1,20")
+    ap.add_argument("--batch-dt", type=float, default=180.0)
+    ap.add_argument("--block", type=int, default=None, help="batched launch shape (default: autotuned)")
+    ap.add_argument("--warps-per-sm", type=int, default=None)
+    ap.add_argument("--sort-interval", type=int, default=None)
+    ap.add_argument("--buckets", type=int, default=None)
+    ap.add_argument("--no-plain", action="store_true", help="skip the one-release-at-a-time arm")
     return ap.parse_args()
 
 
@@ -391,12 +405,7 @@ def b200_arm(a) -> None:
         return
 
     # ---- roofline of the fused kernel -------------------------------------------------
-    peaks = {}
-    try:
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
-    except (OSError, ValueError):
-        pass
-    peak = peaks.get("hbm_gbs") or 6650.0
+    peak = measured_peak_gbs()
     # physical DRAM bytes per fused step of this kernel on this workload, from one ncu capture of the
     # full-size timed launches (profiles/k_ab3_steps_f32_config2_sorted.md: 2.615 GB / 61 steps and
     # 2.585 GB / 59 steps); traffic per launch scales with the steps it runs
@@ -516,10 +525,214 @@ def precision_study(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+def measured_peak_gbs() -> float:
+    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json), else the fallback 6650 GB/s."""
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        peaks = {}
+    return float(peaks.get("hbm_gbs") or 6650.0)
+
+
+class EventPairs:
+    """CUDA events around each launch of a ReleaseBatch (its observer protocol)."""
+
+    def __init__(self) -> None:
+        self.pairs = []
+
+    def before(self) -> None:
+        import torch
+
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.pairs.append([e, None])
+
+    def after(self) -> None:
+        import torch
+
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.pairs[-1][1] = e
+
+    def durations_ms(self) -> list[float]:
+        return [s.elapsed_time(e) for s, e in self.pairs]
+
+
+def batched_workload(a, grid):
+    """The release experiments: log-uniform counts, uniform release times and durations, RK2/AB3 at random."""
+    rng = np.random.default_rng(4)
+    E = a.experiments
+    lo, hi = (float(v) for v in a.count_range.split(","))
+    dlo, dhi = (float(v) for v in a.duration_days.split(","))
+    counts = np.maximum(1, np.round(np.exp(rng.uniform(np.log(lo), np.log(hi), E)) * a.count_scale)).astype(int)
+    t0 = rng.uniform(0.0, a.release_days * 86400.0, E)
+    nsteps = np.floor(rng.uniform(dlo, dhi, E) * 86400.0 / a.batch_dt).astype(int)
+    schemes = np.where(rng.random(E) < 0.5, "rk2", "ab3")
+    return [dict(scheme=str(schemes[e]), t0=float(t0[e]), nsteps=int(nsteps[e]), n=int(counts[e]), seed=5000 + e)
+            for e in range(E)]
+
+
+def batched_study(a) -> None:
+    """Config-4 batched releases: one ReleaseBatch vs the plain path one release at a time.
+
+    Snapshots are generated on the device and stay resident; the plain arm
+    reads them in place, the batched arm streams them device-to-device through
+    a 4-slot ring (fixed slot addresses, so intervals replay CUDA graphs).
+    Both arms start from the same host arrays; the timed regions include
+    building each arm's particle state from them.  Every experiment's final
+    state is compared bit for bit between the arms.
+    """
+    import torch
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200.batching import Release, ReleaseBatch
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    torch.cuda.set_device(0)
+    nz, ny, nx = (int(v) for v in a.batch_grid.split(","))
+    specs = batched_workload(a, None)
+    t_end = max(s["t0"] + s["nsteps"] * a.batch_dt for s in specs)
+    nt = int(math.ceil(t_end / 3600.0)) + 2
+    grid = SyntheticROMS(GridSpec(nx=nx, ny=ny, nz=nz, nt=nt, seed=4, dtype="float32"))
+    t_arr = grid.time_array[:nt]
+    t0 = time.perf_counter()
+    snaps = grid.device_snapshots(nt)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    inputs = [grid.release(s["n"], seed=s["seed"]) for s in specs]
+    total_ps = sum(s["n"] * s["nsteps"] for s in specs)
+    statics = {n: opb.StaticField.from_numpy(arr, *STAGGERS[n])
+               for n, arr in (("h", grid.h), ("dx", grid.dx), ("dy", grid.dy), ("C", grid.C))}
+
+    def fieldset(ring: bool):
+        kw = {n: opb.TimeDependentField.from_tensor(snaps[n], *STAGGERS[n], ring=ring, ring_size=4) for n in TD}
+        return opb.Fieldset(nt, nz, ny, nx, constants={"hc": grid.hc, "NZ": nz}, **kw, **statics)
+
+    def stepper(s):
+        f = opb.roms.rk2_w_advection_timestepper if s["scheme"] == "rk2" else opb.roms.ab3_w_advection_timestepper
+        return f(t_arr, np.float64(a.batch_dt), time=np.float64(s["t0"]))
+
+    # ---- batched ---------------------------------------------------------------
+    fs_ring = fieldset(True)
+    tuned = None
+    if a.block is None or a.warps_per_sm is None or a.sort_interval is None or a.buckets is None:
+        from offline_particles_b200.autotune import autotune
+
+        probe = [Release(stepper(s), s["nsteps"], *inputs[q]) for q, s in enumerate(specs)]
+        tuned = autotune(fs_ring, probe)
+        del probe
+    block = a.block if a.block is not None else tuned["block"]
+    warps = a.warps_per_sm if a.warps_per_sm is not None else tuned["warps_per_sm"]
+    sort_interval = a.sort_interval if a.sort_interval is not None else tuned["sort_interval"]
+    buckets = a.buckets if a.buckets is not None else tuned["buckets"]
+    split = tuned["split_schemes"] if tuned is not None else True
+    torch.cuda.empty_cache()
+    timer = EventPairs()
+    with ClockSampler(0) as clocks:
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_.record()
+        rels = [Release(stepper(s), s["nsteps"], *inputs[q]) for q, s in enumerate(specs)]
+        batch = ReleaseBatch(fs_ring, rels, block=block, warps_per_sm=warps, sort_interval=sort_interval,
+                             buckets=buckets, split_schemes=split)
+        batch.observers.append(timer)
+        batch.run()
+        e_.record()
+        torch.cuda.synchronize()
+        batch_wall = time.perf_counter() - w0
+    batch_s = s_.elapsed_time(e_) * 1e-3
+    launch_ms = timer.durations_ms()
+    errors = [q for q, r in enumerate(rels) if r.error is not None]
+    batch_res = [batch.result(r, ("zidx", "yidx", "xidx", "status")) for r in rels]
+    per_snap = sum(fs_ring[n].storage_bytes_per_snapshot for n in TD)
+    f_pair = 2 * per_snap + 3 * grid.h.nbytes + grid.C.nbytes
+    state_b = {"rk2": 2 * (1 + 3 * 8), "ab3": 2 * (1 + 3 * 8 + 6 * 8)}
+    alg_bytes = sum(s["n"] * s["nsteps"] * state_b[s["scheme"]] for s in specs) + f_pair * sum(
+        st[3] for st in batch.stats)
+    kernel_s = sum(launch_ms) * 1e-3
+    peak = measured_peak_gbs()
+    batched = {"value": total_ps / batch_s, "unit": UNIT, "seconds": batch_s, "wall_s": batch_wall,
+               "launches": batch.launches, "segment_sorts": batch.sorts, "graphs": batch.graphs,
+               "block": block, "warps_per_sm": warps, "sort_interval_intervals": sort_interval, "buckets": buckets,
+               "split_schemes": split,
+               "autotune": tuned,
+               "launch_ms_median": statistics.median(launch_ms) if launch_ms else None,
+               "launch_time_share": kernel_s / batch_s,
+               "roofline": {"bound": "hbm", "achieved": alg_bytes / kernel_s / 1e9, "peak": peak, "unit": "GB/s",
+                            "frac": alg_bytes / kernel_s / 1e9 / peak,
+                            "algorithmic_bytes": alg_bytes,
+                            "definition": "sum over experiments of particle-steps x state bytes (RK2 50 B, AB3 146 B) "
+                                          "+ per interval the snapshot pair and statics x the most steps of one "
+                                          "experiment, over the summed launch times"},
+               "errors": errors, "clocks": clocks.summary()}
+    del batch, fs_ring
+    torch.cuda.empty_cache()
+
+    # ---- plain: one release at a time ------------------------------------------
+    plain = None
+    identical = None
+    if not a.no_plain:
+        fs_res = fieldset(False)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_.record()
+        plain_res = []
+        per = []
+        for q, s in enumerate(specs):
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            sim = opb.SimulationBuilder(stepper(s), fs_res).build_simulation(s["n"])
+            sim.set_indices(*inputs[q])
+            sim.set_particle_field("status", 10 if s["scheme"] == "ab3" else 0)
+            sim.run(s["nsteps"])
+            P = sim.particles
+            plain_res.append({k: P[k] for k in ("zidx", "yidx", "xidx", "status")})
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev1.record()
+            per.append((ev0, ev1))
+            del sim
+        e_.record()
+        torch.cuda.synchronize()
+        plain_s = s_.elapsed_time(e_) * 1e-3
+        # plain rate by release size: where one-at-a-time leaves the GPU idle
+        secs = np.array([a_.elapsed_time(b_) * 1e-3 for a_, b_ in per])
+        ns = np.array([s["n"] for s in specs])
+        ps = np.array([s["n"] * s["nsteps"] for s in specs], dtype=np.float64)
+        bands = {}
+        for lo_, hi_ in ((0, 1e4), (1e4, 1e5), (1e5, 1e7)):
+            m = (ns >= lo_) & (ns < hi_)
+            if m.any():
+                bands[f"{lo_:.0e}-{hi_:.0e}"] = {"releases": int(m.sum()), "particle_steps": float(ps[m].sum()),
+                                                  "seconds": float(secs[m].sum()),
+                                                  "rate": float(ps[m].sum() / secs[m].sum())}
+        plain = {"value": total_ps / plain_s, "unit": UNIT, "seconds": plain_s,
+                 "wall_s": time.perf_counter() - w0, "by_release_size": bands}
+        identical = all(np.array_equal(br[k].view(np.uint8), pr[k].view(np.uint8))
+                        for br, pr in zip(batch_res, plain_res) for k in br)
+    counts = [s["n"] for s in specs]
+    line = {"study": "batched", "metric": METRIC, "unit": UNIT,
+            "value": batched["value"], "vs_plain": (batched["value"] / plain["value"]) if plain else None,
+            "batched": batched, "plain": plain, "identical_to_plain": identical,
+            "workload": {"grid": [nz, ny, nx], "field_dtype": "float32", "snapshots": nt,
+                         "experiments": len(specs), "particles": int(sum(counts)),
+                         "particles_min_max": [int(min(counts)), int(max(counts))],
+                         "rk2": sum(s["scheme"] == "rk2" for s in specs), "dt_s": a.batch_dt,
+                         "particle_steps": int(total_ps), "release_days": a.release_days,
+                         "duration_days": a.duration_days, "count_scale": a.count_scale},
+            "snapshot_generation_s": gen_s,
+            "data": "synthetic; snapshots generated on the device and resident (plain reads them in place, "
+                    "batched copies them into a 4-slot ring)"}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     a = parse()
     if a.study == "precision":
         precision_study(a)
+    elif a.study == "batched":
+        batched_study(a)
     elif a.impl == "reference":
         reference_arm(a)
     else:

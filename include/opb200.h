@@ -177,38 +177,55 @@ typedef struct {
     int32_t validate;    /* 1: the validation kernel runs before every step */
     double dt;
     double alpha;        /* RK2 only */
+    int32_t bucket_row;  /* row of the experiment in the bucket-bounds table (interleaved order) */
+    int32_t _pad;
 } opb_experiment;
 
 /* Per-launch header, in DEVICE memory next to the tables (so one captured
  * CUDA graph serves every launch: only device contents change). */
 typedef struct {
     int32_t nexp;        /* experiments in the table */
-    int32_t _pad;
-    int64_t nchunks;     /* total chunks */
+    int32_t nbuckets;    /* 0: segment-major work order; else spatially interleaved over this many buckets */
+    int64_t nchunks;     /* total chunks (segment-major: set by the caller; interleaved: by the launch) */
     uint64_t next_chunk; /* work counter: zeroed by opb_batched_steps before its kernel */
 } opb_batch_header;
 
 /* Advance the experiments of `header`/`experiments`/`table` (DEVICE arrays)
  * over the particle arena p (all AB3 history pointers required).  A
  * persistent grid (`ctas` CTAs of `block` threads; ctas = 0: as many as stay
- * resident) in which each warp claims chunks until none are left.  block is
- * 128, 256 or 512.  Fields must have the ROMS layout (u, v, w, zeta
- * time-dependent; h, dx, dy, C static).  Results equal running each
+ * resident) in which each warp claims chunks until none are left.  Shapes:
+ * block 256 with warps_per_sm 16, 24 or 32 (register budget per thread 128,
+ * 80 or 64), or block 128 with 16; scheme 0 takes 16 only.  Work order: header->nbuckets = 0 walks each
+ * experiment's segment in turn (chunks from first_chunk); nbuckets > 0 walks
+ * Morton buckets in turn and, within a bucket, every experiment's particles in
+ * it (bucket_bounds as written by opb_sort_segments, row bucket_row per
+ * experiment; item_scratch: nexp * nbuckets + 1 int64 of DEVICE scratch), so
+ * particles of all experiments that share a region are advanced together and
+ * share the field data in L2.  scheme: 0 advances every experiment of the
+ * table with one kernel; OPB_SCHEME_RK2 / OPB_SCHEME_AB3 compiles that scheme
+ * alone (smaller code, fewer registers) and skips experiments of the other.
+ * Fields must have the ROMS layout (u, v, w,
+ * zeta time-dependent; h, dx, dy, C static).  Results equal running each
  * experiment alone with opb_rk2/ab3_w_advection_steps. */
 int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const opb_experiment *experiments,
-                      const opb_scalars *s, const opb_roms_fields *f, const opb_time *table, int32_t block,
-                      int32_t ctas, void *stream);
+                      const opb_scalars *s, const opb_roms_fields *f, const opb_time *table,
+                      const int64_t *bucket_bounds, int64_t *item_scratch, int32_t scheme, int32_t block,
+                      int32_t warps_per_sm, int32_t ctas, void *stream);
 
 /* Spatially sort particles WITHIN each of nseg segments [start, start+count)
  * (host arrays; segments disjoint and ascending).  Each segment is reordered
  * by the Morton key of opb_sort_particles (inactive last, stable); particles
  * never leave their segment.  ids (int64, DEVICE, one per arena particle, or
- * NULL) is permuted with the particles.  No reference counterpart (the
- * reference never reorders particles). */
+ * NULL) is permuted with the particles.  bucket_bounds (DEVICE, nseg rows of
+ * nbuckets + 1 int64, or NULL): row s, entry b = storage index of segment s's
+ * first particle in Morton bucket >= b (nbuckets equal power-of-two key
+ * ranges covering the grid; entry nbuckets = the first inactive particle or
+ * the segment's end).  No reference counterpart (the reference never
+ * reorders particles). */
 size_t opb_sort_segments_workspace_bytes(int64_t total, int32_t nseg);
 int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int64_t *seg_start,
-                      const int64_t *seg_count, int32_t nseg, int64_t *ids, void *workspace, size_t workspace_bytes,
-                      void *stream);
+                      const int64_t *seg_count, int32_t nseg, int64_t *ids, int32_t nbuckets, int64_t *bucket_bounds,
+                      void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---- reduced-precision steppers --------------------------------------------
  * The precision variant of the fused steppers: float32 interpolation and

@@ -23,7 +23,7 @@ INCLUDE = ROOT / "include"
 GENCODE = "-gencode=arch=compute_100a,code=sm_100a"
 # per-file flags, as CMakeLists.txt sets them: the float64 path contracts no
 # multiply-add (bit parity with the reference); the float32 path may
-SOURCE_FLAGS = {"opb_roms.cu": ["-fmad=false"], "opb_fast.cu": ["-prec-div=false", "-ftz=true"]}
+SOURCE_FLAGS = {"opb_roms.cu": ["-fmad=false"], "opb_batched.cu": ["-fmad=false"], "opb_fast.cu": ["-prec-div=false", "-ftz=true"]}
 
 
 def _sources() -> list[Path]:

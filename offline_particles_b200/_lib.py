@@ -63,17 +63,18 @@ class opb_scalars(ctypes.Structure):
 class opb_experiment(ctypes.Structure):
     _fields_ = [("start", ctypes.c_int64), ("count", ctypes.c_int64), ("first_chunk", ctypes.c_int64),
                 ("scheme", ctypes.c_int32), ("nsteps", ctypes.c_int32), ("table_offset", ctypes.c_int32),
-                ("validate", ctypes.c_int32), ("dt", ctypes.c_double), ("alpha", ctypes.c_double)]
+                ("validate", ctypes.c_int32), ("dt", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("bucket_row", ctypes.c_int32), ("_pad", ctypes.c_int32)]
 
 
 class opb_batch_header(ctypes.Structure):
-    _fields_ = [("nexp", ctypes.c_int32), ("_pad", ctypes.c_int32), ("nchunks", ctypes.c_int64),
+    _fields_ = [("nexp", ctypes.c_int32), ("nbuckets", ctypes.c_int32), ("nchunks", ctypes.c_int64),
                 ("next_chunk", ctypes.c_uint64)]
 
 
 SCHEME_RK2, SCHEME_AB3 = 1, 2
 BATCH_CHUNK = 32
-BATCH_BLOCKS = (128, 256, 512)
+BATCH_SHAPES = ((256, 16), (256, 24), (256, 32), (128, 16))  # (block, warps per SM)
 
 _P = ctypes.POINTER
 _VP = ctypes.c_void_p
@@ -100,8 +101,8 @@ SIGNATURES = {
                                        ctypes.c_int32, ctypes.c_int32, _VP],
     "opb_ab3_w_advection_steps_fp32": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP,
                                        ctypes.c_int32, ctypes.c_int32, _VP],
-    "opb_batched_steps": [_P(opb_particles), _VP, _VP, _P(opb_scalars), _P(opb_roms_fields), _VP, ctypes.c_int32,
-                          ctypes.c_int32, _VP],
+    "opb_batched_steps": [_P(opb_particles), _VP, _VP, _P(opb_scalars), _P(opb_roms_fields), _VP, _VP, _VP,
+                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _VP],
     "opb_quantize_levels": [_VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP, _VP],
 }
 
@@ -111,8 +112,8 @@ SIGNATURES_OTHER = {
     "opb_sort_workspace_bytes": ([ctypes.c_int64], ctypes.c_size_t),
     "opb_sort_particles_noalloc": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP], ctypes.c_int),
     "opb_sort_segments_workspace_bytes": ([ctypes.c_int64, ctypes.c_int32], ctypes.c_size_t),
-    "opb_sort_segments": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP, ctypes.c_int32, _VP, _VP,
-                           ctypes.c_size_t, _VP], ctypes.c_int),
+    "opb_sort_segments": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP, ctypes.c_int32, _VP,
+                           ctypes.c_int32, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
 }
 NOALLOC_MAX_PARTICLES = 1 << 20
 

@@ -45,8 +45,8 @@ from .timesteppers import ABTimestepper, RK2Timestepper, Timestepper, _time_depe
 TIME_DTYPE = np.dtype([("prev", "<i4"), ("next", "<i4"), ("ft", "<f8"), ("gt", "<f8")])
 EXPERIMENT_DTYPE = np.dtype([("start", "<i8"), ("count", "<i8"), ("first_chunk", "<i8"), ("scheme", "<i4"),
                              ("nsteps", "<i4"), ("table_offset", "<i4"), ("validate", "<i4"), ("dt", "<f8"),
-                             ("alpha", "<f8")])
-HEADER_DTYPE = np.dtype([("nexp", "<i4"), ("_pad", "<i4"), ("nchunks", "<i8"), ("next_chunk", "<u8")])
+                             ("alpha", "<f8"), ("bucket_row", "<i4"), ("_pad", "<i4")])
+HEADER_DTYPE = np.dtype([("nexp", "<i4"), ("nbuckets", "<i4"), ("nchunks", "<i8"), ("next_chunk", "<u8")])
 assert TIME_DTYPE.itemsize == ctypes.sizeof(_lib.opb_time)
 assert EXPERIMENT_DTYPE.itemsize == ctypes.sizeof(_lib.opb_experiment)
 assert HEADER_DTYPE.itemsize == ctypes.sizeof(_lib.opb_batch_header)
@@ -203,19 +203,35 @@ class ReleaseBatch:
     """Advance many ``Release`` experiments together on one device.
 
     ``fieldset``: the shared fields (u, v, w, zeta time-dependent; h, dx, dy, C
-    static).  ``block``: CTA size of the persistent launch (128, 256, 512).
-    ``ctas``: CTAs of the launch (0: as many as stay resident).
+    static).  ``block``, ``warps_per_sm``: the persistent launch's CTA size
+    and resident warps per SM (register budget per thread 65536 / 32 /
+    warps_per_sm), one of ``_lib.BATCH_SHAPES``.  ``ctas``: CTAs of the launch
+    (0: as many as stay resident).  ``split_schemes``: one launch per scheme,
+    each kernel compiled for RK2 or AB3 alone (less code, fewer registers),
+    instead of one kernel for both.
     ``sort_interval``: snapshot intervals between re-sorts of a release's
     segment (0: never; a release is always sorted when it starts).
     ``graphs``: capture each interval's upload + launch as a CUDA graph (only
     when every time-dependent field streams through a ring, whose slot
-    addresses repeat).
+    addresses repeat).  ``buckets``: 0 walks one release's segment after
+    another; a power of two walks that many Morton buckets of the grid in
+    turn, advancing the particles of every release in a bucket together, so
+    that releases sharing a region share its field data in L2.
     """
 
     def __init__(self, fieldset: Fieldset, releases: list[Release], *, device=None, block: int = 256,
-                 ctas: int = 0, sort_interval: int = 4, graphs: bool = True) -> None:
-        if block not in _lib.BATCH_BLOCKS:
-            raise ValueError(f"block must be one of {_lib.BATCH_BLOCKS}")
+                 warps_per_sm: int = 16, ctas: int = 0, sort_interval: int = 4, graphs: bool = True,
+                 buckets: int = 256, split_schemes: bool = True) -> None:
+        if buckets < 0 or (buckets & (buckets - 1)) or buckets > 65536:
+            raise ValueError("buckets must be 0 or a power of two up to 65536")
+        self.buckets = int(buckets)
+        if (block, warps_per_sm) not in _lib.BATCH_SHAPES:
+            raise ValueError(f"(block, warps_per_sm) must be one of {_lib.BATCH_SHAPES}")
+        if not split_schemes and warps_per_sm != 16:
+            raise ValueError("one kernel for both schemes runs at 16 warps per SM only")
+        self.warps_per_sm = int(warps_per_sm)
+        # one launch per scheme (each kernel compiled for its scheme alone), or one for both
+        self.groups = (_lib.SCHEME_RK2, _lib.SCHEME_AB3) if split_schemes else (0,)
         self.fieldset = fieldset
         self.releases = list(releases)
         self.launcher = Launcher(fieldset)
@@ -253,6 +269,10 @@ class ReleaseBatch:
         self._sort_ws = None
         self.launches = 0
         self.sorts = 0
+        # per launched interval: (interval, experiments, particle-steps, most steps of one experiment)
+        self.stats: list[tuple[int, int, int, int]] = []
+        # objects with before() / after(), called around each interval's launch (timing)
+        self.observers: list = []
 
     # ------------------------------------------------------------------ arena
     def _init_arena(self) -> None:
@@ -286,8 +306,13 @@ class ReleaseBatch:
             entries += per * (int(math.ceil(dT / r.dt)) + 2)
         self.max_experiments = len(self.releases)
         self.max_entries = max(entries, 1)
-        self._off_exp = _align(HEADER_DTYPE.itemsize)
-        self._off_tab = self._off_exp + _align(self.max_experiments * EXPERIMENT_DTYPE.itemsize)
+        # layout: one header and one experiment list per launch group, then the shared stage-time table
+        ng = len(self.groups)
+        self._off_hdr = [g * _align(HEADER_DTYPE.itemsize) for g in range(ng)]
+        base = ng * _align(HEADER_DTYPE.itemsize)
+        exp_bytes = _align(self.max_experiments * EXPERIMENT_DTYPE.itemsize)
+        self._off_exps = [base + g * exp_bytes for g in range(ng)]
+        self._off_tab = base + ng * exp_bytes
         self._nbytes = self._off_tab + _align(self.max_entries * TIME_DTYPE.itemsize)
         # two pinned staging buffers and two device copies, used alternately
         self._host = [torch.zeros(self._nbytes, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
@@ -295,27 +320,36 @@ class ReleaseBatch:
         self._host_free: list[torch.cuda.Event | None] = [None, None]
         self._parity = 0
         self._scalars = None
+        # per release: where each Morton bucket starts in its segment (written by every segment sort)
+        nb = max(self.buckets, 1)
+        self._bounds = torch.zeros((len(self.releases), nb + 1), dtype=torch.int64, device=self.device)
+        self._items = torch.zeros((len(self.groups), len(self.releases) * nb + 1), dtype=torch.int64,
+                                  device=self.device)
 
     # --------------------------------------------------------------- planning
     def _plan(self, j: int):
         return self.planner.plan(self.releases, j)
 
-    def _write_tables(self, j: int, exps, tidx_all, dtype) -> tuple[int, int]:
-        """Fill a pinned staging buffer; return (parity, chunks)."""
+    def _write_tables(self, j: int, exps, tidx_all, dtype) -> int:
+        """Fill a pinned staging buffer (per launch group: header and experiments; the stage-time table);
+        return its parity."""
         b = self._parity
         self._parity ^= 1
         ev = self._host_free[b]
         if ev is not None:
             ev.synchronize()  # the upload that last read this staging buffer has finished
         host = self._host[b].numpy()
-        hdr = host[:HEADER_DTYPE.itemsize].view(HEADER_DTYPE)
-        ex = host[self._off_exp:self._off_exp + len(exps) * EXPERIMENT_DTYPE.itemsize].view(EXPERIMENT_DTYPE)
         chunk = _lib.BATCH_CHUNK
-        nchunks = 0
-        for q, (e, r, k, first) in enumerate(exps):
-            ex[q] = (r.start, len(r), nchunks, r.scheme, k, first, r.validate, r.dt, r.alpha)
-            nchunks += (len(r) + chunk - 1) // chunk
-        hdr[0] = (len(exps), 0, nchunks, 0)
+        for g, scheme in enumerate(self.groups):
+            mine = [x for x in exps if scheme == 0 or x[1].scheme == scheme]
+            hdr = host[self._off_hdr[g]:self._off_hdr[g] + HEADER_DTYPE.itemsize].view(HEADER_DTYPE)
+            off = self._off_exps[g]
+            ex = host[off:off + len(mine) * EXPERIMENT_DTYPE.itemsize].view(EXPERIMENT_DTYPE)
+            nchunks = 0
+            for q, (e, r, k, first) in enumerate(mine):
+                ex[q] = (r.start, len(r), nchunks, r.scheme, k, first, r.validate, r.dt, r.alpha, e, 0)
+                nchunks += (len(r) + chunk - 1) // chunk
+            hdr[0] = (len(mine), self.buckets, nchunks, 0)
         if tidx_all:
             tid = np.asarray(tidx_all, dtype=np.float64)
             It, fr = np.divmod(tid, 1.0)
@@ -327,7 +361,7 @@ class ReleaseBatch:
             tab["next"] = It + 1 - j
             tab["ft"] = ft.astype(np.float64)
             tab["gt"] = gt.astype(np.float64)
-        return b, nchunks
+        return b
 
     # --------------------------------------------------------------- stepping
     @property
@@ -354,11 +388,13 @@ class ReleaseBatch:
         for e, r, k, first in exps:
             last = self._sorted_at.get(e)
             if last is None or (self.sort_interval > 0 and j - last >= self.sort_interval):
-                due.append(r)
+                due.append((e, r))
                 self._sorted_at[e] = j
         if not due:
             return
-        due.sort(key=lambda r: r.start)
+        due.sort(key=lambda er: er[1].start)
+        rows = [e for e, _ in due]
+        due = [r for _, r in due]
         starts = (ctypes.c_int64 * len(due))(*[r.start for r in due])
         counts = (ctypes.c_int64 * len(due))(*[len(r) for r in due])
         total = sum(len(r) for r in due)
@@ -368,9 +404,14 @@ class ReleaseBatch:
             self._sort_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
         fs = self.fieldset
         dims = (ctypes.c_int64 * 3)(fs.z_size, fs.y_size, fs.x_size)
+        nb = max(self.buckets, 1)
+        out = torch.empty((len(due), nb + 1), dtype=torch.int64, device=self.device)
         _lib.call("opb_sort_segments", ctypes.byref(_abi.particles_struct(self.arena)), ctypes.byref(dims), starts,
-                  counts, len(due), self.order.data_ptr(), self._sort_ws.data_ptr(), self._sort_ws.numel(),
-                  _abi.stream(self.arena))
+                  counts, len(due), self.order.data_ptr(), nb, out.data_ptr(), self._sort_ws.data_ptr(),
+                  self._sort_ws.numel(), _abi.stream(self.arena))
+        # pinned source: a pageable one would make the copy wait for the stream to drain
+        rows_dev = torch.tensor(rows, dtype=torch.int64).pin_memory().to(self.device, non_blocking=True)
+        self._bounds.index_copy_(0, rows_dev, out)
         self.sorts += 1
 
     def _launch(self, rf, b: int) -> None:
@@ -378,9 +419,11 @@ class ReleaseBatch:
         host = self._host[b]
         base = dev.data_ptr()
         dev.copy_(host, non_blocking=True)
-        _lib.call("opb_batched_steps", ctypes.byref(_abi.particles_struct(self.arena)), base, base + self._off_exp,
-                  ctypes.byref(self._scalars_struct()), ctypes.byref(rf), base + self._off_tab, self.block,
-                  self.ctas, _abi.stream(self.arena))
+        for g, scheme in enumerate(self.groups):
+            _lib.call("opb_batched_steps", ctypes.byref(_abi.particles_struct(self.arena)), base + self._off_hdr[g],
+                      base + self._off_exps[g], ctypes.byref(self._scalars_struct()), ctypes.byref(rf),
+                      base + self._off_tab, self._bounds.data_ptr(), self._items[g].data_ptr(), scheme, self.block,
+                      self.warps_per_sm, self.ctas, _abi.stream(self.arena))
 
     def _run_launch(self, rf, b: int) -> None:
         if not self.graphs:
@@ -422,9 +465,14 @@ class ReleaseBatch:
         if exps:
             window = list(range(j, min(j + 3, self.num_snapshots)))
             rf, dtype = window_fields(self.launcher, window, self._td)
-            b, nchunks = self._write_tables(j, exps, tidx_all, dtype)
+            b = self._write_tables(j, exps, tidx_all, dtype)
             self._sort_due(j, exps)
+            for obs in self.observers:
+                obs.before()
             self._run_launch(rf, b)
+            for obs in self.observers:
+                obs.after()
+            self.stats.append((j, len(exps), sum(len(r) * k for _, r, k, _ in exps), max(k for _, _, k, _ in exps)))
             ev = torch.cuda.Event()
             ev.record(torch.cuda.current_stream(self.device))
             self._host_free[b] = ev

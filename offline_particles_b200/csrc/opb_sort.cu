@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -157,6 +159,92 @@ __global__ void __launch_bounds__(kBlock) k_segment_put(const __grid_constant__ 
     if (a.d_ids) a.d_ids[i] = a.s_ids[q];
 }
 
+// bucket_bounds[s * (nb + 1) + b]: storage index of segment s's first particle
+// whose cell key is >= b << shift (b = nb: the first inactive particle, or the
+// segment's end).  Keys are sorted within the segment, so this is a lower bound.
+__global__ void __launch_bounds__(kBlock) k_bucket_bounds(const uint64_t *keys, const int64_t *seg_start,
+                                                          const int64_t *seg_cstart, long long m, int nseg, int nb,
+                                                          int shift, int64_t *bounds) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nseg * (nb + 1)) return;
+    const int s = (int)(t / (nb + 1));
+    const int b = (int)(t % (nb + 1));
+    const uint64_t threshold = b == nb ? 0x40000000ull : ((uint64_t)b << shift);
+    long long lo = seg_cstart[s];
+    long long hi = s + 1 < nseg ? seg_cstart[s + 1] : m;
+    const long long first = lo;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if ((keys[mid] & 0xffffffffull) < threshold) lo = mid + 1;
+        else hi = mid;
+    }
+    bounds[t] = seg_start[s] + (lo - first);
+}
+
+// right shift that leaves at most nb distinct buckets of the keys of this grid
+int bucket_shift(const KeyArgs &k, int nb) {
+    auto spread = [](uint32_t v) {
+        uint32_t out = 0;
+        for (int i = 0; i < 10; ++i) out |= ((v >> i) & 1u) << (3 * i);
+        return out;
+    };
+    const uint32_t zmax = (uint32_t)((k.nz - 1) >> k.sz), ymax = (uint32_t)((k.ny - 1) >> k.sy);
+    const uint32_t xmax = (uint32_t)((k.nx - 1) >> k.sx);
+    // every key is below 2^bits, with bits the position of the top set bit of the largest key + 1
+    const uint32_t top = (spread(zmax) << 2) | (spread(ymax) << 1) | spread(xmax);
+    int bits = 0;
+    while (bits < 32 && (top >> bits) != 0) ++bits;
+    int lg = 0;
+    while ((1 << lg) < nb) ++lg;
+    return bits > lg ? bits - lg : 0;
+}
+
+// Pinned staging for small host tables copied to the device inside an
+// asynchronous call: a copy from pageable memory would first wait for the
+// stream to drain (CUDA's rule for pageable host-to-device copies), stalling
+// the caller's host thread behind all queued work.  A ring of pinned slots per
+// device; a slot is reused once the copy that last read it has completed.
+struct PinnedRing {
+    static constexpr int kSlots = 16;
+    static constexpr size_t kSlotBytes = 1 << 20;
+    char *host = nullptr;
+    cudaEvent_t done[kSlots] = {};
+    bool used[kSlots] = {};
+    int next = 0;
+};
+
+// copy `bytes` from host `src` to device `dst` on stream st through pinned memory
+cudaError_t stage_to_device(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+    static std::mutex mu;
+    static std::map<int, PinnedRing> rings;
+    if (bytes > PinnedRing::kSlotBytes) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    PinnedRing &R = rings[dev];
+    if (!R.host) {
+        e = cudaHostAlloc((void **)&R.host, PinnedRing::kSlots * PinnedRing::kSlotBytes, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            R.host = nullptr;
+            return e;
+        }
+        for (int i = 0; i < PinnedRing::kSlots; ++i) {
+            e = cudaEventCreateWithFlags(&R.done[i], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    const int k = R.next;
+    R.next = (R.next + 1) % PinnedRing::kSlots;
+    if (R.used[k] && (e = cudaEventSynchronize(R.done[k])) != cudaSuccess) return e;
+    char *slot = R.host + (size_t)k * PinnedRing::kSlotBytes;
+    std::memcpy(slot, src, bytes);
+    if ((e = cudaMemcpyAsync(dst, slot, bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(R.done[k], st)) != cudaSuccess) return e;
+    R.used[k] = true;
+    return cudaSuccess;
+}
+
 size_t cub_temp_bytes64(long long n, int end_bit) {
     size_t bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
@@ -298,14 +386,16 @@ size_t opb_sort_segments_workspace_bytes(int64_t total, int32_t nseg) {
 }
 
 int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int64_t *seg_start,
-                      const int64_t *seg_count, int32_t nseg, int64_t *ids, void *workspace, size_t workspace_bytes,
-                      void *stream) {
+                      const int64_t *seg_count, int32_t nseg, int64_t *ids, int32_t nbuckets, int64_t *bucket_bounds,
+                      void *workspace, size_t workspace_bytes, void *stream) {
     const char *what = "opb_sort_segments";
     if (!p) return fail(OPB_EINVAL, "%s: particles is NULL", what);
     if (p->n < 0 || p->n > 0x7fffffffLL) return fail(OPB_EINVAL, "%s: particle count out of range", what);
     if (nseg < 0) return fail(OPB_EINVAL, "%s: negative segment count", what);
     if (nseg == 0 || p->n == 0) return OPB_OK;
     if (!seg_start || !seg_count || !shape) return fail(OPB_EINVAL, "%s: NULL argument", what);
+    if (bucket_bounds && (nbuckets < 1 || nbuckets > 65536 || (nbuckets & (nbuckets - 1))))
+        return fail(OPB_EINVAL, "%s: nbuckets must be a power of two in [1, 65536]", what);
     if (!p->status || !p->zidx || !p->yidx || !p->xidx) return fail(OPB_EINVAL, "%s: NULL particle array", what);
     if (shape[0] < 1 || shape[1] < 1 || shape[2] < 1 || shape[0] > (1 << 30) || shape[1] > (1 << 30) ||
         shape[2] > (1 << 30))
@@ -334,7 +424,7 @@ int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int6
         seg[nseg + s] = c;
         c += seg_count[s];
     }
-    cudaError_t e = cudaMemcpyAsync(ws + L.seg, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice, st);
+    cudaError_t e = stage_to_device(ws + L.seg, seg.data(), seg.size() * 8, st);
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     SegArgs a;
     a.k.status = p->status;
@@ -393,6 +483,11 @@ int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int6
     }
     k_segment_take<<<grid, kBlock, 0, st>>>(take, perm, slot);
     k_segment_put<<<grid, kBlock, 0, st>>>(put, slot);
+    if (bucket_bounds) {
+        const long long nt = (long long)nseg * (nbuckets + 1);
+        k_bucket_bounds<<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+            keys_out, a.seg_start, a.seg_cstart, m, nseg, nbuckets, bucket_shift(a.k, nbuckets), bucket_bounds);
+    }
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     opb::clear_error();

@@ -1,0 +1,188 @@
+// Per-particle stage functions shared by the ROMS kernels (opb_roms.cu) and
+// the batched-release kernel (opb_batched.cu): the particle state, the fields
+// of one stage, the level tables, and one function per reference kernel body.
+// Every translation unit that includes this is compiled with -fmad=false
+// (bit-identical float64 arithmetic; see opb_device.cuh).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "opb200.h"
+#include "opb_device.cuh"
+
+namespace opb {
+namespace {
+
+constexpr int kBlock = 256;
+
+// ------------------------------------------------------------ per particle
+struct PState {
+    double zidx, yidx, xidx, z;
+    double k0x, k0y, k0z;  // AB3 k(n)
+    double k1x, k1y, k1z;  // RK2 k1 / AB3 k(n-1)
+    double k2x, k2y, k2z;  // RK2 k2 / AB3 k(n-2)
+    // h and zeta at (yidx, xidx) for the time selection `at`, left by the
+    // previous step's last stage; the next step's first stage needs exactly
+    // these values (same position, same time index) and reuses them
+    double h_at, zeta_at;
+    opb_time at;
+    uint8_t status;
+};
+
+__device__ __forceinline__ bool same_time(const opb_time &a, const opb_time &b) {
+    return a.prev == b.prev && a.next == b.next && a.ft == b.ft && a.gt == b.gt;
+}
+
+__device__ __forceinline__ void raise_zero_division(const DParticles &p) {
+    if (p.err) atomicOr(p.err, (uint32_t)OPB_ERRF_ZERO_DIVISION);
+}
+
+// The fields of one stage.  FIXED: the ROMS layout (u, v, w, zeta
+// time-dependent; h, dx, dy, C static), known at compile time; otherwise each
+// field's kind is read at run time.
+template <typename T, typename I, bool FIXED = false>
+struct Bound {
+    static constexpr int KT = FIXED ? KIND_TD : KIND_ANY;
+    static constexpr int KS = FIXED ? KIND_STATIC : KIND_ANY;
+    View<T, I, KT> u, v, w, zeta;
+    View<T, I, KS> dx, dy, h, C;
+};
+
+template <typename T, typename I, bool FIXED = false>
+__device__ __forceinline__ Bound<T, I, FIXED> bind_all(const DRoms &r, const opb_time &t) {
+    using B = Bound<T, I, FIXED>;
+    B b;
+    b.u = bind<T, I, B::KT>(r.u, t);
+    b.v = bind<T, I, B::KT>(r.v, t);
+    b.w = bind<T, I, B::KT>(r.w, t);
+    b.zeta = bind<T, I, B::KT>(r.zeta, t);
+    b.dx = bind<T, I, B::KS>(r.dx, t);
+    b.dy = bind<T, I, B::KS>(r.dy, t);
+    b.h = bind<T, I, B::KS>(r.h, t);
+    b.C = bind<T, I, B::KS>(r.C, t);  // static float64 (kernels/_core.pyx:5-9)
+    return b;
+}
+
+// Every kernel starts here, before any thread can return: the block's shared
+// tables of the sigma levels (used by compute_zidx).
+#define OPB_LEVELS(r, sc)                                                                            \
+    __shared__ double s_sigma[kMaxLevels];                                                           \
+    __shared__ double s_C[kMaxLevels];                                                               \
+    const Levels L = load_levels((const double *)(r).C.data[0], (r).C.n0, (r).C.o0, (sc).NZ, s_sigma, s_C); \
+    __syncthreads()
+
+// rk2_w_advection.pyx:97-153 (stage 1 for one particle).  Returns false on a
+// zero grid spacing (the reference raises ZeroDivisionError).
+template <typename B>
+__device__ __forceinline__ bool rk2_stage1(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false) {
+    const double h = reuse_hz ? s.h_at : bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
+    const double zeta = reuse_hz ? s.zeta_at : bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    const double Cv = linear(f.C, s.zidx + f.C.o0);
+    s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
+    const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
+    const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
+    const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
+    const double dy = bilinear(f.dy, s.yidx + f.dy.o0, s.xidx + f.dy.o1);
+    if (dx == 0.0 || dy == 0.0) return false;
+    s.k1x = u / dx;
+    s.k1y = v / dy;
+    s.k1z = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    return true;
+}
+
+// rk2_w_advection.pyx:225-275 (stage 2 for one particle)
+template <typename B>
+__device__ __forceinline__ bool rk2_stage2(PState &s, const B &f, const Levels &L, const DScalars &sc) {
+    const double adt = sc.alpha * sc.dt;
+    const double z_int = s.z + adt * s.k1z;
+    const double y_int = s.yidx + adt * s.k1y;
+    const double x_int = s.xidx + adt * s.k1x;
+    const double h = bilinear(f.h, y_int + f.h.o0, x_int + f.h.o1);
+    const double zeta = bilinear(f.zeta, y_int + f.zeta.o0, x_int + f.zeta.o1);
+    const double z_idx = compute_zidx_hint(z_int, h, zeta, sc.hc, L, s.zidx);
+    const double u = trilinear(f.u, z_idx + f.u.o0, y_int + f.u.o1, x_int + f.u.o2);
+    const double v = trilinear(f.v, z_idx + f.v.o0, y_int + f.v.o1, x_int + f.v.o2);
+    const double dx = bilinear(f.dx, y_int + f.dx.o0, x_int + f.dx.o1);
+    const double dy = bilinear(f.dy, y_int + f.dy.o0, x_int + f.dy.o1);
+    if (dx == 0.0 || dy == 0.0) return false;
+    s.k2x = u / dx;
+    s.k2y = v / dy;
+    s.k2z = trilinear(f.w, z_idx + f.w.o0, y_int + f.w.o1, x_int + f.w.o2);
+    return true;
+}
+
+// rk2_w_advection.pyx:316-354 (update for one particle); b1 = 1/(2 alpha)
+// weights k1, the reference's own convention (rk2_w_advection.pyx:317-318).
+template <typename B>
+__device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &L, const DScalars &sc) {
+    const double b1 = 1.0 / (2.0 * sc.alpha);
+    const double b2 = 1.0 - b1;
+    const double b1dt = b1 * sc.dt;
+    const double b2dt = b2 * sc.dt;
+    s.z = s.z + b1dt * s.k1z + b2dt * s.k2z;
+    s.yidx = s.yidx + b1dt * s.k1y + b2dt * s.k2y;
+    s.xidx = s.xidx + b1dt * s.k1x + b2dt * s.k2x;
+    const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
+    const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
+    s.h_at = h;
+    s.zeta_at = zeta;
+}
+
+// ab3_w_advection.pyx:84-178 (AB3 step for one particle)
+template <typename B>
+__device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false) {
+    const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
+    const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
+    if (dx == 0.0) return false;
+    s.k0x = u / dx;
+    const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
+    const double dy = bilinear(f.dy, s.yidx + f.dy.o0, s.xidx + f.dy.o1);
+    if (dy == 0.0) return false;
+    s.k0y = v / dy;
+    s.k0z = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    if (s.status == ST_MULTISTEP_1) {  // ab3_w_advection.pyx:122-131
+        s.k1x = s.k0x;
+        s.k1y = s.k0y;
+        s.k1z = s.k0z;
+        s.k2x = s.k0x;
+        s.k2y = s.k0y;
+        s.k2z = s.k0z;
+        s.status = ST_MULTISTEP_2;
+    } else if (s.status == ST_MULTISTEP_2) {  // ab3_w_advection.pyx:132-138
+        s.k2x = -s.k0x + 2.0 * s.k1x;
+        s.k2y = -s.k0y + 2.0 * s.k1y;
+        s.k2z = -s.k0z + 2.0 * s.k1z;
+        s.status = ST_NORMAL;
+    }
+    const double h = reuse_hz ? s.h_at : bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
+    const double zeta = reuse_hz ? s.zeta_at : bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    const double Cv = linear(f.C, s.zidx + f.C.o0);
+    s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
+    const double dt = sc.dt;
+    s.z = s.z + dt * (23.0 * s.k0z - 16.0 * s.k1z + 5.0 * s.k2z) / 12.0;
+    s.yidx = s.yidx + dt * (23.0 * s.k0y - 16.0 * s.k1y + 5.0 * s.k2y) / 12.0;
+    s.xidx = s.xidx + dt * (23.0 * s.k0x - 16.0 * s.k1x + 5.0 * s.k2x) / 12.0;
+    s.k2z = s.k1z;
+    s.k2x = s.k1x;
+    s.k2y = s.k1y;
+    s.k1z = s.k0z;
+    s.k1x = s.k0x;
+    s.k1y = s.k0y;
+    return true;
+}
+
+// ab3_w_advection.pyx:214-229 (post step for one particle)
+template <typename B>
+__device__ __forceinline__ void ab3_post(PState &s, const B &f, const Levels &L, const DScalars &sc) {
+    const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
+    const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
+    s.h_at = h;
+    s.zeta_at = zeta;
+}
+
+__device__ __forceinline__ long long gtid() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
+
+}  // namespace
+}  // namespace opb

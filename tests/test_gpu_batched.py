@@ -103,16 +103,18 @@ def _check(b, alone):
             assert same_bits(got[k], alone[q][k]), f"release {q} {k}: " + mismatch_report(got[k], alone[q][k])
 
 
-@pytest.mark.parametrize("block", [128, 256, 512])
-def test_batch_equals_each_release_alone(grid, alone, block):
-    b = _batch(grid, block=block)
+@pytest.mark.parametrize("block,warps,split", [(128, 16, True), (256, 16, True), (256, 24, True), (256, 32, True),
+                                               (256, 16, False), (128, 16, False)])
+def test_batch_equals_each_release_alone(grid, alone, block, warps, split):
+    b = _batch(grid, block=block, warps_per_sm=warps, split_schemes=split)
     assert b.graphs  # ring-streamed fields: intervals replay captured graphs
     _check(b, alone)
 
 
-@pytest.mark.parametrize("sort_interval,graphs,ctas", [(0, True, 0), (1, False, 0), (3, True, 7)])
-def test_batch_independent_of_sorting_graphs_and_grid(grid, alone, sort_interval, graphs, ctas):
-    b = _batch(grid, sort_interval=sort_interval, graphs=graphs, ctas=ctas)
+@pytest.mark.parametrize("sort_interval,graphs,ctas,buckets", [(0, True, 0, 256), (1, False, 0, 0),
+                                                                (3, True, 7, 1), (2, True, 0, 4096)])
+def test_batch_independent_of_sorting_graphs_grid_and_order(grid, alone, sort_interval, graphs, ctas, buckets):
+    b = _batch(grid, sort_interval=sort_interval, graphs=graphs, ctas=ctas, buckets=buckets)
     _check(b, alone)
     if sort_interval == 1:
         assert b.sorts >= b.launches
@@ -161,9 +163,11 @@ def test_segment_sort_keeps_segments_and_permutes_ids():
     lib = _lib.load()
     ws = torch.empty(int(lib.opb_sort_segments_workspace_bytes(sum(counts), 3)), dtype=torch.uint8, device="cuda")
     dims = (ctypes.c_int64 * 3)(12, 80, 96)
+    nb = 16
+    bounds = torch.full((3, nb + 1), -1, dtype=torch.int64, device="cuda")
     _lib.call("opb_sort_segments", ctypes.byref(_abi.particles_struct(P)), ctypes.byref(dims),
-              (ctypes.c_int64 * 3)(*starts), (ctypes.c_int64 * 3)(*counts), 3, ids.data_ptr(), ws.data_ptr(),
-              ws.numel(), None)
+              (ctypes.c_int64 * 3)(*starts), (ctypes.c_int64 * 3)(*counts), 3, ids.data_ptr(), nb,
+              bounds.data_ptr(), ws.data_ptr(), ws.numel(), None)
     torch.cuda.synchronize()
     idn = ids.cpu().numpy()
     zn = P["z"].cpu().numpy()
@@ -178,7 +182,14 @@ def test_segment_sort_keeps_segments_and_permutes_ids():
         act = (stn & 0x80) == 0
         assert not np.any(act[np.argmax(~act):]) if (~act).any() else True
     assert np.array_equal(idn[~inside], np.flatnonzero(~inside))  # outside the segments: untouched
+    # bucket bounds: ascending within each segment, first = segment start, last = the first inactive particle
+    bn = bounds.cpu().numpy()
+    stn = P["status"].cpu().numpy()
+    for q, (s, c) in enumerate(zip(starts, counts)):
+        row = bn[q]
+        assert row[0] == s and np.all(np.diff(row) >= 0)
+        assert row[-1] == s + int(((stn[s:s + c] & 0x80) == 0).sum())
     with pytest.raises(ValueError, match="out of order"):
         _lib.call("opb_sort_segments", ctypes.byref(_abi.particles_struct(P)), ctypes.byref(dims),
-                  (ctypes.c_int64 * 2)(5000, 100), (ctypes.c_int64 * 2)(10, 10), 2, None, ws.data_ptr(),
+                  (ctypes.c_int64 * 2)(5000, 100), (ctypes.c_int64 * 2)(10, 10), 2, None, 0, None, ws.data_ptr(),
                   ws.numel(), None)
