@@ -8,10 +8,11 @@ persistent launch (``opb_batched_steps``):
 
 * a per-experiment offset table (segment start and count, scheme, dt, alpha,
   step count, offset into a shared stage-time table) is written to pinned host
-  memory and copied to the device with the launch;
-* the launch, its table upload and its work-counter reset are captured once
-  as a CUDA graph per ring phase and replayed every interval (the snapshots of
-  an interval sit in fixed ring slots, so only device contents change);
+  memory and copied to the device before the launch;
+* the launch (per scheme: work-item planning, work-counter reset, persistent
+  kernel) is captured once as a CUDA graph per ring phase and replayed every
+  interval (the snapshots of an interval sit in fixed ring slots and the
+  tables in fixed device buffers, so only device contents change);
 * a release's segment is Morton-sorted when it starts and every
   ``sort_interval`` intervals after that, in place (``opb_sort_segments``).
 
@@ -115,7 +116,7 @@ class IntervalPlanner:
         exps = []
         tidx_all: list[float] = []
         for e, r in enumerate(releases):
-            if r.finished or r.time >= Tn:
+            if r is None or r.finished or r.time >= Tn:
                 continue
             if r.time < T[j]:
                 raise RuntimeError(f"release {e} is at time {r.time}, before interval {j}")
@@ -162,7 +163,9 @@ class Release:
     name: str | None = None
     # filled in by the batch
     start: int = field(default=-1, init=False)
+    slot: int = field(default=-1, init=False)
     done: int = field(default=0, init=False)
+    reported: bool = field(default=False, init=False)  # returned by ReleaseBatch.tick as finished
     error: BaseException | None = field(default=None, init=False)
 
     def __post_init__(self) -> None:
@@ -199,8 +202,72 @@ class Release:
         return len(self) * self.nsteps
 
 
+class SegmentAllocator:
+    """First-fit allocation of contiguous particle ranges in an arena of ``capacity`` slots."""
+
+    def __init__(self, capacity: int) -> None:
+        self.capacity = int(capacity)
+        self.free_list: list[tuple[int, int]] = [(0, self.capacity)] if capacity > 0 else []  # (start, length)
+
+    def alloc(self, n: int) -> int | None:
+        if n <= 0:
+            return None
+        for q, (s, ln) in enumerate(self.free_list):
+            if ln >= n:
+                if ln == n:
+                    self.free_list.pop(q)
+                else:
+                    self.free_list[q] = (s + n, ln - n)
+                return s
+        return None
+
+    def free(self, start: int, n: int) -> None:
+        if n <= 0:
+            return
+        bisect.insort(self.free_list, (start, n))
+        merged: list[tuple[int, int]] = []
+        for s, ln in self.free_list:
+            if merged and merged[-1][0] + merged[-1][1] == s:
+                merged[-1] = (merged[-1][0], merged[-1][1] + ln)
+            else:
+                merged.append((s, ln))
+        self.free_list = merged
+
+    @property
+    def free_total(self) -> int:
+        return sum(ln for _, ln in self.free_list)
+
+    @property
+    def largest_free(self) -> int:
+        return max((ln for _, ln in self.free_list), default=0)
+
+
+class Collected:
+    """A release's particle fields on their way to pinned host memory (``ReleaseBatch.collect``)."""
+
+    def __init__(self, release: Release, host: dict[str, torch.Tensor], event: torch.cuda.Event) -> None:
+        self.release = release
+        self._host = host
+        self._event = event
+
+    def ready(self) -> bool:
+        return self._event.query()
+
+    def result(self) -> dict[str, np.ndarray]:
+        self._event.synchronize()
+        return {k: v.numpy() for k, v in self._host.items()}
+
+
 class ReleaseBatch:
     """Advance many ``Release`` experiments together on one device.
+
+    Static use: ``ReleaseBatch(fieldset, releases).run()``.  Dynamic use (a
+    request server): ``ReleaseBatch(fieldset, time_array=..., capacity=N,
+    max_releases=R)``, then ``add`` releases at interval boundaries, ``tick``
+    one snapshot interval at a time, and ``collect`` / ``retire`` releases that
+    have finished.  Every release lives in its own contiguous segment of a
+    particle arena of ``capacity`` slots (first-fit); its state stays on the
+    device from ``add`` to ``retire``.
 
     ``fieldset``: the shared fields (u, v, w, zeta time-dependent; h, dx, dy, C
     static).  ``block``, ``warps_per_sm``: the persistent launch's CTA size
@@ -211,15 +278,16 @@ class ReleaseBatch:
     instead of one kernel for both.
     ``sort_interval``: snapshot intervals between re-sorts of a release's
     segment (0: never; a release is always sorted when it starts).
-    ``graphs``: capture each interval's upload + launch as a CUDA graph (only
-    when every time-dependent field streams through a ring, whose slot
-    addresses repeat).  ``buckets``: 0 walks one release's segment after
-    another; a power of two walks that many Morton buckets of the grid in
-    turn, advancing the particles of every release in a bucket together, so
-    that releases sharing a region share its field data in L2.
+    ``graphs``: capture each interval's launches as a CUDA graph (only when
+    every time-dependent field streams through a ring, whose slot addresses
+    repeat).  ``buckets``: 0 walks one release's segment after another; a
+    power of two walks that many Morton buckets of the grid in turn, advancing
+    the particles of every release in a bucket together, so that releases
+    sharing a region share its field data in L2.
     """
 
-    def __init__(self, fieldset: Fieldset, releases: list[Release], *, device=None, block: int = 256,
+    def __init__(self, fieldset: Fieldset, releases: list[Release] = (), *, time_array=None,
+                 capacity: int | None = None, max_releases: int | None = None, device=None, block: int = 256,
                  warps_per_sm: int = 16, ctas: int = 0, sort_interval: int = 4, graphs: bool = True,
                  buckets: int = 256, split_schemes: bool = True) -> None:
         if buckets < 0 or (buckets & (buckets - 1)) or buckets > 65536:
@@ -233,7 +301,7 @@ class ReleaseBatch:
         # one launch per scheme (each kernel compiled for its scheme alone), or one for both
         self.groups = (_lib.SCHEME_RK2, _lib.SCHEME_AB3) if split_schemes else (0,)
         self.fieldset = fieldset
-        self.releases = list(releases)
+        releases = list(releases)
         self.launcher = Launcher(fieldset)
         self.block = int(block)
         self.ctas = int(ctas)
@@ -245,72 +313,132 @@ class ReleaseBatch:
         if len(nts) != 1:
             raise ValueError("time-dependent fields must have the same number of snapshots")
         self.num_snapshots = nts.pop()
-        times = None
-        for r in self.releases:
-            ta = np.asarray(r.timestepper.time_array, dtype=np.float64)
-            if times is None:
-                times = ta
-            elif ta.shape != times.shape or not np.array_equal(ta, times):
-                raise ValueError("every release must use the same time array")
-        if times is None:
-            raise ValueError("no releases")
-        if times.shape[0] > self.num_snapshots:
+        if time_array is None:
+            if not releases:
+                raise ValueError("give releases or a time_array")
+            time_array = releases[0].timestepper.time_array
+        self.time_array = np.asarray(time_array, dtype=np.float64)
+        if self.time_array.shape[0] > self.num_snapshots:
             raise ValueError("the time array has more entries than the fields have snapshots")
-        self.time_array = times
-        self.planner = IntervalPlanner(times, self.num_snapshots)
+        self.planner = IntervalPlanner(self.time_array, self.num_snapshots)
         self._T = self.planner.T
         self.graphs = bool(graphs) and all(f.streamed for f in self._td.values())
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.capacity = int(capacity) if capacity is not None else sum(len(r) for r in releases)
+        self.max_releases = int(max_releases) if max_releases is not None else max(len(releases), 1)
+        self.slots: list[Release | None] = [None] * self.max_releases
+        self.allocator = SegmentAllocator(self.capacity)
         self.interval = None  # index j of the next snapshot interval to run
-        self._init_arena()
-        self._init_tables()
+        self.arena = Particles(self.capacity, device=self.device, **ARENA_FIELDS)
+        # original arena slot of each storage slot: segments keep their ranges, so a particle's index
+        # within its release is order - start
+        self.order = torch.arange(self.capacity, dtype=torch.int64, device=self.device)
+        min_dt = min((r.dt for r in releases), default=60.0)
+        self._init_tables(min_dt)
         self._graphs: dict = {}
         self._sorted_at: dict[int, int] = {}
         self._sort_ws = None
         self.launches = 0
         self.sorts = 0
+        self.retired_particle_steps = 0
         # per launched interval: (interval, experiments, particle-steps, most steps of one experiment)
         self.stats: list[tuple[int, int, int, int]] = []
         # objects with before() / after(), called around each interval's launch (timing)
         self.observers: list = []
+        for r in releases:
+            if not self.add(r):
+                raise ValueError("the releases do not fit the arena")
+
+    @property
+    def releases(self) -> list[Release]:
+        """Releases currently in the batch (slot order)."""
+        return [r for r in self.slots if r is not None]
 
     # ------------------------------------------------------------------ arena
-    def _init_arena(self) -> None:
-        n = 0
-        for r in self.releases:
-            r.start = n
-            n += len(r)
-        self.arena = Particles(n, device=self.device, **ARENA_FIELDS)
-        A = self.arena.arrays
-        for r in self.releases:
-            sl = slice(r.start, r.start + len(r))
-            A["zidx"][sl].copy_(torch.from_numpy(r.zidx))
-            A["yidx"][sl].copy_(torch.from_numpy(r.yidx))
-            A["xidx"][sl].copy_(torch.from_numpy(r.xidx))
-            st = r.status
-            if isinstance(st, (int, np.integer)):
-                A["status"][sl].fill_(int(st))
-            else:
-                A["status"][sl].copy_(torch.from_numpy(np.ascontiguousarray(st, dtype=np.uint8)))
-        # original arena slot of each storage slot: segments keep their ranges, so the slot within a
-        # release is order - start
-        self.order = torch.arange(n, dtype=torch.int64, device=self.device)
-        self.n = n
+    @staticmethod
+    def bytes_per_particle() -> int:
+        """Arena bytes per particle slot: status, positions, z, the RK2 stage / AB3 three-step velocity
+        history (float64 each), and the original-order index."""
+        return 1 + 8 * len(_lib.PARTICLE_POINTERS) + 8
 
-    def _init_tables(self) -> None:
-        # capacity: at most ceil(interval / dt) + 1 steps per release per interval
+    def add(self, r: Release) -> bool:
+        """Place a release in a free slot and segment and upload its initial state; False if it does not fit."""
+        if r.slot >= 0:
+            raise ValueError("the release is already in a batch")
+        ta = np.asarray(r.timestepper.time_array, dtype=np.float64)
+        if ta.shape != self.time_array.shape or not np.array_equal(ta, self.time_array):
+            raise ValueError("every release must use the batch's time array")
+        if self.interval is not None and r.time < self._T[self.interval]:
+            raise ValueError(f"release time {r.time} is before the batch's current interval")
+        try:
+            slot = self.slots.index(None)
+        except ValueError:
+            return False
+        n = len(r)
+        start = self.allocator.alloc(n)
+        if start is None:
+            return False
+        r.start, r.slot = start, slot
+        self.slots[slot] = r
+        self._sorted_at.pop(slot, None)
+        A = self.arena.arrays
+        sl = slice(start, start + n)
+        # pinned sources: a pageable one would make each copy wait for the stream to drain
+        for name, arr in (("zidx", r.zidx), ("yidx", r.yidx), ("xidx", r.xidx)):
+            A[name][sl].copy_(torch.from_numpy(arr).pin_memory(), non_blocking=True)
+        for name in _lib.PARTICLE_POINTERS[3:]:
+            A[name][sl].zero_()
+        st = r.status
+        if isinstance(st, (int, np.integer)):
+            A["status"][sl].fill_(int(st))
+        else:
+            A["status"][sl].copy_(torch.from_numpy(np.ascontiguousarray(st, dtype=np.uint8)).pin_memory(),
+                                  non_blocking=True)
+        self.order[sl].copy_(torch.arange(start, start + n, dtype=torch.int64, device=self.device))
+        return True
+
+    def collect(self, r: Release, names=("zidx", "yidx", "xidx", "status")) -> Collected:
+        """Start copying a release's fields, in its original particle order, to pinned host memory."""
+        if r.slot < 0 or self.slots[r.slot] is not r:
+            raise ValueError("the release is not in this batch")
+        sl = slice(r.start, r.start + len(r))
+        pos = self.order[sl] - r.start
+        host = {}
+        for name in names:
+            key = name if name in self.arena else "_" + name
+            t = self.arena.arrays[key][sl]
+            o = torch.empty_like(t)
+            o.index_copy_(0, pos, t)
+            h = torch.empty(o.shape, dtype=o.dtype, pin_memory=True)
+            h.copy_(o, non_blocking=True)
+            host[name] = h
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.device))
+        return Collected(r, host, ev)
+
+    def retire(self, r: Release) -> None:
+        """Free a release's slot and segment.  Later uploads into the segment are queued on the same
+        stream, so they stay ordered after the work that reads it."""
+        if r.slot < 0 or self.slots[r.slot] is not r:
+            raise ValueError("the release is not in this batch")
+        self.retired_particle_steps += len(r) * r.done
+        self.allocator.free(r.start, len(r))
+        self.slots[r.slot] = None
+        self._sorted_at.pop(r.slot, None)
+        r.slot = -1
+
+    def _init_tables(self, min_dt: float) -> None:
+        # capacity: at most ceil(interval / dt) + 2 steps per release per interval, 3 entries per RK2 step
         dT = float(np.min(np.diff(self.time_array))) if len(self.time_array) > 1 else 1.0
-        entries = 0
-        for r in self.releases:
-            per = (3 if r.scheme == _lib.SCHEME_RK2 else 2)
-            entries += per * (int(math.ceil(dT / r.dt)) + 2)
-        self.max_experiments = len(self.releases)
-        self.max_entries = max(entries, 1)
-        # layout: one header and one experiment list per launch group, then the shared stage-time table
+        self.max_entries = 3 * (int(math.ceil(dT / min_dt)) + 2) * self.max_releases
+        self._layout()
+
+    def _layout(self) -> None:
+        # one header and one experiment list per launch group, then the shared stage-time table
         ng = len(self.groups)
         self._off_hdr = [g * _align(HEADER_DTYPE.itemsize) for g in range(ng)]
         base = ng * _align(HEADER_DTYPE.itemsize)
-        exp_bytes = _align(self.max_experiments * EXPERIMENT_DTYPE.itemsize)
+        exp_bytes = _align(self.max_releases * EXPERIMENT_DTYPE.itemsize)
         self._off_exps = [base + g * exp_bytes for g in range(ng)]
         self._off_tab = base + ng * exp_bytes
         self._nbytes = self._off_tab + _align(self.max_entries * TIME_DTYPE.itemsize)
@@ -320,19 +448,31 @@ class ReleaseBatch:
         self._host_free: list[torch.cuda.Event | None] = [None, None]
         self._parity = 0
         self._scalars = None
-        # per release: where each Morton bucket starts in its segment (written by every segment sort)
+        # per slot: where each Morton bucket starts in its segment (written by every segment sort)
         nb = max(self.buckets, 1)
-        self._bounds = torch.zeros((len(self.releases), nb + 1), dtype=torch.int64, device=self.device)
-        self._items = torch.zeros((len(self.groups), len(self.releases) * nb + 1), dtype=torch.int64,
+        self._bounds = torch.zeros((self.max_releases, nb + 1), dtype=torch.int64, device=self.device)
+        self._items = torch.zeros((len(self.groups), self.max_releases * nb + 1), dtype=torch.int64,
                                   device=self.device)
+        self._graphs = {}
+
+    def _grow_table(self, entries: int) -> None:
+        """Stage-time table too small for this interval (a shorter dt than planned for): double it."""
+        torch.cuda.current_stream(self.device).synchronize()
+        while self.max_entries < entries:
+            self.max_entries *= 2
+        bounds = self._bounds
+        self._layout()
+        self._bounds.copy_(bounds)
 
     # --------------------------------------------------------------- planning
     def _plan(self, j: int):
-        return self.planner.plan(self.releases, j)
+        return self.planner.plan(self.slots, j)
 
     def _write_tables(self, j: int, exps, tidx_all, dtype) -> int:
         """Fill a pinned staging buffer (per launch group: header and experiments; the stage-time table);
         return its parity."""
+        if len(tidx_all) > self.max_entries:
+            self._grow_table(len(tidx_all))
         b = self._parity
         self._parity ^= 1
         ev = self._host_free[b]
@@ -369,7 +509,8 @@ class ReleaseBatch:
         return all(r.finished for r in self.releases)
 
     def _first_interval(self) -> int:
-        t0 = min(r.time for r in self.releases if not r.finished)
+        times = [r.time for r in self.releases if not r.finished]
+        t0 = min(times) if times else self._T[0]
         return max(0, bisect.bisect_right(self._T, t0) - 1)
 
     def _scalars_struct(self):
@@ -414,11 +555,12 @@ class ReleaseBatch:
         self._bounds.index_copy_(0, rows_dev, out)
         self.sorts += 1
 
+    def _upload(self, b: int, nbytes: int) -> None:
+        """Copy the used part of staging buffer b to its device copy (outside any graph: the size varies)."""
+        self._dev[b][:nbytes].copy_(self._host[b][:nbytes], non_blocking=True)
+
     def _launch(self, rf, b: int) -> None:
-        dev = self._dev[b]
-        host = self._host[b]
-        base = dev.data_ptr()
-        dev.copy_(host, non_blocking=True)
+        base = self._dev[b].data_ptr()
         for g, scheme in enumerate(self.groups):
             _lib.call("opb_batched_steps", ctypes.byref(_abi.particles_struct(self.arena)), base + self._off_hdr[g],
                       base + self._off_exps[g], ctypes.byref(self._scalars_struct()), ctypes.byref(rf),
@@ -448,10 +590,16 @@ class ReleaseBatch:
             return  # the eager launch did this interval's work; the capture itself ran nothing
         g.replay()
 
-    def step_interval(self) -> bool:
-        """Run one snapshot interval for every release that has steps in it; False when all are done."""
-        if self.finished:
-            return False
+    def _report(self) -> list[Release]:
+        done = [r for r in self.releases if r.finished and not r.reported]
+        for r in done:
+            r.reported = True
+        return done
+
+    def tick(self) -> list[Release]:
+        """Run snapshot interval ``interval`` for every release with steps in it, then move to the next
+        interval; return the releases that finished (all steps done, or stopped with an error) and were
+        not returned before."""
         if self.interval is None:
             self.interval = self._first_interval()
         j = self.interval
@@ -459,7 +607,7 @@ class ReleaseBatch:
             for r in self.releases:
                 if not r.finished:
                     r.error = IndexError("no snapshot interval left")
-            return False
+            return self._report()
         exps, tidx_all = self._plan(j)
         self.interval = j + 1
         if exps:
@@ -469,6 +617,7 @@ class ReleaseBatch:
             self._sort_due(j, exps)
             for obs in self.observers:
                 obs.before()
+            self._upload(b, self._off_tab + len(tidx_all) * TIME_DTYPE.itemsize)
             self._run_launch(rf, b)
             for obs in self.observers:
                 obs.after()
@@ -480,6 +629,13 @@ class ReleaseBatch:
             for f in self._td.values():
                 f.mark_used(window)
                 f.prefetch(j + 3, set(window[1:]))
+        return self._report()
+
+    def step_interval(self) -> bool:
+        """Run one snapshot interval; False once every release is done."""
+        if self.finished:
+            return False
+        self.tick()
         return not self.finished
 
     def run(self) -> None:
@@ -496,19 +652,10 @@ class ReleaseBatch:
         """Host copies of a release's particle fields in its original particle order."""
         if isinstance(r, int):
             r = self.releases[r]
-        self.synchronize()
-        sl = slice(r.start, r.start + len(r))
-        pos = (self.order[sl] - r.start)
-        out = {}
-        for name in names:
-            key = name if name in self.arena else "_" + name
-            t = self.arena.arrays[key][sl]
-            o = torch.empty_like(t)
-            o.index_copy_(0, pos, t)
-            out[name] = o.cpu().numpy()
-        return out
+        self.arena.check_errors()
+        return self.collect(r, names).result()
 
     @property
     def particle_steps(self) -> int:
-        """Particle-steps planned so far (particles x steps, over all releases)."""
-        return sum(len(r) * r.done for r in self.releases)
+        """Particle-steps planned so far (particles x steps), retired releases included."""
+        return self.retired_particle_steps + sum(len(r) * r.done for r in self.releases)

@@ -259,8 +259,8 @@ class SnapshotRing:
         # everything queued so far before overwriting the slot)
         self.last_use: dict[int, torch.cuda.Event | None] = {}
         self.copy_stream = torch.cuda.Stream(device=device)
-        # a device-resident source is copied device to device: no host staging
-        on_device = isinstance(source, torch.Tensor) and source.is_cuda
+        # a device-resident or device-generated source is copied device to device: no host staging
+        on_device = (isinstance(source, torch.Tensor) and source.is_cuda) or hasattr(source, "produce")
         self.staging = [] if on_device else [torch.empty(tuple(spatial_shape), dtype=torch_dtype(np_dtype),
                                                          pin_memory=True) for _ in range(2)]
         self.staging_free = [None, None]  # events: staging buffer's last H2D copy done
@@ -288,6 +288,20 @@ class SnapshotRing:
 
     def _upload(self, k: int, slot: int, slot_free: torch.cuda.Event) -> None:
         src = self.source
+        if hasattr(src, "produce"):
+            # generated on the device, on the copy stream
+            with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
+                if slot_free is not None:
+                    self.copy_stream.wait_event(slot_free)
+                if self.storage is None:
+                    src.produce(k, self.slots[slot])
+                else:
+                    src.produce(k, self.device_staging)
+                    quantize_levels(self.device_staging, self.slots[slot], self.slot_scales[slot], self.nlev)
+                ev = torch.cuda.Event()
+                ev.record(self.copy_stream)
+            self.ready[k] = ev
+            return
         if isinstance(src, torch.Tensor) and (src.is_pinned() or src.is_cuda):
             # already in pinned host memory (or on the device): one async copy, no staging
             with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):

@@ -277,6 +277,72 @@ class SyntheticROMS:
         return snap
 
     # ------------------------------------------------------- device generation
+    def _device_consts(self, dev) -> dict:
+        """Time-independent tensors of the device construction (float64 on ``dev``)."""
+        import torch
+
+        nx, ny = self.spec.nx, self.spec.ny
+        f64 = dict(dtype=torch.float64, device=dev)
+        rho_t, corner_t = self._taper
+        pad = np.pad(rho_t, ((0, 0), (1, 1)), mode="edge")
+        tu = torch.tensor(np.minimum(pad[:, :-1], pad[:, 1:]), **f64)
+        pad = np.pad(rho_t, ((1, 1), (0, 0)), mode="edge")
+        tv = torch.tensor(np.minimum(pad[:-1, :], pad[1:, :]), **f64)
+        h = torch.tensor(self.h64, **f64)
+        hc = self.spec.hc
+        Sw = (hc * torch.tensor(self.sigma_w, **f64)[:, None, None]
+              + h[None] * torch.tensor(self.Cw64, **f64)[:, None, None]) / (hc + h)[None]
+        return {
+            "corner": torch.tensor(corner_t, **f64), "tu": tu, "tv": tv, "h": h,
+            "mask": torch.tensor(self.mask_rho, **f64), "prof": torch.tensor(self._prof, **f64),
+            "dSw": Sw[1:] - Sw[:-1],
+            "yc": torch.arange(ny + 1, **f64)[:, None] - 0.5, "xc": torch.arange(nx + 1, **f64)[None, :] - 0.5,
+            "yu": torch.arange(ny, **f64)[:, None], "xu": torch.arange(nx + 1, **f64)[None, :] - 0.5,
+            "yv": torch.arange(ny + 1, **f64)[:, None] - 0.5, "xv": torch.arange(nx, **f64)[None, :],
+            "scale": self._velocity_scale(),
+        }
+
+    def _snapshot_time(self, it: int) -> float:
+        return float(self.time_array[it]) if it < len(self.time_array) else it * self.spec.snapshot_interval
+
+    def _device_snapshot(self, it: int, c: dict, td, out: dict | None = None) -> dict:
+        """Snapshot ``it`` of u, v, w, zeta computed on the device in float64, stored in ``td``."""
+        import torch
+
+        nx, ny, nz = self.spec.nx, self.spec.ny, self.spec.nz
+        dev = c["h"].device
+        f64 = dict(dtype=torch.float64, device=dev)
+        if out is None:
+            out = {"u": torch.empty((nz, ny, nx - 1), dtype=td, device=dev),
+                   "v": torch.empty((nz, ny - 1, nx), dtype=td, device=dev),
+                   "w": torch.empty((nz + 1, ny, nx), dtype=td, device=dev),
+                   "zeta": torch.empty((ny, nx), dtype=td, device=dev)}
+        t = self._snapshot_time(it)
+        psi = torch.zeros((ny + 1, nx + 1), **f64)
+        for m in range(self._k.size):
+            ph = self._phi[m] + self._omega[m] * t
+            psi += self._amp[m] * torch.cos(self._k[m] * c["xc"] + self._l[m] * c["yc"] + ph)
+        psi *= c["corner"]
+        uf = -(psi[1:, :] - psi[:-1, :])
+        vf = psi[:, 1:] - psi[:, :-1]
+        for m in range(self._kp.size):
+            a = self._ampp[m]
+            uf += -a * self._kp[m] * torch.sin(self._kp[m] * c["xu"] + self._lp[m] * c["yu"] + self._phip[m]) * c["tu"]
+            vf += -a * self._lp[m] * torch.sin(self._kp[m] * c["xv"] + self._lp[m] * c["yv"] + self._phip[m]) * c["tv"]
+        mod = (1.0 + 0.2 * np.sin(2 * np.pi * t / 86400.0)) * c["scale"]
+        uf *= mod
+        vf *= mod
+        prof = c["prof"]
+        out["u"].copy_(prof[:, None, None] * uf[None, :, 1:-1])
+        out["v"].copy_(prof[:, None, None] * vf[None, 1:-1, :])
+        div = ((uf[:, 1:] - uf[:, :-1]) + (vf[1:, :] - vf[:-1, :])) / self.spec.dx
+        zeta = self.zeta_value(t)
+        Hz = (zeta + c["h"])[None] * c["dSw"]
+        cum = torch.cat([torch.zeros((1, ny, nx), **f64), torch.cumsum(prof[:, None, None] * Hz, dim=0)])
+        out["w"].copy_(-div[None] * cum * c["mask"][None])
+        out["zeta"].fill_(zeta)
+        return out
+
     def device_snapshots(self, nt: int, device=None, dtype=None) -> dict:
         """Snapshots 0..nt-1 of u, v, w, zeta generated on a CUDA device.
 
@@ -289,61 +355,23 @@ class SyntheticROMS:
         import torch
 
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
-        td = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64}[
-            np.dtype(dtype) if dtype is not None else self.dtype]
+        td = _torch_dtype(dtype if dtype is not None else self.dtype)
         nx, ny, nz = self.spec.nx, self.spec.ny, self.spec.nz
-        f64 = dict(dtype=torch.float64, device=dev)
-        rho_t, corner_t = self._taper
-        corner = torch.tensor(corner_t, **f64)
-        pad = np.pad(rho_t, ((0, 0), (1, 1)), mode="edge")
-        tu = torch.tensor(np.minimum(pad[:, :-1], pad[:, 1:]), **f64)
-        pad = np.pad(rho_t, ((1, 1), (0, 0)), mode="edge")
-        tv = torch.tensor(np.minimum(pad[:-1, :], pad[1:, :]), **f64)
-        h = torch.tensor(self.h64, **f64)
-        mask = torch.tensor(self.mask_rho, **f64)
-        prof = torch.tensor(self._prof, **f64)
-        hc = self.spec.hc
-        Sw = (hc * torch.tensor(self.sigma_w, **f64)[:, None, None]
-              + h[None] * torch.tensor(self.Cw64, **f64)[:, None, None]) / (hc + h)[None]
-        dSw = Sw[1:] - Sw[:-1]
-        yc = torch.arange(ny + 1, **f64)[:, None] - 0.5
-        xc = torch.arange(nx + 1, **f64)[None, :] - 0.5
-        yu = torch.arange(ny, **f64)[:, None]
-        xu = torch.arange(nx + 1, **f64)[None, :] - 0.5
-        yv = torch.arange(ny + 1, **f64)[:, None] - 0.5
-        xv = torch.arange(nx, **f64)[None, :]
-        scale = self._velocity_scale()
         out = {
             "u": torch.empty((nt, nz, ny, nx - 1), dtype=td, device=dev),
             "v": torch.empty((nt, nz, ny - 1, nx), dtype=td, device=dev),
             "w": torch.empty((nt, nz + 1, ny, nx), dtype=td, device=dev),
             "zeta": torch.empty((nt, ny, nx), dtype=td, device=dev),
         }
+        c = self._device_consts(dev)
         for it in range(nt):
-            t = float(self.time_array[it]) if it < len(self.time_array) else it * self.spec.snapshot_interval
-            psi = torch.zeros((ny + 1, nx + 1), **f64)
-            for m in range(self._k.size):
-                ph = self._phi[m] + self._omega[m] * t
-                psi += self._amp[m] * torch.cos(self._k[m] * xc + self._l[m] * yc + ph)
-            psi *= corner
-            uf = -(psi[1:, :] - psi[:-1, :])
-            vf = psi[:, 1:] - psi[:, :-1]
-            for m in range(self._kp.size):
-                a = self._ampp[m]
-                uf += -a * self._kp[m] * torch.sin(self._kp[m] * xu + self._lp[m] * yu + self._phip[m]) * tu
-                vf += -a * self._lp[m] * torch.sin(self._kp[m] * xv + self._lp[m] * yv + self._phip[m]) * tv
-            mod = (1.0 + 0.2 * np.sin(2 * np.pi * t / 86400.0)) * scale
-            uf *= mod
-            vf *= mod
-            out["u"][it] = (prof[:, None, None] * uf[None, :, 1:-1]).to(td)
-            out["v"][it] = (prof[:, None, None] * vf[None, 1:-1, :]).to(td)
-            div = ((uf[:, 1:] - uf[:, :-1]) + (vf[1:, :] - vf[:-1, :])) / self.spec.dx
-            zeta = self.zeta_value(t)
-            Hz = (zeta + h)[None] * dSw
-            cum = torch.cat([torch.zeros((1, ny, nx), **f64), torch.cumsum(prof[:, None, None] * Hz, dim=0)])
-            out["w"][it] = (-div[None] * cum * mask[None]).to(td)
-            out["zeta"][it].fill_(zeta)
+            self._device_snapshot(it, c, td, {k: v[it] for k, v in out.items()})
         return out
+
+    def device_source(self, nt: int, device=None, dtype=None, cache: int = 6) -> "DeviceSnapshotSource":
+        """Snapshots 0..nt-1 generated on the device when a field's ring asks for them (no storage for
+        the whole series: serving runs whose model time has no fixed end)."""
+        return DeviceSnapshotSource(self, nt, device, dtype, cache)
 
     # ------------------------------------------------------------ accessors
     def field(self, name: str) -> _LazyField:
@@ -374,6 +402,87 @@ class SyntheticROMS:
         out = {name: self.dense(name) for name in ("u", "v", "w", "zeta")}
         out.update(h=self.h, dx=self.dx, dy=self.dy, C=self.C)
         return out
+
+
+def _torch_dtype(dtype):
+    import torch
+
+    return {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64}[np.dtype(dtype)]
+
+
+class _GeneratedField:
+    """One field of a DeviceSnapshotSource: an array-like ``(nt, ...)`` whose snapshots are produced on
+    the device into a caller's tensor (``produce``), for a TimeDependentField ring."""
+
+    def __init__(self, source: "DeviceSnapshotSource", name: str, spatial_shape: tuple[int, ...]) -> None:
+        self._source = source
+        self.name = name
+        self.shape = (source.nt,) + tuple(spatial_shape)
+        self.ndim = len(self.shape)
+        self.dtype = source.np_dtype
+
+    def __len__(self) -> int:
+        return self.shape[0]
+
+    def produce(self, k: int, out) -> None:
+        self._source.produce(k, self.name, out)
+
+
+class DeviceSnapshotSource:
+    """Synthetic snapshots generated on a CUDA device on demand.
+
+    ``field(name)`` gives the array-like for ``TimeDependentField``; when a
+    field's ring asks for snapshot k, all four fields of k are generated once
+    (on the asking stream) and kept in a small cache, so the other fields'
+    rings copy them instead of generating again.  Generation is deterministic:
+    snapshot k has the same bits every time it is produced.
+    """
+
+    def __init__(self, grid: "SyntheticROMS", nt: int, device=None, dtype=None, cache: int = 6) -> None:
+        import threading
+
+        import torch
+
+        self.grid = grid
+        self.nt = int(nt)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.np_dtype = np.dtype(dtype if dtype is not None else grid.dtype)
+        self.td = _torch_dtype(self.np_dtype)
+        self.cache_size = max(2, int(cache))
+        self._consts = None
+        self._cache: dict[int, tuple[dict, object]] = {}
+        self._lock = threading.Lock()
+        self.generated = 0
+
+    def field(self, name: str) -> _GeneratedField:
+        nz, ny, nx = self.grid.spec.nz, self.grid.spec.ny, self.grid.spec.nx
+        shapes = {"u": (nz, ny, nx - 1), "v": (nz, ny - 1, nx), "w": (nz + 1, ny, nx), "zeta": (ny, nx)}
+        return _GeneratedField(self, name, shapes[name])
+
+    def produce(self, k: int, name: str, out) -> None:
+        """Write field ``name`` of snapshot ``k`` into the device tensor ``out`` on the current stream."""
+        import torch
+
+        if not 0 <= k < self.nt:
+            raise IndexError(k)
+        stream = torch.cuda.current_stream(self.device)
+        with self._lock:
+            entry = self._cache.pop(k, None)
+            if entry is None:
+                if self._consts is None:
+                    self._consts = self.grid._device_consts(self.device)
+                fields = self.grid._device_snapshot(k, self._consts, self.td)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                entry = (fields, ev)
+                self.generated += 1
+            self._cache[k] = entry  # most recently used last
+            while len(self._cache) > self.cache_size:
+                self._cache.pop(next(iter(self._cache)))
+        fields, ev = entry
+        stream.wait_event(ev)
+        out.copy_(fields[name])
+        fields[name].record_stream(stream)
 
 
 # The workloads: grid, snapshots, particles, scheme, dt (seconds).
