@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--dt", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
-    ap.add_argument("--study", choices=("precision", "batched"), default=None,
+    ap.add_argument("--study", choices=("precision", "batched", "serving"), default=None,
                     help="precision: float64 vs float32 arithmetic with float32/float16/bfloat16 storage, "
                          "separation in metres after --days; batched: release experiments in one batch vs "
                          "one after another through the plain path")
@@ -84,6 +84,14 @@ def parse():
     ap.add_argument("--sort-interval", type=int, default=None)
     ap.add_argument("--buckets", type=int, default=None)
     ap.add_argument("--no-plain", action="store_true", help="skip the one-release-at-a-time arm")
+    # serving (--study serving)
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson request rate (1/s)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="arrival window (s)")
+    ap.add_argument("--serve-count", type=str, default="100,2e6", help="log-uniform particles per request")
+    ap.add_argument("--serve-count-scale", type=float, default=0.15)
+    ap.add_argument("--serve-days", type=str, default="1,30", help="request duration range (days)")
+    ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget for particle state")
+    ap.add_argument("--serve-plain", type=int, default=64, help="requests of the trace the plain arm runs")
     return ap.parse_args()
 
 
@@ -727,12 +735,159 @@ def batched_study(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+def serving_trace(a, grid):
+    """Poisson arrivals; per request: log-uniform count, random wet rectangle and sigma band, duration,
+    scheme and dt (config-5 construction, seeded)."""
+    from offline_particles_b200.serving import ReleaseRequest
+
+    rng = np.random.default_rng(5)
+    lo, hi = (float(v) for v in a.serve_count.split(","))
+    dlo, dhi = (float(v) for v in a.serve_days.split(","))
+    t, reqs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / a.serve_rate)
+        if t > a.serve_seconds:
+            break
+        n = max(1, int(round(np.exp(rng.uniform(np.log(lo), np.log(hi))) * a.serve_count_scale)))
+        z, y, x = grid.release_in_box(n, rng)
+        dt = float(rng.choice([60.0, 120.0, 300.0]))
+        days = rng.uniform(dlo, dhi)
+        scheme = "rk2" if rng.random() < 0.5 else "ab3"
+        r = ReleaseRequest(z, y, x, scheme, dt, round(days * 86400.0 / dt) * dt, id=len(reqs))
+        r.offset = t  # arrival time after the start of the run
+        reqs.append(r)
+    return reqs
+
+
+def serving_study(a) -> None:
+    """Config-5 serving: a Poisson request stream served with continuous batching (ReleaseServer), and
+    the plain path serving a prefix of the same trace one request at a time.
+
+    Snapshots of the config-4 grid are generated on the device when a ring
+    asks for them (model time runs as long as the service does).  Served arm:
+    requests are submitted at their arrival times (wall clock) and admitted at
+    interval boundaries by the HBM budget; latency = arrival to result in host
+    memory.  Plain arm: the first --serve-plain requests, each alone through
+    Simulation from the start time the server gave it (FIFO from the same
+    arrival times; its results are compared bit for bit with the served ones).
+    """
+    import torch
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200.serving import ReleaseServer
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    torch.cuda.set_device(0)
+    nz, ny, nx = (int(v) for v in a.batch_grid.split(","))
+    grid = SyntheticROMS(GridSpec(nx=nx, ny=ny, nz=nz, nt=4, seed=4, dtype="float32"))
+    reqs = serving_trace(a, grid)
+    nt = 400_000  # hourly snapshot indices available to the device source (45 model years)
+    t_arr = np.arange(nt, dtype=np.float64) * 3600.0
+    statics = {n: opb.StaticField.from_numpy(arr, *STAGGERS[n])
+               for n, arr in (("h", grid.h), ("dx", grid.dx), ("dy", grid.dy), ("C", grid.C))}
+
+    def fieldset():
+        src = grid.device_source(nt)
+        kw = {n: opb.TimeDependentField(src.field(n), *STAGGERS[n], ring_size=4) for n in TD}
+        return opb.Fieldset(nt, nz, ny, nx, constants={"hc": grid.hc, "NZ": nz}, **kw, **statics)
+
+    budget = int(a.serve_budget_gb * 1e9)
+    server = ReleaseServer(fieldset(), t_arr, hbm_budget=budget, max_releases=1024, block=256, warps_per_sm=16,
+                           buckets=256, sort_interval=4)
+    offered = sum(len(r) * round(r.duration / r.dt) for r in reqs) / a.serve_seconds
+    # warm the kernels (module load, occupancy, graph capture) on a throwaway server
+    warm = ReleaseServer(fieldset(), t_arr, hbm_budget=64 * server.per_particle, max_releases=4)
+    wz, wy, wx = grid.release(32, seed=1)
+    from offline_particles_b200.serving import ReleaseRequest
+    for sch in ("rk2", "ab3"):
+        warm.submit(ReleaseRequest(wz, wy, wx, sch, 300.0, 7200.0))
+    warm.drain()
+    del warm
+    torch.cuda.synchronize()
+
+    with ClockSampler(0) as clocks:
+        t0 = time.perf_counter()
+        i, n = 0, len(reqs)
+        max_running = 0
+        while True:
+            now = time.perf_counter() - t0
+            while i < n and reqs[i].offset <= now:
+                reqs[i].arrival = t0 + reqs[i].offset
+                server.submit(reqs[i])
+                i += 1
+            if not server.queue and not server.running:
+                if i >= n:
+                    break
+                server._poll()
+                time.sleep(max(0.0, min(0.002, reqs[i].offset - (time.perf_counter() - t0))))
+                continue
+            server.tick()
+            max_running = max(max_running, len(server.running))
+        server.drain()
+        t_end = max(r.finished for r in server.done)
+    span = t_end - t0
+    served_ps = sum(len(r) * r.nsteps for r in server.done)
+    lat = server.latencies()
+    served = {"requests": len(server.done), "rejected": len(server.rejected), "value": served_ps / span,
+              "unit": UNIT, "makespan_s": span, "ticks": server.ticks, "launches": server.batch.launches,
+              "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+              "latency_mean_s": float(lat.mean()), "max_running": max_running, "capacity_particles": server.capacity,
+              "bytes_per_particle": server.per_particle, "clocks": clocks.summary()}
+
+    # ---- plain: the same requests one at a time, FIFO ---------------------------
+    plain = None
+    if a.serve_plain > 0:
+        fs = fieldset()
+        k = min(a.serve_plain, len(server.done))
+        prefix = sorted(server.done, key=lambda r: r.id)[:k]
+        free_at, lat_p, ps, busy, same = 0.0, [], 0, 0.0, 0
+        for r in prefix:
+            f = opb.roms.rk2_w_advection_timestepper if r.scheme == "rk2" else opb.roms.ab3_w_advection_timestepper
+            torch.cuda.synchronize()
+            w0 = time.perf_counter()
+            ts = f(t_arr, np.float64(r.dt), time=np.float64(r.start_time))
+            sim = opb.SimulationBuilder(ts, fs).build_simulation(len(r))
+            sim.set_indices(r.zidx, r.yidx, r.xidx)
+            sim.set_particle_field("status", 10 if r.scheme == "ab3" else 0)
+            sim.run(r.nsteps)
+            P = sim.particles
+            res = {key: P[key] for key in ("zidx", "yidx", "xidx", "status")}
+            service = time.perf_counter() - w0
+            del sim
+            busy += service
+            start = max(free_at, r.offset)
+            free_at = start + service
+            lat_p.append(free_at - r.offset)
+            ps += len(r) * r.nsteps
+            same += all(np.array_equal(res[key].view(np.uint8), r.result[key].view(np.uint8)) for key in res)
+        lat_p = np.array(lat_p)
+        plain = {"requests": k, "value": ps / busy, "unit": UNIT, "busy_s": busy,
+                 "latency_p50_s": float(np.percentile(lat_p, 50)), "latency_p99_s": float(np.percentile(lat_p, 99)),
+                 "identical_to_served": f"{same}/{k}",
+                 "note": "service times measured one request at a time; FIFO latencies from the same arrival "
+                         "times"}
+    sizes = [len(r) for r in reqs]
+    line = {"study": "serving", "metric": "served particle-steps/s and request latency p50/p99", "unit": UNIT,
+            "value": served["value"], "vs_plain": served["value"] / plain["value"] if plain else None,
+            "served": served, "plain": plain,
+            "workload": {"grid": [nz, ny, nx], "field_dtype": "float32", "rate_per_s": a.serve_rate,
+                         "window_s": a.serve_seconds, "requests": len(reqs),
+                         "particles_per_request": [int(min(sizes)), int(np.median(sizes)), int(max(sizes))],
+                         "count_range": a.serve_count, "count_scale": a.serve_count_scale,
+                         "duration_days": a.serve_days, "dt_s": [60, 120, 300],
+                         "offered_particle_steps_per_s": offered, "hbm_budget_gb": a.serve_budget_gb},
+            "data": "synthetic; snapshots generated on the device on demand"}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     a = parse()
     if a.study == "precision":
         precision_study(a)
     elif a.study == "batched":
         batched_study(a)
+    elif a.study == "serving":
+        serving_study(a)
     elif a.impl == "reference":
         reference_arm(a)
     else:

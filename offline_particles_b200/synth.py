@@ -397,6 +397,28 @@ class SyntheticROMS:
         z = rng.uniform(0.0, self.spec.nz - 1.0, n)
         return z, y, x
 
+    def release_in_box(self, n: int, rng: np.random.Generator, min_frac: float = 0.05,
+                       max_frac: float = 0.5) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """``n`` particles uniform in the wet cells of a random rectangle (sides ``min_frac`` to
+        ``max_frac`` of the grid's) at uniform random levels of a random sigma band."""
+        ny, nx, nz = self.spec.ny, self.spec.nx, self.spec.nz
+        while True:
+            hy = max(1, int(ny * rng.uniform(min_frac, max_frac)))
+            hx = max(1, int(nx * rng.uniform(min_frac, max_frac)))
+            y0 = int(rng.integers(0, ny - hy + 1))
+            x0 = int(rng.integers(0, nx - hx + 1))
+            box = self.mask_rho[y0:y0 + hy, x0:x0 + hx] > 0
+            wet = np.flatnonzero(box.ravel())
+            if wet.size:
+                break
+        cells = wet[rng.integers(0, wet.size, n)]
+        j, i = np.divmod(cells, hx)
+        y = np.clip(y0 + j + rng.uniform(-0.5, 0.5, n), 0.0, ny - 1.0)
+        x = np.clip(x0 + i + rng.uniform(-0.5, 0.5, n), 0.0, nx - 1.0)
+        za, zb = np.sort(rng.uniform(0.0, nz - 1.0, 2))
+        z = rng.uniform(za, zb, n)
+        return z, y, x
+
     def oracle_fields(self) -> dict[str, np.ndarray]:
         """Dense field dict (u, v, w, zeta with a time axis; h, dx, dy, C)."""
         out = {name: self.dense(name) for name in ("u", "v", "w", "zeta")}
