@@ -48,6 +48,12 @@ extern "C" {
 #define OPB_F32 1
 #define OPB_BF16 2
 #define OPB_F16 3
+/* snapshot pairs (opb_batched_steps only): data[k] holds two consecutive
+ * snapshots interleaved element by element (element 2i from the earlier, 2i+1
+ * from the later), so one load fetches both values a time blend needs; an
+ * opb_time selects the pair with prev (next == prev) */
+#define OPB_F64_PAIRS 4
+#define OPB_F32_PAIRS 5
 
 /* return codes */
 #define OPB_OK 0
@@ -201,7 +207,8 @@ typedef struct {
  * it (bucket_bounds as written by opb_sort_segments, row bucket_row per
  * experiment; item_scratch: nexp * nbuckets + 1 int64 of DEVICE scratch), so
  * particles of all experiments that share a region are advanced together and
- * share the field data in L2.  scheme: 0 advances every experiment of the
+ * share the field data in L2.  The time-dependent fields (u, v, w, zeta) come
+ * as snapshot pairs (OPB_F32_PAIRS / OPB_F64_PAIRS).  scheme: 0 advances every experiment of the
  * table with one kernel; OPB_SCHEME_RK2 / OPB_SCHEME_AB3 compiles that scheme
  * alone (smaller code, fewer registers) and skips experiments of the other.
  * Fields must have the ROMS layout (u, v, w,

@@ -13,6 +13,7 @@ from ._build import LIB_PATH, build_library
 
 MAX_SLOTS = 8
 F64, F32, BF16, F16 = 0, 1, 2, 3
+F64_PAIRS, F32_PAIRS = 4, 5
 ABI_VERSION = 3
 OK, EINVAL, ECUDA = 0, 1, 2
 ERRF_ZERO_DIVISION = 1

@@ -283,7 +283,9 @@ class ReleaseBatch:
     repeat).  ``buckets``: 0 walks one release's segment after another; a
     power of two walks that many Morton buckets of the grid in turn, advancing
     the particles of every release in a bucket together, so that releases
-    sharing a region share its field data in L2.
+    sharing a region share its field data in L2.  The launches read the
+    time-dependent fields as snapshot pairs (two consecutive snapshots
+    interleaved element by element), one load per stencil corner.
     """
 
     def __init__(self, fieldset: Fieldset, releases: list[Release] = (), *, time_array=None,
@@ -336,6 +338,7 @@ class ReleaseBatch:
         min_dt = min((r.dt for r in releases), default=60.0)
         self._init_tables(min_dt)
         self._graphs: dict = {}
+        self._pairs: dict = {}  # field name -> (three pair buffers, pair index held by each)
         self._sorted_at: dict[int, int] = {}
         self._sort_ws = None
         self.launches = 0
@@ -464,6 +467,39 @@ class ReleaseBatch:
         self._layout()
         self._bounds.copy_(bounds)
 
+    # ------------------------------------------------------------- snapshot pairs
+    def _pair_fields(self, j: int, window: list[int], rf) -> None:
+        """Point the time-dependent fields of ``rf`` at snapshot pairs j and j + 1 (slots 0 and 1).
+
+        Pair k interleaves snapshots k and k + 1 element by element, so the kernel fetches both values
+        of a corner's time blend with one load.  Pairs live in a ring of three buffers per field (pair k
+        in buffer k % 3); each interval builds at most the one pair it has not seen, on the compute
+        stream, after the launches that read the buffer's previous pair.
+        """
+        keep = set(window)
+        for name, f in self._td.items():
+            bufs = self._pairs.get(name)
+            if bufs is None:
+                n = int(np.prod(f.spatial_shape))
+                dt = torch.float32 if f.storage == "float32" else torch.float64
+                bufs = (torch.empty((3, 2 * n), dtype=dt, device=self.device), [-1, -1, -1])
+                self._pairs[name] = bufs
+            buf, held = bufs
+            for k in (j, j + 1):
+                if k + 1 > window[-1] or held[k % 3] == k:
+                    continue
+                a = f.snapshot(k, keep).reshape(-1)
+                b = f.snapshot(k + 1, keep).reshape(-1)
+                torch.stack((a, b), dim=1, out=buf[k % 3].view(-1, 2))
+                held[k % 3] = k
+            fld = getattr(rf, name)
+            fld.dtype = _lib.F32_PAIRS if buf.dtype == torch.float32 else _lib.F64_PAIRS
+            fld.data[0] = buf[j % 3].data_ptr()
+            fld.data[1] = buf[(j + 1) % 3].data_ptr() if held[(j + 1) % 3] == j + 1 else fld.data[0]
+            for q in range(2, _lib.MAX_SLOTS):
+                fld.data[q] = None
+            fld.nslots = 2
+
     # --------------------------------------------------------------- planning
     def _plan(self, j: int):
         return self.planner.plan(self.slots, j)
@@ -497,8 +533,8 @@ class ReleaseBatch:
             ft = fr.astype(dtype)
             gt = dtype.type(1) - ft
             tab = host[self._off_tab:self._off_tab + len(tidx_all) * TIME_DTYPE.itemsize].view(TIME_DTYPE)
-            tab["prev"] = It - j
-            tab["next"] = It + 1 - j
+            tab["prev"] = It - j  # pair slot: 0 = snapshots j, j+1; 1 = snapshots j+1, j+2
+            tab["next"] = It - j
             tab["ft"] = ft.astype(np.float64)
             tab["gt"] = gt.astype(np.float64)
         return b
@@ -613,6 +649,7 @@ class ReleaseBatch:
         if exps:
             window = list(range(j, min(j + 3, self.num_snapshots)))
             rf, dtype = window_fields(self.launcher, window, self._td)
+            self._pair_fields(j, window, rf)
             b = self._write_tables(j, exps, tidx_all, dtype)
             self._sort_due(j, exps)
             for obs in self.observers:

@@ -16,7 +16,7 @@ namespace {
 
 // One particle of experiment E through E.nsteps steps of its scheme: the loop
 // bodies of k_rk2_steps / k_ab3_steps (opb_roms.cu) with E's dt, alpha and
-// time table.
+// time table, reading the time-dependent fields as snapshot pairs.
 // SCHEME: OPB_SCHEME_RK2 or OPB_SCHEME_AB3 compiles one scheme only (smaller
 // code, fewer live registers); 0 decides per experiment.
 template <typename T, typename I, int SCHEME>
@@ -50,26 +50,26 @@ __device__ __forceinline__ void batched_particle(const DParticles &p, long long 
         if (ab3) {
             const opb_time t1 = tab[2 * k], t2 = tab[2 * k + 1];
             const bool reuse = k > 0 && same_time(t1, s.at);
-            if (!ab3_step(s, bind_all<T, I, true>(r, t1), sc, reuse)) {
+            if (!ab3_step(s, bind_all<T, I, true, true>(r, t1), sc, reuse)) {
                 raise_zero_division(p);
                 break;
             }
             moved = true;
-            ab3_post(s, bind_all<T, I, true>(r, t2), L, sc);
+            ab3_post(s, bind_all<T, I, true, true>(r, t2), L, sc);
             s.at = t2;
         } else {
             const opb_time t1 = tab[3 * k], t2 = tab[3 * k + 1], t3 = tab[3 * k + 2];
             const bool reuse = k > 0 && same_time(t1, s.at);
-            if (!rk2_stage1(s, bind_all<T, I, true>(r, t1), sc, reuse)) {
+            if (!rk2_stage1(s, bind_all<T, I, true, true>(r, t1), sc, reuse)) {
                 raise_zero_division(p);
                 break;
             }
             moved = true;
-            if (!rk2_stage2(s, bind_all<T, I, true>(r, t2), L, sc)) {
+            if (!rk2_stage2(s, bind_all<T, I, true, true>(r, t2), L, sc)) {
                 raise_zero_division(p);
                 break;
             }
-            rk2_update(s, bind_all<T, I, true>(r, t3), L, sc);
+            rk2_update(s, bind_all<T, I, true, true>(r, t3), L, sc);
             s.at = t3;
         }
     }
@@ -255,7 +255,17 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
     if ((rc = convert_particles(p, dp, what, true))) return rc;
     if (!s) return fail(OPB_EINVAL, "%s: scalars is NULL", what);
     convert_scalars(s, ds);
-    if ((rc = convert_fields(f, dr, what, true, &dtype))) return rc;
+    if (!f) return fail(OPB_EINVAL, "%s: fields is NULL", what);
+    // time-dependent fields come as snapshot pairs: check, then convert with the element dtype
+    opb_roms_fields g = *f;
+    for (opb_field *x : {&g.u, &g.v, &g.w, &g.zeta}) {
+        if (x->is_static) continue;
+        if (x->dtype != OPB_F32_PAIRS && x->dtype != OPB_F64_PAIRS)
+            return fail(OPB_EINVAL, "%s: time-dependent fields must be snapshot pairs (OPB_F32_PAIRS or "
+                        "OPB_F64_PAIRS)", what);
+        x->dtype = x->dtype == OPB_F32_PAIRS ? OPB_F32 : OPB_F64;
+    }
+    if ((rc = convert_fields(&g, dr, what, true, &dtype))) return rc;
     if (!header || !experiments || !table) return fail(OPB_EINVAL, "%s: NULL device array", what);
     const bool shape_ok = (block == 128 && warps_per_sm == 16) ||
                           (block == 256 && (warps_per_sm == 16 || warps_per_sm == 24 || warps_per_sm == 32));

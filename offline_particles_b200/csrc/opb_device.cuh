@@ -59,7 +59,20 @@ struct DScalars {
 // only at run time); KIND_STATIC / KIND_TD fix it at compile time, which lets
 // the compiler drop the per-corner test (the ROMS layout: u, v, w, zeta
 // time-dependent; h, dx, dy, C static).
-constexpr int KIND_ANY = 0, KIND_STATIC = 1, KIND_TD = 2;
+// KIND_PAIRS: time-dependent, both snapshots of the blend interleaved in one
+// buffer (element 2i earlier, 2i+1 later): one 8- or 16-byte load per corner.
+constexpr int KIND_ANY = 0, KIND_STATIC = 1, KIND_TD = 2, KIND_PAIRS = 3;
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+    using type = float2;
+};
+template <>
+struct Vec2<double> {
+    using type = double2;
+};
 
 template <typename T, typename I, int KIND = KIND_ANY>
 struct View {
@@ -76,9 +89,16 @@ struct View {
     // adds in the inputs' dtype).
     __device__ __forceinline__ double at(I i) const {
         if (KIND == KIND_STATIC || (KIND == KIND_ANY && stat)) return __ldg(stat + i);
-        const T a = __ldg(prev + i) * gt;
-        const T b = __ldg(next + i) * ft;
-        return (double)(a + b);
+        if constexpr (KIND == KIND_PAIRS) {
+            const typename Vec2<T>::type v = __ldg((const typename Vec2<T>::type *)prev + i);
+            const T a = v.x * gt;
+            const T b = v.y * ft;
+            return (double)(a + b);
+        } else {
+            const T a = __ldg(prev + i) * gt;
+            const T b = __ldg(next + i) * ft;
+            return (double)(a + b);
+        }
     }
 };
 

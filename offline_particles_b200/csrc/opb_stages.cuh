@@ -40,17 +40,17 @@ __device__ __forceinline__ void raise_zero_division(const DParticles &p) {
 // The fields of one stage.  FIXED: the ROMS layout (u, v, w, zeta
 // time-dependent; h, dx, dy, C static), known at compile time; otherwise each
 // field's kind is read at run time.
-template <typename T, typename I, bool FIXED = false>
+template <typename T, typename I, bool FIXED = false, bool PAIRS = false>
 struct Bound {
-    static constexpr int KT = FIXED ? KIND_TD : KIND_ANY;
+    static constexpr int KT = PAIRS ? KIND_PAIRS : FIXED ? KIND_TD : KIND_ANY;
     static constexpr int KS = FIXED ? KIND_STATIC : KIND_ANY;
     View<T, I, KT> u, v, w, zeta;
     View<T, I, KS> dx, dy, h, C;
 };
 
-template <typename T, typename I, bool FIXED = false>
-__device__ __forceinline__ Bound<T, I, FIXED> bind_all(const DRoms &r, const opb_time &t) {
-    using B = Bound<T, I, FIXED>;
+template <typename T, typename I, bool FIXED = false, bool PAIRS = false>
+__device__ __forceinline__ Bound<T, I, FIXED, PAIRS> bind_all(const DRoms &r, const opb_time &t) {
+    using B = Bound<T, I, FIXED, PAIRS>;
     B b;
     b.u = bind<T, I, B::KT>(r.u, t);
     b.v = bind<T, I, B::KT>(r.v, t);
