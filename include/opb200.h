@@ -48,7 +48,8 @@ extern "C" {
 #define OPB_F32 1
 #define OPB_BF16 2
 #define OPB_F16 3
-/* snapshot pairs (opb_batched_steps only): data[k] holds two consecutive
+/* snapshot pairs (opb_batched_steps and the float64 fused steppers
+ * opb_rk2/ab3_w_advection_steps, ROMS field layout): data[k] holds two consecutive
  * snapshots interleaved element by element (element 2i from the earlier, 2i+1
  * from the later), so one load fetches both values a time blend needs; an
  * opb_time selects the pair with prev (next == prev) */

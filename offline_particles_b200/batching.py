@@ -41,7 +41,8 @@ from .kernels import _abi
 from .kernels.status import ParticleStatus
 from .launcher import Launcher
 from .particles import Particles
-from .timesteppers import ABTimestepper, RK2Timestepper, Timestepper, _time_dependent_fields, window_fields
+from .timesteppers import (ABTimestepper, RK2Timestepper, Timestepper, _time_dependent_fields, pair_fields,
+                           window_fields)
 
 TIME_DTYPE = np.dtype([("prev", "<i4"), ("next", "<i4"), ("ft", "<f8"), ("gt", "<f8")])
 EXPERIMENT_DTYPE = np.dtype([("start", "<i8"), ("count", "<i8"), ("first_chunk", "<i8"), ("scheme", "<i4"),
@@ -338,7 +339,6 @@ class ReleaseBatch:
         min_dt = min((r.dt for r in releases), default=60.0)
         self._init_tables(min_dt)
         self._graphs: dict = {}
-        self._pairs: dict = {}  # field name -> (three pair buffers, pair index held by each)
         self._sorted_at: dict[int, int] = {}
         self._sort_ws = None
         self.launches = 0
@@ -469,36 +469,11 @@ class ReleaseBatch:
 
     # ------------------------------------------------------------- snapshot pairs
     def _pair_fields(self, j: int, window: list[int], rf) -> None:
-        """Point the time-dependent fields of ``rf`` at snapshot pairs j and j + 1 (slots 0 and 1).
-
-        Pair k interleaves snapshots k and k + 1 element by element, so the kernel fetches both values
-        of a corner's time blend with one load.  Pairs live in a ring of three buffers per field (pair k
-        in buffer k % 3); each interval builds at most the one pair it has not seen, on the compute
-        stream, after the launches that read the buffer's previous pair.
-        """
-        keep = set(window)
-        for name, f in self._td.items():
-            bufs = self._pairs.get(name)
-            if bufs is None:
-                n = int(np.prod(f.spatial_shape))
-                dt = torch.float32 if f.storage == "float32" else torch.float64
-                bufs = (torch.empty((3, 2 * n), dtype=dt, device=self.device), [-1, -1, -1])
-                self._pairs[name] = bufs
-            buf, held = bufs
-            for k in (j, j + 1):
-                if k + 1 > window[-1] or held[k % 3] == k:
-                    continue
-                a = f.snapshot(k, keep).reshape(-1)
-                b = f.snapshot(k + 1, keep).reshape(-1)
-                torch.stack((a, b), dim=1, out=buf[k % 3].view(-1, 2))
-                held[k % 3] = k
-            fld = getattr(rf, name)
-            fld.dtype = _lib.F32_PAIRS if buf.dtype == torch.float32 else _lib.F64_PAIRS
-            fld.data[0] = buf[j % 3].data_ptr()
-            fld.data[1] = buf[(j + 1) % 3].data_ptr() if held[(j + 1) % 3] == j + 1 else fld.data[0]
-            for q in range(2, _lib.MAX_SLOTS):
-                fld.data[q] = None
-            fld.nslots = 2
+        """Point the time-dependent fields of ``rf`` at snapshot pairs j and j + 1 (slots 0 and 1;
+        ``TimeDependentField.pair``): the kernel fetches both values of a corner's time blend with one
+        load.  Pair j + 1 exists only when snapshot j + 2 is in the window."""
+        its = [j, j + 1] if j + 2 <= window[-1] else [j]
+        pair_fields(rf, its, self._td)
 
     # --------------------------------------------------------------- planning
     def _plan(self, j: int):

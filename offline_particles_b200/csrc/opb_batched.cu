@@ -255,16 +255,13 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
     if ((rc = convert_particles(p, dp, what, true))) return rc;
     if (!s) return fail(OPB_EINVAL, "%s: scalars is NULL", what);
     convert_scalars(s, ds);
-    if (!f) return fail(OPB_EINVAL, "%s: fields is NULL", what);
     // time-dependent fields come as snapshot pairs: check, then convert with the element dtype
-    opb_roms_fields g = *f;
-    for (opb_field *x : {&g.u, &g.v, &g.w, &g.zeta}) {
-        if (x->is_static) continue;
-        if (x->dtype != OPB_F32_PAIRS && x->dtype != OPB_F64_PAIRS)
-            return fail(OPB_EINVAL, "%s: time-dependent fields must be snapshot pairs (OPB_F32_PAIRS or "
-                        "OPB_F64_PAIRS)", what);
-        x->dtype = x->dtype == OPB_F32_PAIRS ? OPB_F32 : OPB_F64;
-    }
+    opb_roms_fields g;
+    bool pairs = false;
+    if ((rc = unpair_fields(f, g, pairs, what))) return rc;
+    if (!pairs && !(g.u.is_static && g.v.is_static && g.w.is_static && g.zeta.is_static))
+        return fail(OPB_EINVAL, "%s: time-dependent fields must be snapshot pairs (OPB_F32_PAIRS or OPB_F64_PAIRS)",
+                    what);
     if ((rc = convert_fields(&g, dr, what, true, &dtype))) return rc;
     if (!header || !experiments || !table) return fail(OPB_EINVAL, "%s: NULL device array", what);
     const bool shape_ok = (block == 128 && warps_per_sm == 16) ||

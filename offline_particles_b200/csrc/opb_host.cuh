@@ -191,6 +191,26 @@ int stage_common(const char *what, const opb_particles *p, const opb_scalars *s,
     return OPB_OK;
 }
 
+// Time-dependent fields may come as snapshot pairs (OPB_F32_PAIRS / OPB_F64_PAIRS): `out` is `in`
+// with the element dtypes, `pairs` says which form it was.  All of u, v, w, zeta or none.
+int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, bool &pairs, const char *what) {
+    if (!in) return fail(OPB_EINVAL, "%s: fields is NULL", what);
+    out = *in;
+    int npairs = 0, ntd = 0;
+    for (opb_field *x : {&out.u, &out.v, &out.w, &out.zeta}) {
+        if (x->is_static) continue;
+        ++ntd;
+        if (x->dtype == OPB_F32_PAIRS || x->dtype == OPB_F64_PAIRS) {
+            x->dtype = x->dtype == OPB_F32_PAIRS ? OPB_F32 : OPB_F64;
+            ++npairs;
+        }
+    }
+    if (npairs && npairs != ntd)
+        return fail(OPB_EINVAL, "%s: either every time-dependent field is a snapshot pair or none", what);
+    pairs = npairs > 0;
+    return OPB_OK;
+}
+
 int need_fields(const opb_particles *p, const char *what, std::initializer_list<std::pair<const char *, const void *>> req) {
     if (!p || p->n == 0) return OPB_OK;
     for (auto &kv : req)

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3_post(const __grid_constant__ DPa
 // ------------------------------------------------------------ fused kernels
 // `nsteps` RK2 steps (timesteppers.py:241-257) per launch.  table[3*k + j]
 // selects the fields of step k, stage j (t, t + alpha dt, t + dt).
-template <typename T, typename I, bool FIXED>
+template <typename T, typename I, bool FIXED, bool PAIRS = false>
 __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
@@ -200,16 +200,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table[3 * k], t2 = table[3 * k + 1], t3 = table[3 * k + 2];
         const bool reuse = k > 0 && same_time(t1, s.at);
-        if (!rk2_stage1(s, bind_all<T, I, FIXED>(r, t1), sc, reuse)) {
+        if (!rk2_stage1(s, bind_all<T, I, FIXED, PAIRS>(r, t1), sc, reuse)) {
             raise_zero_division(p);
             break;
         }
         moved = true;
-        if (!rk2_stage2(s, bind_all<T, I, FIXED>(r, t2), L, sc)) {
+        if (!rk2_stage2(s, bind_all<T, I, FIXED, PAIRS>(r, t2), L, sc)) {
             raise_zero_division(p);
             break;
         }
-        rk2_update(s, bind_all<T, I, FIXED>(r, t3), L, sc);
+        rk2_update(s, bind_all<T, I, FIXED, PAIRS>(r, t3), L, sc);
         s.at = t3;
     }
     if (s.status != st0) p.status[i] = s.status;
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
 
 // `nsteps` AB3 steps (timesteppers.py:296-305) per launch.  table[2*k + j]
 // selects the fields of step k at t (j = 0) and t + dt (j = 1).
-template <typename T, typename I, bool FIXED>
+template <typename T, typename I, bool FIXED, bool PAIRS = false>
 __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
@@ -255,12 +255,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table[2 * k], t2 = table[2 * k + 1];
         const bool reuse = k > 0 && same_time(t1, s.at);
-        if (!ab3_step(s, bind_all<T, I, FIXED>(r, t1), sc, reuse)) {
+        if (!ab3_step(s, bind_all<T, I, FIXED, PAIRS>(r, t1), sc, reuse)) {
             raise_zero_division(p);
             break;
         }
         moved = true;
-        ab3_post(s, bind_all<T, I, FIXED>(r, t2), L, sc);
+        ab3_post(s, bind_all<T, I, FIXED, PAIRS>(r, t2), L, sc);
         s.at = t2;
     }
     if (s.status != st0) p.status[i] = s.status;
@@ -427,7 +427,12 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     if ((rc = convert_particles(p, dp, what, true))) return rc;
     if (!s) return fail(OPB_EINVAL, "%s: scalars is NULL", what);
     convert_scalars(s, ds);
-    if ((rc = convert_fields(f, dr, what, true, &dtype))) return rc;
+    opb_roms_fields g;
+    bool pairs = false;
+    if ((rc = unpair_fields(f, g, pairs, what))) return rc;
+    if ((rc = convert_fields(&g, dr, what, true, &dtype))) return rc;
+    if (pairs && !roms_layout(dr))
+        return fail(OPB_EINVAL, "%s: snapshot pairs need the ROMS field layout", what);
     if (nsteps < 0) return fail(OPB_EINVAL, "%s: negative step count", what);
     if (nsteps > 0 && !table) return fail(OPB_EINVAL, "%s: step table is NULL", what);
     if (rk2)
@@ -439,18 +444,20 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
                                    {"_dxidx2", p->dxidx2}, {"_dyidx2", p->dyidx2}, {"_dz2", p->dz2}});
     if (rc) return rc;
     if (dp.n == 0 || nsteps == 0) return OPB_OK;
-    const unsigned g = grid_for(dp.n);
+    const unsigned grid = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
     const bool fixed = roms_layout(dr);
     dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {
         using T = decltype(tv);
         using I = decltype(iv);
         if (rk2) {
-            if (fixed) k_rk2_steps<T, I, true><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-            else k_rk2_steps<T, I, false><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            if (pairs) k_rk2_steps<T, I, true, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            else if (fixed) k_rk2_steps<T, I, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            else k_rk2_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
         } else {
-            if (fixed) k_ab3_steps<T, I, true><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-            else k_ab3_steps<T, I, false><<<g, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            if (pairs) k_ab3_steps<T, I, true, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            else if (fixed) k_ab3_steps<T, I, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            else k_ab3_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
         }
     });
     return check_launch(what);

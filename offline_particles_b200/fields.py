@@ -413,12 +413,13 @@ class TimeDependentField(Field):
 
     def __init__(self, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
                  spatial_array_factory=None, output_dtype=np.float64, *, ring_size: int = 4, prefetch: int = 2,
-                 device=None, storage: str | None = None, ring: bool | None = None) -> None:
+                 device=None, storage: str | None = None, ring: bool | None = None, pair_slots: int = 4) -> None:
         """``storage``: keep the snapshots on the device as "bfloat16" or "float16" with one scale
         per level (the float32 steppers only); default: the source dtype.  ``ring``: stream the
         snapshots through a ring of ``ring_size`` device slots (default: yes, unless ``data`` is
         already a CUDA tensor, which is then read in place; ring=True copies such a source slot by
-        slot, so that every launch reads the same slot addresses)."""
+        slot, so that every launch reads the same slot addresses).  ``pair_slots``: how many snapshot
+        pairs (``pair``) are kept on the device."""
         super().__init__(Stagger(z_stagger), Stagger(y_stagger), Stagger(x_stagger))
         if data.ndim < 2:
             raise ValueError(
@@ -460,6 +461,10 @@ class TimeDependentField(Field):
             self._ring = SnapshotRing(data, self._spatial_shape, self._data_dtype, ring_size, self._device,
                                       storage=self._storage)
         self._It = 0
+        if pair_slots < 2:
+            raise ValueError("pair_slots must be at least 2")
+        self._pair_slots = int(pair_slots)
+        self._pairs: collections.OrderedDict[int, torch.Tensor] = collections.OrderedDict()
 
     # ------------------------------------------------------------ properties
     @property
@@ -525,6 +530,42 @@ class TimeDependentField(Field):
         if self._ring is None:
             return self._data[k] if self._q is None else self._q[k]
         return self._ring.acquire(k, keep)
+
+    @property
+    def pair_slots(self) -> int:
+        return self._pair_slots
+
+    def pair(self, k: int, keep: set[int] | frozenset = frozenset()) -> torch.Tensor:
+        """Snapshots k and k + 1 interleaved element by element (shape ``(2 * size,)``; element 2i from
+        snapshot k, 2i + 1 from k + 1): the layout in which the float64 fused steppers fetch both values
+        of a time blend with one load.  Built on the current stream the first time it is asked for; the
+        ``pair_slots`` most recently used pairs stay on the device, and a pair's buffer is reused for a
+        new one in stream order (after the launches queued before it that read the old pair).  Pairs in
+        ``keep`` are not evicted."""
+        if self._storage is not None:
+            raise ValueError("snapshot pairs hold float32/float64 storage only")
+        if k < 0 or k + 1 >= self._num_timesteps:
+            raise IndexError(k)
+        cache = self._pairs
+        if k in cache:
+            cache.move_to_end(k)
+            return cache[k]
+        buf = None
+        if len(cache) >= self._pair_slots:
+            for old in list(cache):
+                if old not in keep:
+                    buf = cache.pop(old)
+                    break
+            if buf is None:
+                raise RuntimeError(f"{self._pair_slots} pair slots cannot hold pairs {sorted(keep)}")
+        if buf is None:
+            n = int(np.prod(self._spatial_shape))
+            buf = torch.empty(2 * n, dtype=torch_dtype(self._data_dtype), device=self._device)
+        a = self.snapshot(k, {k, k + 1}).reshape(-1)
+        b = self.snapshot(k + 1, {k, k + 1}).reshape(-1)
+        torch.stack((a, b), dim=1, out=buf.view(-1, 2))
+        cache[k] = buf
+        return buf
 
     def snapshot_scales(self, k: int) -> torch.Tensor | None:
         """Per-level scales of resident snapshot ``k`` (None for unscaled storage)."""

@@ -168,6 +168,9 @@ class Timestepper(abc.ABC):
         # a streamed field keeps one ring slot free so the next snapshot uploads while this launch runs
         capacity = min([_lib.MAX_SLOTS] + [max(2, f.ring_size - 1) if f.streamed else f.ring_size
                                            for f in td.values()])
+        pairs = use_pairs(launcher, td)
+        pair_capacity = min([_lib.MAX_SLOTS] + [f.pair_slots for f in td.values()])
+        starts: set[int] = set()  # snapshot intervals the launch's stages read (one pair each)
         time = self._time
         steps: list[list] = []
         needed: set[int] = set()
@@ -181,6 +184,9 @@ class Timestepper(abc.ABC):
             more = needed | its | {i + 1 for i in its}
             if len(more) > capacity or any(i + 1 >= f.num_timesteps for f in td.values() for i in its):
                 break
+            if pairs and len(starts | its) > pair_capacity:
+                break
+            starts |= its
             needed = more
             steps.append(tidxs)
             end_times.append(nxt)
@@ -215,18 +221,54 @@ def _time_dependent_fields(launcher: Launcher) -> dict[str, TimeDependentField]:
     return {n: fs[n] for n in _abi.ROMS_FIELDS if n in fs and isinstance(fs[n], TimeDependentField)}
 
 
+# The float64 fused steppers read streamed time-dependent fields as snapshot pairs (one load per stencil
+# corner instead of two).  Building a pair costs a read of two snapshots and a write of both per
+# snapshot interval: measured on the 1024x768x50 AB3 workload, that pays where the snapshots already
+# stream from the host (end to end 4.98 -> 5.42 G particle-steps/s) but not for fields resident on the
+# device (13.74 -> 12.66), so resident fields keep the two-load form.
+SNAPSHOT_PAIRS = True
+
+
+def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField]) -> bool:
+    """Snapshot pairs apply to the float64 steppers on the ROMS layout with float32/float64 storage whose
+    time-dependent fields stream through device rings."""
+    return (SNAPSHOT_PAIRS and launcher.arithmetic == "float64" and set(td) == {"u", "v", "w", "zeta"}
+            and all(f.storage in ("float32", "float64") and f.streamed for f in td.values()))
+
+
+def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField]) -> dict[int, int]:
+    """Point the time-dependent fields of ``rf`` at snapshot pairs ``its`` (slot q holds pair its[q]);
+    return pair -> slot."""
+    keep = set(its)
+    for name, field in td.items():
+        f = getattr(rf, name)
+        f.dtype = _lib.F32_PAIRS if field.storage == "float32" else _lib.F64_PAIRS
+        for q in range(_lib.MAX_SLOTS):
+            f.data[q] = field.pair(its[q], keep).data_ptr() if q < len(its) else None
+            f.scale[q] = None
+        if len(its) == 1:
+            f.data[1] = f.data[0]
+        f.nslots = max(2, len(its))
+    return {k: q for q, k in enumerate(its)}
+
+
 def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: dict[str, TimeDependentField]):
     """opb_roms_fields over the snapshots ``needed`` plus the per-stage opb_time table."""
     rf, dtype = window_fields(launcher, needed, td)
-    slot = {k: j for j, k in enumerate(needed)}
     entries = [t for step in steps for t in step]
+    if use_pairs(launcher, td):
+        pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td)
+        prev_next = lambda It: (pslot[It], pslot[It])  # noqa: E731
+    else:
+        slot = {k: j for j, k in enumerate(needed)}
+        prev_next = lambda It: (slot[It], slot[It + 1])  # noqa: E731
     table = (_lib.opb_time * len(entries))()
     for j, tidx in enumerate(entries):
         It, ft = divmod(tidx, 1)
         It = int(It)
         ft = dtype.type(ft)
         gt = dtype.type(1 - ft)
-        table[j] = _lib.opb_time(slot[It], slot[It + 1], float(ft), float(gt))
+        table[j] = _lib.opb_time(*prev_next(It), float(ft), float(gt))
     # move the field windows the way the stage launches would have
     for field in td.values():
         for tidx in entries:

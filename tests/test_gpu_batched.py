@@ -193,3 +193,33 @@ def test_segment_sort_keeps_segments_and_permutes_ids():
         _lib.call("opb_sort_segments", ctypes.byref(_abi.particles_struct(P)), ctypes.byref(dims),
                   (ctypes.c_int64 * 2)(5000, 100), (ctypes.c_int64 * 2)(10, 10), 2, None, 0, None, ws.data_ptr(),
                   ws.numel(), None)
+
+
+@pytest.mark.parametrize("scheme,dt", [("rk2", 300.0), ("ab3", 120.0)])
+def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
+    """The fused float64 steppers read streamed fields as snapshot pairs; switching pairs off must not
+    change a bit."""
+    from b200_runner import b200_fieldset
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200 import timesteppers
+
+    g, fields = grid
+    t_arr = g.time_array[:fields["u"].shape[0]]
+    z, y, x = g.release(3000, seed=77)
+    out = []
+    for pairs in (True, False):
+        timesteppers.SNAPSHOT_PAIRS = pairs
+        try:
+            f = opb.roms.rk2_w_advection_timestepper if scheme == "rk2" else opb.roms.ab3_w_advection_timestepper
+            sim = opb.SimulationBuilder(f(t_arr, np.float64(dt), time=np.float64(1234.5)),
+                                        b200_fieldset(fields, g.hc, g.spec.nz)).build_simulation(len(z))
+            sim.set_indices(z, y, x)
+            sim.set_particle_field("status", 10 if scheme == "ab3" else 0)
+            sim.run(90)
+            P = sim.particles
+            out.append({k: P[k] for k in NAMES})
+        finally:
+            timesteppers.SNAPSHOT_PAIRS = True
+    for k in NAMES:
+        assert same_bits(out[0][k], out[1][k]), k
