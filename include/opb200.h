@@ -160,6 +160,12 @@ int opb_ab3_w_advection(const opb_particles *p, const opb_scalars *s, const opb_
 int opb_ab3_post_w_advection(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                              const opb_time *t, void *stream);
 
+/* ---- snapshot pairs ------------------------------------------------------------
+ * No reference counterpart (a layout of this library): out[2i] = a[i],
+ * out[2i + 1] = b[i] for i < n, a/b/out DEVICE buffers of dtype OPB_F32 or
+ * OPB_F64 (out holds 2n elements): the snapshot pair of snapshots a and b. */
+int opb_interleave_pairs(const void *a, const void *b, void *out, int64_t n, int32_t dtype, void *stream);
+
 /* ---- batched release experiments ---------------------------------------------
  * No single reference counterpart: the reference advances one release per
  * Simulation (simulation.py:27-229).  Here many releases share one particle

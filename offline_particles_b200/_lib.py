@@ -104,6 +104,7 @@ SIGNATURES = {
                                        ctypes.c_int32, ctypes.c_int32, _VP],
     "opb_batched_steps": [_P(opb_particles), _VP, _VP, _P(opb_scalars), _P(opb_roms_fields), _VP, _VP, _VP,
                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _VP],
+    "opb_interleave_pairs": [_VP, _VP, _VP, ctypes.c_int64, ctypes.c_int32, _VP],
     "opb_quantize_levels": [_VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP, _VP],
 }
 

@@ -1,0 +1,93 @@
+// Snapshot pairs: two consecutive snapshots of a time-dependent field
+// interleaved element by element (out[2i] = a[i], out[2i + 1] = b[i]), the
+// layout in which the float64 steppers fetch both values of a time blend with
+// one load.  Pure data movement at HBM bandwidth: 16-byte loads of a and b,
+// 16-byte stores of the interleaved result.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "opb200.h"
+#include "opb_errors.h"
+
+namespace {
+
+constexpr int kBlock = 256;
+
+// float32: four elements of a and b per thread -> two float4 stores
+__global__ void __launch_bounds__(kBlock) k_pairs_f32(const float4 *__restrict__ a, const float4 *__restrict__ b,
+                                                      float4 *__restrict__ out, long long n4) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (long long)gridDim.x * blockDim.x) {
+        const float4 x = __ldg(a + q), y = __ldg(b + q);
+        out[2 * q] = make_float4(x.x, y.x, x.y, y.y);
+        out[2 * q + 1] = make_float4(x.z, y.z, x.w, y.w);
+    }
+}
+
+// float64: two elements of a and b per thread -> two double2 stores
+__global__ void __launch_bounds__(kBlock) k_pairs_f64(const double2 *__restrict__ a, const double2 *__restrict__ b,
+                                                      double2 *__restrict__ out, long long n2) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += (long long)gridDim.x * blockDim.x) {
+        const double2 x = __ldg(a + q), y = __ldg(b + q);
+        out[2 * q] = make_double2(x.x, y.x);
+        out[2 * q + 1] = make_double2(x.y, y.y);
+    }
+}
+
+// the elements the vector kernels leave (n not a multiple of the vector width, or unaligned buffers)
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_pairs_tail(const T *__restrict__ a, const T *__restrict__ b,
+                                                       T *__restrict__ out, long long first, long long n) {
+    const long long i = first + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[2 * i] = a[i];
+    out[2 * i + 1] = b[i];
+}
+
+int grid_for(long long work) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long want = (work + kBlock - 1) / kBlock;
+    const long long cap = (long long)sms * 8;  // 8 resident CTAs of 256 per SM
+    return (int)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+}  // namespace
+
+extern "C" {
+
+int opb_interleave_pairs(const void *a, const void *b, void *out, int64_t n, int32_t dtype, void *stream) {
+    const char *what = "opb_interleave_pairs";
+    if (n < 0) return opb::fail(OPB_EINVAL, "%s: negative element count", what);
+    if (n == 0) return OPB_OK;
+    if (!a || !b || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
+    if (dtype != OPB_F32 && dtype != OPB_F64) return opb::fail(OPB_EINVAL, "%s: dtype must be OPB_F32 or OPB_F64", what);
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool aligned = ((((uintptr_t)a) | ((uintptr_t)b) | ((uintptr_t)out)) & 15) == 0;
+    long long done = 0;
+    if (dtype == OPB_F32) {
+        if (aligned) {
+            const long long n4 = n / 4;
+            if (n4) k_pairs_f32<<<grid_for(n4), kBlock, 0, st>>>((const float4 *)a, (const float4 *)b, (float4 *)out, n4);
+            done = n4 * 4;
+        }
+        if (done < n)
+            k_pairs_tail<float><<<(unsigned)((n - done + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                (const float *)a, (const float *)b, (float *)out, done, n);
+    } else {
+        if (aligned) {
+            const long long n2 = n / 2;
+            if (n2) k_pairs_f64<<<grid_for(n2), kBlock, 0, st>>>((const double2 *)a, (const double2 *)b, (double2 *)out, n2);
+            done = n2 * 2;
+        }
+        if (done < n)
+            k_pairs_tail<double><<<(unsigned)((n - done + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+                (const double *)a, (const double *)b, (double *)out, done, n);
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+}  // extern "C"

@@ -465,6 +465,8 @@ class TimeDependentField(Field):
             raise ValueError("pair_slots must be at least 2")
         self._pair_slots = int(pair_slots)
         self._pairs: collections.OrderedDict[int, torch.Tensor] = collections.OrderedDict()
+        self._pair_store = None
+        self._pair_free: list[torch.Tensor] | None = None
 
     # ------------------------------------------------------------ properties
     @property
@@ -550,20 +552,29 @@ class TimeDependentField(Field):
         if k in cache:
             cache.move_to_end(k)
             return cache[k]
-        buf = None
-        if len(cache) >= self._pair_slots:
+        if self._pair_free is None:
+            # every pair buffer at once, on first use: a large allocation later could synchronise the device
+            n = int(np.prod(self._spatial_shape))
+            self._pair_store = torch.empty((self._pair_slots, 2 * n), dtype=torch_dtype(self._data_dtype),
+                                           device=self._device)
+            self._pair_free = list(self._pair_store.unbind(0))
+        if self._pair_free:
+            buf = self._pair_free.pop()
+        else:
+            buf = None
             for old in list(cache):
                 if old not in keep:
                     buf = cache.pop(old)
                     break
             if buf is None:
                 raise RuntimeError(f"{self._pair_slots} pair slots cannot hold pairs {sorted(keep)}")
-        if buf is None:
-            n = int(np.prod(self._spatial_shape))
-            buf = torch.empty(2 * n, dtype=torch_dtype(self._data_dtype), device=self._device)
-        a = self.snapshot(k, {k, k + 1}).reshape(-1)
-        b = self.snapshot(k + 1, {k, k + 1}).reshape(-1)
-        torch.stack((a, b), dim=1, out=buf.view(-1, 2))
+        a = self.snapshot(k, {k, k + 1})
+        b = self.snapshot(k + 1, {k, k + 1})
+        from . import _lib
+        from ._device import stream_handle
+
+        _lib.call("opb_interleave_pairs", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(),
+                  _lib.F32 if a.dtype == torch.float32 else _lib.F64, stream_handle(self._device))
         cache[k] = buf
         return buf
 

@@ -168,7 +168,7 @@ class Timestepper(abc.ABC):
         # a streamed field keeps one ring slot free so the next snapshot uploads while this launch runs
         capacity = min([_lib.MAX_SLOTS] + [max(2, f.ring_size - 1) if f.streamed else f.ring_size
                                            for f in td.values()])
-        pairs = use_pairs(launcher, td)
+        pairs = use_pairs(launcher, td, len(particles))
         pair_capacity = min([_lib.MAX_SLOTS] + [f.pair_slots for f in td.values()])
         starts: set[int] = set()  # snapshot intervals the launch's stages read (one pair each)
         time = self._time
@@ -221,19 +221,27 @@ def _time_dependent_fields(launcher: Launcher) -> dict[str, TimeDependentField]:
     return {n: fs[n] for n in _abi.ROMS_FIELDS if n in fs and isinstance(fs[n], TimeDependentField)}
 
 
-# The float64 fused steppers read streamed time-dependent fields as snapshot pairs (one load per stencil
-# corner instead of two).  Building a pair costs a read of two snapshots and a write of both per
-# snapshot interval: measured on the 1024x768x50 AB3 workload, that pays where the snapshots already
-# stream from the host (end to end 4.98 -> 5.42 G particle-steps/s) but not for fields resident on the
-# device (13.74 -> 12.66), so resident fields keep the two-load form.
-SNAPSHOT_PAIRS = True
+# The float64 fused steppers can read the time-dependent fields as snapshot pairs: one load per stencil
+# corner instead of two, about 11 % less kernel time on the 1024x768x50 AB3 workload.  A pair costs one
+# pass over two snapshots and a write of both per snapshot interval, so it pays when the particles'
+# work per interval outweighs that: measured, and by the cost model, when there is at least one particle
+# per 32 grid cells (4.19 M particles on 39.3 M cells: 13.8 -> 15.0 G particle-steps/s; a release of a
+# thousand particles would pay more for the pairs than it saves).
+# "auto" (default: that rule), "always" or "never".
+SNAPSHOT_PAIRS = "auto"
+PAIR_CELLS_PER_PARTICLE = 32
 
 
-def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField]) -> bool:
-    """Snapshot pairs apply to the float64 steppers on the ROMS layout with float32/float64 storage whose
-    time-dependent fields stream through device rings."""
-    return (SNAPSHOT_PAIRS and launcher.arithmetic == "float64" and set(td) == {"u", "v", "w", "zeta"}
-            and all(f.storage in ("float32", "float64") and f.streamed for f in td.values()))
+def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField], nparticles: int) -> bool:
+    """Snapshot pairs apply to the float64 steppers on the ROMS layout with float32/float64 storage."""
+    if SNAPSHOT_PAIRS == "never" or launcher.arithmetic != "float64" or set(td) != {"u", "v", "w", "zeta"}:
+        return False
+    if not all(f.storage in ("float32", "float64") for f in td.values()):
+        return False
+    if SNAPSHOT_PAIRS == "always":
+        return True
+    fs = launcher.fieldset
+    return nparticles * PAIR_CELLS_PER_PARTICLE >= fs.z_size * fs.y_size * fs.x_size
 
 
 def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField]) -> dict[int, int]:
@@ -252,11 +260,12 @@ def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField]) -> dict[i
     return {k: q for q, k in enumerate(its)}
 
 
-def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: dict[str, TimeDependentField]):
+def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: dict[str, TimeDependentField],
+                  nparticles: int):
     """opb_roms_fields over the snapshots ``needed`` plus the per-stage opb_time table."""
     rf, dtype = window_fields(launcher, needed, td)
     entries = [t for step in steps for t in step]
-    if use_pairs(launcher, td):
+    if use_pairs(launcher, td, nparticles):
         pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td)
         prev_next = lambda It: (pslot[It], pslot[It])  # noqa: E731
     else:
@@ -417,7 +426,7 @@ class RK2Timestepper(Timestepper):
             launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
 
     def _launch_fused(self, particles, launcher, steps, needed, td) -> None:
-        rf, table = _fused_fields(launcher, steps, needed, td)
+        rf, table = _fused_fields(launcher, steps, needed, td, len(particles))
         sc = _abi.scalars_struct({
             "hc": launcher.scalar("hc", self._tidx), "NZ": launcher.scalar("NZ", self._tidx),
             "_dt": self._normalised_dt, "_RK2_alpha": self._alpha,
@@ -481,7 +490,7 @@ class ABTimestepper(Timestepper):
             launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
 
     def _launch_fused(self, particles, launcher, steps, needed, td) -> None:
-        rf, table = _fused_fields(launcher, steps, needed, td)
+        rf, table = _fused_fields(launcher, steps, needed, td, len(particles))
         sc = _abi.scalars_struct({
             "hc": launcher.scalar("hc", self._tidx), "NZ": launcher.scalar("NZ", self._tidx),
             "_dt": self._normalised_dt,

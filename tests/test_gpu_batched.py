@@ -208,7 +208,7 @@ def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
     t_arr = g.time_array[:fields["u"].shape[0]]
     z, y, x = g.release(3000, seed=77)
     out = []
-    for pairs in (True, False):
+    for pairs in ("always", "never"):
         timesteppers.SNAPSHOT_PAIRS = pairs
         try:
             f = opb.roms.rk2_w_advection_timestepper if scheme == "rk2" else opb.roms.ab3_w_advection_timestepper
@@ -220,6 +220,23 @@ def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
             P = sim.particles
             out.append({k: P[k] for k in NAMES})
         finally:
-            timesteppers.SNAPSHOT_PAIRS = True
+            timesteppers.SNAPSHOT_PAIRS = "auto"
     for k in NAMES:
         assert same_bits(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("dtype,n,offset", [("float32", 1_000_003, 0), ("float32", 4096, 1), ("float64", 777_777, 0),
+                                            ("float64", 10, 1)])
+def test_interleave_pairs_matches_torch(dtype, n, offset):
+    import torch
+
+    from offline_particles_b200 import _lib
+
+    td = getattr(torch, dtype)
+    a = torch.randn(n + offset, dtype=torch.float64, device="cuda").to(td)[offset:]
+    b = torch.randn(n + offset, dtype=torch.float64, device="cuda").to(td)[offset:]
+    out = torch.full((2 * n + offset,), float("nan"), dtype=td, device="cuda")[offset:]
+    _lib.call("opb_interleave_pairs", a.data_ptr(), b.data_ptr(), out.data_ptr(), n,
+              _lib.F32 if dtype == "float32" else _lib.F64, None)
+    torch.cuda.synchronize()
+    assert torch.equal(out.view(-1, 2), torch.stack((a, b), dim=1))
