@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define OPB_ABI_VERSION 3
+#define OPB_ABI_VERSION 4
 #define OPB_MAX_SLOTS 8
 
 /* storage dtypes of time-dependent fields (the float64-exact entry points take
@@ -120,6 +120,7 @@ typedef struct {
     double *dxidx1, *dyidx1, *dz1;
     double *dxidx2, *dyidx2, *dz2;
     uint32_t *err; /* device error word (OPB_ERRF_*), may be NULL */
+    double *rho_t; /* target density of the isopycnal follower (ab3_isopycnal_following.pyx:41), or NULL */
 } opb_particles;
 
 /* Scalars the ROMS kernels declare (rk2_w_advection.pyx:382-385,412-417;
@@ -131,6 +132,8 @@ typedef struct {
     double dt;
     double alpha;
     double bounds[6]; /* zmin, zmax, ymin, ymax, xmin, xmax */
+    double w_max;     /* isopycnal follower (ab3_isopycnal_following.pyx:54-55) */
+    double rho_scale;
 } opb_scalars;
 
 /* ---- one entry point per reference kernel function ---------------------- */
@@ -159,6 +162,15 @@ int opb_ab3_w_advection(const opb_particles *p, const opb_scalars *s, const opb_
 /* kernels/roms/ab3_w_advection.pyx:180-229 (ab3_post_w_advection) */
 int opb_ab3_post_w_advection(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                              const opb_time *t, void *stream);
+
+/* kernels/roms/ab3_isopycnal_following.pyx:26-192 (ab3_isopycnal_following):
+ * the AB3 step with dz0 = w_max * drho / (rho_scale + |drho|), drho = rho -
+ * rho_t.  The density field is passed in f->w (staggered at rho points),
+ * p->rho_t and s->w_max, s->rho_scale are required.  The post step
+ * (ab3_isopycnal_following.pyx:194-241) is the same computation as
+ * opb_ab3_post_w_advection, which serves it. */
+int opb_ab3_isopycnal_following(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                const opb_time *t, void *stream);
 
 /* ---- snapshot pairs ------------------------------------------------------------
  * No reference counterpart (a layout of this library): out[2i] = a[i],
@@ -290,6 +302,12 @@ int opb_rk2_w_advection_steps(const opb_particles *p, const opb_scalars *s, cons
  * `table`: DEVICE array of 2*nsteps opb_time entries (t, t + dt per step). */
 int opb_ab3_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                               const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
+
+/* ABTimestepper.timestep_particles with ab3_isopycnal_following_timestepper's
+ * kernels (models/roms/__init__.py:109-141): nsteps fused steps, as
+ * opb_ab3_w_advection_steps with the isopycnal follower's vertical velocity. */
+int opb_ab3_isopycnal_following_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                      const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
 
 /* ---- spatial ordering ------------------------------------------------------
  * No counterpart in the reference, which keeps particles in release order and

@@ -14,7 +14,7 @@ from ._build import LIB_PATH, build_library
 MAX_SLOTS = 8
 F64, F32, BF16, F16 = 0, 1, 2, 3
 F64_PAIRS, F32_PAIRS = 4, 5
-ABI_VERSION = 3
+ABI_VERSION = 4
 OK, EINVAL, ECUDA = 0, 1, 2
 ERRF_ZERO_DIVISION = 1
 
@@ -47,7 +47,7 @@ PARTICLE_POINTERS = ("zidx", "yidx", "xidx", "z", "_dxidx0", "_dyidx0", "_dz0", 
 class opb_particles(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("status", ctypes.c_void_p)] + [
         (name.lstrip("_"), ctypes.c_void_p) for name in PARTICLE_POINTERS
-    ] + [("err", ctypes.c_void_p)]
+    ] + [("err", ctypes.c_void_p), ("rho_t", ctypes.c_void_p)]
 
 
 class opb_scalars(ctypes.Structure):
@@ -58,6 +58,8 @@ class opb_scalars(ctypes.Structure):
         ("dt", ctypes.c_double),
         ("alpha", ctypes.c_double),
         ("bounds", ctypes.c_double * 6),
+        ("w_max", ctypes.c_double),
+        ("rho_scale", ctypes.c_double),
     ]
 
 
@@ -91,6 +93,9 @@ SIGNATURES = {
     "opb_rk2_w_advection_update": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _P(opb_time), _VP],
     "opb_ab3_w_advection": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _P(opb_time), _VP],
     "opb_ab3_post_w_advection": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _P(opb_time), _VP],
+    "opb_ab3_isopycnal_following": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _P(opb_time), _VP],
+    "opb_ab3_isopycnal_following_steps": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP,
+                                          ctypes.c_int32, ctypes.c_int32, _VP],
     "opb_linear_interpolation": [_P(opb_particles), _VP, _P(opb_field), _P(opb_time), _VP, _VP],
     "opb_bilinear_interpolation": [_P(opb_particles), _VP, _VP, _P(opb_field), _P(opb_time), _VP, _VP],
     "opb_trilinear_interpolation": [_P(opb_particles), _P(opb_field), _P(opb_time), _VP, _VP],

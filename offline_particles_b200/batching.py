@@ -171,8 +171,8 @@ class Release:
 
     def __post_init__(self) -> None:
         ts = self.timestepper
-        if not isinstance(ts, (RK2Timestepper, ABTimestepper)) or not ts.fused():
-            raise TypeError("a Release needs a stock ROMS RK2 or AB3 timestepper (models.roms presets)")
+        if not isinstance(ts, (RK2Timestepper, ABTimestepper)) or not ts.fused() or getattr(ts, "isopycnal", False):
+            raise TypeError("a Release needs a stock ROMS RK2 or AB3 w-advection timestepper (models.roms presets)")
         if not isinstance(ts.time, (float, np.floating)):
             raise TypeError("batched releases use float64 times")
         if self.nsteps < 0:

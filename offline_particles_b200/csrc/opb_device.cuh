@@ -40,6 +40,7 @@ struct DParticles {
     double *dxidx1, *dyidx1, *dz1;
     double *dxidx2, *dyidx2, *dz2;
     uint32_t *err;
+    const double *rho_t;
 };
 
 struct DScalars {
@@ -47,6 +48,7 @@ struct DScalars {
     int NZ;
     double dt, alpha;
     double bounds[6];
+    double w_max, rho_scale;
 };
 
 // ------------------------------------------------------------------ fields

@@ -99,6 +99,7 @@ int convert_particles(const opb_particles *in, DParticles &out, const char *what
     out.dyidx2 = in->dyidx2;
     out.dz2 = in->dz2;
     out.err = in->err;
+    out.rho_t = in->rho_t;
     return OPB_OK;
 }
 
@@ -108,6 +109,8 @@ void convert_scalars(const opb_scalars *in, DScalars &out) {
     out.dt = in->dt;
     out.alpha = in->alpha;
     for (int k = 0; k < 6; ++k) out.bounds[k] = in->bounds[k];
+    out.w_max = in->w_max;
+    out.rho_scale = in->rho_scale;
 }
 
 int convert_field(const opb_field &in, DField &out, int ndim, const char *what, const char *name, int *dtype) {

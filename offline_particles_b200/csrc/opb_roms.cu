@@ -123,7 +123,14 @@ __global__ void __launch_bounds__(kBlock) k_rk2_update(const __grid_constant__ D
     p.zidx[i] = s.zidx;
 }
 
-template <typename T, typename I>
+template <typename T, typename I, bool ISO>
+__device__ __forceinline__ bool ab3_any(PState &s, const Bound<T, I> &f, const DScalars &sc, const DParticles &p,
+                                        long long i) {
+    if constexpr (ISO) return ab3_step(s, f, sc, false, IsoVel{p.rho_t[i], sc.w_max, sc.rho_scale});
+    else return ab3_step(s, f, sc);
+}
+
+template <typename T, typename I, bool ISO = false>
 __global__ void __launch_bounds__(kBlock) k_ab3(const __grid_constant__ DParticles p,
                                                 const __grid_constant__ DScalars sc,
                                                 const __grid_constant__ DRoms r, opb_time t) {
@@ -141,7 +148,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3(const __grid_constant__ DParticl
     s.k2x = p.dxidx2[i];
     s.k2y = p.dyidx2[i];
     s.k2z = p.dz2[i];
-    if (!ab3_step(s, bind_all<T, I>(r, t), sc)) {
+    if (!ab3_any<T, I, ISO>(s, bind_all<T, I>(r, t), sc, p, i)) {
         raise_zero_division(p);
         return;
     }
@@ -228,7 +235,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
 
 // `nsteps` AB3 steps (timesteppers.py:296-305) per launch.  table[2*k + j]
 // selects the fields of step k at t (j = 0) and t + dt (j = 1).
-template <typename T, typename I, bool FIXED, bool PAIRS = false>
+template <typename T, typename I, bool FIXED, bool PAIRS = false, bool ISO = false>
 __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
@@ -248,6 +255,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
     s.k2x = p.dxidx2[i];
     s.k2y = p.dyidx2[i];
     s.k2z = p.dz2[i];
+    const double rho_t = ISO ? p.rho_t[i] : 0.0;
     const uint8_t st0 = s.status;
     bool moved = false;
     for (int k = 0; k < nsteps; ++k) {
@@ -255,7 +263,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table[2 * k], t2 = table[2 * k + 1];
         const bool reuse = k > 0 && same_time(t1, s.at);
-        if (!ab3_step(s, bind_all<T, I, FIXED, PAIRS>(r, t1), sc, reuse)) {
+        bool ok;
+        if constexpr (ISO) ok = ab3_step(s, bind_all<T, I, FIXED, PAIRS>(r, t1), sc, reuse, IsoVel{rho_t, sc.w_max,
+                                                                                                     sc.rho_scale});
+        else ok = ab3_step(s, bind_all<T, I, FIXED, PAIRS>(r, t1), sc, reuse);
+        if (!ok) {
             raise_zero_division(p);
             break;
         }
@@ -358,7 +370,7 @@ static int stage_launch(const char *what, int which, const opb_particles *p, con
     DScalars ds;
     DRoms dr;
     int dtype, rc;
-    const bool need_vel = (which == 0 || which == 1 || which == 3);
+    const bool need_vel = (which == 0 || which == 1 || which == 3 || which == 5);
     if ((rc = stage_common(what, p, s, f, t, need_vel, dp, ds, dr, dtype))) return rc;
     switch (which) {
         case 0: rc = need_fields(p, what, {{"z", p->z}, {"_dxidx1", p->dxidx1}, {"_dyidx1", p->dyidx1}, {"_dz1", p->dz1}}); break;
@@ -368,9 +380,11 @@ static int stage_launch(const char *what, int which, const opb_particles *p, con
                                        {"_dxidx2", p->dxidx2}, {"_dyidx2", p->dyidx2}, {"_dz2", p->dz2}});
             break;
         case 3:
+        case 5:
             rc = need_fields(p, what, {{"z", p->z}, {"_dxidx0", p->dxidx0}, {"_dyidx0", p->dyidx0}, {"_dz0", p->dz0},
                                        {"_dxidx1", p->dxidx1}, {"_dyidx1", p->dyidx1}, {"_dz1", p->dz1},
                                        {"_dxidx2", p->dxidx2}, {"_dyidx2", p->dyidx2}, {"_dz2", p->dz2}});
+            if (!rc && which == 5) rc = need_fields(p, what, {{"rho_t", p->rho_t}});
             break;
         default: rc = need_fields(p, what, {{"z", p->z}}); break;
     }
@@ -386,6 +400,7 @@ static int stage_launch(const char *what, int which, const opb_particles *p, con
             case 1: k_rk2_step_2<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
             case 2: k_rk2_update<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
             case 3: k_ab3<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
+            case 5: k_ab3<T, I, true><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
             default: k_ab3_post<T, I><<<g, kBlock, 0, st>>>(dp, ds, dr, *t); break;
         }
     });
@@ -419,7 +434,7 @@ int opb_ab3_post_w_advection(const opb_particles *p, const opb_scalars *s, const
 
 static int steps_launch(const char *what, bool rk2, const opb_particles *p, const opb_scalars *s,
                         const opb_roms_fields *f, const opb_time *table, int32_t nsteps, int32_t validate_pre,
-                        void *stream) {
+                        void *stream, bool iso = false) {
     DParticles dp;
     DScalars ds;
     DRoms dr;
@@ -442,6 +457,7 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
         rc = need_fields(p, what, {{"z", p->z}, {"_dxidx0", p->dxidx0}, {"_dyidx0", p->dyidx0}, {"_dz0", p->dz0},
                                    {"_dxidx1", p->dxidx1}, {"_dyidx1", p->dyidx1}, {"_dz1", p->dz1},
                                    {"_dxidx2", p->dxidx2}, {"_dyidx2", p->dyidx2}, {"_dz2", p->dz2}});
+    if (!rc && iso) rc = need_fields(p, what, {{"rho_t", p->rho_t}});
     if (rc) return rc;
     if (dp.n == 0 || nsteps == 0) return OPB_OK;
     const unsigned grid = grid_for(dp.n);
@@ -454,6 +470,12 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
             if (pairs) k_rk2_steps<T, I, true, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
             else if (fixed) k_rk2_steps<T, I, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
             else k_rk2_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        } else if (iso) {
+            if (pairs)
+                k_ab3_steps<T, I, true, true, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            else if (fixed)
+                k_ab3_steps<T, I, true, false, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            else k_ab3_steps<T, I, false, false, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
         } else {
             if (pairs) k_ab3_steps<T, I, true, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
             else if (fixed) k_ab3_steps<T, I, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
@@ -461,6 +483,16 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
         }
     });
     return check_launch(what);
+}
+
+int opb_ab3_isopycnal_following(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                const opb_time *t, void *stream) {
+    return stage_launch("opb_ab3_isopycnal_following", 5, p, s, f, t, stream);
+}
+
+int opb_ab3_isopycnal_following_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                      const opb_time *table, int32_t nsteps, int32_t validate, void *stream) {
+    return steps_launch("opb_ab3_isopycnal_following_steps", false, p, s, f, table, nsteps, validate, stream, true);
 }
 
 int opb_rk2_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,

@@ -130,8 +130,34 @@ __device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &
 }
 
 // ab3_w_advection.pyx:84-178 (AB3 step for one particle)
-template <typename B>
-__device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false) {
+// The AB3 step's vertical velocity: the w field (ab3_w_advection.pyx:141-146),
+// or the isopycnal follower's w_max * drho / (rho_scale + |drho|) with drho =
+// rho(x) - rho_t from the density field in the w slot
+// (ab3_isopycnal_following.pyx:124-132).  False on a zero divisor.
+struct WVel {
+    template <typename B>
+    __device__ __forceinline__ bool operator()(const B &f, const PState &s, double &k) const {
+        k = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+        return true;
+    }
+};
+
+struct IsoVel {
+    double rho_t, w_max, rho_scale;
+    template <typename B>
+    __device__ __forceinline__ bool operator()(const B &f, const PState &s, double &k) const {
+        const double rho = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+        const double drho = rho - rho_t;
+        const double den = rho_scale + fabs(drho);
+        if (den == 0.0) return false;
+        k = w_max * drho / den;
+        return true;
+    }
+};
+
+template <typename B, typename VZ = WVel>
+__device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false,
+                                         const VZ &vz = VZ{}) {
     const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
     const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
     if (dx == 0.0) return false;
@@ -140,7 +166,7 @@ __device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &
     const double dy = bilinear(f.dy, s.yidx + f.dy.o0, s.xidx + f.dy.o1);
     if (dy == 0.0) return false;
     s.k0y = v / dy;
-    s.k0z = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    if (!vz(f, s, s.k0z)) return false;
     if (s.status == ST_MULTISTEP_1) {  // ab3_w_advection.pyx:122-131
         s.k1x = s.k0x;
         s.k1y = s.k0y;

@@ -40,7 +40,10 @@ def particles_struct_for(arrays: Mapping[str, torch.Tensor], n: int, err: torch.
         raise TypeError("particle field status must be uint8")
     if status.shape[0] != n:
         raise ValueError("particle arrays do not match the particle count")
-    return _lib.opb_particles(n=n, status=_ptr(status), err=_ptr(err), **kw)
+    rho_t = arrays.get("rho_t")
+    if rho_t is not None and rho_t.dtype != torch.float64:
+        raise TypeError("particle field rho_t must be float64")
+    return _lib.opb_particles(n=n, status=_ptr(status), err=_ptr(err), rho_t=_ptr(rho_t), **kw)
 
 
 def particles_struct(particles) -> _lib.opb_particles:
@@ -65,6 +68,8 @@ def scalars_struct(scalars: Mapping[str, object]) -> _lib.opb_scalars:
     s.alpha = float(scalars.get("_RK2_alpha", 0.0))
     for k, name in enumerate(("zidx_min", "zidx_max", "yidx_min", "yidx_max", "xidx_min", "xidx_max")):
         s.bounds[k] = float(scalars.get(name, 0.0))
+    s.w_max = float(scalars.get("w_max", 0.0))
+    s.rho_scale = float(scalars.get("rho_scale", 0.0))
     return s
 
 
@@ -105,11 +110,15 @@ def field_struct(fd: FieldData, ndim: int, name: str, slots: dict[int, int] | No
     return f
 
 
-def roms_struct(fielddata: Mapping[str, FieldData], names=ROMS_FIELDS) -> tuple[_lib.opb_roms_fields, _lib.opb_time]:
-    """opb_roms_fields + opb_time for one launch (all time-dependent fields at one time index)."""
+def roms_struct(fielddata: Mapping[str, FieldData], names=ROMS_FIELDS,
+                sources: Mapping[str, str] | None = None) -> tuple[_lib.opb_roms_fields, _lib.opb_time]:
+    """opb_roms_fields + opb_time for one launch (all time-dependent fields at one time index).  ``names``:
+    the slots the kernel reads; ``sources``: slot -> fielddata key where they differ (the isopycnal
+    follower's density in the w slot)."""
     rf = _lib.opb_roms_fields()
     t = _lib.opb_time(0, 1, 0.0, 1.0)
     weights = None
+    sources = sources or {}
     for name in ROMS_FIELDS:
         if name not in names:
             # unused by this kernel: a placeholder static field
@@ -117,7 +126,7 @@ def roms_struct(fielddata: Mapping[str, FieldData], names=ROMS_FIELDS) -> tuple[
             g.is_static = 1
             g.ndim = ROMS_NDIM[name]
             continue
-        fd = fielddata[name]
+        fd = fielddata[sources.get(name, name)]
         setattr(rf, name, field_struct(fd, ROMS_NDIM[name], name))
         if isinstance(fd.array, BlendedArray):
             w = (fd.array.It, float(fd.array.ft), float(fd.array.gt), np.dtype(fd.array.dtype))

@@ -11,6 +11,8 @@ import numpy as np
 import numpy.typing as npt
 
 from ...kernels.roms import (
+    ab3_isopycnal_following_kernel,
+    ab3_post_isopycnal_following_kernel,
     ab3_post_w_advection_kernel,
     ab3_w_advection_kernel,
     compute_z_kernel,
@@ -23,6 +25,9 @@ from ...timesteppers import ABTimestepper, RK2Timestepper
 
 __all__ = [
     "compute_z_kernel",
+    "ab3_isopycnal_following_kernel",
+    "ab3_post_isopycnal_following_kernel",
+    "ab3_isopycnal_following_timestepper",
     "ab3_w_advection_kernel",
     "ab3_post_w_advection_kernel",
     "ab3_w_advection_timestepper",
@@ -60,4 +65,19 @@ def ab3_w_advection_timestepper(time_array: npt.NDArray, dt: D, *, time: T | Non
         time=time, time_unit=time_unit, iteration=iteration, index_padding=index_padding,
         pre_step_kernel=validation_kernel,
         post_step_kernel=ab3_post_w_advection_kernel,
+    )
+
+
+def ab3_isopycnal_following_timestepper(time_array: npt.NDArray, dt: D, *, time: T | None = None,
+                                        time_unit: D | None = None, iteration: int = 0,
+                                        index_padding: int = 5) -> ABTimestepper:
+    """AB3 timestepper with the ROMS isopycnal-following kernels, validation pre-step and zidx post-step
+    (models/roms/__init__.py:109-141 of the reference).  The fieldset needs a time-dependent ``rho`` and
+    the constants ``w_max`` and ``rho_scale``; particles carry ``rho_t``."""
+    return ABTimestepper(
+        time_array, dt,
+        ab_kernel=ab3_isopycnal_following_kernel,
+        time=time, time_unit=time_unit, iteration=iteration, index_padding=index_padding,
+        pre_step_kernel=validation_kernel,
+        post_step_kernel=ab3_post_isopycnal_following_kernel,
     )

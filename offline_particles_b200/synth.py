@@ -397,6 +397,22 @@ class SyntheticROMS:
         z = rng.uniform(0.0, self.spec.nz - 1.0, n)
         return z, y, x
 
+    def density(self, nt: int | None = None) -> np.ndarray:
+        """A seeded density field at rho points, ``(nt, nz, ny, nx)`` in the grid's dtype (kg/m^3): a
+        stable stratification (denser at depth) with a slowly moving horizontal wave, for the isopycnal
+        follower.  Deterministic in the grid's spec."""
+        nt = self.spec.nt if nt is None else nt
+        nz, ny, nx = self.spec.nz, self.spec.ny, self.spec.nx
+        k = np.arange(nz, dtype=np.float64)[:, None, None]
+        j = np.arange(ny, dtype=np.float64)[None, :, None]
+        i = np.arange(nx, dtype=np.float64)[None, None, :]
+        out = np.empty((nt, nz, ny, nx), dtype=self.dtype)
+        for it in range(nt):
+            t = self._snapshot_time(it) / 86400.0
+            out[it] = (1026.5 - 1.5 * k / max(nz - 1, 1)
+                       + 0.3 * np.sin(2 * np.pi * j / ny + 0.7 * t) * np.cos(2 * np.pi * i / nx - 0.3 * t))
+        return out
+
     def release_in_box(self, n: int, rng: np.random.Generator, min_frac: float = 0.05,
                        max_frac: float = 0.5) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
         """``n`` particles uniform in the wet cells of a random rectangle (sides ``min_frac`` to

@@ -152,6 +152,11 @@ class Timestepper(abc.ABC):
         """True when the kernels are the stock ROMS ones and steps can run fused."""
         return False
 
+    @property
+    def field_roles(self) -> dict[str, str]:
+        """C-ABI field slot -> fieldset name, where the stepper's kernels read another field."""
+        return {}
+
     def timestep_particles_many(self, particles, launcher: Launcher, nsteps: int) -> None:
         """Advance ``nsteps`` steps; fused launches where possible, else step by step."""
         if not self.fused():
@@ -164,7 +169,7 @@ class Timestepper(abc.ABC):
 
     def _fused_chunk(self, particles, launcher: Launcher, max_steps: int) -> int:
         """Plan and launch as many steps as fit in one fused launch; return the number taken."""
-        td = _time_dependent_fields(launcher)
+        td = _time_dependent_fields(launcher, self.field_roles)
         # a streamed field keeps one ring slot free so the next snapshot uploads while this launch runs
         capacity = min([_lib.MAX_SLOTS] + [max(2, f.ring_size - 1) if f.streamed else f.ring_size
                                            for f in td.values()])
@@ -216,9 +221,18 @@ def _require_float64(launcher: Launcher) -> None:
                          "stage-by-stage float64 path")
 
 
-def _time_dependent_fields(launcher: Launcher) -> dict[str, TimeDependentField]:
+def _time_dependent_fields(launcher: Launcher, roles: dict[str, str] | None = None
+                           ) -> dict[str, TimeDependentField]:
+    """The time-dependent fields by C-ABI slot name; ``roles`` maps a slot to the fieldset name that fills
+    it where they differ (the isopycnal follower's rho in the w slot)."""
     fs = launcher.fieldset
-    return {n: fs[n] for n in _abi.ROMS_FIELDS if n in fs and isinstance(fs[n], TimeDependentField)}
+    roles = roles or {}
+    out = {}
+    for n in _abi.ROMS_FIELDS:
+        src = roles.get(n, n)
+        if src in fs and isinstance(fs[src], TimeDependentField):
+            out[n] = fs[src]
+    return out
 
 
 # The float64 fused steppers can read the time-dependent fields as snapshot pairs: one load per stencil
@@ -261,9 +275,9 @@ def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField]) -> dict[i
 
 
 def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: dict[str, TimeDependentField],
-                  nparticles: int):
+                  nparticles: int, roles: dict[str, str] | None = None):
     """opb_roms_fields over the snapshots ``needed`` plus the per-stage opb_time table."""
-    rf, dtype = window_fields(launcher, needed, td)
+    rf, dtype = window_fields(launcher, needed, td, roles)
     entries = [t for step in steps for t in step]
     if use_pairs(launcher, td, nparticles):
         pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td)
@@ -285,13 +299,15 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
     return rf, table
 
 
-def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDependentField]):
+def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDependentField],
+                  roles: dict[str, str] | None = None):
     """opb_roms_fields whose slot j of every time-dependent field holds snapshot ``needed[j]``, and the
     storage dtype of the time-dependent fields (numpy float64 or float32)."""
     fs = launcher.fieldset
+    roles = roles or {}
     for name in _abi.ROMS_FIELDS:
-        if name not in fs:
-            raise KeyError(f"Field '{name}' does not exist in Fieldset.")
+        if roles.get(name, name) not in fs:
+            raise KeyError(f"Field '{roles.get(name, name)}' does not exist in Fieldset.")
     dtypes = {np.dtype(f.dtype) for f in td.values()}
     if len(dtypes) > 1:
         raise ValueError("time-dependent fields of one launch must share one storage dtype")
@@ -304,7 +320,7 @@ def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDepen
     keep = set(needed)
     rf = _lib.opb_roms_fields()
     for name in _abi.ROMS_FIELDS:
-        field = fs[name]
+        field = fs[roles.get(name, name)]
         if name in td:
             f = _lib.opb_field()
             f.is_static = 0
@@ -459,13 +475,25 @@ class ABTimestepper(Timestepper):
         post = (self._post_step_kernel,) if self._post_step_kernel is not None else ()
         return pre + (self._ab_kernel,) + post
 
+    @property
+    def isopycnal(self) -> bool:
+        """True for the ROMS isopycnal-following kernels (models/roms/__init__.py:109-141)."""
+        from .kernels.roms import ab3_isopycnal_following as iso
+
+        return (self._ab_kernel is iso.ab3_isopycnal_following_kernel
+                and self._post_step_kernel is iso.ab3_post_isopycnal_following_kernel)
+
+    @property
+    def field_roles(self) -> dict[str, str]:
+        return {"w": "rho"} if self.isopycnal else {}
+
     def fused(self) -> bool:
         from .kernels.roms import ab3_w_advection as ab
         from .kernels.validation import validation_kernel
 
-        return (self._ab_kernel is ab.ab3_w_advection_kernel
-                and self._post_step_kernel is ab.ab3_post_w_advection_kernel
-                and self._pre_step_kernel in (None, validation_kernel))
+        stock = (self._ab_kernel is ab.ab3_w_advection_kernel
+                 and self._post_step_kernel is ab.ab3_post_w_advection_kernel)
+        return (stock or self.isopycnal) and self._pre_step_kernel in (None, validation_kernel)
 
     def _stage_times(self, time):
         tidx1 = self.get_time_index(time)
@@ -490,15 +518,20 @@ class ABTimestepper(Timestepper):
             launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
 
     def _launch_fused(self, particles, launcher, steps, needed, td) -> None:
-        rf, table = _fused_fields(launcher, steps, needed, td, len(particles))
+        rf, table = _fused_fields(launcher, steps, needed, td, len(particles), self.field_roles)
+        iso = self.isopycnal
         sc = _abi.scalars_struct({
             "hc": launcher.scalar("hc", self._tidx), "NZ": launcher.scalar("NZ", self._tidx),
             "_dt": self._normalised_dt,
             **{n: launcher.scalar(n, self._tidx) for n in ("zidx_min", "zidx_max", "yidx_min", "yidx_max",
-                                                           "xidx_min", "xidx_max")}})
+                                                           "xidx_min", "xidx_max")},
+            **({n: launcher.scalar(n, self._tidx) for n in ("w_max", "rho_scale")} if iso else {})})
+        if iso and launcher.arithmetic != "float64":
+            raise ValueError("the isopycnal follower has float64 steppers only")
+        entry = "opb_ab3_isopycnal_following_steps" if iso else _entry("opb_ab3_w_advection_steps", launcher)
         dev_table = _upload_table(table, particles.device)
         _notify("before", len(steps))
-        _lib.call(_entry("opb_ab3_w_advection_steps", launcher), ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
+        _lib.call(entry, ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
                   ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
         _notify("after", len(steps))

@@ -331,7 +331,56 @@ int oracle_ab3(const oparticles *p, const oscalars *s, const oroms_fields *F) {
     return (int)(nzero > 0x7fffffff ? 0x7fffffff : nzero);
 }
 
-/* kernels/roms/ab3_w_advection.pyx:180-229 */
+/* kernels/roms/ab3_isopycnal_following.pyx:26-192: ab3_w_advection's step with
+ * the vertical velocity of an isopycnal follower, dz0 = w_max * drho /
+ * (rho_scale + |drho|), drho = rho(x) - rho_t (:124-132).  F->w holds rho.
+ * A zero divisor (dx, dy, or rho_scale + |drho|) skips the particle and is
+ * counted: the reference raises ZeroDivisionError (cdivision=False). */
+int oracle_ab3_isopycnal(const oparticles *p, const oscalars *s, const oroms_fields *F, const double *rho_t,
+                         double w_max, double rho_scale) {
+    int64_t nzero = 0;
+    const double dt = s->dt;
+    #pragma omp parallel for schedule(static) reduction(+:nzero)
+    for (int64_t i = 0; i < p->n; ++i) {
+        if (p->status[i] & OST_INACTIVE) continue;
+        double zi = p->zidx[i], yi = p->yidx[i], xi = p->xidx[i];
+        double u = o_trilin(&F->u, zi + F->u.o0, yi + F->u.o1, xi + F->u.o2);
+        double dx = o_bilin(&F->dx, yi + F->dx.o0, xi + F->dx.o1);
+        if (dx == 0.0) { nzero++; continue; }
+        p->dxidx0[i] = u / dx;
+        double v = o_trilin(&F->v, zi + F->v.o0, yi + F->v.o1, xi + F->v.o2);
+        double dy = o_bilin(&F->dy, yi + F->dy.o0, xi + F->dy.o1);
+        if (dy == 0.0) { nzero++; continue; }
+        p->dyidx0[i] = v / dy;
+        double rho = o_trilin(&F->w, zi + F->w.o0, yi + F->w.o1, xi + F->w.o2);
+        double drho = rho - rho_t[i];
+        double den = rho_scale + fabs(drho);
+        if (den == 0.0) { nzero++; continue; }
+        p->dz0[i] = w_max * drho / den;
+        if (p->status[i] == OST_MULTISTEP_1) {
+            p->dxidx1[i] = p->dxidx0[i]; p->dyidx1[i] = p->dyidx0[i]; p->dz1[i] = p->dz0[i];
+            p->dxidx2[i] = p->dxidx0[i]; p->dyidx2[i] = p->dyidx0[i]; p->dz2[i] = p->dz0[i];
+            p->status[i] = OST_MULTISTEP_2;
+        } else if (p->status[i] == OST_MULTISTEP_2) {
+            p->dxidx2[i] = -p->dxidx0[i] + 2.0 * p->dxidx1[i];
+            p->dyidx2[i] = -p->dyidx0[i] + 2.0 * p->dyidx1[i];
+            p->dz2[i] = -p->dz0[i] + 2.0 * p->dz1[i];
+            p->status[i] = OST_NORMAL;
+        }
+        double h = o_bilin(&F->h, yi + F->h.o0, xi + F->h.o1);
+        double zeta = o_bilin(&F->zeta, yi + F->zeta.o0, xi + F->zeta.o1);
+        double C = o_lin(&F->C, zi + F->C.o0);
+        p->z[i] = o_compute_z(zi, s->NZ, s->hc, h, C, zeta);
+        p->z[i] += dt * (23.0 * p->dz0[i] - 16.0 * p->dz1[i] + 5.0 * p->dz2[i]) / 12.0;
+        p->yidx[i] += dt * (23.0 * p->dyidx0[i] - 16.0 * p->dyidx1[i] + 5.0 * p->dyidx2[i]) / 12.0;
+        p->xidx[i] += dt * (23.0 * p->dxidx0[i] - 16.0 * p->dxidx1[i] + 5.0 * p->dxidx2[i]) / 12.0;
+        p->dz2[i] = p->dz1[i]; p->dxidx2[i] = p->dxidx1[i]; p->dyidx2[i] = p->dyidx1[i];
+        p->dz1[i] = p->dz0[i]; p->dxidx1[i] = p->dxidx0[i]; p->dyidx1[i] = p->dyidx0[i];
+    }
+    return (int)(nzero > 0x7fffffff ? 0x7fffffff : nzero);
+}
+
+/* kernels/roms/ab3_w_advection.pyx:180-229 (and ab3_isopycnal_following.pyx:194-241, the same post step) */
 int oracle_ab3_post(const oparticles *p, const oscalars *s, const oroms_fields *F) {
     #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < p->n; ++i) {

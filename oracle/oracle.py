@@ -51,6 +51,7 @@ ROMS_STAGGERS = {
     "dx": ("invariant", "center", "center"),
     "dy": ("invariant", "center", "center"),
     "C": ("center", "invariant", "invariant"),
+    "rho": ("center", "center", "center"),  # density at rho points (ab3_isopycnal_following)
 }
 TIME_DEPENDENT = ("u", "v", "w", "zeta")
 
@@ -122,6 +123,10 @@ def lib() -> ctypes.CDLL:
             getattr(_lib, name).argtypes = [ctypes.POINTER(OParticles), ctypes.POINTER(OScalars),
                                             ctypes.POINTER(ORomsFields)]
             getattr(_lib, name).restype = ctypes.c_int
+        _lib.oracle_ab3_isopycnal.argtypes = [ctypes.POINTER(OParticles), ctypes.POINTER(OScalars),
+                                              ctypes.POINTER(ORomsFields), ctypes.c_void_p, ctypes.c_double,
+                                              ctypes.c_double]
+        _lib.oracle_ab3_isopycnal.restype = ctypes.c_int
         _lib.oracle_compute_z.argtypes = [ctypes.POINTER(OParticles), ctypes.c_void_p, ctypes.POINTER(OScalars),
                                           ctypes.POINTER(ORomsFields)]
         _lib.oracle_trilinear.argtypes = [ctypes.POINTER(OF3), ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -200,7 +205,9 @@ class OracleROMS:
 
     ``fields`` maps the ROMS field names to numpy arrays: ``u, v, w, zeta`` with
     a leading time axis, ``h, dx, dy`` 2-D and ``C`` 1-D.  ``particles`` maps
-    particle-field names to arrays (copied).
+    particle-field names to arrays (copied).  Scheme "ab3_iso": the AB3
+    isopycnal follower (models/roms/__init__.py:109-141), with ``rho`` in place
+    of ``w``, the particle field ``rho_t`` and scalars ``w_max``, ``rho_scale``.
     """
 
     def __init__(
@@ -215,9 +222,13 @@ class OracleROMS:
         bounds: tuple[float, float, float, float, float, float] | None = None,
         time=None,
         staggers: Mapping[str, tuple[str, str, str]] = ROMS_STAGGERS,
+        w_max: float = 0.0,
+        rho_scale: float = 1.0,
     ) -> None:
-        if scheme not in ("rk2", "ab3"):
+        if scheme not in ("rk2", "ab3", "ab3_iso"):
             raise ValueError(scheme)
+        self.w_max = np.float64(w_max)
+        self.rho_scale = np.float64(rho_scale)
         self.scheme = scheme
         self.time_array = np.asarray(time_array)
         self.fields = dict(fields)
@@ -259,8 +270,10 @@ class OracleROMS:
         td = {}
         for name in TIME_DEPENDENT:
             if name in names:
-                data = self.fields[name]
-                td[name] = make_field(time_blend(data[It], data[It + 1], ft), active_offsets(self.staggers[name]))
+                # the isopycnal follower reads rho where the w-advection kernels read w
+                data = self.fields["rho" if (name == "w" and self.scheme == "ab3_iso") else name]
+                sname = "rho" if (name == "w" and self.scheme == "ab3_iso") else name
+                td[name] = make_field(time_blend(data[It], data[It + 1], ft), active_offsets(self.staggers[sname]))
             else:
                 td[name] = OF3() if name != "zeta" else OF2()
         f = ORomsFields(td["u"], td["v"], td["w"], self._static["dx"], self._static["dy"], self._static["h"],
@@ -308,6 +321,12 @@ class OracleROMS:
             self._check(L.oracle_rk2_step_2(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(tidx_int))))
             self.advance_time()
             L.oracle_rk2_update(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(self.tidx, ("zeta",))))
+        elif self.scheme == "ab3_iso":  # timesteppers.py:296-305 with the isopycnal kernels
+            self._check(L.oracle_ab3_isopycnal(ctypes.byref(op), ctypes.byref(sc),
+                                               ctypes.byref(self.fielddata(self.tidx)), _ptr(p["rho_t"]),
+                                               float(self.w_max), float(self.rho_scale)))
+            self.advance_time()
+            L.oracle_ab3_post(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(self.tidx, ("zeta",))))
         else:  # timesteppers.py:296-305
             self._check(L.oracle_ab3(ctypes.byref(op), ctypes.byref(sc), ctypes.byref(self.fielddata(self.tidx))))
             self.advance_time()
@@ -325,7 +344,8 @@ def particle_fields(scheme: str) -> tuple[str, ...]:
     base = ("status", "zidx", "yidx", "xidx", "z")
     if scheme == "rk2":
         return base + ("_dxidx1", "_dyidx1", "_dz1", "_dxidx2", "_dyidx2", "_dz2")
-    return base + ("_dz0", "_dz1", "_dz2", "_dyidx0", "_dyidx1", "_dyidx2", "_dxidx0", "_dxidx1", "_dxidx2")
+    ab3 = base + ("_dz0", "_dz1", "_dz2", "_dyidx0", "_dyidx1", "_dyidx2", "_dxidx0", "_dxidx1", "_dxidx2")
+    return ab3 + ("rho_t",) if scheme == "ab3_iso" else ab3
 
 
 def new_particles(n: int, scheme: str) -> dict[str, np.ndarray]:

@@ -13,21 +13,23 @@ STAGGERS = {
     "dx": ("invariant", "center", "center"),
     "dy": ("invariant", "center", "center"),
     "C": ("center", "invariant", "invariant"),
+    "rho": ("center", "center", "center"),
 }
 
 
-def b200_fieldset(fields: dict, hc: float, nz: int, ring_size: int = 4, storage: str | None = None):
+def b200_fieldset(fields: dict, hc: float, nz: int, ring_size: int = 4, storage: str | None = None,
+                  **constants):
     import offline_particles_b200 as opb
 
     nt, _, ny, nxu = fields["u"].shape
     kw = {}
     for name, arr in fields.items():
         st = STAGGERS[name]
-        if name in ("u", "v", "w", "zeta"):
+        if name in ("u", "v", "w", "zeta", "rho"):
             kw[name] = opb.TimeDependentField.from_numpy(arr, *st, ring_size=ring_size, storage=storage)
         else:
             kw[name] = opb.StaticField.from_numpy(arr, *st)
-    return opb.Fieldset(nt, nz, ny, nxu + 1, constants={"hc": hc, "NZ": nz}, **kw)
+    return opb.Fieldset(nt, nz, ny, nxu + 1, constants={"hc": hc, "NZ": nz, **constants}, **kw)
 
 
 def build_sim(fields, *, hc, nz, scheme, dt, z, y, x, status=None, unfused=False, ring_size=4, time=None,

@@ -27,6 +27,9 @@ ab3_f32.npz        AB3 on a 96x80x16 float32 grid, 6 snapshots, 4096 particles,
 edge_cases.npz     NaN land, inactive / out-of-domain / non-finite particles,
                    steps that land exactly on snapshot times, RK2 and AB3.
 zero_division.json the reference's error for a zero grid spacing.
+iso_f32.npz        the AB3 isopycnal follower (ab3_isopycnal_following.pyx) on a
+                   96x80x16 float32 grid with a synthetic density field,
+                   4096 particles with target densities, dt=120 s, 149 steps.
 """
 
 from __future__ import annotations
@@ -55,7 +58,12 @@ STAGGERS = {
     "dx": ("invariant", "center", "center"),
     "dy": ("invariant", "center", "center"),
     "C": ("center", "invariant", "invariant"),
+    "rho": ("center", "center", "center"),
 }
+
+# the isopycnal follower (models/roms/__init__.py:109-141): AB3 with dz from density
+ISO_CASE = dict(grid=GridSpec(nx=96, ny=80, nz=16, nt=6, seed=13, dtype="float32"), n=4096, dt=120.0, steps=149,
+                record_every=30, record_n=256, w_max=2.0e-3, rho_scale=0.05)
 
 CASES = {
     "config1_rk2": dict(grid=GridSpec(nx=128, ny=96, nz=20, nt=26, seed=1, dtype="float64"),
@@ -76,16 +84,54 @@ def fingerprint(fields: dict[str, np.ndarray]) -> str:
     return h.hexdigest()
 
 
-def ref_fieldset(op, fields: dict[str, np.ndarray], hc: float, nz: int):
+def ref_fieldset(op, fields: dict[str, np.ndarray], hc: float, nz: int, **constants):
     nt, _, ny, nxu = fields["u"].shape
     kw = {}
     for name, arr in fields.items():
         st = STAGGERS[name]
-        if name in ("u", "v", "w", "zeta"):
+        if name in ("u", "v", "w", "zeta", "rho"):
             kw[name] = op.TimeDependentField.from_numpy(arr, *st)
         else:
             kw[name] = op.StaticField.from_numpy(arr, *st)
-    return op.Fieldset(nt, nz, ny, nxu + 1, constants={"hc": hc, "NZ": nz}, **kw)
+    return op.Fieldset(nt, nz, ny, nxu + 1, constants={"hc": hc, "NZ": nz, **constants}, **kw)
+
+
+def iso_inputs(c):
+    """Fields (rho in place of w), release and target densities of the isopycnal case."""
+    g = SyntheticROMS(c["grid"])
+    fields = g.oracle_fields()
+    del fields["w"]
+    fields["rho"] = g.density()
+    z, y, x = g.release(c["n"])
+    rng = np.random.default_rng(17)
+    rho_t = 1026.5 - 1.5 * rng.uniform(0.0, 1.0, c["n"])
+    return g, fields, z, y, x, rho_t
+
+
+def make_isopycnal(op) -> None:
+    from offline_particles.models.roms import ab3_isopycnal_following_timestepper
+
+    c = ISO_CASE
+    g, fields, z, y, x, rho_t = iso_inputs(c)
+    t_arr = np.arange(fields["u"].shape[0], dtype=np.float64) * 3600.0
+    fs = ref_fieldset(op, fields, g.hc, g.spec.nz, w_max=c["w_max"], rho_scale=c["rho_scale"])
+    ts = ab3_isopycnal_following_timestepper(t_arr, np.float64(c["dt"]))
+    sim = op.SimulationBuilder(ts, fs).build_simulation(len(z))
+    sim.set_indices(z, y, x)
+    sim.set_particle_field("status", 10)
+    sim.set_particle_field("rho_t", rho_t)
+    ridx = np.sort(np.random.default_rng(5).choice(c["n"], c["record_n"], replace=False))
+    rec = []
+    for k in range(c["steps"]):
+        sim.step()
+        if (k + 1) % c["record_every"] == 0:
+            P = sim.particles
+            rec.append(np.stack([np.asarray(P[n])[ridx] for n in ("zidx", "yidx", "xidx")]))
+    P = sim.particles
+    final = {name: np.array(P[name]) for name in P.arrays}
+    np.savez_compressed(HERE / "iso_f32.npz", fingerprint=fingerprint(fields), z0=z, y0=y, x0=x, rho_t0=rho_t,
+                        record_idx=ridx, record=np.stack(rec), **final)
+    print("iso_f32 status", np.unique(final["status"], return_counts=True))
 
 
 def run_reference(op, fields, *, hc, nz, scheme, dt, steps, z, y, x, status=None, record_every=0, record_idx=None,
@@ -311,6 +357,7 @@ def main() -> None:
     make_workloads(op)
     make_edge_cases(op)
     make_zero_division(op)
+    make_isopycnal(op)
     for p in sorted(HERE.glob("*.npz")) + sorted(HERE.glob("*.json")):
         print(p.name, p.stat().st_size)
 

@@ -108,3 +108,22 @@ EDGE_KEYS = [(d, s, nl) for d in ("float64", "float32") for s in ("rk2", "ab3") 
 
 def edge_key(dtype: str, scheme: str, nan_land: bool) -> str:
     return f"{dtype}_{scheme}_{'nanland' if nan_land else 'plain'}"
+
+
+# The isopycnal-follower fixture (tests/golden/make_golden.py: ISO_CASE, iso_inputs).
+def iso_case():
+    from offline_particles_b200.synth import GridSpec
+
+    return dict(grid=GridSpec(nx=96, ny=80, nz=16, nt=6, seed=13, dtype="float32"), n=4096, dt=120.0, steps=149,
+                record_every=30, record_n=256, w_max=2.0e-3, rho_scale=0.05)
+
+
+def iso_fields():
+    """The case's grid and fields: the synthetic ROMS fields with the density field in place of w."""
+    from offline_particles_b200.synth import SyntheticROMS
+
+    g = SyntheticROMS(iso_case()["grid"])
+    fields = g.oracle_fields()
+    del fields["w"]
+    fields["rho"] = g.density()
+    return g, fields

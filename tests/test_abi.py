@@ -51,7 +51,9 @@ int main(void) {
     S(opb_roms_fields); F(opb_roms_fields, zeta); F(opb_roms_fields, C);
     S(opb_time); F(opb_time, ft); F(opb_time, gt);
     S(opb_particles); F(opb_particles, status); F(opb_particles, z); F(opb_particles, dz2); F(opb_particles, err);
+    F(opb_particles, rho_t);
     S(opb_scalars); F(opb_scalars, NZ); F(opb_scalars, dt); F(opb_scalars, alpha); F(opb_scalars, bounds);
+    F(opb_scalars, w_max); F(opb_scalars, rho_scale);
     S(opb_experiment); F(opb_experiment, count); F(opb_experiment, first_chunk); F(opb_experiment, scheme);
     F(opb_experiment, nsteps); F(opb_experiment, table_offset); F(opb_experiment, validate);
     F(opb_experiment, dt); F(opb_experiment, alpha);
@@ -120,6 +122,13 @@ def test_argument_errors_need_no_gpu():
     t.next = 5
     rc = lib.opb_rk2_w_advection_step_1(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), ctypes.byref(t), None)
     assert rc == _lib.EINVAL and b"slot out of range" in lib.opb_last_error()
+    # the isopycnal follower needs the particles' target density
+    t.next = 1
+    p.dxidx0 = p.dyidx0 = p.dz0 = p.dxidx2 = p.dyidx2 = p.dz2 = 16
+    rc = lib.opb_ab3_isopycnal_following(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), ctypes.byref(t), None)
+    assert rc == _lib.EINVAL and b"rho_t" in lib.opb_last_error()
+    rc = lib.opb_ab3_isopycnal_following_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"rho_t" in lib.opb_last_error()
 
 
 def test_call_raises_value_error():

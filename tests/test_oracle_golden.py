@@ -121,3 +121,28 @@ def test_cannot_step_onto_last_snapshot():
     orc.step(p)
     with pytest.raises(IndexError):
         orc.step(p)
+
+
+def test_isopycnal_follower_matches_reference():
+    """ab3_isopycnal_following_timestepper (models/roms/__init__.py:109-141) restated: bit for bit."""
+    from helpers import iso_case, iso_fields
+
+    c = iso_case()
+    gold = load("iso_f32.npz")
+    g, fields = iso_fields()
+    assert fingerprint(fields) == str(gold["fingerprint"]), "synthetic inputs drifted from the fixture"
+    orc = O.OracleROMS(g.time_array, fields, hc=g.hc, scheme="ab3_iso", dt=np.float64(c["dt"]), w_max=c["w_max"],
+                       rho_scale=c["rho_scale"])
+    p = O.new_particles(c["n"], "ab3_iso")
+    p["zidx"][:], p["yidx"][:], p["xidx"][:] = gold["z0"], gold["y0"], gold["x0"]
+    p["rho_t"][:] = gold["rho_t0"]
+    p["status"][:] = O.MULTISTEP_1
+    ridx = gold["record_idx"]
+    rec = []
+    for k in range(c["steps"]):
+        orc.step(p)
+        if (k + 1) % c["record_every"] == 0:
+            rec.append(np.stack([p[n][ridx] for n in ("zidx", "yidx", "xidx")]))
+    assert same_bits(np.stack(rec), gold["record"]), mismatch_report(np.stack(rec), gold["record"])
+    for name in ("status", "zidx", "yidx", "xidx", "z", "_dz0", "_dz1", "_dz2", "_dxidx1", "_dyidx2"):
+        assert same_bits(p[name], gold[name]), f"{name}: {mismatch_report(p[name], gold[name])}"
