@@ -7,7 +7,7 @@ same Python API over hand-written sm_100a CUDA kernels reached through a C ABI
 (include/opb200.h).  There is no CPU fallback.
 """
 
-from . import kernels
+from . import kernels, output
 from .events import Event, SimulationState
 from .fields import BlendedArray, FieldData, StaticField, TimeDependentField
 from .fieldset import Fieldset
@@ -33,6 +33,7 @@ __all__ = [
     "DeviceArray",
     "NumpyArray",
     "kernels",
+    "output",
     "roms",
 ]
 

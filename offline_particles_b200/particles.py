@@ -224,6 +224,14 @@ class ParticlesView:
         """The device tensor of a particle field in STORAGE order (no copy; do not modify)."""
         return object.__getattribute__(self, "_parent").arrays[name]
 
+    def device_original(self, name: str) -> torch.Tensor:
+        """A device copy of a particle field in ORIGINAL order, queued on the current stream (no
+        synchronisation, no error check: for asynchronous readers such as output writers)."""
+        parent = object.__getattribute__(self, "_parent")
+        if name not in parent:
+            raise KeyError(name)
+        return parent.original(name)
+
     @property
     def arrays(self) -> Mapping:
         return object.__getattribute__(self, "_parent").arrays

@@ -201,6 +201,17 @@ class Simulation:
         torch.cuda.synchronize(self._particles.device)
         self._particles.check_errors()
 
+    @property
+    def output_writers(self) -> Mapping[str, object]:
+        return self._output_writers
+
+    def close_outputs(self) -> None:
+        """Finish every output writer that buffers rows (files complete on disk)."""
+        for w in self._output_writers.values():
+            close = getattr(w, "close", None)
+            if close is not None:
+                close()
+
 
 class SimulationBuilder:
     """Builds a Simulation from a timestepper, a fieldset and events."""
@@ -242,12 +253,22 @@ class SimulationBuilder:
             raise ValueError("Either n or dt must be specified.")
 
     def add_output_writer(self, builder, *, n=None, dt=None, first=None) -> None:
-        """Output writers (zarr) are outside this package's scope."""
-        raise NotImplementedError("output writers are not part of offline_particles_b200")
+        """Add an output writer (simulation.py:320-342): its events fire every ``n`` iterations or ``dt``."""
+        name = builder.name
+        if name in self._output_writers:
+            raise ValueError(f"Output writer '{name}' already exists.")
+        self._output_writers[name] = (builder, {"n": n, "dt": dt, "first": first})
 
     def build_simulation(self, nparticles: int, *, device=None, sort_interval: int = DEFAULT_SORT_INTERVAL,
                          arithmetic: str = "float64") -> Simulation:
+        """Build the writers, schedule their events (simulation.py:344-369) and the Simulation."""
+        writers = {}
+        time_type = np.asarray(self._timestepper.time_array).dtype
+        for name, (builder, kwargs) in self._output_writers.items():
+            writers[name] = builder.build(nparticles, time_type)
+            for event in writers[name].create_events():
+                self.add_event(event, **kwargs)
         return Simulation(nparticles=nparticles, timestepper=self._timestepper, fieldset=self._fieldset,
                           iteration_scheduler=self._iteration_scheduler, time_scheduler=self._time_scheduler,
-                          output_writers=types.MappingProxyType({}), device=device, sort_interval=sort_interval,
+                          output_writers=types.MappingProxyType(writers), device=device, sort_interval=sort_interval,
                           arithmetic=arithmetic)

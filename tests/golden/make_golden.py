@@ -27,6 +27,8 @@ ab3_f32.npz        AB3 on a 96x80x16 float32 grid, 6 snapshots, 4096 particles,
 edge_cases.npz     NaN land, inactive / out-of-domain / non-finite particles,
                    steps that land exactly on snapshot times, RK2 and AB3.
 zero_division.json the reference's error for a zero grid spacing.
+outputs.npz        rows of the reference's output events: linearly_interpolate_fields
+                   (h, u, zeta, w) every 1800 s of an RK2 run, time and values.
 iso_f32.npz        the AB3 isopycnal follower (ab3_isopycnal_following.pyx) on a
                    96x80x16 float32 grid with a synthetic density field,
                    4096 particles with target densities, dt=120 s, 149 steps.
@@ -350,6 +352,74 @@ def make_zero_division(op) -> None:
     (HERE / "zero_division.json").write_text(json.dumps(result, indent=1) + "\n")
 
 
+OUTPUT_CASE = dict(grid=GridSpec(nx=48, ny=40, nz=8, nt=4, seed=41, dtype="float32"), n=512, dt=300.0, steps=24,
+                   every=1800.0, variables=("h", "u", "zeta", "w"))
+
+
+def make_outputs(op) -> None:
+    """Rows the reference's output events produce: linearly_interpolate_fields outputs written every
+    `every` seconds by an in-memory writer on the reference's own AbstractOutputWriter interface (the
+    reference's zarr writer needs zarr, which is absent)."""
+    from offline_particles.models.roms import rk2_w_advection_timestepper
+    from offline_particles.output import AbstractOutputWriter, AbstractOutputWriterBuilder, linearly_interpolate_fields
+
+    class MemoryWriter(AbstractOutputWriter):
+        def __init__(self, outputs):
+            self._outputs = outputs
+            self.times, self.rows = [], {k: [] for k in outputs}
+
+        name = "mem"
+        outputs = property(lambda self: self._outputs)
+
+        def write_time(self, state):
+            self.times.append(state.time)
+
+        def write_output(self, name, state):
+            self.rows[name].append(np.array(state.particles[self._outputs[name].particle_field]))
+
+        def finalise_write_round(self, state):
+            pass
+
+    class MemoryBuilder(AbstractOutputWriterBuilder):
+        name = "mem"
+
+        def __init__(self):
+            self._outputs = {}
+            self.writer = None
+
+        outputs = property(lambda self: self._outputs)
+
+        def add_output(self, *outputs, **kwargs):
+            for o in outputs:
+                self._outputs[o.name] = o
+
+        def remove_output(self, name):
+            del self._outputs[name]
+
+        def build(self, nparticles, time_type=np.dtype(np.float64)):
+            self.writer = MemoryWriter(dict(self._outputs))
+            return self.writer
+
+    c = OUTPUT_CASE
+    g = SyntheticROMS(c["grid"])
+    fields = g.oracle_fields()
+    fs = ref_fieldset(op, fields, g.hc, g.spec.nz)
+    t_arr = np.arange(fields["u"].shape[0], dtype=np.float64) * 3600.0
+    sb = op.SimulationBuilder(rk2_w_advection_timestepper(t_arr, np.float64(c["dt"])), fs)
+    mb = MemoryBuilder()
+    mb.add_output(*linearly_interpolate_fields(fs, *c["variables"]))
+    sb.add_output_writer(mb, dt=np.float64(c["every"]))
+    z, y, x = g.release(c["n"], seed=3)
+    sim = sb.build_simulation(c["n"])
+    sim.set_indices(z, y, x)
+    for _ in range(c["steps"]):
+        sim.step()
+    w = mb.writer
+    np.savez_compressed(HERE / "outputs.npz", fingerprint=fingerprint(fields), z0=z, y0=y, x0=x,
+                        time=np.array(w.times), **{f"out_{k}": np.stack(v) for k, v in w.rows.items()})
+    print("outputs rows", len(w.times), {k: np.stack(v).shape for k, v in w.rows.items()})
+
+
 def main() -> None:
     op = import_reference()
     make_interp_kat(op)
@@ -358,6 +428,7 @@ def main() -> None:
     make_edge_cases(op)
     make_zero_division(op)
     make_isopycnal(op)
+    make_outputs(op)
     for p in sorted(HERE.glob("*.npz")) + sorted(HERE.glob("*.json")):
         print(p.name, p.stat().st_size)
 

@@ -1,0 +1,67 @@
+"""Output writers on the GPU against the reference's own output rows (tests/golden/outputs.npz).
+
+linearly_interpolate_fields (h, u, zeta, w) written every 1800 s of an RK2 run
+(output/_linear_interpolation.py, output/_output.py, simulation.py:320-369 of
+the reference): the same events, kernels and row format, through
+NpyOutputBuilder; rows bit for bit, stepping one step at a time and with
+fused multi-step runs that the output events split.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import load, mismatch_report, same_bits
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("mode", ["step", "run"])
+def test_output_rows_match_reference(tmp_path, mode):
+    from b200_runner import b200_fieldset
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200.output import NpyOutputBuilder, linearly_interpolate_fields
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    gold = load("outputs.npz")
+    g = SyntheticROMS(GridSpec(nx=48, ny=40, nz=8, nt=4, seed=41, dtype="float32"))
+    fields = g.oracle_fields()
+    fs = b200_fieldset(fields, g.hc, g.spec.nz)
+    t_arr = np.arange(fields["u"].shape[0], dtype=np.float64) * 3600.0
+    sb = opb.SimulationBuilder(opb.roms.rk2_w_advection_timestepper(t_arr, np.float64(300.0)), fs)
+    ob = NpyOutputBuilder("npy", tmp_path / "out")
+    ob.add_output(*linearly_interpolate_fields(fs, "h", "u", "zeta", "w"))
+    sb.add_output_writer(ob, dt=np.float64(1800.0))
+    sim = sb.build_simulation(512)
+    sim.set_indices(gold["z0"], gold["y0"], gold["x0"])
+    if mode == "step":
+        for _ in range(24):
+            sim.step()
+    else:
+        sim.run(24)
+    sim.synchronize()
+    sim.close_outputs()
+    out = tmp_path / "out"
+    assert same_bits(np.load(out / "time.npy"), gold["time"])
+    for name in ("h", "u", "zeta", "w"):
+        got = np.load(out / f"{name}.npy")
+        assert got.shape == gold[f"out_{name}"].shape
+        assert same_bits(got, gold[f"out_{name}"]), f"{name}: {mismatch_report(got, gold[f'out_{name}'])}"
+
+
+def test_output_writer_errors(tmp_path):
+    from offline_particles_b200.kernels.validation import validation_kernel
+    from offline_particles_b200.output import NpyOutputBuilder, Output
+
+    with pytest.raises(ValueError, match="not found"):
+        Output("nope", validation_kernel)
+    ob = NpyOutputBuilder("npy", tmp_path)
+    o = Output("zidx", validation_kernel)
+    ob.add_output(o)
+    with pytest.raises(KeyError):
+        ob.add_output(o)
+    ob.remove_output("zidx")
+    with pytest.raises(KeyError):
+        ob.remove_output("zidx")
