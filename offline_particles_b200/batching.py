@@ -163,6 +163,7 @@ class Release:
     status: int | np.ndarray | None = None
     name: str | None = None
     # filled in by the batch
+    records: list = field(default_factory=list, init=False, repr=False)  # (model time, Collected) rows
     start: int = field(default=-1, init=False)
     slot: int = field(default=-1, init=False)
     done: int = field(default=0, init=False)
@@ -201,6 +202,17 @@ class Release:
     @property
     def particle_steps(self) -> int:
         return len(self) * self.nsteps
+
+    def trajectory(self) -> dict[str, np.ndarray]:
+        """The recorded rows (``ReleaseBatch(record_every=...)``): ``time`` (rounds,) and each recorded
+        field (rounds, particles) in the release's original particle order."""
+        if not self.records:
+            return {"time": np.zeros(0)}
+        rows = [c.result() for _, c in self.records]
+        out = {"time": np.array([t for t, _ in self.records])}
+        for k in rows[0]:
+            out[k] = np.stack([r[k] for r in rows])
+        return out
 
 
 class SegmentAllocator:
@@ -287,12 +299,21 @@ class ReleaseBatch:
     sharing a region share its field data in L2.  The launches read the
     time-dependent fields as snapshot pairs (two consecutive snapshots
     interleaved element by element), one load per stencil corner.
+    ``record_every``: every that many snapshot intervals (at the interval
+    boundaries the launches replay on, so output never splits a launch),
+    copy ``record_fields`` of every running release to pinned host memory,
+    asynchronously; ``Release.trajectory()`` returns the rows.
     """
 
     def __init__(self, fieldset: Fieldset, releases: list[Release] = (), *, time_array=None,
                  capacity: int | None = None, max_releases: int | None = None, device=None, block: int = 256,
                  warps_per_sm: int = 16, ctas: int = 0, sort_interval: int = 4, graphs: bool = True,
-                 buckets: int = 256, split_schemes: bool = True) -> None:
+                 buckets: int = 256, split_schemes: bool = True, record_every: int = 0,
+                 record_fields=("zidx", "yidx", "xidx", "status")) -> None:
+        if record_every < 0:
+            raise ValueError("record_every must be non-negative")
+        self.record_every = int(record_every)
+        self.record_fields = tuple(record_fields)
         if buckets < 0 or (buckets & (buckets - 1)) or buckets > 65536:
             raise ValueError("buckets must be 0 or a power of two up to 65536")
         self.buckets = int(buckets)
@@ -641,6 +662,12 @@ class ReleaseBatch:
             for f in self._td.values():
                 f.mark_used(window)
                 f.prefetch(j + 3, set(window[1:]))
+        if self.record_every and (j + 1) % self.record_every == 0:
+            for r in self.releases:
+                if r.done and (r.done < r.nsteps or not r.reported) and r.error is None:
+                    if r.records and r.records[-1][0] == r.time:
+                        continue  # already recorded at this model time
+                    r.records.append((r.time, self.collect(r, self.record_fields)))
         return self._report()
 
     def step_interval(self) -> bool:

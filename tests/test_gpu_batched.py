@@ -240,3 +240,34 @@ def test_interleave_pairs_matches_torch(dtype, n, offset):
               _lib.F32 if dtype == "float32" else _lib.F64, None)
     torch.cuda.synchronize()
     assert torch.equal(out.view(-1, 2), torch.stack((a, b), dim=1))
+
+
+def test_batch_records_trajectories_like_a_simulation(grid):
+    """Rows recorded every 2 snapshot intervals equal a Simulation run alone read at the same model times."""
+    from b200_runner import b200_fieldset
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200.batching import Release, ReleaseBatch
+
+    g, fields = grid
+    t_arr = g.time_array[:fields["u"].shape[0]]
+    z, y, x = g.release(1500, seed=44)
+    specs = [("ab3", 180.0, 0.0, 150), ("rk2", 300.0, 3600.0, 70)]
+    rels = [Release(_stepper(s, t_arr, dt, t0), n, z, y, x) for s, dt, t0, n in specs]
+    b = ReleaseBatch(b200_fieldset(fields, g.hc, g.spec.nz), rels, record_every=2)
+    b.run()
+    b.synchronize()
+    for (scheme, dt, t0, nsteps), r in zip(specs, rels):
+        tr = r.trajectory()
+        assert len(tr["time"]) >= 2
+        sim = opb.SimulationBuilder(_stepper(scheme, t_arr, dt, t0),
+                                    b200_fieldset(fields, g.hc, g.spec.nz)).build_simulation(len(z))
+        sim.set_indices(z, y, x)
+        sim.set_particle_field("status", 10 if scheme == "ab3" else 0)
+        for q, t in enumerate(tr["time"]):
+            steps = int(round((t - t0) / dt)) - sim.iteration
+            sim.run(steps)
+            assert sim.time == t
+            P = sim.particles
+            for k in ("zidx", "yidx", "xidx", "status"):
+                assert same_bits(tr[k][q], P[k]), (scheme, q, k)

@@ -65,3 +65,41 @@ def test_output_writer_errors(tmp_path):
     ob.remove_output("zidx")
     with pytest.raises(KeyError):
         ob.remove_output("zidx")
+
+
+def test_simulation_from_roms_history_files(tmp_path):
+    """Fields streamed from NetCDF history files give the same particles as the same fields in memory."""
+    from b200_runner import STAGGERS
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200.roms_history import RomsHistory, write_history
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    g = SyntheticROMS(GridSpec(nx=64, ny=48, nz=10, nt=6, seed=61, dtype="float32"))
+    f = g.oracle_fields()
+    write_history(tmp_path / "a.nc", {**f, **{n: f[n][:4] for n in ("u", "v", "w", "zeta")}}, g.time_array[:4],
+                  hc=g.hc, mask_rho=g.mask_rho, fill_land=1e37)
+    write_history(tmp_path / "b.nc", {**f, **{n: f[n][4:] for n in ("u", "v", "w", "zeta")}}, g.time_array[4:],
+                  hc=g.hc, mask_rho=g.mask_rho, fill_land=1e37)
+    h = RomsHistory([tmp_path / "a.nc", tmp_path / "b.nc"])
+    z, y, x = g.release(2000, seed=8)
+    outs = []
+    for source in ("files", "memory"):
+        if source == "files":
+            fs = h.fieldset()
+        else:
+            kw = {n: opb.TimeDependentField.from_numpy(np.asarray(h.variable(n)), *STAGGERS[n])
+                  for n in ("u", "v", "w", "zeta")}
+            for n, arr in h.statics().items():
+                kw[n] = opb.StaticField.from_numpy(arr, *STAGGERS[n])
+            fs = opb.Fieldset(6, 10, 48, 64, constants={"hc": h.hc, "NZ": 10}, **kw)
+        ts = opb.roms.ab3_w_advection_timestepper(h.time_array, np.float64(120.0))
+        sim = opb.SimulationBuilder(ts, fs).build_simulation(len(z))
+        sim.set_indices(z, y, x)
+        sim.set_particle_field("status", 10)
+        sim.run(140)
+        P = sim.particles
+        outs.append({k: P[k] for k in ("status", "zidx", "yidx", "xidx", "z")})
+    h.close()
+    for k in outs[0]:
+        assert same_bits(outs[0][k], outs[1][k]), k
