@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--ny", type=int, default=768)
     ap.add_argument("--nz", type=int, default=50)
     ap.add_argument("--dt", type=float, default=120.0)
+    ap.add_argument("--ring-size", type=int, default=8, help="device snapshot slots of the end-to-end arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
     ap.add_argument("--study", choices=("precision", "batched", "serving"), default=None,
@@ -375,12 +376,12 @@ def b200_arm(a) -> None:
     h2d_gbs = 3 * probe.numel() * probe.element_size() / (hs.elapsed_time(he) * 1e-3) / 1e9
     del probe
     # untimed warm-up of the same path (allocator, ring, copy stream)
-    simw, _ = build_sim(grid, psrc, n, a, ring_size=4)
+    simw, _ = build_sim(grid, psrc, n, a, ring_size=a.ring_size)
     simw.set_indices(hz, hy, hx)
     simw.run(a.warmup)
     simw.synchronize()
     del simw
-    sim3, fs3 = build_sim(grid, psrc, n, a, ring_size=4)
+    sim3, fs3 = build_sim(grid, psrc, n, a, ring_size=a.ring_size)
     barrier(world)
     torch.cuda.synchronize()
     s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

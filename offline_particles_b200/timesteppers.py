@@ -360,14 +360,20 @@ def _upload_table(table, device) -> torch.Tensor:
 
 
 def _prefetch_after(td: dict[str, TimeDependentField], needed: list[int]) -> None:
-    """After a launch: mark its snapshots' slots as read by it, then start uploading the next snapshot."""
+    """After a launch: mark its snapshots' slots as read by it, then start uploading the snapshots that
+    follow into every slot the next launch does not need (the last two are kept): with a deeper ring the
+    host stream never waits for a launch to free a slot."""
     if not needed:
         return
     last = needed[-1]
     for f in td.values():
         f.mark_used(needed)
+        if not f.streamed:
+            continue
         keep = {needed[-2], last} if len(needed) > 1 else {last}
-        f.prefetch(last + 1, keep)
+        for j in range(1, max(1, f.ring_size - len(keep)) + 1):
+            keep.add(last + j)
+            f.prefetch(last + j, keep)
 
 
 class RK2Timestepper(Timestepper):
