@@ -83,10 +83,12 @@ __device__ __forceinline__ bool rk2_stage1(PState &s, const B &f, const DScalars
     const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
     const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
     const double dy = bilinear(f.dy, s.yidx + f.dy.o0, s.xidx + f.dy.o1);
+    // gathered before the check (pure reads): every stencil's loads are in flight together
+    const double w = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
     if (dx == 0.0 || dy == 0.0) return false;
     s.k1x = u / dx;
     s.k1y = v / dy;
-    s.k1z = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    s.k1z = w;
     return true;
 }
 
@@ -104,10 +106,11 @@ __device__ __forceinline__ bool rk2_stage2(PState &s, const B &f, const Levels &
     const double v = trilinear(f.v, z_idx + f.v.o0, y_int + f.v.o1, x_int + f.v.o2);
     const double dx = bilinear(f.dx, y_int + f.dx.o0, x_int + f.dx.o1);
     const double dy = bilinear(f.dy, y_int + f.dy.o0, x_int + f.dy.o1);
+    const double w = trilinear(f.w, z_idx + f.w.o0, y_int + f.w.o1, x_int + f.w.o2);
     if (dx == 0.0 || dy == 0.0) return false;
     s.k2x = u / dx;
     s.k2y = v / dy;
-    s.k2z = trilinear(f.w, z_idx + f.w.o0, y_int + f.w.o1, x_int + f.w.o2);
+    s.k2z = w;
     return true;
 }
 
@@ -134,19 +137,17 @@ __device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &
 // or the isopycnal follower's w_max * drho / (rho_scale + |drho|) with drho =
 // rho(x) - rho_t from the density field in the w slot
 // (ab3_isopycnal_following.pyx:124-132).  False on a zero divisor.
+// finish(g, k): g is the trilinear value of the w-slot field at the particle.
 struct WVel {
-    template <typename B>
-    __device__ __forceinline__ bool operator()(const B &f, const PState &s, double &k) const {
-        k = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    __device__ __forceinline__ bool finish(double g, double &k) const {
+        k = g;
         return true;
     }
 };
 
 struct IsoVel {
     double rho_t, w_max, rho_scale;
-    template <typename B>
-    __device__ __forceinline__ bool operator()(const B &f, const PState &s, double &k) const {
-        const double rho = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    __device__ __forceinline__ bool finish(double rho, double &k) const {
         const double drho = rho - rho_t;
         const double den = rho_scale + fabs(drho);
         if (den == 0.0) return false;
@@ -158,15 +159,18 @@ struct IsoVel {
 template <typename B, typename VZ = WVel>
 __device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false,
                                          const VZ &vz = VZ{}) {
+    // every gather first (pure reads, so their loads are in flight together), then the divisions and
+    // their zero checks in the reference's order: dx, dy, then the vertical velocity's
     const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
     const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
-    if (dx == 0.0) return false;
-    s.k0x = u / dx;
     const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
     const double dy = bilinear(f.dy, s.yidx + f.dy.o0, s.xidx + f.dy.o1);
+    const double wg = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    if (dx == 0.0) return false;
+    s.k0x = u / dx;
     if (dy == 0.0) return false;
     s.k0y = v / dy;
-    if (!vz(f, s, s.k0z)) return false;
+    if (!vz.finish(wg, s.k0z)) return false;
     if (s.status == ST_MULTISTEP_1) {  // ab3_w_advection.pyx:122-131
         s.k1x = s.k0x;
         s.k1y = s.k0y;
