@@ -398,6 +398,14 @@ class SnapshotRing:
     def resident(self) -> list[int]:
         return sorted(self.slot_of)
 
+    def is_ready(self, k: int) -> bool:
+        """Snapshot k is in its slot and its upload has completed."""
+        with self.lock:
+            if k not in self.slot_of or (k in self.pending and not self.pending[k].done()):
+                return False
+            ev = self.ready.get(k)
+        return ev is None or ev.query()
+
     def close(self) -> None:
         self.pool.shutdown(wait=True)
 
@@ -601,6 +609,10 @@ class TimeDependentField(Field):
     def prefetch(self, k: int, keep: set[int]) -> None:
         if self._ring is not None and 0 <= k < self._num_timesteps:
             self._ring.prefetch(k, keep)
+
+    def is_ready(self, k: int) -> bool:
+        """Snapshot k can be read without waiting for an upload (always, for a device-resident source)."""
+        return self._ring is None or self._ring.is_ready(k)
 
     def mark_used(self, ks) -> None:
         """Tell the ring that the launches queued so far are the last readers of snapshots ``ks``."""

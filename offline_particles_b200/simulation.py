@@ -186,7 +186,16 @@ class Simulation:
         return n
 
     def run(self, nsteps: int) -> None:
-        """Advance ``nsteps`` steps: fused multi-step launches between event firings."""
+        """Advance ``nsteps`` steps: fused multi-step launches between event firings.  Snapshots are
+        prefetched up to the last one these steps read (no uploads past the run's end)."""
+        ts = self._timestepper
+        ts._prefetch_limit = ts.snapshot_horizon(nsteps)
+        try:
+            self._run(nsteps)
+        finally:
+            ts._prefetch_limit = None
+
+    def _run(self, nsteps: int) -> None:
         done = 0
         while done < nsteps:
             k = min(self.steps_to_next_event(nsteps - done), self._maybe_sort())

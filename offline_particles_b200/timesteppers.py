@@ -157,6 +157,19 @@ class Timestepper(abc.ABC):
         """C-ABI field slot -> fieldset name, where the stepper's kernels read another field."""
         return {}
 
+    # last snapshot index worth prefetching (set by Simulation.run for its horizon; None: no limit)
+    _prefetch_limit: int | None = None
+
+    def snapshot_horizon(self, nsteps: int) -> int | None:
+        """The last snapshot index the next ``nsteps`` steps read (None when past the time array)."""
+        t = self._time
+        for _ in range(nsteps):
+            t = t + self.dt
+        try:
+            return int(divmod(self.get_time_index(t), 1)[0]) + 1
+        except (ValueError, IndexError):
+            return None
+
     def timestep_particles_many(self, particles, launcher: Launcher, nsteps: int) -> None:
         """Advance ``nsteps`` steps; fused launches where possible, else step by step."""
         if not self.fused():
@@ -170,10 +183,13 @@ class Timestepper(abc.ABC):
     def _fused_chunk(self, particles, launcher: Launcher, max_steps: int) -> int:
         """Plan and launch as many steps as fit in one fused launch; return the number taken."""
         td = _time_dependent_fields(launcher, self.field_roles)
-        # a streamed field keeps one ring slot free so the next snapshot uploads while this launch runs
-        capacity = min([_lib.MAX_SLOTS] + [max(2, f.ring_size - 1) if f.streamed else f.ring_size
+        # streamed fields: a launch spans at most one snapshot interval (3 snapshots) and a slot stays free,
+        # so each launch waits for at most one new upload and the next ones stream in while it runs (a launch
+        # spanning n intervals would first wait for all n + 2 uploads)
+        capacity = min([_lib.MAX_SLOTS] + [min(3, max(2, f.ring_size - 1)) if f.streamed else f.ring_size
                                            for f in td.values()])
         pairs = use_pairs(launcher, td, len(particles))
+        streamed = any(f.streamed for f in td.values())
         pair_capacity = min([_lib.MAX_SLOTS] + [f.pair_slots for f in td.values()])
         starts: set[int] = set()  # snapshot intervals the launch's stages read (one pair each)
         time = self._time
@@ -191,6 +207,15 @@ class Timestepper(abc.ABC):
                 break
             if pairs and len(starts | its) > pair_capacity:
                 break
+            # pipelining over streamed snapshots: a launch waits only for the uploads its first step waits
+            # for (and for one if that step waits for none), so compute starts as soon as they land and the
+            # next snapshots stream in behind it
+            if streamed:
+                pending = {k for k in more if not all(f.is_ready(k) for f in td.values())}
+                if not steps:
+                    allowed = max(1, len(pending))
+                elif len(pending) > allowed:
+                    break
             starts |= its
             needed = more
             steps.append(tidxs)
@@ -359,7 +384,7 @@ def _upload_table(table, device) -> torch.Tensor:
     return raw.to(device, non_blocking=True)
 
 
-def _prefetch_after(td: dict[str, TimeDependentField], needed: list[int]) -> None:
+def _prefetch_after(td: dict[str, TimeDependentField], needed: list[int], limit: int | None = None) -> None:
     """After a launch: mark its snapshots' slots as read by it, then start uploading the snapshots that
     follow into every slot the next launch does not need (the last two are kept): with a deeper ring the
     host stream never waits for a launch to free a slot."""
@@ -372,6 +397,8 @@ def _prefetch_after(td: dict[str, TimeDependentField], needed: list[int]) -> Non
             continue
         keep = {needed[-2], last} if len(needed) > 1 else {last}
         for j in range(1, max(1, f.ring_size - len(keep)) + 1):
+            if limit is not None and last + j > limit:
+                break  # past the snapshots the current run needs
             keep.add(last + j)
             f.prefetch(last + j, keep)
 
@@ -460,7 +487,7 @@ class RK2Timestepper(Timestepper):
                   ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
         _notify("after", len(steps))
-        _prefetch_after(td, needed)
+        _prefetch_after(td, needed, self._prefetch_limit)
 
 
 class ABTimestepper(Timestepper):
@@ -541,4 +568,4 @@ class ABTimestepper(Timestepper):
                   ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
         _notify("after", len(steps))
-        _prefetch_after(td, needed)
+        _prefetch_after(td, needed, self._prefetch_limit)
