@@ -12,7 +12,7 @@ from .events import Event, SimulationState
 from .fields import BlendedArray, FieldData, StaticField, TimeDependentField
 from .fieldset import Fieldset
 from .models import roms
-from .simulation import Simulation, SimulationBuilder
+from .simulation import Checkpoint, Simulation, SimulationBuilder, load_checkpoint
 from .spatial_arrays import DeviceArray, NumpyArray, Stagger
 from .timesteppers import ABTimestepper, RK2Timestepper, Timestepper
 
@@ -24,6 +24,8 @@ __all__ = [
     "Fieldset",
     "Simulation",
     "SimulationBuilder",
+    "Checkpoint",
+    "load_checkpoint",
     "Event",
     "SimulationState",
     "RK2Timestepper",

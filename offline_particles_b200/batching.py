@@ -643,6 +643,7 @@ class ReleaseBatch:
         exps, tidx_all = self._plan(j)
         self.interval = j + 1
         if exps:
+            torch.cuda.nvtx.range_push(f"opb interval {j}: {len(exps)} releases")
             window = list(range(j, min(j + 3, self.num_snapshots)))
             rf, dtype = window_fields(self.launcher, window, self._td)
             self._pair_fields(j, window, rf)
@@ -662,6 +663,7 @@ class ReleaseBatch:
             for f in self._td.values():
                 f.mark_used(window)
                 f.prefetch(j + 3, set(window[1:]))
+            torch.cuda.nvtx.range_pop()
         if self.record_every and (j + 1) % self.record_every == 0:
             for r in self.releases:
                 if r.done and (r.done < r.nsteps or not r.reported) and r.error is None:

@@ -229,6 +229,10 @@ def quantize_levels(src: torch.Tensor, dst: torch.Tensor, scales: torch.Tensor, 
               stream_handle(src.device))
 
 
+class SnapshotLoadError(RuntimeError):
+    """A snapshot could not be brought to the device: its source raised, or delivered nothing in time."""
+
+
 class SnapshotRing:
     """Device slots for the snapshots of one time-dependent field.
 
@@ -238,8 +242,9 @@ class SnapshotRing:
     """
 
     def __init__(self, source, spatial_shape: tuple[int, ...], np_dtype: np.dtype, nslots: int,
-                 device: torch.device, storage: torch.dtype | None = None) -> None:
+                 device: torch.device, storage: torch.dtype | None = None, load_timeout: float | None = 600.0) -> None:
         self.source = source
+        self.load_timeout = load_timeout
         self.np_dtype = np.dtype(np_dtype)
         self.device = device
         self.nslots = nslots
@@ -376,7 +381,21 @@ class SnapshotRing:
             # a launch that follows may read the slot and nobody may mark it: forget the last-use event
             self.last_use[self.slot_of[k]] = None
         if fut is not None:
-            fut.result()
+            try:
+                fut.result(timeout=self.load_timeout)
+            except concurrent.futures.TimeoutError:
+                with self.lock:
+                    self.pending[k] = fut  # still loading: a later acquire waits for it again
+                raise SnapshotLoadError(f"snapshot {k}: the source delivered nothing in {self.load_timeout} s") from None
+            except Exception as e:
+                with self.lock:  # forget the failed snapshot: a later acquire loads it again
+                    slot = self.slot_of.pop(k, None)
+                    if k in self.lru:
+                        self.lru.remove(k)
+                    self.ready.pop(k, None)
+                    if slot is not None:
+                        self.last_use.pop(slot, None)
+                raise SnapshotLoadError(f"snapshot {k}: the source raised {type(e).__name__}: {e}") from e
         ev = self.ready.get(k)
         if ev is not None:
             torch.cuda.current_stream(self.device).wait_event(ev)
@@ -421,13 +440,15 @@ class TimeDependentField(Field):
 
     def __init__(self, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
                  spatial_array_factory=None, output_dtype=np.float64, *, ring_size: int = 4, prefetch: int = 2,
-                 device=None, storage: str | None = None, ring: bool | None = None, pair_slots: int = 4) -> None:
+                 device=None, storage: str | None = None, ring: bool | None = None, pair_slots: int = 4,
+                 load_timeout: float | None = 600.0) -> None:
         """``storage``: keep the snapshots on the device as "bfloat16" or "float16" with one scale
         per level (the float32 steppers only); default: the source dtype.  ``ring``: stream the
         snapshots through a ring of ``ring_size`` device slots (default: yes, unless ``data`` is
         already a CUDA tensor, which is then read in place; ring=True copies such a source slot by
         slot, so that every launch reads the same slot addresses).  ``pair_slots``: how many snapshot
-        pairs (``pair``) are kept on the device."""
+        pairs (``pair``) are kept on the device.  ``load_timeout``: seconds a launch waits for a snapshot
+        from the source before ``SnapshotLoadError`` (None: no limit)."""
         super().__init__(Stagger(z_stagger), Stagger(y_stagger), Stagger(x_stagger))
         if data.ndim < 2:
             raise ValueError(
@@ -467,7 +488,7 @@ class TimeDependentField(Field):
             if ring_size < 2 or ring_size > 8:
                 raise ValueError("ring_size must be between 2 and 8")
             self._ring = SnapshotRing(data, self._spatial_shape, self._data_dtype, ring_size, self._device,
-                                      storage=self._storage)
+                                      storage=self._storage, load_timeout=load_timeout)
         self._It = 0
         if pair_slots < 2:
             raise ValueError("pair_slots must be at least 2")

@@ -39,6 +39,10 @@ from .fieldset import Fieldset
 from .models.roms import ab3_w_advection_timestepper, rk2_w_advection_timestepper
 
 
+class RequestCancelled(Exception):
+    """The request was withdrawn (``ReleaseServer.cancel``)."""
+
+
 @dataclass
 class ReleaseRequest:
     """A release to serve: ``zidx``/``yidx``/``xidx`` (float64 index-space positions), ``scheme``
@@ -102,6 +106,7 @@ class ReleaseServer:
         self.collecting: list[tuple[ReleaseRequest, Collected]] = []
         self.done: list[ReleaseRequest] = []
         self.rejected: list[ReleaseRequest] = []
+        self.cancelled: list[ReleaseRequest] = []
         self.ticks = 0
         # the segment sort's scratch for the whole arena, allocated up front so that admission never
         # has to find device memory
@@ -156,6 +161,23 @@ class ReleaseServer:
         if b.interval is None and n:
             b.interval = j
         return n
+
+    def cancel(self, req: ReleaseRequest) -> bool:
+        """Withdraw a request: from the queue, or from the device (its particles are dropped and its
+        segment freed at once; the launches already queued finish with it).  False when it has already
+        finished."""
+        queued = [q for q in self.queue if q is req]
+        if queued:
+            self.queue = collections.deque(q for q in self.queue if q is not req)
+        elif req.release is not None and id(req.release) in self.running:
+            self.running.pop(id(req.release))
+            self.batch.retire(req.release)
+        else:
+            return False
+        req.error = RequestCancelled(f"request {req.id} cancelled")
+        req.finished = time.perf_counter()
+        self.cancelled.append(req)
+        return True
 
     # ---------------------------------------------------------------- serving
     def _poll(self, wait: bool = False) -> None:

@@ -210,6 +210,26 @@ class Simulation:
         torch.cuda.synchronize(self._particles.device)
         self._particles.check_errors()
 
+    # ---------------------------------------------------------- checkpoint
+    def save_checkpoint(self, path) -> None:
+        """Write the particle arrays (every field, the AB3 history included, in original order), the time
+        and the iteration to ``path`` (.npz).  Resume with ``load_checkpoint`` and ``restore_particles`` on a
+        Simulation built with a timestepper at that time and iteration (the reference's manual restart:
+        ``Timestepper(time=..., iteration=...)``, ``set_particle_field``)."""
+        self.synchronize()
+        arrays = {f"p_{k}": self._particles.original(k).cpu().numpy() for k in self._particles.arrays}
+        np.savez(path, time=np.asarray(self.time), iteration=np.int64(self.iteration), **arrays)
+
+    def restore_particles(self, particles: Mapping[str, np.ndarray]) -> None:
+        """Set every particle field from ``particles`` (original order), e.g. ``load_checkpoint(...).particles``."""
+        missing = set(self._particles.arrays) - set(particles)
+        if missing:
+            raise KeyError(f"checkpoint lacks particle fields {sorted(missing)}")
+        for k, v in particles.items():
+            if k in self._particles.arrays:
+                self._particles.assign(k, torch.from_numpy(np.ascontiguousarray(v)))
+        self._steps_since_sort = None
+
     @property
     def output_writers(self) -> Mapping[str, object]:
         return self._output_writers
@@ -220,6 +240,22 @@ class Simulation:
             close = getattr(w, "close", None)
             if close is not None:
                 close()
+
+
+class Checkpoint:
+    """What ``Simulation.save_checkpoint`` wrote: ``time``, ``iteration`` and ``particles`` (name -> array)."""
+
+    def __init__(self, time, iteration: int, particles: dict[str, np.ndarray]) -> None:
+        self.time = time
+        self.iteration = iteration
+        self.particles = particles
+
+
+def load_checkpoint(path) -> Checkpoint:
+    with np.load(path) as z:
+        particles = {k[2:]: z[k] for k in z.files if k.startswith("p_")}
+        t = z["time"]
+        return Checkpoint(t[()] if t.ndim == 0 else t, int(z["iteration"]), particles)
 
 
 class SimulationBuilder:
