@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--nz", type=int, default=50)
     ap.add_argument("--dt", type=float, default=120.0)
     ap.add_argument("--ring-size", type=int, default=8, help="device snapshot slots of the end-to-end arm")
+    ap.add_argument("--layout", choices=("auto", "quads", "pairs", "plain"), default="auto",
+                    help="how the kernels read snapshots: auto (quads for float32 storage where pairs pay), "
+                         "quads, pairs, or plain snapshots")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
     ap.add_argument("--study", choices=("precision", "batched", "serving"), default=None,
@@ -304,6 +307,7 @@ def b200_arm(a) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import offline_particles_b200 as opb
+    from offline_particles_b200 import fields as fmod
     from offline_particles_b200 import particles as pmod
     from offline_particles_b200 import timesteppers
 
@@ -321,8 +325,10 @@ def b200_arm(a) -> None:
     sim.synchronize()
     timer = LaunchTimer()
     sorts = []
+    builds = []
     timesteppers.launch_observers.append(timer)
     pmod.sort_observers.append(lambda: sorts.append(1))
+    fmod.pair_observers.append(lambda: builds.append(1))
     barrier(world)
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
@@ -333,6 +339,7 @@ def b200_arm(a) -> None:
         torch.cuda.synchronize()
     timesteppers.launch_observers.remove(timer)
     pmod.sort_observers.clear()
+    fmod.pair_observers.clear()
     sim.synchronize()
     run_ms = dist_max(s.elapsed_time(e), world)
     launch_ms = timer.durations_ms()
@@ -447,8 +454,10 @@ def b200_arm(a) -> None:
                      "algorithmic_bytes_per_step": b_step, "bytes_per_particle_step": b_step / n,
                      "steps_per_launch": avg_launch_steps, "launch_ms": avg_launch_ms,
                      "kernel": "k_ab3_steps<float>"},
-        "gpu_launches": len(launch_ms) + 2 * len(sorts),
+        "gpu_launches": len(launch_ms) + 2 * len(sorts) + len(builds),
         "sorts_in_timed_region": len(sorts),
+        "pair_builds_in_timed_region": len(builds),
+        "snapshot_layout": a.layout,
         "active_particles_end": active,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
@@ -881,8 +890,21 @@ def serving_study(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+def set_layout(layout: str) -> None:
+    """The snapshot layout of every launch in this process (``--layout``)."""
+    from offline_particles_b200 import timesteppers
+
+    if layout == "quads":
+        timesteppers.SNAPSHOT_PAIRS, timesteppers.SNAPSHOT_QUADS = "always", True
+    elif layout == "pairs":
+        timesteppers.SNAPSHOT_PAIRS, timesteppers.SNAPSHOT_QUADS = "always", False
+    elif layout == "plain":
+        timesteppers.SNAPSHOT_PAIRS = "never"
+
+
 def main() -> None:
     a = parse()
+    set_layout(a.layout)
     if a.study == "precision":
         precision_study(a)
     elif a.study == "batched":

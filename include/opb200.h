@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define OPB_ABI_VERSION 4
+#define OPB_ABI_VERSION 5
 #define OPB_MAX_SLOTS 8
 
 /* storage dtypes of time-dependent fields (the float64-exact entry points take
@@ -55,6 +55,14 @@ extern "C" {
  * opb_time selects the pair with prev (next == prev) */
 #define OPB_F64_PAIRS 4
 #define OPB_F32_PAIRS 5
+/* snapshot quads (the same entry points, float32 storage): data[k] holds, for
+ * element i, the four floats {a[i], b[i], a[i+1], b[i+1]} of the earlier (a) and
+ * later (b) snapshot, so one 16-byte load fetches a stencil's two x-neighbouring
+ * corners with both values of their time blends.  Quads come with x-pairs of the
+ * static fields h, dx and dy (OPB_F64_XPAIRS; C stays OPB_F64) */
+#define OPB_F32_QUADS 6
+/* x-pairs of a static float64 field: data[0] holds {s[i], s[i+1]} for element i */
+#define OPB_F64_XPAIRS 7
 
 /* return codes */
 #define OPB_OK 0
@@ -177,6 +185,17 @@ int opb_ab3_isopycnal_following(const opb_particles *p, const opb_scalars *s, co
  * out[2i + 1] = b[i] for i < n, a/b/out DEVICE buffers of dtype OPB_F32 or
  * OPB_F64 (out holds 2n elements): the snapshot pair of snapshots a and b. */
 int opb_interleave_pairs(const void *a, const void *b, void *out, int64_t n, int32_t dtype, void *stream);
+
+/* No reference counterpart (a layout of this library): the snapshot quads of
+ * float32 snapshots a and b, out[4i .. 4i+3] = a[i], b[i], a[i+1], b[i+1] for
+ * i < n - 1 and a[n-1], b[n-1], a[n-1], b[n-1] for the last element (out holds
+ * 4n floats; DEVICE buffers, out 16-byte aligned). */
+int opb_interleave_quads(const float *a, const float *b, float *out, int64_t n, void *stream);
+
+/* No reference counterpart: the x-pairs of a static float64 field s,
+ * out[2i] = s[i], out[2i+1] = s[i+1] for i < n - 1 and s[n-1] twice for the last
+ * element (out holds 2n doubles; DEVICE buffers, out 16-byte aligned). */
+int opb_neighbour_pairs(const double *s, double *out, int64_t n, void *stream);
 
 /* ---- batched release experiments ---------------------------------------------
  * No single reference counterpart: the reference advances one release per

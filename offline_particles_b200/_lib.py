@@ -14,7 +14,8 @@ from ._build import LIB_PATH, build_library
 MAX_SLOTS = 8
 F64, F32, BF16, F16 = 0, 1, 2, 3
 F64_PAIRS, F32_PAIRS = 4, 5
-ABI_VERSION = 4
+F32_QUADS, F64_XPAIRS = 6, 7
+ABI_VERSION = 5
 OK, EINVAL, ECUDA = 0, 1, 2
 ERRF_ZERO_DIVISION = 1
 
@@ -110,6 +111,8 @@ SIGNATURES = {
     "opb_batched_steps": [_P(opb_particles), _VP, _VP, _P(opb_scalars), _P(opb_roms_fields), _VP, _VP, _VP,
                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _VP],
     "opb_interleave_pairs": [_VP, _VP, _VP, ctypes.c_int64, ctypes.c_int32, _VP],
+    "opb_interleave_quads": [_VP, _VP, _VP, ctypes.c_int64, _VP],
+    "opb_neighbour_pairs": [_VP, _VP, ctypes.c_int64, _VP],
     "opb_quantize_levels": [_VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP, _VP],
 }
 

@@ -5,6 +5,8 @@
 // bit-identical to the fused single-release steppers.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "opb200.h"
 #include "opb_device.cuh"
 #include "opb_errors.h"
@@ -16,10 +18,10 @@ namespace {
 
 // One particle of experiment E through E.nsteps steps of its scheme: the loop
 // bodies of k_rk2_steps / k_ab3_steps (opb_roms.cu) with E's dt, alpha and
-// time table, reading the time-dependent fields as snapshot pairs.
-// SCHEME: OPB_SCHEME_RK2 or OPB_SCHEME_AB3 compiles one scheme only (smaller
-// code, fewer live registers); 0 decides per experiment.
-template <typename T, typename I, int SCHEME>
+// time table, reading the time-dependent fields as snapshot pairs or quads
+// (LAYOUT).  SCHEME: OPB_SCHEME_RK2 or OPB_SCHEME_AB3 compiles one scheme only
+// (smaller code, fewer live registers); 0 decides per experiment.
+template <typename T, typename I, int SCHEME, int LAYOUT>
 __device__ __forceinline__ void batched_particle(const DParticles &p, long long i, const opb_experiment &E,
                                                  const DScalars &sc0, const DRoms &r, const opb_time *table,
                                                  const Levels &L) {
@@ -50,26 +52,26 @@ __device__ __forceinline__ void batched_particle(const DParticles &p, long long 
         if (ab3) {
             const opb_time t1 = tab[2 * k], t2 = tab[2 * k + 1];
             const bool reuse = k > 0 && same_time(t1, s.at);
-            if (!ab3_step(s, bind_all<T, I, true, true>(r, t1), sc, reuse)) {
+            if (!ab3_step(s, bind_all<T, I, true, LAYOUT>(r, t1), sc, reuse)) {
                 raise_zero_division(p);
                 break;
             }
             moved = true;
-            ab3_post(s, bind_all<T, I, true, true>(r, t2), L, sc);
+            ab3_post(s, bind_all<T, I, true, LAYOUT>(r, t2), L, sc);
             s.at = t2;
         } else {
             const opb_time t1 = tab[3 * k], t2 = tab[3 * k + 1], t3 = tab[3 * k + 2];
             const bool reuse = k > 0 && same_time(t1, s.at);
-            if (!rk2_stage1(s, bind_all<T, I, true, true>(r, t1), sc, reuse)) {
+            if (!rk2_stage1(s, bind_all<T, I, true, LAYOUT>(r, t1), sc, reuse)) {
                 raise_zero_division(p);
                 break;
             }
             moved = true;
-            if (!rk2_stage2(s, bind_all<T, I, true, true>(r, t2), L, sc)) {
+            if (!rk2_stage2(s, bind_all<T, I, true, LAYOUT>(r, t2), L, sc)) {
                 raise_zero_division(p);
                 break;
             }
-            rk2_update(s, bind_all<T, I, true, true>(r, t3), L, sc);
+            rk2_update(s, bind_all<T, I, true, LAYOUT>(r, t3), L, sc);
             s.at = t3;
         }
     }
@@ -157,7 +159,7 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan_items(opb_batch_header *_
 // one experiment's segment, so the 32 lanes of a warp share a scheme, a step
 // count and a time table and never diverge on them.  MINB CTAs of BLOCK
 // threads per SM: the register budget per thread is 65536 / (BLOCK * MINB).
-template <typename T, typename I, int BLOCK, int MINB, int SCHEME>
+template <typename T, typename I, int BLOCK, int MINB, int SCHEME, int LAYOUT>
 __global__ void __launch_bounds__(BLOCK, MINB) k_batched_steps(const __grid_constant__ DParticles p,
                                                             opb_batch_header *__restrict__ hdr,
                                                             const opb_experiment *__restrict__ exps,
@@ -208,12 +210,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_batched_steps(const __grid_cons
         if (i >= end || i < E.start || i >= E.start + E.count || E.nsteps <= 0) continue;
         if (i < 0 || i >= p.n) continue;
         if (SCHEME != 0 && E.scheme != SCHEME) continue;  // another launch's experiment
-        batched_particle<T, I, SCHEME>(p, i, E, sc, r, table, L);
+        batched_particle<T, I, SCHEME, LAYOUT>(p, i, E, sc, r, table, L);
     }
 }
 
 // launch the <BLOCK, MINB> instance; false if the shape is not compiled
-template <typename T, typename I, int SCHEME>
+template <typename T, typename I, int SCHEME, int LAYOUT>
 bool launch_batched(int block, int warps_per_sm, int ctas, cudaStream_t st, const DParticles &dp,
                     opb_batch_header *hdr, const opb_experiment *exps, const DScalars &ds, const DRoms &dr,
                     const opb_time *table, const int64_t *bounds, const int64_t *items, int *launched) {
@@ -228,10 +230,10 @@ bool launch_batched(int block, int warps_per_sm, int ctas, cudaStream_t st, cons
     // the combined kernel (SCHEME 0) only at 16 warps: its register budget already spills at 80
     if (SCHEME == 0 && warps_per_sm != 16) return false;
     switch (key) {
-        case 12816: return go(k_batched_steps<T, I, 128, 4, SCHEME>, 128);
-        case 25616: return go(k_batched_steps<T, I, 256, 2, SCHEME>, 256);
-        case 25624: return go(k_batched_steps<T, I, 256, 3, SCHEME != 0 ? SCHEME : OPB_SCHEME_RK2>, 256);
-        case 25632: return go(k_batched_steps<T, I, 256, 4, SCHEME != 0 ? SCHEME : OPB_SCHEME_RK2>, 256);
+        case 12816: return go(k_batched_steps<T, I, 128, 4, SCHEME, LAYOUT>, 128);
+        case 25616: return go(k_batched_steps<T, I, 256, 2, SCHEME, LAYOUT>, 256);
+        case 25624: return go(k_batched_steps<T, I, 256, 3, SCHEME != 0 ? SCHEME : OPB_SCHEME_RK2, LAYOUT>, 256);
+        case 25632: return go(k_batched_steps<T, I, 256, 4, SCHEME != 0 ? SCHEME : OPB_SCHEME_RK2, LAYOUT>, 256);
         default: return false;
     }
 }
@@ -255,13 +257,13 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
     if ((rc = convert_particles(p, dp, what, true))) return rc;
     if (!s) return fail(OPB_EINVAL, "%s: scalars is NULL", what);
     convert_scalars(s, ds);
-    // time-dependent fields come as snapshot pairs: check, then convert with the element dtype
+    // time-dependent fields come as snapshot pairs or quads: check, then convert with the element dtype
     opb_roms_fields g;
-    bool pairs = false;
-    if ((rc = unpair_fields(f, g, pairs, what))) return rc;
-    if (!pairs && !(g.u.is_static && g.v.is_static && g.w.is_static && g.zeta.is_static))
-        return fail(OPB_EINVAL, "%s: time-dependent fields must be snapshot pairs (OPB_F32_PAIRS or OPB_F64_PAIRS)",
-                    what);
+    int layout = LAYOUT_PLAIN;
+    if ((rc = unpair_fields(f, g, layout, what))) return rc;
+    if (layout == LAYOUT_PLAIN && !(g.u.is_static && g.v.is_static && g.w.is_static && g.zeta.is_static))
+        return fail(OPB_EINVAL, "%s: time-dependent fields must be snapshot pairs (OPB_F32_PAIRS or OPB_F64_PAIRS) "
+                    "or quads (OPB_F32_QUADS)", what);
     if ((rc = convert_fields(&g, dr, what, true, &dtype))) return rc;
     if (!header || !experiments || !table) return fail(OPB_EINVAL, "%s: NULL device array", what);
     const bool shape_ok = (block == 128 && warps_per_sm == 16) ||
@@ -293,19 +295,28 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
         if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     }
     int launched = 0;
-    dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {
+    auto go = [&](auto tv, auto iv, auto lv) {
         using T = decltype(tv);
         using I = decltype(iv);
+        constexpr int LAYOUT = decltype(lv)::value;
         if (scheme == OPB_SCHEME_RK2)
-            launch_batched<T, I, OPB_SCHEME_RK2>(block, warps_per_sm, ctas, st, dp, header, experiments, ds, dr, table,
-                                                 bucket_bounds, item_scratch, &launched);
+            launch_batched<T, I, OPB_SCHEME_RK2, LAYOUT>(block, warps_per_sm, ctas, st, dp, header, experiments, ds,
+                                                         dr, table, bucket_bounds, item_scratch, &launched);
         else if (scheme == OPB_SCHEME_AB3)
-            launch_batched<T, I, OPB_SCHEME_AB3>(block, warps_per_sm, ctas, st, dp, header, experiments, ds, dr, table,
-                                                 bucket_bounds, item_scratch, &launched);
+            launch_batched<T, I, OPB_SCHEME_AB3, LAYOUT>(block, warps_per_sm, ctas, st, dp, header, experiments, ds,
+                                                         dr, table, bucket_bounds, item_scratch, &launched);
         else
-            launch_batched<T, I, 0>(block, warps_per_sm, ctas, st, dp, header, experiments, ds, dr, table,
-                                    bucket_bounds, item_scratch, &launched);
-    });
+            launch_batched<T, I, 0, LAYOUT>(block, warps_per_sm, ctas, st, dp, header, experiments, ds, dr, table,
+                                            bucket_bounds, item_scratch, &launched);
+    };
+    if (layout == LAYOUT_QUADS) {
+        if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads hold float32 storage", what);
+        if (fits_int(dr)) go(float{}, int{}, std::integral_constant<int, LAYOUT_QUADS>{});
+        else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_QUADS>{});
+    } else {
+        // snapshot pairs (roms_layout above rules out the all-static fields that passed the layout check)
+        dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) { go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{}); });
+    }
     if (!launched) return fail(OPB_ECUDA, "%s: occupancy query failed", what);
     return check_launch(what);
 }

@@ -63,7 +63,16 @@ struct DScalars {
 // time-dependent; h, dx, dy, C static).
 // KIND_PAIRS: time-dependent, both snapshots of the blend interleaved in one
 // buffer (element 2i earlier, 2i+1 later): one 8- or 16-byte load per corner.
-constexpr int KIND_ANY = 0, KIND_STATIC = 1, KIND_TD = 2, KIND_PAIRS = 3;
+// KIND_QUADS (float32 storage): time-dependent, element i holds {earlier[i],
+// later[i], earlier[i+1], later[i+1]}: a stencil's two x-neighbouring corners
+// with both snapshots of their blends in one 16-byte load.
+// KIND_XPAIRS: static float64, element i holds {s[i], s[i+1]}: the two
+// x-neighbouring corners in one 16-byte load.
+constexpr int KIND_ANY = 0, KIND_STATIC = 1, KIND_TD = 2, KIND_PAIRS = 3, KIND_QUADS = 4, KIND_XPAIRS = 5;
+
+// How a launch reads its fields: plain snapshots, snapshot pairs, or snapshot
+// quads with x-pairs of the static fields h, dx, dy.
+constexpr int LAYOUT_PLAIN = 0, LAYOUT_PAIRS = 1, LAYOUT_QUADS = 2;
 
 template <typename T>
 struct Vec2;
@@ -79,6 +88,7 @@ struct Vec2<double> {
 template <typename T, typename I, int KIND = KIND_ANY>
 struct View {
     using index_type = I;
+    static_assert(KIND != KIND_QUADS || sizeof(T) == 4, "snapshot quads hold float32 storage");
     const T *prev;
     const T *next;
     const double *stat;  // non-null: static float64 field
@@ -89,17 +99,41 @@ struct View {
     // fields.py:423-428: both products and their sum in the storage dtype,
     // then widened to float64 (np.add(..., out=float64, casting="unsafe")
     // adds in the inputs' dtype).
+    __device__ __forceinline__ double blend(T a, T b) const {
+        const T x = a * gt;
+        const T y = b * ft;
+        return (double)(x + y);
+    }
+
     __device__ __forceinline__ double at(I i) const {
-        if (KIND == KIND_STATIC || (KIND == KIND_ANY && stat)) return __ldg(stat + i);
-        if constexpr (KIND == KIND_PAIRS) {
+        if constexpr (KIND == KIND_XPAIRS) {
+            return __ldg(stat + 2 * (long long)i);
+        } else if constexpr (KIND == KIND_QUADS) {
+            const float2 v = __ldg((const float2 *)prev + 2 * (long long)i);
+            return blend(v.x, v.y);
+        } else if constexpr (KIND == KIND_PAIRS) {
             const typename Vec2<T>::type v = __ldg((const typename Vec2<T>::type *)prev + i);
-            const T a = v.x * gt;
-            const T b = v.y * ft;
-            return (double)(a + b);
+            return blend(v.x, v.y);
         } else {
-            const T a = __ldg(prev + i) * gt;
-            const T b = __ldg(next + i) * ft;
-            return (double)(a + b);
+            if (KIND == KIND_STATIC || (KIND == KIND_ANY && stat)) return __ldg(stat + i);
+            return blend(__ldg(prev + i), __ldg(next + i));
+        }
+    }
+
+    // the values at i and i + 1 (x-neighbours: i + 1 stays in i's row for every
+    // stencil, whose lowest corner index is clamped to n - 2)
+    __device__ __forceinline__ void at2(I i, double &lo, double &hi) const {
+        if constexpr (KIND == KIND_XPAIRS) {
+            const double2 v = __ldg((const double2 *)stat + i);
+            lo = v.x;
+            hi = v.y;
+        } else if constexpr (KIND == KIND_QUADS) {
+            const float4 v = __ldg((const float4 *)prev + i);
+            lo = blend(v.x, v.y);
+            hi = blend(v.z, v.w);
+        } else {
+            lo = at(i);
+            hi = at(i + 1);
         }
     }
 };
@@ -155,7 +189,9 @@ __device__ __forceinline__ double linear(const F &f, double idx) {
     const I I0 = trunc_index(idx, (I)(f.n0 - 2));
     const double f0 = idx - (double)I0;
     const double g0 = 1.0 - f0;
-    return g0 * f.at(I0) + f0 * f.at(I0 + 1);
+    double v0, v1;
+    f.at2(I0, v0, v1);
+    return g0 * v0 + f0 * v1;
 }
 
 // linear.pxd:19-33
@@ -169,10 +205,9 @@ __device__ __forceinline__ double bilinear(const F &f, double idx0, double idx1)
     const double g0 = 1.0 - f0;
     const double g1 = 1.0 - f1;
     const I b = I0 * f.n1 + I1;
-    const double v00 = f.at(b);
-    const double v01 = f.at(b + 1);
-    const double v10 = f.at(b + f.n1);
-    const double v11 = f.at(b + f.n1 + 1);
+    double v00, v01, v10, v11;
+    f.at2(b, v00, v01);
+    f.at2(b + f.n1, v10, v11);
     return g0 * g1 * v00 + g0 * f1 * v01 + f0 * g1 * v10 + f0 * f1 * v11;
 }
 
@@ -192,14 +227,11 @@ __device__ __forceinline__ double trilinear(const F &f, double idx0, double idx1
     const I s1 = f.n2;
     const I s0 = f.n1 * f.n2;
     const I b = I0 * s0 + I1 * s1 + I2;
-    const double v000 = f.at(b);
-    const double v001 = f.at(b + 1);
-    const double v010 = f.at(b + s1);
-    const double v011 = f.at(b + s1 + 1);
-    const double v100 = f.at(b + s0);
-    const double v101 = f.at(b + s0 + 1);
-    const double v110 = f.at(b + s0 + s1);
-    const double v111 = f.at(b + s0 + s1 + 1);
+    double v000, v001, v010, v011, v100, v101, v110, v111;
+    f.at2(b, v000, v001);
+    f.at2(b + s1, v010, v011);
+    f.at2(b + s0, v100, v101);
+    f.at2(b + s0 + s1, v110, v111);
     return (g0 * g1 * g2 * v000 +
             g0 * g1 * f2 * v001 +
             g0 * f1 * g2 * v010 +

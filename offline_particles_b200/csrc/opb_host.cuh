@@ -194,23 +194,37 @@ int stage_common(const char *what, const opb_particles *p, const opb_scalars *s,
     return OPB_OK;
 }
 
-// Time-dependent fields may come as snapshot pairs (OPB_F32_PAIRS / OPB_F64_PAIRS): `out` is `in`
-// with the element dtypes, `pairs` says which form it was.  All of u, v, w, zeta or none.
-int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, bool &pairs, const char *what) {
+// Time-dependent fields may come as snapshot pairs (OPB_F32_PAIRS / OPB_F64_PAIRS) or snapshot quads
+// (OPB_F32_QUADS, with h, dx, dy as OPB_F64_XPAIRS): `out` is `in` with the element dtypes, `layout`
+// says which form it was (LAYOUT_PLAIN, LAYOUT_PAIRS, LAYOUT_QUADS).  All of u, v, w, zeta or none.
+int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, int &layout, const char *what) {
     if (!in) return fail(OPB_EINVAL, "%s: fields is NULL", what);
     out = *in;
-    int npairs = 0, ntd = 0;
+    int npairs = 0, nquads = 0, ntd = 0, nx = 0;
     for (opb_field *x : {&out.u, &out.v, &out.w, &out.zeta}) {
         if (x->is_static) continue;
         ++ntd;
         if (x->dtype == OPB_F32_PAIRS || x->dtype == OPB_F64_PAIRS) {
             x->dtype = x->dtype == OPB_F32_PAIRS ? OPB_F32 : OPB_F64;
             ++npairs;
+        } else if (x->dtype == OPB_F32_QUADS) {
+            x->dtype = OPB_F32;
+            ++nquads;
         }
     }
-    if (npairs && npairs != ntd)
-        return fail(OPB_EINVAL, "%s: either every time-dependent field is a snapshot pair or none", what);
-    pairs = npairs > 0;
+    for (opb_field *x : {&out.h, &out.dx, &out.dy}) {
+        if (x->is_static && x->dtype == OPB_F64_XPAIRS) {
+            x->dtype = OPB_F64;
+            ++nx;
+        }
+    }
+    if ((npairs && npairs != ntd) || (nquads && nquads != ntd))
+        return fail(OPB_EINVAL, "%s: either every time-dependent field is a snapshot pair (or quad) or none", what);
+    if (nquads && nx != 3)
+        return fail(OPB_EINVAL, "%s: snapshot quads need h, dx and dy as static x-pairs (OPB_F64_XPAIRS)", what);
+    if (nx && !nquads)
+        return fail(OPB_EINVAL, "%s: static x-pairs (OPB_F64_XPAIRS) come with snapshot quads only", what);
+    layout = nquads ? LAYOUT_QUADS : npairs ? LAYOUT_PAIRS : LAYOUT_PLAIN;
     return OPB_OK;
 }
 

@@ -1,8 +1,10 @@
 // Snapshot pairs: two consecutive snapshots of a time-dependent field
 // interleaved element by element (out[2i] = a[i], out[2i + 1] = b[i]), the
 // layout in which the float64 steppers fetch both values of a time blend with
-// one load.  Pure data movement at HBM bandwidth: 16-byte loads of a and b,
-// 16-byte stores of the interleaved result.
+// one load.  Snapshot quads extend each pair with its x-neighbour's
+// ({a[i], b[i], a[i+1], b[i+1]}: one 16-byte load per two stencil corners), and
+// x-pairs do the same for a static float64 field ({s[i], s[i+1]}).  Pure data
+// movement at HBM bandwidth: 16-byte loads, 16-byte stores.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -42,6 +44,39 @@ __global__ void __launch_bounds__(kBlock) k_pairs_tail(const T *__restrict__ a, 
     if (i >= n) return;
     out[2 * i] = a[i];
     out[2 * i + 1] = b[i];
+}
+
+// float32 quads: four elements per thread (one float4 of a and of b, plus the
+// next element of each) -> four float4 stores; the caller handles the tail
+__global__ void __launch_bounds__(kBlock) k_quads_f32(const float *__restrict__ a, const float *__restrict__ b,
+                                                      float4 *__restrict__ out, long long n4, long long n) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (long long)gridDim.x * blockDim.x) {
+        const long long i = 4 * q;
+        const float4 x = __ldg((const float4 *)a + q), y = __ldg((const float4 *)b + q);
+        const long long j = i + 4 < n ? i + 4 : n - 1;
+        const float xn = __ldg(a + j), yn = __ldg(b + j);
+        out[i] = make_float4(x.x, y.x, x.y, y.y);
+        out[i + 1] = make_float4(x.y, y.y, x.z, y.z);
+        out[i + 2] = make_float4(x.z, y.z, x.w, y.w);
+        out[i + 3] = make_float4(x.w, y.w, xn, yn);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_quads_tail(const float *__restrict__ a, const float *__restrict__ b,
+                                                       float4 *__restrict__ out, long long first, long long n) {
+    const long long i = first + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long j = i + 1 < n ? i + 1 : n - 1;
+    out[i] = make_float4(a[i], b[i], a[j], b[j]);
+}
+
+// float64 x-pairs, one element per thread
+__global__ void __launch_bounds__(kBlock) k_xpairs_f64(const double *__restrict__ s, double2 *__restrict__ out,
+                                                       long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long j = i + 1 < n ? i + 1 : n - 1;
+        out[i] = make_double2(__ldg(s + i), __ldg(s + j));
+    }
 }
 
 int grid_for(long long work) {
@@ -84,6 +119,41 @@ int opb_interleave_pairs(const void *a, const void *b, void *out, int64_t n, int
             k_pairs_tail<double><<<(unsigned)((n - done + kBlock - 1) / kBlock), kBlock, 0, st>>>(
                 (const double *)a, (const double *)b, (double *)out, done, n);
     }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+int opb_interleave_quads(const float *a, const float *b, float *out, int64_t n, void *stream) {
+    const char *what = "opb_interleave_quads";
+    if (n < 0) return opb::fail(OPB_EINVAL, "%s: negative element count", what);
+    if (n == 0) return OPB_OK;
+    if (!a || !b || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
+    if (((uintptr_t)out) & 15) return opb::fail(OPB_EINVAL, "%s: out is not 16-byte aligned", what);
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool aligned = ((((uintptr_t)a) | ((uintptr_t)b)) & 15) == 0;
+    long long done = 0;
+    if (aligned) {
+        const long long n4 = n / 4;
+        if (n4) k_quads_f32<<<grid_for(n4), kBlock, 0, st>>>(a, b, (float4 *)out, n4, n);
+        done = n4 * 4;
+    }
+    if (done < n)
+        k_quads_tail<<<(unsigned)((n - done + kBlock - 1) / kBlock), kBlock, 0, st>>>(a, b, (float4 *)out, done, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+int opb_neighbour_pairs(const double *s, double *out, int64_t n, void *stream) {
+    const char *what = "opb_neighbour_pairs";
+    if (n < 0) return opb::fail(OPB_EINVAL, "%s: negative element count", what);
+    if (n == 0) return OPB_OK;
+    if (!s || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
+    if (((uintptr_t)out) & 15) return opb::fail(OPB_EINVAL, "%s: out is not 16-byte aligned", what);
+    k_xpairs_f64<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(s, (double2 *)out, n);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     opb::clear_error();

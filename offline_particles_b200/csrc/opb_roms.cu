@@ -14,6 +14,7 @@
 #include <cstring>
 #include <initializer_list>
 #include <string>
+#include <type_traits>
 #include <utility>
 
 #include "opb200.h"
@@ -186,7 +187,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3_post(const __grid_constant__ DPa
 // ------------------------------------------------------------ fused kernels
 // `nsteps` RK2 steps (timesteppers.py:241-257) per launch.  table[3*k + j]
 // selects the fields of step k, stage j (t, t + alpha dt, t + dt).
-template <typename T, typename I, bool FIXED, bool PAIRS = false>
+template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN>
 __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
@@ -207,16 +208,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table[3 * k], t2 = table[3 * k + 1], t3 = table[3 * k + 2];
         const bool reuse = k > 0 && same_time(t1, s.at);
-        if (!rk2_stage1(s, bind_all<T, I, FIXED, PAIRS>(r, t1), sc, reuse)) {
+        if (!rk2_stage1(s, bind_all<T, I, FIXED, LAYOUT>(r, t1), sc, reuse)) {
             raise_zero_division(p);
             break;
         }
         moved = true;
-        if (!rk2_stage2(s, bind_all<T, I, FIXED, PAIRS>(r, t2), L, sc)) {
+        if (!rk2_stage2(s, bind_all<T, I, FIXED, LAYOUT>(r, t2), L, sc)) {
             raise_zero_division(p);
             break;
         }
-        rk2_update(s, bind_all<T, I, FIXED, PAIRS>(r, t3), L, sc);
+        rk2_update(s, bind_all<T, I, FIXED, LAYOUT>(r, t3), L, sc);
         s.at = t3;
     }
     if (s.status != st0) p.status[i] = s.status;
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
 
 // `nsteps` AB3 steps (timesteppers.py:296-305) per launch.  table[2*k + j]
 // selects the fields of step k at t (j = 0) and t + dt (j = 1).
-template <typename T, typename I, bool FIXED, bool PAIRS = false, bool ISO = false>
+template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool ISO = false>
 __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
@@ -264,15 +265,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
         const opb_time t1 = table[2 * k], t2 = table[2 * k + 1];
         const bool reuse = k > 0 && same_time(t1, s.at);
         bool ok;
-        if constexpr (ISO) ok = ab3_step(s, bind_all<T, I, FIXED, PAIRS>(r, t1), sc, reuse, IsoVel{rho_t, sc.w_max,
+        if constexpr (ISO) ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT>(r, t1), sc, reuse, IsoVel{rho_t, sc.w_max,
                                                                                                      sc.rho_scale});
-        else ok = ab3_step(s, bind_all<T, I, FIXED, PAIRS>(r, t1), sc, reuse);
+        else ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT>(r, t1), sc, reuse);
         if (!ok) {
             raise_zero_division(p);
             break;
         }
         moved = true;
-        ab3_post(s, bind_all<T, I, FIXED, PAIRS>(r, t2), L, sc);
+        ab3_post(s, bind_all<T, I, FIXED, LAYOUT>(r, t2), L, sc);
         s.at = t2;
     }
     if (s.status != st0) p.status[i] = s.status;
@@ -443,10 +444,10 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     if (!s) return fail(OPB_EINVAL, "%s: scalars is NULL", what);
     convert_scalars(s, ds);
     opb_roms_fields g;
-    bool pairs = false;
-    if ((rc = unpair_fields(f, g, pairs, what))) return rc;
+    int layout = LAYOUT_PLAIN;
+    if ((rc = unpair_fields(f, g, layout, what))) return rc;
     if ((rc = convert_fields(&g, dr, what, true, &dtype))) return rc;
-    if (pairs && !roms_layout(dr))
+    if (layout != LAYOUT_PLAIN && !roms_layout(dr))
         return fail(OPB_EINVAL, "%s: snapshot pairs need the ROMS field layout", what);
     if (nsteps < 0) return fail(OPB_EINVAL, "%s: negative step count", what);
     if (nsteps > 0 && !table) return fail(OPB_EINVAL, "%s: step table is NULL", what);
@@ -463,24 +464,31 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     const unsigned grid = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
     const bool fixed = roms_layout(dr);
+    auto go = [&](auto tv, auto iv, auto lv) {
+        using T = decltype(tv);
+        using I = decltype(iv);
+        constexpr int LAYOUT = decltype(lv)::value;
+        if (rk2) k_rk2_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        else if (iso)
+            k_ab3_steps<T, I, true, LAYOUT, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        else k_ab3_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+    };
+    if (layout == LAYOUT_QUADS) {
+        if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads hold float32 storage", what);
+        if (fits_int(dr)) go(float{}, int{}, std::integral_constant<int, LAYOUT_QUADS>{});
+        else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_QUADS>{});
+        return check_launch(what);
+    }
     dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {
         using T = decltype(tv);
         using I = decltype(iv);
-        if (rk2) {
-            if (pairs) k_rk2_steps<T, I, true, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-            else if (fixed) k_rk2_steps<T, I, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-            else k_rk2_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-        } else if (iso) {
-            if (pairs)
-                k_ab3_steps<T, I, true, true, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-            else if (fixed)
-                k_ab3_steps<T, I, true, false, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-            else k_ab3_steps<T, I, false, false, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-        } else {
-            if (pairs) k_ab3_steps<T, I, true, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-            else if (fixed) k_ab3_steps<T, I, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-            else k_ab3_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-        }
+        if (layout == LAYOUT_PAIRS) go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{});
+        else if (fixed) go(tv, iv, std::integral_constant<int, LAYOUT_PLAIN>{});
+        else if (rk2) k_rk2_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        else if (iso)
+            k_ab3_steps<T, I, false, LAYOUT_PLAIN, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps,
+                                                                                 validate_pre);
+        else k_ab3_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
     });
     return check_launch(what);
 }

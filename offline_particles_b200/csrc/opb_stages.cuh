@@ -39,18 +39,24 @@ __device__ __forceinline__ void raise_zero_division(const DParticles &p) {
 
 // The fields of one stage.  FIXED: the ROMS layout (u, v, w, zeta
 // time-dependent; h, dx, dy, C static), known at compile time; otherwise each
-// field's kind is read at run time.
-template <typename T, typename I, bool FIXED = false, bool PAIRS = false>
+// field's kind is read at run time.  LAYOUT (FIXED only): how the
+// time-dependent fields, and with LAYOUT_QUADS the static h, dx, dy, are read.
+template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN>
 struct Bound {
-    static constexpr int KT = PAIRS ? KIND_PAIRS : FIXED ? KIND_TD : KIND_ANY;
-    static constexpr int KS = FIXED ? KIND_STATIC : KIND_ANY;
+    static_assert(FIXED || LAYOUT == LAYOUT_PLAIN, "pair layouts need the ROMS field layout");
+    static constexpr int KT = LAYOUT == LAYOUT_QUADS ? KIND_QUADS
+                              : LAYOUT == LAYOUT_PAIRS ? KIND_PAIRS
+                              : FIXED ? KIND_TD : KIND_ANY;
+    static constexpr int KS = LAYOUT == LAYOUT_QUADS ? KIND_XPAIRS : FIXED ? KIND_STATIC : KIND_ANY;
+    static constexpr int KC = FIXED ? KIND_STATIC : KIND_ANY;
     View<T, I, KT> u, v, w, zeta;
-    View<T, I, KS> dx, dy, h, C;
+    View<T, I, KS> dx, dy, h;
+    View<T, I, KC> C;
 };
 
-template <typename T, typename I, bool FIXED = false, bool PAIRS = false>
-__device__ __forceinline__ Bound<T, I, FIXED, PAIRS> bind_all(const DRoms &r, const opb_time &t) {
-    using B = Bound<T, I, FIXED, PAIRS>;
+template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN>
+__device__ __forceinline__ Bound<T, I, FIXED, LAYOUT> bind_all(const DRoms &r, const opb_time &t) {
+    using B = Bound<T, I, FIXED, LAYOUT>;
     B b;
     b.u = bind<T, I, B::KT>(r.u, t);
     b.v = bind<T, I, B::KT>(r.v, t);
@@ -59,7 +65,7 @@ __device__ __forceinline__ Bound<T, I, FIXED, PAIRS> bind_all(const DRoms &r, co
     b.dx = bind<T, I, B::KS>(r.dx, t);
     b.dy = bind<T, I, B::KS>(r.dy, t);
     b.h = bind<T, I, B::KS>(r.h, t);
-    b.C = bind<T, I, B::KS>(r.C, t);  // static float64 (kernels/_core.pyx:5-9)
+    b.C = bind<T, I, B::KC>(r.C, t);  // static float64 (kernels/_core.pyx:5-9)
     return b;
 }
 

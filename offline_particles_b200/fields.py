@@ -33,6 +33,9 @@ import torch
 from ._device import cuda_device, torch_dtype
 from .spatial_arrays import BBox, DeviceArray, SpatialArray, Stagger
 
+# Observers of snapshot pair/quad builds: callables run after each build launch (used for counting launches).
+pair_observers: list = []
+
 FieldData = collections.namedtuple("FieldData", ["array", "offsets"])
 
 SUPPORTED_DTYPES = (np.dtype(np.float64), np.dtype(np.float32))
@@ -168,6 +171,7 @@ class StaticField(Field):
         if data.data.dtype != torch.float64:
             data = DeviceArray(data.data, data.z_stagger, data.y_stagger, data.x_stagger, dtype=torch.float64)
         self._data = data
+        self._xpairs: tuple[torch.Tensor, torch.Tensor] | None = None
 
     @property
     def data(self) -> DeviceArray:
@@ -194,6 +198,20 @@ class StaticField(Field):
         """The float64 device array and its offsets; ``time_index`` is ignored."""
         array, offsets = self._data.get_data_subset(bbox)
         return FieldData(array, offsets)
+
+    def xpairs(self) -> torch.Tensor:
+        """The field's x-pairs (shape ``(2 * size,)``; element i holds values i and i + 1,
+        ``opb_neighbour_pairs``): the static companion of snapshot quads.  Built once, on the current
+        stream."""
+        if self._xpairs is None:
+            from . import _lib
+            from ._device import stream_handle
+
+            src = self._data.data.contiguous()
+            out = torch.empty(2 * src.numel(), dtype=torch.float64, device=src.device)
+            _lib.call("opb_neighbour_pairs", src.data_ptr(), out.data_ptr(), src.numel(), stream_handle(src.device))
+            self._xpairs = (src, out)  # src kept alive until the build has run
+        return self._xpairs[1]
 
     @classmethod
     def from_numpy(cls, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
@@ -429,6 +447,17 @@ class SnapshotRing:
         self.pool.shutdown(wait=True)
 
 
+class _PairCache:
+    """Device buffers of one pair layout of a field: the pairs by first snapshot (LRU) and free buffers."""
+
+    __slots__ = ("cache", "store", "free")
+
+    def __init__(self) -> None:
+        self.cache: collections.OrderedDict[int, torch.Tensor] = collections.OrderedDict()
+        self.store: torch.Tensor | None = None
+        self.free: list[torch.Tensor] | None = None
+
+
 class TimeDependentField(Field):
     """A field with a leading time axis, streamed to the device snapshot by snapshot.
 
@@ -493,9 +522,7 @@ class TimeDependentField(Field):
         if pair_slots < 2:
             raise ValueError("pair_slots must be at least 2")
         self._pair_slots = int(pair_slots)
-        self._pairs: collections.OrderedDict[int, torch.Tensor] = collections.OrderedDict()
-        self._pair_store = None
-        self._pair_free: list[torch.Tensor] | None = None
+        self._pair_caches: dict[bool, _PairCache] = {}  # snapshot pairs (False) and quads (True)
 
     # ------------------------------------------------------------ properties
     @property
@@ -566,29 +593,34 @@ class TimeDependentField(Field):
     def pair_slots(self) -> int:
         return self._pair_slots
 
-    def pair(self, k: int, keep: set[int] | frozenset = frozenset()) -> torch.Tensor:
+    def pair(self, k: int, keep: set[int] | frozenset = frozenset(), *, quads: bool = False) -> torch.Tensor:
         """Snapshots k and k + 1 interleaved element by element (shape ``(2 * size,)``; element 2i from
         snapshot k, 2i + 1 from k + 1): the layout in which the float64 fused steppers fetch both values
-        of a time blend with one load.  Built on the current stream the first time it is asked for; the
-        ``pair_slots`` most recently used pairs stay on the device, and a pair's buffer is reused for a
-        new one in stream order (after the launches queued before it that read the old pair).  Pairs in
+        of a time blend with one load.  ``quads`` (float32 storage): each element's pair followed by its
+        x-neighbour's (shape ``(4 * size,)``; ``opb_interleave_quads``), so one 16-byte load fetches two
+        stencil corners.  Built on the current stream the first time it is asked for; the ``pair_slots``
+        most recently used pairs (and as many quads) stay on the device, and a buffer is reused for a
+        new one in stream order (after the launches queued before it that read the old one).  Pairs in
         ``keep`` are not evicted."""
         if self._storage is not None:
             raise ValueError("snapshot pairs hold float32/float64 storage only")
+        if quads and self._data_dtype != np.float32:
+            raise ValueError("snapshot quads hold float32 storage only")
         if k < 0 or k + 1 >= self._num_timesteps:
             raise IndexError(k)
-        cache = self._pairs
+        pc = self._pair_caches.setdefault(bool(quads), _PairCache())
+        cache = pc.cache
         if k in cache:
             cache.move_to_end(k)
             return cache[k]
-        if self._pair_free is None:
-            # every pair buffer at once, on first use: a large allocation later could synchronise the device
+        if pc.free is None:
+            # every buffer at once, on first use: a large allocation later could synchronise the device
             n = int(np.prod(self._spatial_shape))
-            self._pair_store = torch.empty((self._pair_slots, 2 * n), dtype=torch_dtype(self._data_dtype),
-                                           device=self._device)
-            self._pair_free = list(self._pair_store.unbind(0))
-        if self._pair_free:
-            buf = self._pair_free.pop()
+            pc.store = torch.empty((self._pair_slots, (4 if quads else 2) * n), dtype=torch_dtype(self._data_dtype),
+                                   device=self._device)
+            pc.free = list(pc.store.unbind(0))
+        if pc.free:
+            buf = pc.free.pop()
         else:
             buf = None
             for old in list(cache):
@@ -602,8 +634,14 @@ class TimeDependentField(Field):
         from . import _lib
         from ._device import stream_handle
 
-        _lib.call("opb_interleave_pairs", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(),
-                  _lib.F32 if a.dtype == torch.float32 else _lib.F64, stream_handle(self._device))
+        if quads:
+            _lib.call("opb_interleave_quads", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(),
+                      stream_handle(self._device))
+        else:
+            _lib.call("opb_interleave_pairs", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(),
+                      _lib.F32 if a.dtype == torch.float32 else _lib.F64, stream_handle(self._device))
+        for obs in pair_observers:
+            obs()
         cache[k] = buf
         return buf
 

@@ -20,7 +20,7 @@ import numpy.typing as npt
 import torch
 
 from . import _lib
-from .fields import TimeDependentField
+from .fields import StaticField, TimeDependentField
 from .kernels import ParticleKernel
 from .kernels import _abi
 from .launcher import Launcher, ScalarSource
@@ -288,19 +288,49 @@ def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField], nparticles:
     return nparticles * PAIR_CELLS_PER_PARTICLE >= fs.z_size * fs.y_size * fs.x_size
 
 
-def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField]) -> dict[int, int]:
+# Snapshot quads (float32 storage): each element's snapshot pair followed by its x-neighbour's, with the
+# static h, dx, dy as x-pairs, so a stencil's two x-neighbouring corners come in one 16-byte load: half
+# the gather requests of pairs.  They replace the pairs wherever pairs are used and storage is float32.
+SNAPSHOT_QUADS = True
+QUAD_STATICS = ("h", "dx", "dy")
+
+
+def quad_statics(launcher: Launcher, td: dict[str, TimeDependentField],
+                 roles: dict[str, str] | None = None) -> dict[str, StaticField] | None:
+    """The static fields read as x-pairs beside snapshot quads, or None when the pairs stay pairs."""
+    if not SNAPSHOT_QUADS or not td or not all(f.storage == "float32" for f in td.values()):
+        return None
+    fs = launcher.fieldset
+    roles = roles or {}
+    out = {n: fs[roles.get(n, n)] for n in QUAD_STATICS if roles.get(n, n) in fs}
+    if len(out) != len(QUAD_STATICS) or not all(isinstance(f, StaticField) for f in out.values()):
+        return None
+    return out
+
+
+def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField],
+                statics: dict[str, StaticField] | None = None) -> dict[int, int]:
     """Point the time-dependent fields of ``rf`` at snapshot pairs ``its`` (slot q holds pair its[q]);
-    return pair -> slot."""
+    return pair -> slot.  ``statics`` (``quad_statics``): snapshot quads instead, with those static
+    fields as x-pairs."""
     keep = set(its)
+    quads = statics is not None
     for name, field in td.items():
         f = getattr(rf, name)
-        f.dtype = _lib.F32_PAIRS if field.storage == "float32" else _lib.F64_PAIRS
+        if quads:
+            f.dtype = _lib.F32_QUADS
+        else:
+            f.dtype = _lib.F32_PAIRS if field.storage == "float32" else _lib.F64_PAIRS
         for q in range(_lib.MAX_SLOTS):
-            f.data[q] = field.pair(its[q], keep).data_ptr() if q < len(its) else None
+            f.data[q] = field.pair(its[q], keep, quads=quads).data_ptr() if q < len(its) else None
             f.scale[q] = None
         if len(its) == 1:
             f.data[1] = f.data[0]
         f.nslots = max(2, len(its))
+    for name, field in (statics or {}).items():
+        g = getattr(rf, name)
+        g.dtype = _lib.F64_XPAIRS
+        g.data[0] = field.xpairs().data_ptr()
     return {k: q for q, k in enumerate(its)}
 
 
@@ -310,7 +340,8 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
     rf, dtype = window_fields(launcher, needed, td, roles)
     entries = [t for step in steps for t in step]
     if use_pairs(launcher, td, nparticles):
-        pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td)
+        pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td,
+                            quad_statics(launcher, td, roles))
         prev_next = lambda It: (pslot[It], pslot[It])  # noqa: E731
     else:
         slot = {k: j for j, k in enumerate(needed)}

@@ -129,6 +129,22 @@ def test_argument_errors_need_no_gpu():
     assert rc == _lib.EINVAL and b"rho_t" in lib.opb_last_error()
     rc = lib.opb_ab3_isopycnal_following_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
     assert rc == _lib.EINVAL and b"rho_t" in lib.opb_last_error()
+    # snapshot quads come with x-pairs of h, dx and dy, all four time-dependent fields quads, float32 only
+    for name in ("u", "v", "w", "zeta"):
+        getattr(rf, name).dtype = _lib.F32_QUADS
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"static x-pairs" in lib.opb_last_error()
+    rf.zeta.dtype = _lib.F32_PAIRS
+    for name in ("h", "dx", "dy"):
+        getattr(rf, name).dtype = _lib.F64_XPAIRS
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"every time-dependent field" in lib.opb_last_error()
+    for name in ("u", "v", "w", "zeta"):
+        getattr(rf, name).dtype = _lib.F32
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"come with snapshot quads only" in lib.opb_last_error()
+    assert lib.opb_interleave_quads(16, 16, 20, 4, None) == _lib.EINVAL
+    assert b"16-byte aligned" in lib.opb_last_error()
 
 
 def test_call_raises_value_error():

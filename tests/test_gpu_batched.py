@@ -197,8 +197,8 @@ def test_segment_sort_keeps_segments_and_permutes_ids():
 
 @pytest.mark.parametrize("scheme,dt", [("rk2", 300.0), ("ab3", 120.0)])
 def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
-    """The fused float64 steppers read streamed fields as snapshot pairs; switching pairs off must not
-    change a bit."""
+    """The fused float64 steppers read streamed fields as plain snapshots, snapshot pairs or snapshot quads
+    (with static x-pairs); the three layouts give the same bits."""
     from b200_runner import b200_fieldset
 
     import offline_particles_b200 as opb
@@ -208,8 +208,9 @@ def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
     t_arr = g.time_array[:fields["u"].shape[0]]
     z, y, x = g.release(3000, seed=77)
     out = []
-    for pairs in ("always", "never"):
+    for pairs, quads in (("never", False), ("always", False), ("always", True)):
         timesteppers.SNAPSHOT_PAIRS = pairs
+        timesteppers.SNAPSHOT_QUADS = quads
         try:
             f = opb.roms.rk2_w_advection_timestepper if scheme == "rk2" else opb.roms.ab3_w_advection_timestepper
             sim = opb.SimulationBuilder(f(t_arr, np.float64(dt), time=np.float64(1234.5)),
@@ -221,8 +222,58 @@ def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
             out.append({k: P[k] for k in NAMES})
         finally:
             timesteppers.SNAPSHOT_PAIRS = "auto"
+            timesteppers.SNAPSHOT_QUADS = True
     for k in NAMES:
         assert same_bits(out[0][k], out[1][k]), k
+        assert same_bits(out[0][k], out[2][k]), k
+
+
+def test_batch_same_with_snapshot_pairs_and_quads(grid):
+    """The batched launch reads float32 fields as snapshot quads; with quads off it reads pairs, and every
+    release ends with the same bits."""
+    from b200_runner import b200_fieldset
+
+    from offline_particles_b200 import timesteppers
+    from offline_particles_b200.batching import ReleaseBatch
+
+    g, fields = grid
+    t_arr = g.time_array[:fields["u"].shape[0]]
+    out = []
+    for quads in (True, False):
+        timesteppers.SNAPSHOT_QUADS = quads
+        try:
+            rels = _releases(g, t_arr, SPECS)
+            b = ReleaseBatch(b200_fieldset(fields, g.hc, g.spec.nz), rels, buckets=64)
+            b.run()
+            b.synchronize()
+            out.append([b.result(r) for r in rels])
+        finally:
+            timesteppers.SNAPSHOT_QUADS = True
+    for q, (a, c) in enumerate(zip(*out)):
+        for k in NAMES:
+            assert same_bits(a[k], c[k]), (q, k)
+
+
+@pytest.mark.parametrize("n,offset", [(1_000_003, 0), (4096, 1), (5, 0), (1, 0)])
+def test_interleave_quads_and_xpairs_match_torch(n, offset):
+    import torch
+
+    from offline_particles_b200 import _lib
+
+    a = torch.randn(n + offset, dtype=torch.float32, device="cuda")[offset:]
+    b = torch.randn(n + offset, dtype=torch.float32, device="cuda")[offset:]
+    out = torch.full((4 * n,), float("nan"), dtype=torch.float32, device="cuda")
+    _lib.call("opb_interleave_quads", a.data_ptr(), b.data_ptr(), out.data_ptr(), n, None)
+    nxt = torch.cat((torch.arange(1, n, device="cuda"), torch.tensor([n - 1], device="cuda")))
+    want = torch.stack((a, b, a[nxt], b[nxt]), dim=1)
+    s = torch.randn(n + offset, dtype=torch.float64, device="cuda")[offset:]
+    xp = torch.full((2 * n,), float("nan"), dtype=torch.float64, device="cuda")
+    _lib.call("opb_neighbour_pairs", s.data_ptr(), xp.data_ptr(), n, None)
+    torch.cuda.synchronize()
+    assert torch.equal(out.view(-1, 4), want)
+    assert torch.equal(xp.view(-1, 2), torch.stack((s, s[nxt]), dim=1))
+    with pytest.raises(ValueError, match="16-byte"):
+        _lib.call("opb_interleave_quads", a.data_ptr(), b.data_ptr(), out.data_ptr() + 4, n, None)
 
 
 @pytest.mark.parametrize("dtype,n,offset", [("float32", 1_000_003, 0), ("float32", 4096, 1), ("float64", 777_777, 0),
