@@ -65,8 +65,8 @@ def parse():
     ap.add_argument("--nz", type=int, default=50)
     ap.add_argument("--dt", type=float, default=120.0)
     ap.add_argument("--ring-size", type=int, default=8, help="device snapshot slots of the end-to-end arm")
-    ap.add_argument("--layout", choices=("auto", "quads", "pairs", "plain"), default="auto",
-                    help="how the kernels read snapshots: auto (quads for float32 storage where pairs pay), "
+    ap.add_argument("--layout", choices=("auto", "octets", "quads", "pairs", "plain"), default="auto",
+                    help="how the kernels read snapshots: auto (the library default where pairs pay), octets, "
                          "quads, pairs, or plain snapshots")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
@@ -894,10 +894,8 @@ def set_layout(layout: str) -> None:
     """The snapshot layout of every launch in this process (``--layout``)."""
     from offline_particles_b200 import timesteppers
 
-    if layout == "quads":
-        timesteppers.SNAPSHOT_PAIRS, timesteppers.SNAPSHOT_QUADS = "always", True
-    elif layout == "pairs":
-        timesteppers.SNAPSHOT_PAIRS, timesteppers.SNAPSHOT_QUADS = "always", False
+    if layout in ("octets", "quads", "pairs"):
+        timesteppers.SNAPSHOT_PAIRS, timesteppers.SNAPSHOT_LAYOUT = "always", layout
     elif layout == "plain":
         timesteppers.SNAPSHOT_PAIRS = "never"
 

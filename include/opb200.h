@@ -63,6 +63,16 @@ extern "C" {
 #define OPB_F32_QUADS 6
 /* x-pairs of a static float64 field: data[0] holds {s[i], s[i+1]} for element i */
 #define OPB_F64_XPAIRS 7
+/* snapshot octets (the same entry points, float32 storage): data[k] holds, for
+ * element i, the earlier/later pairs of elements i, i+1, i+R and i+R+1 (R: the
+ * field's last dimension), so one 32-byte load fetches the four corners of a
+ * stencil face with both values of their time blends.  Octets come with yx-pairs
+ * of h, dx and dy (OPB_F64_YXPAIRS; C stays OPB_F64).  Pair buffers must be
+ * aligned to their load: 8 bytes (OPB_F32_PAIRS), 16 (OPB_F64_PAIRS, quads,
+ * x-pairs) or 32 (octets, yx-pairs) */
+#define OPB_F32_OCTS 8
+/* yx-pairs of a static float64 field: data[0] holds {s[i], s[i+1], s[i+R], s[i+R+1]} */
+#define OPB_F64_YXPAIRS 9
 
 /* return codes */
 #define OPB_OK 0
@@ -196,6 +206,18 @@ int opb_interleave_quads(const float *a, const float *b, float *out, int64_t n, 
  * out[2i] = s[i], out[2i+1] = s[i+1] for i < n - 1 and s[n-1] twice for the last
  * element (out holds 2n doubles; DEVICE buffers, out 16-byte aligned). */
 int opb_neighbour_pairs(const double *s, double *out, int64_t n, void *stream);
+
+/* No reference counterpart: the snapshot octets of float32 snapshots a and b with
+ * row length `row`, out[8i .. 8i+7] = a[j], b[j] for j = i, i+1, i+row, i+row+1 in
+ * turn, each j past the end replaced by n - 1 (out holds 8n floats; DEVICE
+ * buffers, out 32-byte aligned). */
+int opb_interleave_octets(const float *a, const float *b, float *out, int64_t n, int64_t row, void *stream);
+
+/* No reference counterpart: the yx-pairs of a static float64 field s with row
+ * length `row`, out[4i .. 4i+3] = s[i], s[i+1], s[i+row], s[i+row+1], each index
+ * past the end replaced by n - 1 (out holds 4n doubles; DEVICE buffers, out
+ * 32-byte aligned). */
+int opb_neighbour_quads(const double *s, double *out, int64_t n, int64_t row, void *stream);
 
 /* ---- batched release experiments ---------------------------------------------
  * No single reference counterpart: the reference advances one release per

@@ -15,6 +15,7 @@ MAX_SLOTS = 8
 F64, F32, BF16, F16 = 0, 1, 2, 3
 F64_PAIRS, F32_PAIRS = 4, 5
 F32_QUADS, F64_XPAIRS = 6, 7
+F32_OCTS, F64_YXPAIRS = 8, 9
 ABI_VERSION = 5
 OK, EINVAL, ECUDA = 0, 1, 2
 ERRF_ZERO_DIVISION = 1
@@ -113,6 +114,8 @@ SIGNATURES = {
     "opb_interleave_pairs": [_VP, _VP, _VP, ctypes.c_int64, ctypes.c_int32, _VP],
     "opb_interleave_quads": [_VP, _VP, _VP, ctypes.c_int64, _VP],
     "opb_neighbour_pairs": [_VP, _VP, ctypes.c_int64, _VP],
+    "opb_interleave_octets": [_VP, _VP, _VP, ctypes.c_int64, ctypes.c_int64, _VP],
+    "opb_neighbour_quads": [_VP, _VP, ctypes.c_int64, ctypes.c_int64, _VP],
     "opb_quantize_levels": [_VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP, _VP],
 }
 

@@ -42,7 +42,7 @@ from .kernels.status import ParticleStatus
 from .launcher import Launcher
 from .particles import Particles
 from .timesteppers import (ABTimestepper, RK2Timestepper, Timestepper, _time_dependent_fields, pair_fields,
-                           quad_statics, window_fields)
+                           pair_layout, window_fields)
 
 TIME_DTYPE = np.dtype([("prev", "<i4"), ("next", "<i4"), ("ft", "<f8"), ("gt", "<f8")])
 EXPERIMENT_DTYPE = np.dtype([("start", "<i8"), ("count", "<i8"), ("first_chunk", "<i8"), ("scheme", "<i4"),
@@ -492,10 +492,10 @@ class ReleaseBatch:
     def _pair_fields(self, j: int, window: list[int], rf) -> None:
         """Point the time-dependent fields of ``rf`` at snapshot pairs j and j + 1 (slots 0 and 1;
         ``TimeDependentField.pair``): the kernel fetches both values of a corner's time blend with one
-        load (snapshot quads with float32 storage: two corners per load).  Pair j + 1 exists only when
+        load (quads or octets with float32 storage: two or four corners per load).  Pair j + 1 exists only when
         snapshot j + 2 is in the window."""
         its = [j, j + 1] if j + 2 <= window[-1] else [j]
-        pair_fields(rf, its, self._td, quad_statics(self.launcher, self._td))
+        pair_fields(rf, its, self._td, *pair_layout(self.launcher, self._td))
 
     # --------------------------------------------------------------- planning
     def _plan(self, j: int):

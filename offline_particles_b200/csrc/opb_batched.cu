@@ -262,8 +262,8 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
     int layout = LAYOUT_PLAIN;
     if ((rc = unpair_fields(f, g, layout, what))) return rc;
     if (layout == LAYOUT_PLAIN && !(g.u.is_static && g.v.is_static && g.w.is_static && g.zeta.is_static))
-        return fail(OPB_EINVAL, "%s: time-dependent fields must be snapshot pairs (OPB_F32_PAIRS or OPB_F64_PAIRS) "
-                    "or quads (OPB_F32_QUADS)", what);
+        return fail(OPB_EINVAL, "%s: time-dependent fields must be snapshot pairs (OPB_F32_PAIRS or OPB_F64_PAIRS), "
+                    "quads (OPB_F32_QUADS) or octets (OPB_F32_OCTS)", what);
     if ((rc = convert_fields(&g, dr, what, true, &dtype))) return rc;
     if (!header || !experiments || !table) return fail(OPB_EINVAL, "%s: NULL device array", what);
     const bool shape_ok = (block == 128 && warps_per_sm == 16) ||
@@ -309,10 +309,16 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
             launch_batched<T, I, 0, LAYOUT>(block, warps_per_sm, ctas, st, dp, header, experiments, ds, dr, table,
                                             bucket_bounds, item_scratch, &launched);
     };
-    if (layout == LAYOUT_QUADS) {
-        if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads hold float32 storage", what);
-        if (fits_int(dr)) go(float{}, int{}, std::integral_constant<int, LAYOUT_QUADS>{});
-        else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_QUADS>{});
+    if (layout == LAYOUT_QUADS || layout == LAYOUT_OCTS) {
+        if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads and octets hold float32 storage", what);
+        const bool small = fits_int(dr);
+        if (layout == LAYOUT_QUADS) {
+            if (small) go(float{}, int{}, std::integral_constant<int, LAYOUT_QUADS>{});
+            else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_QUADS>{});
+        } else {
+            if (small) go(float{}, int{}, std::integral_constant<int, LAYOUT_OCTS>{});
+            else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_OCTS>{});
+        }
     } else {
         // snapshot pairs (roms_layout above rules out the all-static fields that passed the layout check)
         dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) { go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{}); });

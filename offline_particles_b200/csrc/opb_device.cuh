@@ -68,11 +68,40 @@ struct DScalars {
 // with both snapshots of their blends in one 16-byte load.
 // KIND_XPAIRS: static float64, element i holds {s[i], s[i+1]}: the two
 // x-neighbouring corners in one 16-byte load.
-constexpr int KIND_ANY = 0, KIND_STATIC = 1, KIND_TD = 2, KIND_PAIRS = 3, KIND_QUADS = 4, KIND_XPAIRS = 5;
+// KIND_OCTS (float32 storage): time-dependent, element i holds the snapshot
+// pairs of i, i+1, i+R, i+R+1 (R: the field's row length, its x size), so one
+// 32-byte load fetches the four corners of a stencil face at one level.
+// KIND_YXPAIRS: static float64, element i holds {s[i], s[i+1], s[i+R],
+// s[i+R+1]}: a bilinear stencil in one 32-byte load.
+constexpr int KIND_ANY = 0, KIND_STATIC = 1, KIND_TD = 2, KIND_PAIRS = 3, KIND_QUADS = 4, KIND_XPAIRS = 5,
+              KIND_OCTS = 6, KIND_YXPAIRS = 7;
 
-// How a launch reads its fields: plain snapshots, snapshot pairs, or snapshot
-// quads with x-pairs of the static fields h, dx, dy.
-constexpr int LAYOUT_PLAIN = 0, LAYOUT_PAIRS = 1, LAYOUT_QUADS = 2;
+// How a launch reads its fields: plain snapshots, snapshot pairs, snapshot
+// quads with x-pairs of the static fields h, dx, dy, or snapshot octets with
+// yx-pairs of h, dx, dy.
+constexpr int LAYOUT_PLAIN = 0, LAYOUT_PAIRS = 1, LAYOUT_QUADS = 2, LAYOUT_OCTS = 3;
+
+// 32-byte read-only loads (sm_100: ld.global.nc.v8.f32 / .v4.f64); the
+// address must be 32-byte aligned
+struct alignas(32) F8 {
+    float v[8];
+};
+struct alignas(32) D4 {
+    double v[4];
+};
+__device__ __forceinline__ F8 ldg256(const F8 *p) {
+    F8 r;
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]), "=f"(r.v[6]),
+          "=f"(r.v[7])
+        : "l"(p));
+    return r;
+}
+__device__ __forceinline__ D4 ldg256(const D4 *p) {
+    D4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3]) : "l"(p));
+    return r;
+}
 
 template <typename T>
 struct Vec2;
@@ -88,7 +117,8 @@ struct Vec2<double> {
 template <typename T, typename I, int KIND = KIND_ANY>
 struct View {
     using index_type = I;
-    static_assert(KIND != KIND_QUADS || sizeof(T) == 4, "snapshot quads hold float32 storage");
+    static_assert((KIND != KIND_QUADS && KIND != KIND_OCTS) || sizeof(T) == 4,
+                  "snapshot quads and octets hold float32 storage");
     const T *prev;
     const T *next;
     const double *stat;  // non-null: static float64 field
@@ -106,7 +136,12 @@ struct View {
     }
 
     __device__ __forceinline__ double at(I i) const {
-        if constexpr (KIND == KIND_XPAIRS) {
+        if constexpr (KIND == KIND_YXPAIRS) {
+            return __ldg(stat + 4 * (long long)i);
+        } else if constexpr (KIND == KIND_OCTS) {
+            const float2 v = __ldg((const float2 *)prev + 4 * (long long)i);
+            return blend(v.x, v.y);
+        } else if constexpr (KIND == KIND_XPAIRS) {
             return __ldg(stat + 2 * (long long)i);
         } else if constexpr (KIND == KIND_QUADS) {
             const float2 v = __ldg((const float2 *)prev + 2 * (long long)i);
@@ -123,7 +158,15 @@ struct View {
     // the values at i and i + 1 (x-neighbours: i + 1 stays in i's row for every
     // stencil, whose lowest corner index is clamped to n - 2)
     __device__ __forceinline__ void at2(I i, double &lo, double &hi) const {
-        if constexpr (KIND == KIND_XPAIRS) {
+        if constexpr (KIND == KIND_YXPAIRS) {
+            const double2 v = __ldg((const double2 *)stat + 2 * (long long)i);
+            lo = v.x;
+            hi = v.y;
+        } else if constexpr (KIND == KIND_OCTS) {
+            const float4 v = __ldg((const float4 *)prev + 2 * (long long)i);
+            lo = blend(v.x, v.y);
+            hi = blend(v.z, v.w);
+        } else if constexpr (KIND == KIND_XPAIRS) {
             const double2 v = __ldg((const double2 *)stat + i);
             lo = v.x;
             hi = v.y;
@@ -134,6 +177,27 @@ struct View {
         } else {
             lo = at(i);
             hi = at(i + 1);
+        }
+    }
+
+    // the values at i, i + 1, i + row, i + row + 1 (row: the field's x size; the
+    // lowest corner's indices are clamped so that all four lie in the field)
+    __device__ __forceinline__ void at4(I i, I row, double &v00, double &v01, double &v10, double &v11) const {
+        if constexpr (KIND == KIND_YXPAIRS) {
+            const D4 v = ldg256((const D4 *)stat + i);
+            v00 = v.v[0];
+            v01 = v.v[1];
+            v10 = v.v[2];
+            v11 = v.v[3];
+        } else if constexpr (KIND == KIND_OCTS) {
+            const F8 v = ldg256((const F8 *)prev + i);
+            v00 = blend(v.v[0], v.v[1]);
+            v01 = blend(v.v[2], v.v[3]);
+            v10 = blend(v.v[4], v.v[5]);
+            v11 = blend(v.v[6], v.v[7]);
+        } else {
+            at2(i, v00, v01);
+            at2(i + row, v10, v11);
         }
     }
 };
@@ -206,8 +270,7 @@ __device__ __forceinline__ double bilinear(const F &f, double idx0, double idx1)
     const double g1 = 1.0 - f1;
     const I b = I0 * f.n1 + I1;
     double v00, v01, v10, v11;
-    f.at2(b, v00, v01);
-    f.at2(b + f.n1, v10, v11);
+    f.at4(b, f.n1, v00, v01, v10, v11);
     return g0 * g1 * v00 + g0 * f1 * v01 + f0 * g1 * v10 + f0 * f1 * v11;
 }
 
@@ -228,10 +291,8 @@ __device__ __forceinline__ double trilinear(const F &f, double idx0, double idx1
     const I s0 = f.n1 * f.n2;
     const I b = I0 * s0 + I1 * s1 + I2;
     double v000, v001, v010, v011, v100, v101, v110, v111;
-    f.at2(b, v000, v001);
-    f.at2(b + s1, v010, v011);
-    f.at2(b + s0, v100, v101);
-    f.at2(b + s0 + s1, v110, v111);
+    f.at4(b, s1, v000, v001, v010, v011);
+    f.at4(b + s0, s1, v100, v101, v110, v111);
     return (g0 * g1 * g2 * v000 +
             g0 * g1 * f2 * v001 +
             g0 * f1 * g2 * v010 +

@@ -194,13 +194,31 @@ int stage_common(const char *what, const opb_particles *p, const opb_scalars *s,
     return OPB_OK;
 }
 
-// Time-dependent fields may come as snapshot pairs (OPB_F32_PAIRS / OPB_F64_PAIRS) or snapshot quads
-// (OPB_F32_QUADS, with h, dx, dy as OPB_F64_XPAIRS): `out` is `in` with the element dtypes, `layout`
-// says which form it was (LAYOUT_PLAIN, LAYOUT_PAIRS, LAYOUT_QUADS).  All of u, v, w, zeta or none.
+// Time-dependent fields may come as snapshot pairs (OPB_F32_PAIRS / OPB_F64_PAIRS), snapshot quads
+// (OPB_F32_QUADS, with h, dx, dy as OPB_F64_XPAIRS) or snapshot octets (OPB_F32_OCTS, with h, dx, dy as
+// OPB_F64_YXPAIRS): `out` is `in` with the element dtypes, `layout` says which form it was (LAYOUT_PLAIN,
+// LAYOUT_PAIRS, LAYOUT_QUADS, LAYOUT_OCTS).  All of u, v, w, zeta or none.
 int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, int &layout, const char *what) {
     if (!in) return fail(OPB_EINVAL, "%s: fields is NULL", what);
+    // every vector load of a layout starts on its own size: the buffers must be aligned to it
+    auto misaligned = [](const opb_field &x, uintptr_t align) {
+        const int n = x.is_static ? 1 : (x.nslots < OPB_MAX_SLOTS ? x.nslots : OPB_MAX_SLOTS);
+        for (int k = 0; k < n; ++k)
+            if (((uintptr_t)x.data[k]) & (align - 1)) return true;
+        return false;
+    };
+    for (const opb_field *x : {&in->u, &in->v, &in->w, &in->zeta, &in->h, &in->dx, &in->dy}) {
+        const uintptr_t align = x->dtype == OPB_F32_PAIRS                                  ? 8
+                                : x->dtype == OPB_F64_PAIRS || x->dtype == OPB_F32_QUADS ||
+                                          x->dtype == OPB_F64_XPAIRS                       ? 16
+                                : x->dtype == OPB_F32_OCTS || x->dtype == OPB_F64_YXPAIRS ? 32
+                                                                                           : 1;
+        if (align > 1 && misaligned(*x, align))
+            return fail(OPB_EINVAL, "%s: a snapshot pair/quad/octet or x/yx-pair buffer is not %d-byte aligned",
+                        what, (int)align);
+    }
     out = *in;
-    int npairs = 0, nquads = 0, ntd = 0, nx = 0;
+    int npairs = 0, nquads = 0, nocts = 0, ntd = 0, nx = 0, nyx = 0;
     for (opb_field *x : {&out.u, &out.v, &out.w, &out.zeta}) {
         if (x->is_static) continue;
         ++ntd;
@@ -210,21 +228,32 @@ int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, int &layout, 
         } else if (x->dtype == OPB_F32_QUADS) {
             x->dtype = OPB_F32;
             ++nquads;
+        } else if (x->dtype == OPB_F32_OCTS) {
+            x->dtype = OPB_F32;
+            ++nocts;
         }
     }
     for (opb_field *x : {&out.h, &out.dx, &out.dy}) {
         if (x->is_static && x->dtype == OPB_F64_XPAIRS) {
             x->dtype = OPB_F64;
             ++nx;
+        } else if (x->is_static && x->dtype == OPB_F64_YXPAIRS) {
+            x->dtype = OPB_F64;
+            ++nyx;
         }
     }
-    if ((npairs && npairs != ntd) || (nquads && nquads != ntd))
-        return fail(OPB_EINVAL, "%s: either every time-dependent field is a snapshot pair (or quad) or none", what);
+    if ((npairs && npairs != ntd) || (nquads && nquads != ntd) || (nocts && nocts != ntd))
+        return fail(OPB_EINVAL, "%s: either every time-dependent field is a snapshot pair (or quad, or octet) or none",
+                    what);
     if (nquads && nx != 3)
         return fail(OPB_EINVAL, "%s: snapshot quads need h, dx and dy as static x-pairs (OPB_F64_XPAIRS)", what);
+    if (nocts && nyx != 3)
+        return fail(OPB_EINVAL, "%s: snapshot octets need h, dx and dy as static yx-pairs (OPB_F64_YXPAIRS)", what);
     if (nx && !nquads)
         return fail(OPB_EINVAL, "%s: static x-pairs (OPB_F64_XPAIRS) come with snapshot quads only", what);
-    layout = nquads ? LAYOUT_QUADS : npairs ? LAYOUT_PAIRS : LAYOUT_PLAIN;
+    if (nyx && !nocts)
+        return fail(OPB_EINVAL, "%s: static yx-pairs (OPB_F64_YXPAIRS) come with snapshot octets only", what);
+    layout = nocts ? LAYOUT_OCTS : nquads ? LAYOUT_QUADS : npairs ? LAYOUT_PAIRS : LAYOUT_PLAIN;
     return OPB_OK;
 }
 

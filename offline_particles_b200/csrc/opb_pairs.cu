@@ -3,8 +3,9 @@
 // layout in which the float64 steppers fetch both values of a time blend with
 // one load.  Snapshot quads extend each pair with its x-neighbour's
 // ({a[i], b[i], a[i+1], b[i+1]}: one 16-byte load per two stencil corners), and
-// x-pairs do the same for a static float64 field ({s[i], s[i+1]}).  Pure data
-// movement at HBM bandwidth: 16-byte loads, 16-byte stores.
+// x-pairs do the same for a static float64 field ({s[i], s[i+1]}).  Octets
+// (and yx-pairs) add the next row's two elements: one 32-byte load per stencil
+// face.  Pure data movement at HBM bandwidth.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -76,6 +77,33 @@ __global__ void __launch_bounds__(kBlock) k_xpairs_f64(const double *__restrict_
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const long long j = i + 1 < n ? i + 1 : n - 1;
         out[i] = make_double2(__ldg(s + i), __ldg(s + j));
+    }
+}
+
+// float32 octets, one element per thread: the pairs of i, i+1, i+row, i+row+1
+// (indices past the end clamped to n - 1) -> two float4 stores
+__global__ void __launch_bounds__(kBlock) k_octets_f32(const float *__restrict__ a, const float *__restrict__ b,
+                                                       float4 *__restrict__ out, long long n, long long row) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long last = n - 1;
+        const long long i1 = i + 1 < n ? i + 1 : last;
+        const long long i2 = i + row < n ? i + row : last;
+        const long long i3 = i + row + 1 < n ? i + row + 1 : last;
+        out[2 * i] = make_float4(__ldg(a + i), __ldg(b + i), __ldg(a + i1), __ldg(b + i1));
+        out[2 * i + 1] = make_float4(__ldg(a + i2), __ldg(b + i2), __ldg(a + i3), __ldg(b + i3));
+    }
+}
+
+// float64 yx-pairs, one element per thread -> two double2 stores
+__global__ void __launch_bounds__(kBlock) k_yxpairs_f64(const double *__restrict__ s, double2 *__restrict__ out,
+                                                        long long n, long long row) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long last = n - 1;
+        const long long i1 = i + 1 < n ? i + 1 : last;
+        const long long i2 = i + row < n ? i + row : last;
+        const long long i3 = i + row + 1 < n ? i + row + 1 : last;
+        out[2 * i] = make_double2(__ldg(s + i), __ldg(s + i1));
+        out[2 * i + 1] = make_double2(__ldg(s + i2), __ldg(s + i3));
     }
 }
 
@@ -154,6 +182,32 @@ int opb_neighbour_pairs(const double *s, double *out, int64_t n, void *stream) {
     if (!s || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
     if (((uintptr_t)out) & 15) return opb::fail(OPB_EINVAL, "%s: out is not 16-byte aligned", what);
     k_xpairs_f64<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(s, (double2 *)out, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+int opb_interleave_octets(const float *a, const float *b, float *out, int64_t n, int64_t row, void *stream) {
+    const char *what = "opb_interleave_octets";
+    if (n < 0 || row < 0) return opb::fail(OPB_EINVAL, "%s: negative element count or row length", what);
+    if (n == 0) return OPB_OK;
+    if (!a || !b || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
+    if (((uintptr_t)out) & 31) return opb::fail(OPB_EINVAL, "%s: out is not 32-byte aligned", what);
+    k_octets_f32<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(a, b, (float4 *)out, n, row);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+int opb_neighbour_quads(const double *s, double *out, int64_t n, int64_t row, void *stream) {
+    const char *what = "opb_neighbour_quads";
+    if (n < 0 || row < 0) return opb::fail(OPB_EINVAL, "%s: negative element count or row length", what);
+    if (n == 0) return OPB_OK;
+    if (!s || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
+    if (((uintptr_t)out) & 31) return opb::fail(OPB_EINVAL, "%s: out is not 32-byte aligned", what);
+    k_yxpairs_f64<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(s, (double2 *)out, n, row);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     opb::clear_error();

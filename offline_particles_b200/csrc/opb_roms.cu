@@ -473,10 +473,16 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
             k_ab3_steps<T, I, true, LAYOUT, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
         else k_ab3_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
     };
-    if (layout == LAYOUT_QUADS) {
-        if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads hold float32 storage", what);
-        if (fits_int(dr)) go(float{}, int{}, std::integral_constant<int, LAYOUT_QUADS>{});
-        else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_QUADS>{});
+    if (layout == LAYOUT_QUADS || layout == LAYOUT_OCTS) {
+        if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads and octets hold float32 storage", what);
+        const bool small = fits_int(dr);
+        if (layout == LAYOUT_QUADS) {
+            if (small) go(float{}, int{}, std::integral_constant<int, LAYOUT_QUADS>{});
+            else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_QUADS>{});
+        } else {
+            if (small) go(float{}, int{}, std::integral_constant<int, LAYOUT_OCTS>{});
+            else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_OCTS>{});
+        }
         return check_launch(what);
     }
     dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {

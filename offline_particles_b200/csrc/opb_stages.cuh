@@ -40,14 +40,18 @@ __device__ __forceinline__ void raise_zero_division(const DParticles &p) {
 // The fields of one stage.  FIXED: the ROMS layout (u, v, w, zeta
 // time-dependent; h, dx, dy, C static), known at compile time; otherwise each
 // field's kind is read at run time.  LAYOUT (FIXED only): how the
-// time-dependent fields, and with LAYOUT_QUADS the static h, dx, dy, are read.
+// time-dependent fields, and with LAYOUT_QUADS / LAYOUT_OCTS the static h, dx,
+// dy, are read.
 template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN>
 struct Bound {
     static_assert(FIXED || LAYOUT == LAYOUT_PLAIN, "pair layouts need the ROMS field layout");
-    static constexpr int KT = LAYOUT == LAYOUT_QUADS ? KIND_QUADS
+    static constexpr int KT = LAYOUT == LAYOUT_OCTS ? KIND_OCTS
+                              : LAYOUT == LAYOUT_QUADS ? KIND_QUADS
                               : LAYOUT == LAYOUT_PAIRS ? KIND_PAIRS
                               : FIXED ? KIND_TD : KIND_ANY;
-    static constexpr int KS = LAYOUT == LAYOUT_QUADS ? KIND_XPAIRS : FIXED ? KIND_STATIC : KIND_ANY;
+    static constexpr int KS = LAYOUT == LAYOUT_OCTS ? KIND_YXPAIRS
+                              : LAYOUT == LAYOUT_QUADS ? KIND_XPAIRS
+                              : FIXED ? KIND_STATIC : KIND_ANY;
     static constexpr int KC = FIXED ? KIND_STATIC : KIND_ANY;
     View<T, I, KT> u, v, w, zeta;
     View<T, I, KS> dx, dy, h;

@@ -33,8 +33,11 @@ import torch
 from ._device import cuda_device, torch_dtype
 from .spatial_arrays import BBox, DeviceArray, SpatialArray, Stagger
 
-# Observers of snapshot pair/quad builds: callables run after each build launch (used for counting launches).
+# Observers of snapshot pair/quad/octet builds: callables run after each build launch (used for counting
+# launches).
 pair_observers: list = []
+# elements of the storage dtype per grid element in each pair layout
+PAIR_WIDTH = {"pairs": 2, "quads": 4, "octets": 8}
 
 FieldData = collections.namedtuple("FieldData", ["array", "offsets"])
 
@@ -171,7 +174,7 @@ class StaticField(Field):
         if data.data.dtype != torch.float64:
             data = DeviceArray(data.data, data.z_stagger, data.y_stagger, data.x_stagger, dtype=torch.float64)
         self._data = data
-        self._xpairs: tuple[torch.Tensor, torch.Tensor] | None = None
+        self._neighbours: dict[str, tuple[torch.Tensor, torch.Tensor]] = {}
 
     @property
     def data(self) -> DeviceArray:
@@ -199,19 +202,27 @@ class StaticField(Field):
         array, offsets = self._data.get_data_subset(bbox)
         return FieldData(array, offsets)
 
-    def xpairs(self) -> torch.Tensor:
-        """The field's x-pairs (shape ``(2 * size,)``; element i holds values i and i + 1,
-        ``opb_neighbour_pairs``): the static companion of snapshot quads.  Built once, on the current
-        stream."""
-        if self._xpairs is None:
+    def neighbours(self, kind: str = "xpairs") -> torch.Tensor:
+        """The field's neighbour layout, the static companion of snapshot quads and octets: "xpairs"
+        (shape ``(2 * size,)``, element i holds values i and i + 1; ``opb_neighbour_pairs``) or
+        "yxpairs" (shape ``(4 * size,)``, values i, i + 1, i + R, i + R + 1 with R the x size;
+        ``opb_neighbour_quads``).  Built once per kind, on the current stream."""
+        if kind not in ("xpairs", "yxpairs"):
+            raise ValueError(f"unknown neighbour layout {kind!r}")
+        if kind not in self._neighbours:
             from . import _lib
             from ._device import stream_handle
 
             src = self._data.data.contiguous()
-            out = torch.empty(2 * src.numel(), dtype=torch.float64, device=src.device)
-            _lib.call("opb_neighbour_pairs", src.data_ptr(), out.data_ptr(), src.numel(), stream_handle(src.device))
-            self._xpairs = (src, out)  # src kept alive until the build has run
-        return self._xpairs[1]
+            st = stream_handle(src.device)
+            if kind == "xpairs":
+                out = torch.empty(2 * src.numel(), dtype=torch.float64, device=src.device)
+                _lib.call("opb_neighbour_pairs", src.data_ptr(), out.data_ptr(), src.numel(), st)
+            else:
+                out = torch.empty(4 * src.numel(), dtype=torch.float64, device=src.device)
+                _lib.call("opb_neighbour_quads", src.data_ptr(), out.data_ptr(), src.numel(), src.shape[-1], st)
+            self._neighbours[kind] = (src, out)  # src kept alive until the build has run
+        return self._neighbours[kind][1]
 
     @classmethod
     def from_numpy(cls, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
@@ -522,7 +533,7 @@ class TimeDependentField(Field):
         if pair_slots < 2:
             raise ValueError("pair_slots must be at least 2")
         self._pair_slots = int(pair_slots)
-        self._pair_caches: dict[bool, _PairCache] = {}  # snapshot pairs (False) and quads (True)
+        self._pair_caches: dict[str, _PairCache] = {}  # by layout: pairs, quads, octets
 
     # ------------------------------------------------------------ properties
     @property
@@ -593,22 +604,27 @@ class TimeDependentField(Field):
     def pair_slots(self) -> int:
         return self._pair_slots
 
-    def pair(self, k: int, keep: set[int] | frozenset = frozenset(), *, quads: bool = False) -> torch.Tensor:
+    def pair(self, k: int, keep: set[int] | frozenset = frozenset(), *, layout: str = "pairs") -> torch.Tensor:
         """Snapshots k and k + 1 interleaved element by element (shape ``(2 * size,)``; element 2i from
         snapshot k, 2i + 1 from k + 1): the layout in which the float64 fused steppers fetch both values
-        of a time blend with one load.  ``quads`` (float32 storage): each element's pair followed by its
-        x-neighbour's (shape ``(4 * size,)``; ``opb_interleave_quads``), so one 16-byte load fetches two
-        stencil corners.  Built on the current stream the first time it is asked for; the ``pair_slots``
-        most recently used pairs (and as many quads) stay on the device, and a buffer is reused for a
-        new one in stream order (after the launches queued before it that read the old one).  Pairs in
-        ``keep`` are not evicted."""
+        of a time blend with one load.  ``layout`` (float32 storage for the last two): "pairs"; "quads",
+        each element's pair followed by its x-neighbour's (shape ``(4 * size,)``,
+        ``opb_interleave_quads``: one 16-byte load per two stencil corners); "octets", the pairs of
+        elements i, i + 1, i + R, i + R + 1 with R the x size (shape ``(8 * size,)``,
+        ``opb_interleave_octets``: one 32-byte load per stencil face).  Built on the current stream the
+        first time it is asked for; the ``pair_slots`` most recently used pairs of each layout stay on
+        the device, and a buffer is reused for a new one in stream order (after the launches queued
+        before it that read the old one).  Pairs in ``keep`` are not evicted."""
+        width = PAIR_WIDTH.get(layout)
+        if width is None:
+            raise ValueError(f"unknown pair layout {layout!r}")
         if self._storage is not None:
             raise ValueError("snapshot pairs hold float32/float64 storage only")
-        if quads and self._data_dtype != np.float32:
-            raise ValueError("snapshot quads hold float32 storage only")
+        if width > 2 and self._data_dtype != np.float32:
+            raise ValueError("snapshot quads and octets hold float32 storage only")
         if k < 0 or k + 1 >= self._num_timesteps:
             raise IndexError(k)
-        pc = self._pair_caches.setdefault(bool(quads), _PairCache())
+        pc = self._pair_caches.setdefault(layout, _PairCache())
         cache = pc.cache
         if k in cache:
             cache.move_to_end(k)
@@ -616,7 +632,7 @@ class TimeDependentField(Field):
         if pc.free is None:
             # every buffer at once, on first use: a large allocation later could synchronise the device
             n = int(np.prod(self._spatial_shape))
-            pc.store = torch.empty((self._pair_slots, (4 if quads else 2) * n), dtype=torch_dtype(self._data_dtype),
+            pc.store = torch.empty((self._pair_slots, width * n), dtype=torch_dtype(self._data_dtype),
                                    device=self._device)
             pc.free = list(pc.store.unbind(0))
         if pc.free:
@@ -634,12 +650,15 @@ class TimeDependentField(Field):
         from . import _lib
         from ._device import stream_handle
 
-        if quads:
-            _lib.call("opb_interleave_quads", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(),
-                      stream_handle(self._device))
+        st = stream_handle(self._device)
+        if layout == "octets":
+            _lib.call("opb_interleave_octets", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(),
+                      self._spatial_shape[-1], st)
+        elif layout == "quads":
+            _lib.call("opb_interleave_quads", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(), st)
         else:
             _lib.call("opb_interleave_pairs", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(),
-                      _lib.F32 if a.dtype == torch.float32 else _lib.F64, stream_handle(self._device))
+                      _lib.F32 if a.dtype == torch.float32 else _lib.F64, st)
         for obs in pair_observers:
             obs()
         cache[k] = buf

@@ -288,49 +288,56 @@ def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField], nparticles:
     return nparticles * PAIR_CELLS_PER_PARTICLE >= fs.z_size * fs.y_size * fs.x_size
 
 
-# Snapshot quads (float32 storage): each element's snapshot pair followed by its x-neighbour's, with the
-# static h, dx, dy as x-pairs, so a stencil's two x-neighbouring corners come in one 16-byte load: half
-# the gather requests of pairs.  They replace the pairs wherever pairs are used and storage is float32.
-SNAPSHOT_QUADS = True
-QUAD_STATICS = ("h", "dx", "dy")
+# With float32 storage the pairs can be wider: "quads" (each element's snapshot pair followed by its
+# x-neighbour's, static h, dx, dy as x-pairs: a stencil's two x-neighbouring corners in one 16-byte load)
+# or "octets" (the pairs of a stencil face's four corners, static h, dx, dy as yx-pairs: one 32-byte load
+# per face, one per bilinear stencil).  They replace the pairs wherever pairs are used and storage is
+# float32; "pairs" keeps the plain pairs.
+SNAPSHOT_LAYOUT = "quads"
+NEIGHBOUR_STATICS = ("h", "dx", "dy")
+_STATIC_KIND = {"quads": "xpairs", "octets": "yxpairs"}
+_PAIR_CODE = {"quads": _lib.F32_QUADS, "octets": _lib.F32_OCTS}
+_STATIC_CODE = {"xpairs": _lib.F64_XPAIRS, "yxpairs": _lib.F64_YXPAIRS}
 
 
-def quad_statics(launcher: Launcher, td: dict[str, TimeDependentField],
-                 roles: dict[str, str] | None = None) -> dict[str, StaticField] | None:
-    """The static fields read as x-pairs beside snapshot quads, or None when the pairs stay pairs."""
-    if not SNAPSHOT_QUADS or not td or not all(f.storage == "float32" for f in td.values()):
-        return None
+def pair_layout(launcher: Launcher, td: dict[str, TimeDependentField], roles: dict[str, str] | None = None
+                ) -> tuple[str, dict[str, StaticField] | None]:
+    """The pair layout of a launch that reads pairs ("pairs", "quads" or "octets") and, for the wider
+    two, the static fields read beside them as neighbour layouts."""
+    if SNAPSHOT_LAYOUT == "pairs" or not td or not all(f.storage == "float32" for f in td.values()):
+        return "pairs", None
     fs = launcher.fieldset
     roles = roles or {}
-    out = {n: fs[roles.get(n, n)] for n in QUAD_STATICS if roles.get(n, n) in fs}
-    if len(out) != len(QUAD_STATICS) or not all(isinstance(f, StaticField) for f in out.values()):
-        return None
-    return out
+    statics = {n: fs[roles.get(n, n)] for n in NEIGHBOUR_STATICS if roles.get(n, n) in fs}
+    if len(statics) != len(NEIGHBOUR_STATICS) or not all(isinstance(f, StaticField) for f in statics.values()):
+        return "pairs", None
+    return SNAPSHOT_LAYOUT, statics
 
 
-def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField],
+def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField], layout: str = "pairs",
                 statics: dict[str, StaticField] | None = None) -> dict[int, int]:
-    """Point the time-dependent fields of ``rf`` at snapshot pairs ``its`` (slot q holds pair its[q]);
-    return pair -> slot.  ``statics`` (``quad_statics``): snapshot quads instead, with those static
-    fields as x-pairs."""
+    """Point the time-dependent fields of ``rf`` at snapshot pairs ``its`` (slot q holds pair its[q]) in
+    ``layout`` (``pair_layout``), and for quads and octets the ``statics`` at their neighbour layouts;
+    return pair -> slot."""
     keep = set(its)
-    quads = statics is not None
     for name, field in td.items():
         f = getattr(rf, name)
-        if quads:
-            f.dtype = _lib.F32_QUADS
+        if layout in _PAIR_CODE:
+            f.dtype = _PAIR_CODE[layout]
         else:
             f.dtype = _lib.F32_PAIRS if field.storage == "float32" else _lib.F64_PAIRS
         for q in range(_lib.MAX_SLOTS):
-            f.data[q] = field.pair(its[q], keep, quads=quads).data_ptr() if q < len(its) else None
+            f.data[q] = field.pair(its[q], keep, layout=layout).data_ptr() if q < len(its) else None
             f.scale[q] = None
         if len(its) == 1:
             f.data[1] = f.data[0]
         f.nslots = max(2, len(its))
-    for name, field in (statics or {}).items():
-        g = getattr(rf, name)
-        g.dtype = _lib.F64_XPAIRS
-        g.data[0] = field.xpairs().data_ptr()
+    if layout in _STATIC_KIND:
+        kind = _STATIC_KIND[layout]
+        for name, field in statics.items():
+            g = getattr(rf, name)
+            g.dtype = _STATIC_CODE[kind]
+            g.data[0] = field.neighbours(kind).data_ptr()
     return {k: q for q, k in enumerate(its)}
 
 
@@ -341,7 +348,7 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
     entries = [t for step in steps for t in step]
     if use_pairs(launcher, td, nparticles):
         pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td,
-                            quad_statics(launcher, td, roles))
+                            *pair_layout(launcher, td, roles))
         prev_next = lambda It: (pslot[It], pslot[It])  # noqa: E731
     else:
         slot = {k: j for j, k in enumerate(needed)}

@@ -143,6 +143,29 @@ def test_argument_errors_need_no_gpu():
         getattr(rf, name).dtype = _lib.F32
     rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
     assert rc == _lib.EINVAL and b"come with snapshot quads only" in lib.opb_last_error()
+    # a vector layout's buffers must be aligned to its load width
+    for name in ("u", "v", "w", "zeta"):
+        getattr(rf, name).dtype = _lib.F32_QUADS
+    rf.h.data[0] = 24
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"not 16-byte aligned" in lib.opb_last_error()
+    rf.h.data[0] = 16
+    rf.u.data[1] = 8
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"not 16-byte aligned" in lib.opb_last_error()
+    rf.u.data[1] = 16
+    # octets come with yx-pairs, 32-byte aligned
+    for name in ("u", "v", "w", "zeta"):
+        g = getattr(rf, name)
+        g.dtype, g.data[0], g.data[1] = _lib.F32_OCTS, 32, 32
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"static yx-pairs" in lib.opb_last_error()
+    for name in ("h", "dx", "dy"):
+        getattr(rf, name).dtype = _lib.F64_YXPAIRS
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"not 32-byte aligned" in lib.opb_last_error()
+    assert lib.opb_interleave_octets(16, 16, 48, 4, 2, None) == _lib.EINVAL
+    assert b"32-byte aligned" in lib.opb_last_error()
     assert lib.opb_interleave_quads(16, 16, 20, 4, None) == _lib.EINVAL
     assert b"16-byte aligned" in lib.opb_last_error()
 

@@ -197,8 +197,8 @@ def test_segment_sort_keeps_segments_and_permutes_ids():
 
 @pytest.mark.parametrize("scheme,dt", [("rk2", 300.0), ("ab3", 120.0)])
 def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
-    """The fused float64 steppers read streamed fields as plain snapshots, snapshot pairs or snapshot quads
-    (with static x-pairs); the three layouts give the same bits."""
+    """The fused float64 steppers read streamed fields as plain snapshots, snapshot pairs, quads (static
+    x-pairs beside them) or octets (static yx-pairs); every layout gives the same bits."""
     from b200_runner import b200_fieldset
 
     import offline_particles_b200 as opb
@@ -208,9 +208,10 @@ def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
     t_arr = g.time_array[:fields["u"].shape[0]]
     z, y, x = g.release(3000, seed=77)
     out = []
-    for pairs, quads in (("never", False), ("always", False), ("always", True)):
+    default = timesteppers.SNAPSHOT_LAYOUT
+    for pairs, layout in (("never", "pairs"), ("always", "pairs"), ("always", "quads"), ("always", "octets")):
         timesteppers.SNAPSHOT_PAIRS = pairs
-        timesteppers.SNAPSHOT_QUADS = quads
+        timesteppers.SNAPSHOT_LAYOUT = layout
         try:
             f = opb.roms.rk2_w_advection_timestepper if scheme == "rk2" else opb.roms.ab3_w_advection_timestepper
             sim = opb.SimulationBuilder(f(t_arr, np.float64(dt), time=np.float64(1234.5)),
@@ -222,15 +223,16 @@ def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
             out.append({k: P[k] for k in NAMES})
         finally:
             timesteppers.SNAPSHOT_PAIRS = "auto"
-            timesteppers.SNAPSHOT_QUADS = True
+            timesteppers.SNAPSHOT_LAYOUT = default
     for k in NAMES:
-        assert same_bits(out[0][k], out[1][k]), k
-        assert same_bits(out[0][k], out[2][k]), k
+        for j in (1, 2, 3):
+            assert same_bits(out[0][k], out[j][k]), (k, j)
 
 
-def test_batch_same_with_snapshot_pairs_and_quads(grid):
-    """The batched launch reads float32 fields as snapshot quads; with quads off it reads pairs, and every
-    release ends with the same bits."""
+@pytest.mark.parametrize("layout", ["pairs", "quads", "octets"])
+def test_batch_same_in_every_pair_layout(grid, alone, layout):
+    """The batched launch reads float32 fields as snapshot pairs, quads or octets; every release ends with
+    the bits of its run alone."""
     from b200_runner import b200_fieldset
 
     from offline_particles_b200 import timesteppers
@@ -238,20 +240,19 @@ def test_batch_same_with_snapshot_pairs_and_quads(grid):
 
     g, fields = grid
     t_arr = g.time_array[:fields["u"].shape[0]]
-    out = []
-    for quads in (True, False):
-        timesteppers.SNAPSHOT_QUADS = quads
-        try:
-            rels = _releases(g, t_arr, SPECS)
-            b = ReleaseBatch(b200_fieldset(fields, g.hc, g.spec.nz), rels, buckets=64)
-            b.run()
-            b.synchronize()
-            out.append([b.result(r) for r in rels])
-        finally:
-            timesteppers.SNAPSHOT_QUADS = True
-    for q, (a, c) in enumerate(zip(*out)):
+    default = timesteppers.SNAPSHOT_LAYOUT
+    timesteppers.SNAPSHOT_LAYOUT = layout
+    try:
+        rels = _releases(g, t_arr, SPECS)
+        b = ReleaseBatch(b200_fieldset(fields, g.hc, g.spec.nz), rels, buckets=64)
+        b.run()
+        b.synchronize()
+        got = [b.result(r) for r in rels]
+    finally:
+        timesteppers.SNAPSHOT_LAYOUT = default
+    for q, want in enumerate(alone):
         for k in NAMES:
-            assert same_bits(a[k], c[k]), (q, k)
+            assert same_bits(got[q][k], want[k]), (q, k, mismatch_report(got[q][k], want[k]))
 
 
 @pytest.mark.parametrize("n,offset", [(1_000_003, 0), (4096, 1), (5, 0), (1, 0)])
@@ -274,6 +275,29 @@ def test_interleave_quads_and_xpairs_match_torch(n, offset):
     assert torch.equal(xp.view(-1, 2), torch.stack((s, s[nxt]), dim=1))
     with pytest.raises(ValueError, match="16-byte"):
         _lib.call("opb_interleave_quads", a.data_ptr(), b.data_ptr(), out.data_ptr() + 4, n, None)
+
+
+@pytest.mark.parametrize("n,row,offset", [(1_000_003, 1021, 0), (4096, 64, 1), (6, 3, 0), (1, 1, 0)])
+def test_interleave_octets_and_yxpairs_match_torch(n, row, offset):
+    import torch
+
+    from offline_particles_b200 import _lib
+
+    a = torch.randn(n + offset, dtype=torch.float32, device="cuda")[offset:]
+    b = torch.randn(n + offset, dtype=torch.float32, device="cuda")[offset:]
+    out = torch.full((8 * n,), float("nan"), dtype=torch.float32, device="cuda")
+    _lib.call("opb_interleave_octets", a.data_ptr(), b.data_ptr(), out.data_ptr(), n, row, None)
+    i = torch.arange(n, device="cuda")
+    idx = [torch.clamp(i + d, max=n - 1) for d in (0, 1, row, row + 1)]
+    want = torch.stack([t for j in idx for t in (a[j], b[j])], dim=1)
+    s = torch.randn(n + offset, dtype=torch.float64, device="cuda")[offset:]
+    yx = torch.full((4 * n,), float("nan"), dtype=torch.float64, device="cuda")
+    _lib.call("opb_neighbour_quads", s.data_ptr(), yx.data_ptr(), n, row, None)
+    torch.cuda.synchronize()
+    assert torch.equal(out.view(-1, 8), want)
+    assert torch.equal(yx.view(-1, 4), torch.stack([s[j] for j in idx], dim=1))
+    with pytest.raises(ValueError, match="32-byte"):
+        _lib.call("opb_interleave_octets", a.data_ptr(), b.data_ptr(), out.data_ptr() + 16, n, row, None)
 
 
 @pytest.mark.parametrize("dtype,n,offset", [("float32", 1_000_003, 0), ("float32", 4096, 1), ("float64", 777_777, 0),
