@@ -66,8 +66,9 @@ def parse():
     ap.add_argument("--dt", type=float, default=120.0)
     ap.add_argument("--ring-size", type=int, default=8, help="device snapshot slots of the end-to-end arm")
     ap.add_argument("--layout", choices=("auto", "octets", "quads", "pairs", "plain"), default="auto",
-                    help="how the kernels read snapshots: auto (the library default where pairs pay), octets, "
-                         "quads, pairs, or plain snapshots")
+                    help="how the kernels read snapshots: auto (the library defaults: pairs in the fused "
+                         "steppers where they pay, quads in the batched launch), octets, quads, pairs (every "
+                         "launch), or plain snapshots")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
     ap.add_argument("--study", choices=("precision", "batched", "serving"), default=None,
@@ -396,13 +397,20 @@ def b200_arm(a) -> None:
     s3.record()
     sim3.set_indices(hz, hy, hx)
     sim3.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+    w1 = time.perf_counter()
     sim3.run(a.steps)
+    w2 = time.perf_counter()
     P = sim3.device_particles
     for k in outs:
         outs[k].copy_(P.original(k), non_blocking=True)
     e3.record()
+    w3 = time.perf_counter()
     torch.cuda.synchronize()
     wall_e2e = time.perf_counter() - w0
+    # where the host spent the end-to-end region (the calls are asynchronous; a large share in one call
+    # means the host blocked there)
+    e2e_host_ms = {"set_indices": (w1 - w0) * 1e3, "run": (w2 - w1) * 1e3, "collect": (w3 - w2) * 1e3,
+                   "wait": (wall_e2e - (w3 - w0)) * 1e3}
     sim3.synchronize()
     e2e_ms = dist_max(max(s3.elapsed_time(e3), wall_e2e * 1e3), world)
     h2d = 3 * 8 * n + sum(fs3[k].h2d_bytes for k in TD)
@@ -445,7 +453,8 @@ def b200_arm(a) -> None:
                 "d2h_bytes_per_step": int(d2h / a.steps),
                 "path": "Simulation.set_indices from pinned host + run(K) streaming every snapshot from pinned "
                         "host memory + D2H of zidx/yidx/xidx/status",
-                "h2d_gbs_measured": h2d_gbs,
+                "h2d_gbs_measured": h2d_gbs, "device_ms": s3.elapsed_time(e3), "wall_ms": wall_e2e * 1e3,
+                "host_ms": e2e_host_ms,
                 "h2d_bound_value": total / ((h2d + d2h) / (h2d_gbs * 1e9)) if h2d_gbs else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic_per_step * avg_launch_steps if traffic_per_step else None,
@@ -895,7 +904,8 @@ def set_layout(layout: str) -> None:
     from offline_particles_b200 import timesteppers
 
     if layout in ("octets", "quads", "pairs"):
-        timesteppers.SNAPSHOT_PAIRS, timesteppers.SNAPSHOT_LAYOUT = "always", layout
+        timesteppers.SNAPSHOT_PAIRS = "always"
+        timesteppers.SNAPSHOT_LAYOUT = timesteppers.BATCH_LAYOUT = layout
     elif layout == "plain":
         timesteppers.SNAPSHOT_PAIRS = "never"
 

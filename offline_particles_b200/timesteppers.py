@@ -291,27 +291,35 @@ def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField], nparticles:
 # With float32 storage the pairs can be wider: "quads" (each element's snapshot pair followed by its
 # x-neighbour's, static h, dx, dy as x-pairs: a stencil's two x-neighbouring corners in one 16-byte load)
 # or "octets" (the pairs of a stencil face's four corners, static h, dx, dy as yx-pairs: one 32-byte load
-# per face, one per bilinear stencil).  They replace the pairs wherever pairs are used and storage is
-# float32; "pairs" keeps the plain pairs.
-SNAPSHOT_LAYOUT = "quads"
+# per face, one per bilinear stencil); "pairs" keeps the plain pairs.  Measured on B200 (1024x768x50,
+# 4.19 M particles, AB3): the fused kernel runs 1.4 % (quads) and 2.9 % (octets) faster per step, but the
+# wider build per snapshot interval costs more than that, so the fused steppers keep pairs.  The batched
+# launch, whose particles do far more work per interval than one build, gains 9 % with quads (its
+# gathers are bound by L1 requests) and 2 % with octets (four times the bytes per element in L1).
+SNAPSHOT_LAYOUT = "pairs"  # the fused steppers
+BATCH_LAYOUT = "quads"  # ReleaseBatch
 NEIGHBOUR_STATICS = ("h", "dx", "dy")
 _STATIC_KIND = {"quads": "xpairs", "octets": "yxpairs"}
 _PAIR_CODE = {"quads": _lib.F32_QUADS, "octets": _lib.F32_OCTS}
 _STATIC_CODE = {"xpairs": _lib.F64_XPAIRS, "yxpairs": _lib.F64_YXPAIRS}
 
 
-def pair_layout(launcher: Launcher, td: dict[str, TimeDependentField], roles: dict[str, str] | None = None
-                ) -> tuple[str, dict[str, StaticField] | None]:
-    """The pair layout of a launch that reads pairs ("pairs", "quads" or "octets") and, for the wider
-    two, the static fields read beside them as neighbour layouts."""
-    if SNAPSHOT_LAYOUT == "pairs" or not td or not all(f.storage == "float32" for f in td.values()):
+def pair_layout(launcher: Launcher, td: dict[str, TimeDependentField], roles: dict[str, str] | None = None,
+                layout: str | None = None) -> tuple[str, dict[str, StaticField] | None]:
+    """The pair layout of a launch that reads pairs ("pairs", "quads" or "octets"; ``layout``, default
+    ``SNAPSHOT_LAYOUT``) and, for the wider two, the static fields read beside them as neighbour
+    layouts.  The wider layouts need float32 storage and static h, dx, dy; otherwise "pairs"."""
+    layout = SNAPSHOT_LAYOUT if layout is None else layout
+    if layout not in ("pairs", "quads", "octets"):
+        raise ValueError(f"unknown pair layout {layout!r}")
+    if layout == "pairs" or not td or not all(f.storage == "float32" for f in td.values()):
         return "pairs", None
     fs = launcher.fieldset
     roles = roles or {}
     statics = {n: fs[roles.get(n, n)] for n in NEIGHBOUR_STATICS if roles.get(n, n) in fs}
     if len(statics) != len(NEIGHBOUR_STATICS) or not all(isinstance(f, StaticField) for f in statics.values()):
         return "pairs", None
-    return SNAPSHOT_LAYOUT, statics
+    return layout, statics
 
 
 def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField], layout: str = "pairs",

@@ -240,8 +240,8 @@ def test_batch_same_in_every_pair_layout(grid, alone, layout):
 
     g, fields = grid
     t_arr = g.time_array[:fields["u"].shape[0]]
-    default = timesteppers.SNAPSHOT_LAYOUT
-    timesteppers.SNAPSHOT_LAYOUT = layout
+    default = timesteppers.BATCH_LAYOUT
+    timesteppers.BATCH_LAYOUT = layout
     try:
         rels = _releases(g, t_arr, SPECS)
         b = ReleaseBatch(b200_fieldset(fields, g.hc, g.spec.nz), rels, buckets=64)
@@ -249,7 +249,7 @@ def test_batch_same_in_every_pair_layout(grid, alone, layout):
         b.synchronize()
         got = [b.result(r) for r in rels]
     finally:
-        timesteppers.SNAPSHOT_LAYOUT = default
+        timesteppers.BATCH_LAYOUT = default
     for q, want in enumerate(alone):
         for k in NAMES:
             assert same_bits(got[q][k], want[k]), (q, k, mismatch_report(got[q][k], want[k]))
