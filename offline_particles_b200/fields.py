@@ -262,12 +262,88 @@ class SnapshotLoadError(RuntimeError):
     """A snapshot could not be brought to the device: its source raised, or delivered nothing in time."""
 
 
+class TicketOrder:
+    """Issue in ticket order: ``ticket()`` hands out 0, 1, 2, ...; ``wait_turn(t)`` returns once every
+    ticket below ``t`` is released, or after ``limit`` seconds, when it passes the stuck ones over for
+    everyone after them; ``release(t)`` marks ticket ``t`` issued (or abandoned).  Host logic only."""
+
+    def __init__(self, limit: float = 2.0) -> None:
+        self.limit = limit
+        self.cv = threading.Condition()
+        self.next_ticket = 0
+        self.issued_below = 0  # every ticket below this has been released (or passed over)
+        self.done: set[int] = set()
+
+    def ticket(self) -> int:
+        with self.cv:
+            t = self.next_ticket
+            self.next_ticket += 1
+            return t
+
+    def wait_turn(self, t: int, limit: float | None = None) -> bool:
+        """True if every earlier ticket was released in time, False if they were passed over."""
+        with self.cv:
+            if self.cv.wait_for(lambda: self.issued_below >= t, timeout=self.limit if limit is None else limit):
+                return True
+            self.issued_below = t
+            self.done = {d for d in self.done if d >= t}
+            self.cv.notify_all()
+            return False
+
+    def release(self, t: int) -> None:
+        with self.cv:
+            if t < self.issued_below:
+                return  # passed over while it was stuck
+            self.done.add(t)
+            while self.issued_below in self.done:
+                self.done.remove(self.issued_below)
+                self.issued_below += 1
+            self.cv.notify_all()
+
+
+class _CopyQueue:
+    """The copy stream of one device, shared by every snapshot ring on it, and the order in which the
+    rings issue onto it: the order in which their uploads were scheduled (``TicketOrder``).
+
+    A copy engine serves several streams with queued copies one stream at a time rather than in the
+    order the copies were queued, so rings with streams of their own deliver every snapshot of one field
+    before the first of the next, and a launch that needs snapshot k of every field waits for all the
+    later snapshots of the fields served first.  On one stream in scheduling order, snapshot k of every
+    field lands before snapshot k + 1 of any.  Host staging still runs in each ring's own thread; only
+    the issue of the copy waits for the uploads scheduled before it, at most ``TURN_TIMEOUT`` seconds and
+    a quarter of the ring's ``load_timeout`` (a stalled source then gives up the order, never the
+    progress of the others, and is the one whose snapshot times out).
+
+    One stream cannot deadlock the rings: a launch waits only for uploads that were issued before it
+    was queued (``acquire`` returns once its upload is issued), and an upload waits only for launches
+    queued before it (the last reader of its slot)."""
+
+    TURN_TIMEOUT = 2.0
+    _by_device: dict = {}
+    _registry_lock = threading.Lock()
+
+    @classmethod
+    def of(cls, device: torch.device) -> "_CopyQueue":
+        index = device.index if device.index is not None else torch.cuda.current_device()
+        with cls._registry_lock:
+            q = cls._by_device.get(index)
+            if q is None:
+                q = cls._by_device[index] = cls(torch.device("cuda", index))
+            return q
+
+    def __init__(self, device: torch.device) -> None:
+        self.stream = torch.cuda.Stream(device=device)
+        self.order = TicketOrder(self.TURN_TIMEOUT)
+
+
 class SnapshotRing:
     """Device slots for the snapshots of one time-dependent field.
 
     ``acquire(k)`` returns the device tensor of snapshot ``k`` and makes the
-    current stream wait for its upload.  Uploads run on a side stream from a
-    background thread: host read -> pinned staging buffer -> async H2D copy.
+    current stream wait for its upload.  Uploads run on the device's copy stream
+    (``_CopyQueue``, shared by every ring on the device, in scheduling order)
+    from a background thread: host read -> pinned staging buffer -> async H2D
+    copy.
     """
 
     def __init__(self, source, spatial_shape: tuple[int, ...], np_dtype: np.dtype, nslots: int,
@@ -292,7 +368,8 @@ class SnapshotRing:
         # per slot: event recorded after the last launch known to read it (None: unknown -> wait for
         # everything queued so far before overwriting the slot)
         self.last_use: dict[int, torch.cuda.Event | None] = {}
-        self.copy_stream = torch.cuda.Stream(device=device)
+        self.queue = _CopyQueue.of(device)
+        self.copy_stream = self.queue.stream
         # a device-resident or device-generated source is copied device to device: no host staging
         on_device = (isinstance(source, torch.Tensor) and source.is_cuda) or hasattr(source, "produce")
         self.staging = [] if on_device else [torch.empty(tuple(spatial_shape), dtype=torch_dtype(np_dtype),
@@ -320,10 +397,21 @@ class SnapshotRing:
     def scales(self, k: int) -> torch.Tensor | None:
         return None if self.storage is None else self.slot_scales[self.slot_of[k]]
 
-    def _upload(self, k: int, slot: int, slot_free: torch.cuda.Event) -> None:
+    def _wait_turn(self, ticket: int) -> None:
+        lt = self.load_timeout
+        self.queue.order.wait_turn(ticket, None if lt is None else min(_CopyQueue.TURN_TIMEOUT, 0.25 * lt))
+
+    def _upload(self, k: int, slot: int, slot_free: torch.cuda.Event, ticket: int) -> None:
+        try:
+            self._upload_in_turn(k, slot, slot_free, ticket)
+        finally:
+            self.queue.order.release(ticket)
+
+    def _upload_in_turn(self, k: int, slot: int, slot_free: torch.cuda.Event, ticket: int) -> None:
         src = self.source
         if hasattr(src, "produce"):
             # generated on the device, on the copy stream
+            self._wait_turn(ticket)
             with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
                 if slot_free is not None:
                     self.copy_stream.wait_event(slot_free)
@@ -338,6 +426,7 @@ class SnapshotRing:
             return
         if isinstance(src, torch.Tensor) and (src.is_pinned() or src.is_cuda):
             # already in pinned host memory (or on the device): one async copy, no staging
+            self._wait_turn(ticket)
             with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
                 if slot_free is not None:
                     self.copy_stream.wait_event(slot_free)
@@ -356,6 +445,7 @@ class SnapshotRing:
                 self.staging_free[b].synchronize()
             stage = self.staging[b]
             stage.copy_(torch.from_numpy(host))
+            self._wait_turn(ticket)
             with torch.cuda.stream(self.copy_stream):
                 if slot_free is not None:
                     self.copy_stream.wait_event(slot_free)
@@ -397,7 +487,12 @@ class SnapshotRing:
         self.last_use[slot] = None
         self.slot_of[k] = slot
         self.lru.append(k)
-        self.pending[k] = self.pool.submit(self._upload, k, slot, slot_free)
+        ticket = self.queue.order.ticket()
+        try:
+            self.pending[k] = self.pool.submit(self._upload, k, slot, slot_free, ticket)
+        except BaseException:
+            self.queue.order.release(ticket)
+            raise
         return True
 
     def acquire(self, k: int, keep: set[int] | frozenset = frozenset()) -> torch.Tensor:
