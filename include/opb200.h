@@ -330,17 +330,26 @@ int opb_trilinear_interpolation(const opb_particles *p, const opb_field *f, cons
 
 /* ---- fused steppers ------------------------------------------------------ */
 
+/* Step tables of the fused entry points (the *_steps functions, float64 and
+ * float32): a DEVICE array, or a HOST array (pageable or pinned) of at most
+ * OPB_INLINE_TABLE entries, which the call copies into the launch's parameters.
+ * A host table needs no copy engine, so the launch does not queue behind
+ * host-to-device copies issued before it (snapshot uploads); the caller may
+ * reuse the array as soon as the call returns. */
+#define OPB_INLINE_TABLE 720
+
 /* `nsteps` whole RK2 steps in one launch: per step, the preset's validation
  * pre-step, step_1 at t, step_2 at t + alpha dt, update at t + dt
- * (timesteppers.py:241-257; models/roms/__init__.py:37-62).  `table` is a
- * DEVICE array of 3*nsteps opb_time entries (t, t + alpha dt, t + dt per
- * step).  validate = 0 drops the pre-step.  Results equal `nsteps` rounds of
+ * (timesteppers.py:241-257; models/roms/__init__.py:37-62).  `table` is an
+ * array of 3*nsteps opb_time entries (t, t + alpha dt, t + dt per step), on the
+ * device or on the host (OPB_INLINE_TABLE).  validate = 0 drops the pre-step.  Results equal `nsteps` rounds of
  * the stage entry points; k1/k2 and z hold the last step's values. */
 int opb_rk2_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                               const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
 /* `nsteps` whole AB3 steps in one launch: validation pre-step, ab3 at t,
  * ab3_post at t + dt (timesteppers.py:296-305; models/roms/__init__.py:65-96).
- * `table`: DEVICE array of 2*nsteps opb_time entries (t, t + dt per step). */
+ * `table`: 2*nsteps opb_time entries (t, t + dt per step), on the device or on
+ * the host (OPB_INLINE_TABLE). */
 int opb_ab3_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                               const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
 

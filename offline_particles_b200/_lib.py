@@ -16,6 +16,7 @@ F64, F32, BF16, F16 = 0, 1, 2, 3
 F64_PAIRS, F32_PAIRS = 4, 5
 F32_QUADS, F64_XPAIRS = 6, 7
 F32_OCTS, F64_YXPAIRS = 8, 9
+INLINE_TABLE = 720  # OPB_INLINE_TABLE: opb_time entries a host step table may hold
 ABI_VERSION = 5
 OK, EINVAL, ECUDA = 0, 1, 2
 ERRF_ZERO_DIVISION = 1

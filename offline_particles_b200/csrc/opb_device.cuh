@@ -9,6 +9,7 @@
 #include <cstdint>
 
 #include "opb200.h"
+#include "opb_steptable.cuh"
 
 namespace opb {
 

@@ -23,11 +23,14 @@
 
 #include "opb200.h"
 #include "opb_errors.h"
+#include "opb_steptable.cuh"
 
 namespace opb_fast {
 namespace {
 
 using opb::fail;
+using opb::make_step_table;
+using opb::StepTable;
 
 constexpr int kBlock = 256;
 constexpr int kMaxLevels = 128;
@@ -564,7 +567,7 @@ template <typename S, bool SCALED>
 __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps_fp32(const __grid_constant__ FParticles p,
                                                               const __grid_constant__ FScalars sc,
                                                               const __grid_constant__ FRoms r,
-                                                              const opb_time *__restrict__ table, int nsteps,
+                                                              const __grid_constant__ StepTable table, int nsteps,
                                                               int validate_pre) {
     FAST_LEVELS(r, sc);
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -578,7 +581,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps_fp32(const __grid_const
     for (int k = 0; k < nsteps; ++k) {
         if (validate_pre) s.status = validate(s.status, s.zidx, cval(s.y), cval(s.x), sc.bounds);
         if (s.status & ST_INACTIVE) break;
-        const opb_time t1 = table[2 * k], t2 = table[2 * k + 1];
+        const opb_time t1 = table.at(2 * k), t2 = table.at(2 * k + 1);
         const bool reuse = k > 0 && same_time(t1, s.at);
         if (!ab3_step(s, bind_all<S, SCALED>(r, t1), sc, reuse)) {
             raise_zero_division(p);
@@ -609,7 +612,7 @@ template <typename S, bool SCALED>
 __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps_fp32(const __grid_constant__ FParticles p,
                                                               const __grid_constant__ FScalars sc,
                                                               const __grid_constant__ FRoms r,
-                                                              const opb_time *__restrict__ table, int nsteps,
+                                                              const __grid_constant__ StepTable table, int nsteps,
                                                               int validate_pre) {
     FAST_LEVELS(r, sc);
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -623,7 +626,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps_fp32(const __grid_const
     for (int k = 0; k < nsteps; ++k) {
         if (validate_pre) s.status = validate(s.status, s.zidx, cval(s.y), cval(s.x), sc.bounds);
         if (s.status & ST_INACTIVE) break;
-        const opb_time t1 = table[3 * k], t2 = table[3 * k + 1], t3 = table[3 * k + 2];
+        const opb_time t1 = table.at(3 * k), t2 = table.at(3 * k + 1), t3 = table.at(3 * k + 2);
         const bool reuse = k > 0 && same_time(t1, s.at);
         if (!rk2_stage1(s, bind_all<S, SCALED>(r, t1), sc, reuse)) {
             raise_zero_division(p);
@@ -782,12 +785,14 @@ int steps_fp32(const char *what, bool rk2, const opb_particles *p, const opb_sca
     if (nsteps < 0) return fail(OPB_EINVAL, "%s: negative step count", what);
     if (nsteps > 0 && !table) return fail(OPB_EINVAL, "%s: step table is NULL", what);
     if (fp.n == 0 || nsteps == 0) return OPB_OK;
+    static thread_local StepTable tab;  // up to 17 KB: kept off the stack
+    if ((rc = make_step_table(table, (long long)nsteps * (rk2 ? 3 : 2), tab, what))) return rc;
     const unsigned g = (unsigned)((fp.n + kBlock - 1) / kBlock);
     cudaStream_t st = (cudaStream_t)stream;
 #define OPB_FAST_LAUNCH(S, SC)                                                                  \
     do {                                                                                        \
-        if (rk2) k_rk2_steps_fp32<S, SC><<<g, kBlock, 0, st>>>(fp, fs, fr, table, nsteps, validate_pre); \
-        else k_ab3_steps_fp32<S, SC><<<g, kBlock, 0, st>>>(fp, fs, fr, table, nsteps, validate_pre);     \
+        if (rk2) k_rk2_steps_fp32<S, SC><<<g, kBlock, 0, st>>>(fp, fs, fr, tab, nsteps, validate_pre); \
+        else k_ab3_steps_fp32<S, SC><<<g, kBlock, 0, st>>>(fp, fs, fr, tab, nsteps, validate_pre);     \
     } while (0)
     if (dtype == OPB_F32) {
         if (scaled) OPB_FAST_LAUNCH(float, true);

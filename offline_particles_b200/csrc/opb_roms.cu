@@ -191,7 +191,8 @@ template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN>
 __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
-                                                      const opb_time *__restrict__ table, int nsteps, int validate_pre) {
+                                                      const __grid_constant__ StepTable table, int nsteps,
+                                                      int validate_pre) {
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
     for (int k = 0; k < nsteps; ++k) {
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
-        const opb_time t1 = table[3 * k], t2 = table[3 * k + 1], t3 = table[3 * k + 2];
+        const opb_time t1 = table.at(3 * k), t2 = table.at(3 * k + 1), t3 = table.at(3 * k + 2);
         const bool reuse = k > 0 && same_time(t1, s.at);
         if (!rk2_stage1(s, bind_all<T, I, FIXED, LAYOUT>(r, t1), sc, reuse)) {
             raise_zero_division(p);
@@ -240,7 +241,8 @@ template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool IS
 __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
-                                                      const opb_time *__restrict__ table, int nsteps, int validate_pre) {
+                                                      const __grid_constant__ StepTable table, int nsteps,
+                                                      int validate_pre) {
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
@@ -262,7 +264,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
     for (int k = 0; k < nsteps; ++k) {
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
-        const opb_time t1 = table[2 * k], t2 = table[2 * k + 1];
+        const opb_time t1 = table.at(2 * k), t2 = table.at(2 * k + 1);
         const bool reuse = k > 0 && same_time(t1, s.at);
         bool ok;
         if constexpr (ISO) ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT>(r, t1), sc, reuse, IsoVel{rho_t, sc.w_max,
@@ -461,6 +463,8 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     if (!rc && iso) rc = need_fields(p, what, {{"rho_t", p->rho_t}});
     if (rc) return rc;
     if (dp.n == 0 || nsteps == 0) return OPB_OK;
+    static thread_local StepTable tab;  // up to 17 KB: kept off the stack
+    if ((rc = make_step_table(table, (long long)nsteps * (rk2 ? 3 : 2), tab, what))) return rc;
     const unsigned grid = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
     const bool fixed = roms_layout(dr);
@@ -468,10 +472,10 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
         using T = decltype(tv);
         using I = decltype(iv);
         constexpr int LAYOUT = decltype(lv)::value;
-        if (rk2) k_rk2_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        if (rk2) k_rk2_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
         else if (iso)
-            k_ab3_steps<T, I, true, LAYOUT, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
-        else k_ab3_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+            k_ab3_steps<T, I, true, LAYOUT, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        else k_ab3_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
     };
     if (layout == LAYOUT_QUADS || layout == LAYOUT_OCTS) {
         if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads and octets hold float32 storage", what);
@@ -490,11 +494,11 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
         using I = decltype(iv);
         if (layout == LAYOUT_PAIRS) go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{});
         else if (fixed) go(tv, iv, std::integral_constant<int, LAYOUT_PLAIN>{});
-        else if (rk2) k_rk2_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        else if (rk2) k_rk2_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
         else if (iso)
-            k_ab3_steps<T, I, false, LAYOUT_PLAIN, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps,
+            k_ab3_steps<T, I, false, LAYOUT_PLAIN, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps,
                                                                                  validate_pre);
-        else k_ab3_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, table, nsteps, validate_pre);
+        else k_ab3_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
     });
     return check_launch(what);
 }

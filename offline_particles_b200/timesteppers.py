@@ -430,9 +430,15 @@ def _entry(name: str, launcher: Launcher) -> str:
     return name + ("_fp32" if launcher.arithmetic == "float32" else "")
 
 
-def _upload_table(table, device) -> torch.Tensor:
+def _table_arg(table, device):
+    """The step-table argument of a fused launch, and what must stay alive until the call returns: the
+    host table itself while it fits the launch's parameters (no copy, so the launch does not queue
+    behind the snapshot uploads already issued), else a device copy."""
+    if len(table) <= _lib.INLINE_TABLE:
+        return ctypes.addressof(table), table
     raw = torch.frombuffer(bytearray(bytes(table)), dtype=torch.uint8).pin_memory()
-    return raw.to(device, non_blocking=True)
+    dev = raw.to(device, non_blocking=True)
+    return dev.data_ptr(), dev
 
 
 def _prefetch_after(td: dict[str, TimeDependentField], needed: list[int], limit: int | None = None) -> None:
@@ -532,10 +538,10 @@ class RK2Timestepper(Timestepper):
             "_dt": self._normalised_dt, "_RK2_alpha": self._alpha,
             **{n: launcher.scalar(n, self._tidx) for n in ("zidx_min", "zidx_max", "yidx_min", "yidx_max",
                                                            "xidx_min", "xidx_max")}})
-        dev_table = _upload_table(table, particles.device)
+        table_ptr, _keep = _table_arg(table, particles.device)
         _notify("before", len(steps))
         _lib.call(_entry("opb_rk2_w_advection_steps", launcher), ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
-                  ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
+                  ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
         _notify("after", len(steps))
         _prefetch_after(td, needed, self._prefetch_limit)
@@ -613,10 +619,10 @@ class ABTimestepper(Timestepper):
         if iso and launcher.arithmetic != "float64":
             raise ValueError("the isopycnal follower has float64 steppers only")
         entry = "opb_ab3_isopycnal_following_steps" if iso else _entry("opb_ab3_w_advection_steps", launcher)
-        dev_table = _upload_table(table, particles.device)
+        table_ptr, _keep = _table_arg(table, particles.device)
         _notify("before", len(steps))
         _lib.call(entry, ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
-                  ctypes.byref(rf), dev_table.data_ptr(), len(steps), int(self._pre_step_kernel is not None),
+                  ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None),
                   _abi.stream(particles))
         _notify("after", len(steps))
         _prefetch_after(td, needed, self._prefetch_limit)

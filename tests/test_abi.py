@@ -173,3 +173,31 @@ def test_argument_errors_need_no_gpu():
 def test_call_raises_value_error():
     with pytest.raises(ValueError, match="NULL"):
         _lib.call("opb_validation", None, None, None)
+
+
+CONSTANT_PROBE = r"""
+#include <stdio.h>
+#include "opb200.h"
+#define C(name) printf(#name " %d\n", (int)(name))
+int main(void) {
+    C(OPB_ABI_VERSION); C(OPB_MAX_SLOTS); C(OPB_F64); C(OPB_F32); C(OPB_BF16); C(OPB_F16); C(OPB_F64_PAIRS);
+    C(OPB_F32_PAIRS); C(OPB_F32_QUADS); C(OPB_F64_XPAIRS); C(OPB_F32_OCTS); C(OPB_F64_YXPAIRS);
+    C(OPB_INLINE_TABLE); C(OPB_EINVAL); C(OPB_ECUDA);
+    return 0;
+}
+"""
+
+
+def test_header_constants_match_the_binding(tmp_path):
+    src = tmp_path / "consts.c"
+    src.write_text(CONSTANT_PROBE)
+    exe = tmp_path / "consts"
+    subprocess.run(["gcc", "-std=c99", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    c = {k: int(v) for k, v in (line.split() for line in out if line)}
+    py = {"OPB_ABI_VERSION": _lib.ABI_VERSION, "OPB_MAX_SLOTS": _lib.MAX_SLOTS, "OPB_F64": _lib.F64,
+          "OPB_F32": _lib.F32, "OPB_BF16": _lib.BF16, "OPB_F16": _lib.F16, "OPB_F64_PAIRS": _lib.F64_PAIRS,
+          "OPB_F32_PAIRS": _lib.F32_PAIRS, "OPB_F32_QUADS": _lib.F32_QUADS, "OPB_F64_XPAIRS": _lib.F64_XPAIRS,
+          "OPB_F32_OCTS": _lib.F32_OCTS, "OPB_F64_YXPAIRS": _lib.F64_YXPAIRS,
+          "OPB_INLINE_TABLE": _lib.INLINE_TABLE, "OPB_EINVAL": _lib.EINVAL, "OPB_ECUDA": _lib.ECUDA}
+    assert c == py

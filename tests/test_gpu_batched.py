@@ -346,3 +346,30 @@ def test_batch_records_trajectories_like_a_simulation(grid):
             P = sim.particles
             for k in ("zidx", "yidx", "xidx", "status"):
                 assert same_bits(tr[k][q], P[k]), (scheme, q, k)
+
+
+@pytest.mark.parametrize("scheme,dt", [("rk2", 300.0), ("ab3", 120.0)])
+def test_host_and_device_step_tables_give_the_same_bits(grid, scheme, dt, monkeypatch):
+    """A fused launch takes its step table from host memory (in the launch's parameters) or from device
+    memory; both give the same bits."""
+    from b200_runner import b200_fieldset
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200 import _lib
+
+    g, fields = grid
+    t_arr = g.time_array[:fields["u"].shape[0]]
+    z, y, x = g.release(2000, seed=78)
+    out = []
+    for inline in (_lib.INLINE_TABLE, 0):
+        monkeypatch.setattr(_lib, "INLINE_TABLE", inline)
+        f = opb.roms.rk2_w_advection_timestepper if scheme == "rk2" else opb.roms.ab3_w_advection_timestepper
+        sim = opb.SimulationBuilder(f(t_arr, np.float64(dt), time=np.float64(600.0)),
+                                    b200_fieldset(fields, g.hc, g.spec.nz)).build_simulation(len(z))
+        sim.set_indices(z, y, x)
+        sim.set_particle_field("status", 10 if scheme == "ab3" else 0)
+        sim.run(70)
+        P = sim.particles
+        out.append({k: P[k] for k in NAMES})
+    for k in NAMES:
+        assert same_bits(out[0][k], out[1][k]), k
