@@ -450,14 +450,20 @@ def _prefetch_after(td: dict[str, TimeDependentField], needed: list[int], limit:
     last = needed[-1]
     for f in td.values():
         f.mark_used(needed)
-        if not f.streamed:
-            continue
-        keep = {needed[-2], last} if len(needed) > 1 else {last}
-        for j in range(1, max(1, f.ring_size - len(keep)) + 1):
-            if limit is not None and last + j > limit:
-                break  # past the snapshots the current run needs
-            keep.add(last + j)
-            f.prefetch(last + j, keep)
+    streamed = [f for f in td.values() if f.streamed]
+    if not streamed:
+        return
+    keep = {needed[-2], last} if len(needed) > 1 else {last}
+    depth = {id(f): max(1, f.ring_size - len(keep)) for f in streamed}
+    # snapshot by snapshot, every field of one before any of the next: the copy stream delivers them in
+    # that order, so the next launch's snapshots are not queued behind later ones of other fields
+    for j in range(1, max(depth.values()) + 1):
+        if limit is not None and last + j > limit:
+            break  # past the snapshots the current run needs
+        keep.add(last + j)
+        for f in streamed:
+            if j <= depth[id(f)]:
+                f.prefetch(last + j, set(keep))
 
 
 class RK2Timestepper(Timestepper):
