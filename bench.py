@@ -69,6 +69,8 @@ def parse():
                     help="how the kernels read snapshots: auto (the library defaults: pairs in the fused "
                          "steppers where they pay, quads in the batched launch), octets, quads, pairs (every "
                          "launch), or plain snapshots")
+    ap.add_argument("--no-bundles", action="store_true",
+                    help="read h, zeta, dx, dy as separate fields (no 2-D bundles)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
     ap.add_argument("--study", choices=("precision", "batched", "serving"), default=None,
@@ -466,7 +468,7 @@ def b200_arm(a) -> None:
         "gpu_launches": len(launch_ms) + 2 * len(sorts) + len(builds),
         "sorts_in_timed_region": len(sorts),
         "pair_builds_in_timed_region": len(builds),
-        "snapshot_layout": a.layout,
+        "snapshot_layout": a.layout, "bundles_2d": not a.no_bundles,
         "active_particles_end": active,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
@@ -913,6 +915,10 @@ def set_layout(layout: str) -> None:
 def main() -> None:
     a = parse()
     set_layout(a.layout)
+    if a.no_bundles:
+        from offline_particles_b200 import timesteppers
+
+        timesteppers.BUNDLE_2D = False
     if a.study == "precision":
         precision_study(a)
     elif a.study == "batched":

@@ -73,6 +73,19 @@ extern "C" {
 #define OPB_F32_OCTS 8
 /* yx-pairs of a static float64 field: data[0] holds {s[i], s[i+1], s[i+R], s[i+R+1]} */
 #define OPB_F64_YXPAIRS 9
+/* 2-D bundles (with snapshot pairs or quads of float32 u, v, w): h, zeta, dx and
+ * dy share one stagger, so two of them can share one load per two stencil
+ * corners.  zeta as OPB_F32_ZETA_H: data[k] holds, per element i, the 64-bit
+ * words {h[i], zeta pair[i], h[i+1], zeta pair[i+1]} (a zeta pair: the earlier
+ * snapshot's float in the low half, the later's in the high half; pair slot k as
+ * for OPB_F32_PAIRS), with h as OPB_F64_IN_ZETA (read from zeta's bundle; same
+ * shape and offsets).  dx as OPB_F64_DX_DY: data[0] holds {dx[i], dy[i], dx[i+1],
+ * dy[i+1]}, with dy as OPB_F64_IN_DX (same shape and offsets).  Bundle buffers
+ * are 32-byte aligned; all four codes come together. */
+#define OPB_F32_ZETA_H 10
+#define OPB_F64_IN_ZETA 11
+#define OPB_F64_DX_DY 12
+#define OPB_F64_IN_DX 13
 
 /* return codes */
 #define OPB_OK 0
@@ -218,6 +231,16 @@ int opb_interleave_octets(const float *a, const float *b, float *out, int64_t n,
  * past the end replaced by n - 1 (out holds 4n doubles; DEVICE buffers, out
  * 32-byte aligned). */
 int opb_neighbour_quads(const double *s, double *out, int64_t n, int64_t row, void *stream);
+
+/* No reference counterpart: the zeta-with-h bundle of float32 zeta snapshots a
+ * (earlier) and b (later) and float64 h, n elements each (OPB_F32_ZETA_H; out
+ * holds 32 bytes per element, 32-byte aligned; the last element's neighbour is
+ * itself). */
+int opb_bundle_zeta_h(const float *a, const float *b, const double *h, void *out, int64_t n, void *stream);
+
+/* No reference counterpart: the dx-with-dy bundle of float64 dx and dy, n
+ * elements each (OPB_F64_DX_DY; out holds 4n doubles, 32-byte aligned). */
+int opb_bundle_dx_dy(const double *dx, const double *dy, double *out, int64_t n, void *stream);
 
 /* ---- batched release experiments ---------------------------------------------
  * No single reference counterpart: the reference advances one release per

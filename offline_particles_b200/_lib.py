@@ -16,6 +16,7 @@ F64, F32, BF16, F16 = 0, 1, 2, 3
 F64_PAIRS, F32_PAIRS = 4, 5
 F32_QUADS, F64_XPAIRS = 6, 7
 F32_OCTS, F64_YXPAIRS = 8, 9
+F32_ZETA_H, F64_IN_ZETA, F64_DX_DY, F64_IN_DX = 10, 11, 12, 13
 INLINE_TABLE = 720  # OPB_INLINE_TABLE: opb_time entries a host step table may hold
 ABI_VERSION = 5
 OK, EINVAL, ECUDA = 0, 1, 2
@@ -117,6 +118,8 @@ SIGNATURES = {
     "opb_neighbour_pairs": [_VP, _VP, ctypes.c_int64, _VP],
     "opb_interleave_octets": [_VP, _VP, _VP, ctypes.c_int64, ctypes.c_int64, _VP],
     "opb_neighbour_quads": [_VP, _VP, ctypes.c_int64, ctypes.c_int64, _VP],
+    "opb_bundle_zeta_h": [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP],
+    "opb_bundle_dx_dy": [_VP, _VP, _VP, ctypes.c_int64, _VP],
     "opb_quantize_levels": [_VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP, _VP],
 }
 

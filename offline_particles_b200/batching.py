@@ -495,7 +495,7 @@ class ReleaseBatch:
         load (quads or octets with float32 storage: two or four corners per load).  Pair j + 1 exists only when
         snapshot j + 2 is in the window."""
         its = [j, j + 1] if j + 2 <= window[-1] else [j]
-        pair_fields(rf, its, self._td, *pair_layout(self.launcher, self._td, layout=timesteppers.BATCH_LAYOUT))
+        pair_fields(rf, its, self._td, pair_layout(self.launcher, self._td, layout=timesteppers.BATCH_LAYOUT))
 
     # --------------------------------------------------------------- planning
     def _plan(self, j: int):

@@ -21,7 +21,7 @@ namespace {
 // time table, reading the time-dependent fields as snapshot pairs or quads
 // (LAYOUT).  SCHEME: OPB_SCHEME_RK2 or OPB_SCHEME_AB3 compiles one scheme only
 // (smaller code, fewer live registers); 0 decides per experiment.
-template <typename T, typename I, int SCHEME, int LAYOUT>
+template <typename T, typename I, int SCHEME, int LAYOUT, bool B2>
 __device__ __forceinline__ void batched_particle(const DParticles &p, long long i, const opb_experiment &E,
                                                  const DScalars &sc0, const DRoms &r, const opb_time *table,
                                                  const Levels &L) {
@@ -52,26 +52,26 @@ __device__ __forceinline__ void batched_particle(const DParticles &p, long long 
         if (ab3) {
             const opb_time t1 = tab[2 * k], t2 = tab[2 * k + 1];
             const bool reuse = k > 0 && same_time(t1, s.at);
-            if (!ab3_step(s, bind_all<T, I, true, LAYOUT>(r, t1), sc, reuse)) {
+            if (!ab3_step(s, bind_all<T, I, true, LAYOUT, B2>(r, t1), sc, reuse)) {
                 raise_zero_division(p);
                 break;
             }
             moved = true;
-            ab3_post(s, bind_all<T, I, true, LAYOUT>(r, t2), L, sc);
+            ab3_post(s, bind_all<T, I, true, LAYOUT, B2>(r, t2), L, sc);
             s.at = t2;
         } else {
             const opb_time t1 = tab[3 * k], t2 = tab[3 * k + 1], t3 = tab[3 * k + 2];
             const bool reuse = k > 0 && same_time(t1, s.at);
-            if (!rk2_stage1(s, bind_all<T, I, true, LAYOUT>(r, t1), sc, reuse)) {
+            if (!rk2_stage1(s, bind_all<T, I, true, LAYOUT, B2>(r, t1), sc, reuse)) {
                 raise_zero_division(p);
                 break;
             }
             moved = true;
-            if (!rk2_stage2(s, bind_all<T, I, true, LAYOUT>(r, t2), L, sc)) {
+            if (!rk2_stage2(s, bind_all<T, I, true, LAYOUT, B2>(r, t2), L, sc)) {
                 raise_zero_division(p);
                 break;
             }
-            rk2_update(s, bind_all<T, I, true, LAYOUT>(r, t3), L, sc);
+            rk2_update(s, bind_all<T, I, true, LAYOUT, B2>(r, t3), L, sc);
             s.at = t3;
         }
     }
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan_items(opb_batch_header *_
 // one experiment's segment, so the 32 lanes of a warp share a scheme, a step
 // count and a time table and never diverge on them.  MINB CTAs of BLOCK
 // threads per SM: the register budget per thread is 65536 / (BLOCK * MINB).
-template <typename T, typename I, int BLOCK, int MINB, int SCHEME, int LAYOUT>
+template <typename T, typename I, int BLOCK, int MINB, int SCHEME, int LAYOUT, bool B2>
 __global__ void __launch_bounds__(BLOCK, MINB) k_batched_steps(const __grid_constant__ DParticles p,
                                                             opb_batch_header *__restrict__ hdr,
                                                             const opb_experiment *__restrict__ exps,
@@ -210,12 +210,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_batched_steps(const __grid_cons
         if (i >= end || i < E.start || i >= E.start + E.count || E.nsteps <= 0) continue;
         if (i < 0 || i >= p.n) continue;
         if (SCHEME != 0 && E.scheme != SCHEME) continue;  // another launch's experiment
-        batched_particle<T, I, SCHEME, LAYOUT>(p, i, E, sc, r, table, L);
+        batched_particle<T, I, SCHEME, LAYOUT, B2>(p, i, E, sc, r, table, L);
     }
 }
 
 // launch the <BLOCK, MINB> instance; false if the shape is not compiled
-template <typename T, typename I, int SCHEME, int LAYOUT>
+template <typename T, typename I, int SCHEME, int LAYOUT, bool B2>
 bool launch_batched(int block, int warps_per_sm, int ctas, cudaStream_t st, const DParticles &dp,
                     opb_batch_header *hdr, const opb_experiment *exps, const DScalars &ds, const DRoms &dr,
                     const opb_time *table, const int64_t *bounds, const int64_t *items, int *launched) {
@@ -230,10 +230,10 @@ bool launch_batched(int block, int warps_per_sm, int ctas, cudaStream_t st, cons
     // the combined kernel (SCHEME 0) only at 16 warps: its register budget already spills at 80
     if (SCHEME == 0 && warps_per_sm != 16) return false;
     switch (key) {
-        case 12816: return go(k_batched_steps<T, I, 128, 4, SCHEME, LAYOUT>, 128);
-        case 25616: return go(k_batched_steps<T, I, 256, 2, SCHEME, LAYOUT>, 256);
-        case 25624: return go(k_batched_steps<T, I, 256, 3, SCHEME != 0 ? SCHEME : OPB_SCHEME_RK2, LAYOUT>, 256);
-        case 25632: return go(k_batched_steps<T, I, 256, 4, SCHEME != 0 ? SCHEME : OPB_SCHEME_RK2, LAYOUT>, 256);
+        case 12816: return go(k_batched_steps<T, I, 128, 4, SCHEME, LAYOUT, B2>, 128);
+        case 25616: return go(k_batched_steps<T, I, 256, 2, SCHEME, LAYOUT, B2>, 256);
+        case 25624: return go(k_batched_steps<T, I, 256, 3, SCHEME != 0 ? SCHEME : OPB_SCHEME_RK2, LAYOUT, B2>, 256);
+        case 25632: return go(k_batched_steps<T, I, 256, 4, SCHEME != 0 ? SCHEME : OPB_SCHEME_RK2, LAYOUT, B2>, 256);
         default: return false;
     }
 }
@@ -260,7 +260,8 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
     // time-dependent fields come as snapshot pairs or quads: check, then convert with the element dtype
     opb_roms_fields g;
     int layout = LAYOUT_PLAIN;
-    if ((rc = unpair_fields(f, g, layout, what))) return rc;
+    bool bundled = false;
+    if ((rc = unpair_fields(f, g, layout, bundled, what))) return rc;
     if (layout == LAYOUT_PLAIN && !(g.u.is_static && g.v.is_static && g.w.is_static && g.zeta.is_static))
         return fail(OPB_EINVAL, "%s: time-dependent fields must be snapshot pairs (OPB_F32_PAIRS or OPB_F64_PAIRS), "
                     "quads (OPB_F32_QUADS) or octets (OPB_F32_OCTS)", what);
@@ -295,33 +296,45 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
         if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     }
     int launched = 0;
-    auto go = [&](auto tv, auto iv, auto lv) {
+    auto go = [&](auto tv, auto iv, auto lv, auto bv) {
         using T = decltype(tv);
         using I = decltype(iv);
         constexpr int LAYOUT = decltype(lv)::value;
+        constexpr bool B2 = decltype(bv)::value;
         if (scheme == OPB_SCHEME_RK2)
-            launch_batched<T, I, OPB_SCHEME_RK2, LAYOUT>(block, warps_per_sm, ctas, st, dp, header, experiments, ds,
-                                                         dr, table, bucket_bounds, item_scratch, &launched);
+            launch_batched<T, I, OPB_SCHEME_RK2, LAYOUT, B2>(block, warps_per_sm, ctas, st, dp, header, experiments,
+                                                             ds, dr, table, bucket_bounds, item_scratch, &launched);
         else if (scheme == OPB_SCHEME_AB3)
-            launch_batched<T, I, OPB_SCHEME_AB3, LAYOUT>(block, warps_per_sm, ctas, st, dp, header, experiments, ds,
-                                                         dr, table, bucket_bounds, item_scratch, &launched);
+            launch_batched<T, I, OPB_SCHEME_AB3, LAYOUT, B2>(block, warps_per_sm, ctas, st, dp, header, experiments,
+                                                             ds, dr, table, bucket_bounds, item_scratch, &launched);
         else
-            launch_batched<T, I, 0, LAYOUT>(block, warps_per_sm, ctas, st, dp, header, experiments, ds, dr, table,
-                                            bucket_bounds, item_scratch, &launched);
+            launch_batched<T, I, 0, LAYOUT, B2>(block, warps_per_sm, ctas, st, dp, header, experiments, ds, dr, table,
+                                                bucket_bounds, item_scratch, &launched);
     };
-    if (layout == LAYOUT_QUADS || layout == LAYOUT_OCTS) {
-        if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads and octets hold float32 storage", what);
-        const bool small = fits_int(dr);
-        if (layout == LAYOUT_QUADS) {
-            if (small) go(float{}, int{}, std::integral_constant<int, LAYOUT_QUADS>{});
-            else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_QUADS>{});
+    using NoB = std::false_type;
+    using Bun = std::true_type;
+    const bool small = fits_int(dr);
+    if (layout == LAYOUT_QUADS || layout == LAYOUT_OCTS || bundled) {
+        if (dtype != OPB_F32)
+            return fail(OPB_EINVAL, "%s: snapshot quads, octets and 2-D bundles hold float32 storage", what);
+        using Q = std::integral_constant<int, LAYOUT_QUADS>;
+        using O = std::integral_constant<int, LAYOUT_OCTS>;
+        using P = std::integral_constant<int, LAYOUT_PAIRS>;
+        if (layout == LAYOUT_OCTS) {
+            if (small) go(float{}, int{}, O{}, NoB{});
+            else go(float{}, (long long){}, O{}, NoB{});
+        } else if (layout == LAYOUT_QUADS) {
+            if (small) bundled ? go(float{}, int{}, Q{}, Bun{}) : go(float{}, int{}, Q{}, NoB{});
+            else bundled ? go(float{}, (long long){}, Q{}, Bun{}) : go(float{}, (long long){}, Q{}, NoB{});
         } else {
-            if (small) go(float{}, int{}, std::integral_constant<int, LAYOUT_OCTS>{});
-            else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_OCTS>{});
+            if (small) go(float{}, int{}, P{}, Bun{});
+            else go(float{}, (long long){}, P{}, Bun{});
         }
     } else {
         // snapshot pairs (roms_layout above rules out the all-static fields that passed the layout check)
-        dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) { go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{}); });
+        dispatch(dtype, small, [&](auto tv, auto iv) {
+            go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{}, NoB{});
+        });
     }
     if (!launched) return fail(OPB_ECUDA, "%s: occupancy query failed", what);
     return check_launch(what);

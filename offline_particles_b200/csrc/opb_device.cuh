@@ -203,6 +203,63 @@ struct View {
     }
 };
 
+// ------------------------------------------------------ 2-D field bundles
+// h, zeta, dx and dy share one stagger in the ROMS layout, so one bilinear
+// stencil serves them all.  A bundle holds two of them element by element with
+// the x-neighbour, 32 bytes per element, so one load fetches both fields' values
+// at two corners:
+//   zeta with h (zeta float32, time-dependent): {h[i], zeta pair[i], h[i+1],
+//     zeta pair[i+1]} as four 64-bit words (a zeta pair: the earlier snapshot's
+//     value in the low half, the later's in the high half);
+//   dx with dy (static): {dx[i], dy[i], dx[i+1], dy[i+1]}.
+struct alignas(32) U4 {
+    unsigned long long v[4];
+};
+__device__ __forceinline__ U4 ldg256(const U4 *p) {
+    U4 r;
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(r.v[0]), "=l"(r.v[1]), "=l"(r.v[2]), "=l"(r.v[3]) : "l"(p));
+    return r;
+}
+
+template <typename I>
+struct ZetaHView {
+    using index_type = I;
+    const U4 *p;
+    float ft, gt;
+    I n0, n1;
+    double o0, o1;
+    // the blend of one zeta pair word, as View::blend in float32
+    __device__ __forceinline__ double zeta(unsigned long long w) const {
+        const float x = __uint_as_float((unsigned)(w & 0xffffffffull)) * gt;
+        const float y = __uint_as_float((unsigned)(w >> 32)) * ft;
+        return (double)(x + y);
+    }
+    // h and zeta at i and i + 1
+    __device__ __forceinline__ void at2(I i, double &h0, double &z0, double &h1, double &z1) const {
+        const U4 w = ldg256(p + i);
+        h0 = __longlong_as_double((long long)w.v[0]);
+        z0 = zeta(w.v[1]);
+        h1 = __longlong_as_double((long long)w.v[2]);
+        z1 = zeta(w.v[3]);
+    }
+};
+
+template <typename I>
+struct DxDyView {
+    using index_type = I;
+    const D4 *p;
+    I n0, n1;
+    double o0, o1;
+    // dx and dy at i and i + 1
+    __device__ __forceinline__ void at2(I i, double &a0, double &b0, double &a1, double &b1) const {
+        const D4 w = ldg256(p + i);
+        a0 = w.v[0];
+        b0 = w.v[1];
+        a1 = w.v[2];
+        b1 = w.v[3];
+    }
+};
+
 template <typename T, typename I, int KIND = KIND_ANY>
 __device__ __forceinline__ View<T, I, KIND> bind(const DField &f, const opb_time &t) {
     View<T, I, KIND> v;
@@ -273,6 +330,25 @@ __device__ __forceinline__ double bilinear(const F &f, double idx0, double idx1)
     double v00, v01, v10, v11;
     f.at4(b, f.n1, v00, v01, v10, v11);
     return g0 * g1 * v00 + g0 * f1 * v01 + f0 * g1 * v10 + f0 * f1 * v11;
+}
+
+// Two fields of one bundle on one stencil: each is bilinear() of its own values
+// (the same weights, the same expression, so the same bits).
+template <typename F>
+__device__ __forceinline__ void bilinear_pair(const F &f, double idx0, double idx1, double &a, double &b) {
+    using I = typename F::index_type;
+    const I I0 = trunc_index(idx0, (I)(f.n0 - 2));
+    const I I1 = trunc_index(idx1, (I)(f.n1 - 2));
+    const double f0 = idx0 - (double)I0;
+    const double f1 = idx1 - (double)I1;
+    const double g0 = 1.0 - f0;
+    const double g1 = 1.0 - f1;
+    const I base = I0 * f.n1 + I1;
+    double a00, b00, a01, b01, a10, b10, a11, b11;
+    f.at2(base, a00, b00, a01, b01);
+    f.at2(base + f.n1, a10, b10, a11, b11);
+    a = g0 * g1 * a00 + g0 * f1 * a01 + f0 * g1 * a10 + f0 * f1 * a11;
+    b = g0 * g1 * b00 + g0 * f1 * b01 + f0 * g1 * b10 + f0 * f1 * b11;
 }
 
 // linear.pxd:35-65

@@ -196,9 +196,11 @@ int stage_common(const char *what, const opb_particles *p, const opb_scalars *s,
 
 // Time-dependent fields may come as snapshot pairs (OPB_F32_PAIRS / OPB_F64_PAIRS), snapshot quads
 // (OPB_F32_QUADS, with h, dx, dy as OPB_F64_XPAIRS) or snapshot octets (OPB_F32_OCTS, with h, dx, dy as
-// OPB_F64_YXPAIRS): `out` is `in` with the element dtypes, `layout` says which form it was (LAYOUT_PLAIN,
-// LAYOUT_PAIRS, LAYOUT_QUADS, LAYOUT_OCTS).  All of u, v, w, zeta or none.
-int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, int &layout, const char *what) {
+// OPB_F64_YXPAIRS), and the 2-D fields as bundles (zeta with h, dx with dy; float32 pairs or quads):
+// `out` is `in` with the element dtypes, `layout` says which form it was (LAYOUT_PLAIN, LAYOUT_PAIRS,
+// LAYOUT_QUADS, LAYOUT_OCTS) and `bundled` whether the 2-D fields are bundled.  All of u, v, w, zeta or
+// none.
+int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, int &layout, bool &bundled, const char *what) {
     if (!in) return fail(OPB_EINVAL, "%s: fields is NULL", what);
     // every vector load of a layout starts on its own size: the buffers must be aligned to it
     auto misaligned = [](const opb_field &x, uintptr_t align) {
@@ -211,16 +213,37 @@ int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, int &layout, 
         const uintptr_t align = x->dtype == OPB_F32_PAIRS                                  ? 8
                                 : x->dtype == OPB_F64_PAIRS || x->dtype == OPB_F32_QUADS ||
                                           x->dtype == OPB_F64_XPAIRS                       ? 16
-                                : x->dtype == OPB_F32_OCTS || x->dtype == OPB_F64_YXPAIRS ? 32
+                                : x->dtype == OPB_F32_OCTS || x->dtype == OPB_F64_YXPAIRS ||
+                                          x->dtype == OPB_F32_ZETA_H || x->dtype == OPB_F64_DX_DY ? 32
                                                                                            : 1;
         if (align > 1 && misaligned(*x, align))
-            return fail(OPB_EINVAL, "%s: a snapshot pair/quad/octet or x/yx-pair buffer is not %d-byte aligned",
+            return fail(OPB_EINVAL, "%s: a snapshot pair/quad/octet, x/yx-pair or bundle buffer is not %d-byte aligned",
                         what, (int)align);
     }
     out = *in;
+    // 2-D bundles: all four codes or none
+    const int nb = (in->zeta.dtype == OPB_F32_ZETA_H && !in->zeta.is_static) + (in->h.dtype == OPB_F64_IN_ZETA) +
+                   (in->dx.dtype == OPB_F64_DX_DY && in->dx.is_static) + (in->dy.dtype == OPB_F64_IN_DX);
+    if (nb != 0 && nb != 4)
+        return fail(OPB_EINVAL, "%s: 2-D bundles need zeta as OPB_F32_ZETA_H, h as OPB_F64_IN_ZETA, dx as "
+                    "OPB_F64_DX_DY and dy as OPB_F64_IN_DX together", what);
+    bundled = nb == 4;
+    if (bundled) {
+        if (in->h.ndim != in->zeta.ndim || in->h.shape[0] != in->zeta.shape[0] || in->h.shape[1] != in->zeta.shape[1] ||
+            in->h.offset[0] != in->zeta.offset[0] || in->h.offset[1] != in->zeta.offset[1] ||
+            in->dy.ndim != in->dx.ndim || in->dy.shape[0] != in->dx.shape[0] || in->dy.shape[1] != in->dx.shape[1] ||
+            in->dy.offset[0] != in->dx.offset[0] || in->dy.offset[1] != in->dx.offset[1])
+            return fail(OPB_EINVAL, "%s: bundled fields must share their shape and offsets (h with zeta, dy with dx)",
+                        what);
+        out.zeta.dtype = OPB_F32;
+        out.h.dtype = out.dx.dtype = out.dy.dtype = OPB_F64;
+        // h and dy are read from the bundles: their own buffers are not needed
+        if (!out.h.data[0]) out.h.data[0] = in->zeta.data[0];
+        if (!out.dy.data[0]) out.dy.data[0] = in->dx.data[0];
+    }
     int npairs = 0, nquads = 0, nocts = 0, ntd = 0, nx = 0, nyx = 0;
     for (opb_field *x : {&out.u, &out.v, &out.w, &out.zeta}) {
-        if (x->is_static) continue;
+        if (x->is_static || (bundled && x == &out.zeta)) continue;
         ++ntd;
         if (x->dtype == OPB_F32_PAIRS || x->dtype == OPB_F64_PAIRS) {
             x->dtype = x->dtype == OPB_F32_PAIRS ? OPB_F32 : OPB_F64;
@@ -245,7 +268,9 @@ int unpair_fields(const opb_roms_fields *in, opb_roms_fields &out, int &layout, 
     if ((npairs && npairs != ntd) || (nquads && nquads != ntd) || (nocts && nocts != ntd))
         return fail(OPB_EINVAL, "%s: either every time-dependent field is a snapshot pair (or quad, or octet) or none",
                     what);
-    if (nquads && nx != 3)
+    if (bundled && !(ntd > 0 && ((npairs == ntd && in->u.dtype == OPB_F32_PAIRS) || nquads == ntd)))
+        return fail(OPB_EINVAL, "%s: 2-D bundles come with float32 snapshot pairs or quads of u, v, w", what);
+    if (nquads && !bundled && nx != 3)
         return fail(OPB_EINVAL, "%s: snapshot quads need h, dx and dy as static x-pairs (OPB_F64_XPAIRS)", what);
     if (nocts && nyx != 3)
         return fail(OPB_EINVAL, "%s: snapshot octets need h, dx and dy as static yx-pairs (OPB_F64_YXPAIRS)", what);

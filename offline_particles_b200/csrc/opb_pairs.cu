@@ -107,6 +107,34 @@ __global__ void __launch_bounds__(kBlock) k_yxpairs_f64(const double *__restrict
     }
 }
 
+// zeta-with-h bundles, one element per thread: {h[i], (a[i], b[i]), h[j], (a[j], b[j])} as 64-bit
+// words, j = i + 1 (the last element's neighbour is itself) -> two 16-byte stores
+__device__ __forceinline__ unsigned long long pack_pair(float lo, float hi) {
+    return (unsigned long long)__float_as_uint(lo) | ((unsigned long long)__float_as_uint(hi) << 32);
+}
+
+__global__ void __launch_bounds__(kBlock) k_bundle_zeta_h(const float *__restrict__ a, const float *__restrict__ b,
+                                                          const double *__restrict__ h, ulonglong2 *__restrict__ out,
+                                                          long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long j = i + 1 < n ? i + 1 : n - 1;
+        out[2 * i] = make_ulonglong2((unsigned long long)__double_as_longlong(__ldg(h + i)),
+                                     pack_pair(__ldg(a + i), __ldg(b + i)));
+        out[2 * i + 1] = make_ulonglong2((unsigned long long)__double_as_longlong(__ldg(h + j)),
+                                         pack_pair(__ldg(a + j), __ldg(b + j)));
+    }
+}
+
+// dx-with-dy bundles, one element per thread: {dx[i], dy[i], dx[j], dy[j]}, j = i + 1 (clamped)
+__global__ void __launch_bounds__(kBlock) k_bundle_dx_dy(const double *__restrict__ dx, const double *__restrict__ dy,
+                                                         double2 *__restrict__ out, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long j = i + 1 < n ? i + 1 : n - 1;
+        out[2 * i] = make_double2(__ldg(dx + i), __ldg(dy + i));
+        out[2 * i + 1] = make_double2(__ldg(dx + j), __ldg(dy + j));
+    }
+}
+
 int grid_for(long long work) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -208,6 +236,32 @@ int opb_neighbour_quads(const double *s, double *out, int64_t n, int64_t row, vo
     if (!s || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
     if (((uintptr_t)out) & 31) return opb::fail(OPB_EINVAL, "%s: out is not 32-byte aligned", what);
     k_yxpairs_f64<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(s, (double2 *)out, n, row);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+int opb_bundle_zeta_h(const float *a, const float *b, const double *h, void *out, int64_t n, void *stream) {
+    const char *what = "opb_bundle_zeta_h";
+    if (n < 0) return opb::fail(OPB_EINVAL, "%s: negative element count", what);
+    if (n == 0) return OPB_OK;
+    if (!a || !b || !h || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
+    if (((uintptr_t)out) & 31) return opb::fail(OPB_EINVAL, "%s: out is not 32-byte aligned", what);
+    k_bundle_zeta_h<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(a, b, h, (ulonglong2 *)out, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    opb::clear_error();
+    return OPB_OK;
+}
+
+int opb_bundle_dx_dy(const double *dx, const double *dy, double *out, int64_t n, void *stream) {
+    const char *what = "opb_bundle_dx_dy";
+    if (n < 0) return opb::fail(OPB_EINVAL, "%s: negative element count", what);
+    if (n == 0) return OPB_OK;
+    if (!dx || !dy || !out) return opb::fail(OPB_EINVAL, "%s: NULL buffer", what);
+    if (((uintptr_t)out) & 31) return opb::fail(OPB_EINVAL, "%s: out is not 32-byte aligned", what);
+    k_bundle_dx_dy<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(dx, dy, (double2 *)out, n);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return opb::fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     opb::clear_error();

@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3_post(const __grid_constant__ DPa
 // ------------------------------------------------------------ fused kernels
 // `nsteps` RK2 steps (timesteppers.py:241-257) per launch.  table[3*k + j]
 // selects the fields of step k, stage j (t, t + alpha dt, t + dt).
-template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN>
+template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool B2 = false>
 __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
@@ -209,16 +209,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table.at(3 * k), t2 = table.at(3 * k + 1), t3 = table.at(3 * k + 2);
         const bool reuse = k > 0 && same_time(t1, s.at);
-        if (!rk2_stage1(s, bind_all<T, I, FIXED, LAYOUT>(r, t1), sc, reuse)) {
+        if (!rk2_stage1(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, reuse)) {
             raise_zero_division(p);
             break;
         }
         moved = true;
-        if (!rk2_stage2(s, bind_all<T, I, FIXED, LAYOUT>(r, t2), L, sc)) {
+        if (!rk2_stage2(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t2), L, sc)) {
             raise_zero_division(p);
             break;
         }
-        rk2_update(s, bind_all<T, I, FIXED, LAYOUT>(r, t3), L, sc);
+        rk2_update(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t3), L, sc);
         s.at = t3;
     }
     if (s.status != st0) p.status[i] = s.status;
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
 
 // `nsteps` AB3 steps (timesteppers.py:296-305) per launch.  table[2*k + j]
 // selects the fields of step k at t (j = 0) and t + dt (j = 1).
-template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool ISO = false>
+template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool ISO = false, bool B2 = false>
 __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
@@ -267,15 +267,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
         const opb_time t1 = table.at(2 * k), t2 = table.at(2 * k + 1);
         const bool reuse = k > 0 && same_time(t1, s.at);
         bool ok;
-        if constexpr (ISO) ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT>(r, t1), sc, reuse, IsoVel{rho_t, sc.w_max,
+        if constexpr (ISO) ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, reuse, IsoVel{rho_t, sc.w_max,
                                                                                                      sc.rho_scale});
-        else ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT>(r, t1), sc, reuse);
+        else ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, reuse);
         if (!ok) {
             raise_zero_division(p);
             break;
         }
         moved = true;
-        ab3_post(s, bind_all<T, I, FIXED, LAYOUT>(r, t2), L, sc);
+        ab3_post(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t2), L, sc);
         s.at = t2;
     }
     if (s.status != st0) p.status[i] = s.status;
@@ -447,7 +447,8 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     convert_scalars(s, ds);
     opb_roms_fields g;
     int layout = LAYOUT_PLAIN;
-    if ((rc = unpair_fields(f, g, layout, what))) return rc;
+    bool bundled = false;
+    if ((rc = unpair_fields(f, g, layout, bundled, what))) return rc;
     if ((rc = convert_fields(&g, dr, what, true, &dtype))) return rc;
     if (layout != LAYOUT_PLAIN && !roms_layout(dr))
         return fail(OPB_EINVAL, "%s: snapshot pairs need the ROMS field layout", what);
@@ -468,32 +469,42 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     const unsigned grid = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
     const bool fixed = roms_layout(dr);
-    auto go = [&](auto tv, auto iv, auto lv) {
+    auto go = [&](auto tv, auto iv, auto lv, auto bv) {
         using T = decltype(tv);
         using I = decltype(iv);
         constexpr int LAYOUT = decltype(lv)::value;
-        if (rk2) k_rk2_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        constexpr bool B2 = decltype(bv)::value;
+        if (rk2) k_rk2_steps<T, I, true, LAYOUT, B2><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
         else if (iso)
-            k_ab3_steps<T, I, true, LAYOUT, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
-        else k_ab3_steps<T, I, true, LAYOUT><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+            k_ab3_steps<T, I, true, LAYOUT, true, B2><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        else k_ab3_steps<T, I, true, LAYOUT, false, B2><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
     };
-    if (layout == LAYOUT_QUADS || layout == LAYOUT_OCTS) {
-        if (dtype != OPB_F32) return fail(OPB_EINVAL, "%s: snapshot quads and octets hold float32 storage", what);
-        const bool small = fits_int(dr);
-        if (layout == LAYOUT_QUADS) {
-            if (small) go(float{}, int{}, std::integral_constant<int, LAYOUT_QUADS>{});
-            else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_QUADS>{});
+    using NoB = std::false_type;
+    using Bun = std::true_type;
+    const bool small = fits_int(dr);
+    if (layout == LAYOUT_QUADS || layout == LAYOUT_OCTS || bundled) {
+        if (dtype != OPB_F32)
+            return fail(OPB_EINVAL, "%s: snapshot quads, octets and 2-D bundles hold float32 storage", what);
+        using Q = std::integral_constant<int, LAYOUT_QUADS>;
+        using O = std::integral_constant<int, LAYOUT_OCTS>;
+        using P = std::integral_constant<int, LAYOUT_PAIRS>;
+        if (layout == LAYOUT_OCTS) {
+            if (small) go(float{}, int{}, O{}, NoB{});
+            else go(float{}, (long long){}, O{}, NoB{});
+        } else if (layout == LAYOUT_QUADS) {
+            if (small) bundled ? go(float{}, int{}, Q{}, Bun{}) : go(float{}, int{}, Q{}, NoB{});
+            else bundled ? go(float{}, (long long){}, Q{}, Bun{}) : go(float{}, (long long){}, Q{}, NoB{});
         } else {
-            if (small) go(float{}, int{}, std::integral_constant<int, LAYOUT_OCTS>{});
-            else go(float{}, (long long){}, std::integral_constant<int, LAYOUT_OCTS>{});
+            if (small) go(float{}, int{}, P{}, Bun{});
+            else go(float{}, (long long){}, P{}, Bun{});
         }
         return check_launch(what);
     }
-    dispatch(dtype, fits_int(dr), [&](auto tv, auto iv) {
+    dispatch(dtype, small, [&](auto tv, auto iv) {
         using T = decltype(tv);
         using I = decltype(iv);
-        if (layout == LAYOUT_PAIRS) go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{});
-        else if (fixed) go(tv, iv, std::integral_constant<int, LAYOUT_PLAIN>{});
+        if (layout == LAYOUT_PAIRS) go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{}, NoB{});
+        else if (fixed) go(tv, iv, std::integral_constant<int, LAYOUT_PLAIN>{}, NoB{});
         else if (rk2) k_rk2_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
         else if (iso)
             k_ab3_steps<T, I, false, LAYOUT_PLAIN, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps,

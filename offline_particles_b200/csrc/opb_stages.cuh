@@ -42,9 +42,10 @@ __device__ __forceinline__ void raise_zero_division(const DParticles &p) {
 // field's kind is read at run time.  LAYOUT (FIXED only): how the
 // time-dependent fields, and with LAYOUT_QUADS / LAYOUT_OCTS the static h, dx,
 // dy, are read.
-template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN>
+template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN, bool B2 = false>
 struct Bound {
     static_assert(FIXED || LAYOUT == LAYOUT_PLAIN, "pair layouts need the ROMS field layout");
+    static_assert(!B2 || (LAYOUT != LAYOUT_PLAIN && sizeof(T) == 4), "2-D bundles come with float32 pairs");
     static constexpr int KT = LAYOUT == LAYOUT_OCTS ? KIND_OCTS
                               : LAYOUT == LAYOUT_QUADS ? KIND_QUADS
                               : LAYOUT == LAYOUT_PAIRS ? KIND_PAIRS
@@ -53,24 +54,64 @@ struct Bound {
                               : LAYOUT == LAYOUT_QUADS ? KIND_XPAIRS
                               : FIXED ? KIND_STATIC : KIND_ANY;
     static constexpr int KC = FIXED ? KIND_STATIC : KIND_ANY;
+    static constexpr bool BUNDLED = B2;
     View<T, I, KT> u, v, w, zeta;
     View<T, I, KS> dx, dy, h;
     View<T, I, KC> C;
+    ZetaHView<I> zh;  // B2: zeta with h
+    DxDyView<I> dd;   // B2: dx with dy
 };
 
-template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN>
-__device__ __forceinline__ Bound<T, I, FIXED, LAYOUT> bind_all(const DRoms &r, const opb_time &t) {
-    using B = Bound<T, I, FIXED, LAYOUT>;
+template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN, bool B2 = false>
+__device__ __forceinline__ Bound<T, I, FIXED, LAYOUT, B2> bind_all(const DRoms &r, const opb_time &t) {
+    using B = Bound<T, I, FIXED, LAYOUT, B2>;
     B b;
     b.u = bind<T, I, B::KT>(r.u, t);
     b.v = bind<T, I, B::KT>(r.v, t);
     b.w = bind<T, I, B::KT>(r.w, t);
-    b.zeta = bind<T, I, B::KT>(r.zeta, t);
-    b.dx = bind<T, I, B::KS>(r.dx, t);
-    b.dy = bind<T, I, B::KS>(r.dy, t);
-    b.h = bind<T, I, B::KS>(r.h, t);
     b.C = bind<T, I, B::KC>(r.C, t);  // static float64 (kernels/_core.pyx:5-9)
+    if constexpr (B2) {
+        b.zh.p = (const U4 *)r.zeta.data[t.prev];
+        b.zh.ft = (float)t.ft;  // exact: the host rounded ft, gt to float32
+        b.zh.gt = (float)t.gt;
+        b.zh.n0 = (I)r.zeta.n0;
+        b.zh.n1 = (I)r.zeta.n1;
+        b.zh.o0 = r.zeta.o0;
+        b.zh.o1 = r.zeta.o1;
+        b.dd.p = (const D4 *)r.dx.data[0];
+        b.dd.n0 = (I)r.dx.n0;
+        b.dd.n1 = (I)r.dx.n1;
+        b.dd.o0 = r.dx.o0;
+        b.dd.o1 = r.dx.o1;
+    } else {
+        b.zeta = bind<T, I, B::KT>(r.zeta, t);
+        b.dx = bind<T, I, B::KS>(r.dx, t);
+        b.dy = bind<T, I, B::KS>(r.dy, t);
+        b.h = bind<T, I, B::KS>(r.h, t);
+    }
     return b;
+}
+
+// h and zeta at (y, x): one stencil for both when they are bundled
+template <typename B>
+__device__ __forceinline__ void hz_at(const B &f, double y, double x, double &h, double &zeta) {
+    if constexpr (B::BUNDLED) {
+        bilinear_pair(f.zh, y + f.zh.o0, x + f.zh.o1, h, zeta);
+    } else {
+        h = bilinear(f.h, y + f.h.o0, x + f.h.o1);
+        zeta = bilinear(f.zeta, y + f.zeta.o0, x + f.zeta.o1);
+    }
+}
+
+// dx and dy at (y, x)
+template <typename B>
+__device__ __forceinline__ void dxdy_at(const B &f, double y, double x, double &dx, double &dy) {
+    if constexpr (B::BUNDLED) {
+        bilinear_pair(f.dd, y + f.dd.o0, x + f.dd.o1, dx, dy);
+    } else {
+        dx = bilinear(f.dx, y + f.dx.o0, x + f.dx.o1);
+        dy = bilinear(f.dy, y + f.dy.o0, x + f.dy.o1);
+    }
 }
 
 // Every kernel starts here, before any thread can return: the block's shared
@@ -85,14 +126,19 @@ __device__ __forceinline__ Bound<T, I, FIXED, LAYOUT> bind_all(const DRoms &r, c
 // zero grid spacing (the reference raises ZeroDivisionError).
 template <typename B>
 __device__ __forceinline__ bool rk2_stage1(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false) {
-    const double h = reuse_hz ? s.h_at : bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
-    const double zeta = reuse_hz ? s.zeta_at : bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    double h, zeta;
+    if (reuse_hz) {
+        h = s.h_at;
+        zeta = s.zeta_at;
+    } else {
+        hz_at(f, s.yidx, s.xidx, h, zeta);
+    }
     const double Cv = linear(f.C, s.zidx + f.C.o0);
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
     const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
-    const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
-    const double dy = bilinear(f.dy, s.yidx + f.dy.o0, s.xidx + f.dy.o1);
+    double dx, dy;
+    dxdy_at(f, s.yidx, s.xidx, dx, dy);
     // gathered before the check (pure reads): every stencil's loads are in flight together
     const double w = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
     if (dx == 0.0 || dy == 0.0) return false;
@@ -109,13 +155,13 @@ __device__ __forceinline__ bool rk2_stage2(PState &s, const B &f, const Levels &
     const double z_int = s.z + adt * s.k1z;
     const double y_int = s.yidx + adt * s.k1y;
     const double x_int = s.xidx + adt * s.k1x;
-    const double h = bilinear(f.h, y_int + f.h.o0, x_int + f.h.o1);
-    const double zeta = bilinear(f.zeta, y_int + f.zeta.o0, x_int + f.zeta.o1);
+    double h, zeta;
+    hz_at(f, y_int, x_int, h, zeta);
     const double z_idx = compute_zidx_hint(z_int, h, zeta, sc.hc, L, s.zidx);
     const double u = trilinear(f.u, z_idx + f.u.o0, y_int + f.u.o1, x_int + f.u.o2);
     const double v = trilinear(f.v, z_idx + f.v.o0, y_int + f.v.o1, x_int + f.v.o2);
-    const double dx = bilinear(f.dx, y_int + f.dx.o0, x_int + f.dx.o1);
-    const double dy = bilinear(f.dy, y_int + f.dy.o0, x_int + f.dy.o1);
+    double dx, dy;
+    dxdy_at(f, y_int, x_int, dx, dy);
     const double w = trilinear(f.w, z_idx + f.w.o0, y_int + f.w.o1, x_int + f.w.o2);
     if (dx == 0.0 || dy == 0.0) return false;
     s.k2x = u / dx;
@@ -135,8 +181,8 @@ __device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &
     s.z = s.z + b1dt * s.k1z + b2dt * s.k2z;
     s.yidx = s.yidx + b1dt * s.k1y + b2dt * s.k2y;
     s.xidx = s.xidx + b1dt * s.k1x + b2dt * s.k2x;
-    const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
-    const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    double h, zeta;
+    hz_at(f, s.yidx, s.xidx, h, zeta);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
     s.h_at = h;
     s.zeta_at = zeta;
@@ -172,9 +218,9 @@ __device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &
     // every gather first (pure reads, so their loads are in flight together), then the divisions and
     // their zero checks in the reference's order: dx, dy, then the vertical velocity's
     const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
-    const double dx = bilinear(f.dx, s.yidx + f.dx.o0, s.xidx + f.dx.o1);
+    double dx, dy;
+    dxdy_at(f, s.yidx, s.xidx, dx, dy);
     const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
-    const double dy = bilinear(f.dy, s.yidx + f.dy.o0, s.xidx + f.dy.o1);
     const double wg = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
     if (dx == 0.0) return false;
     s.k0x = u / dx;
@@ -195,8 +241,13 @@ __device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &
         s.k2z = -s.k0z + 2.0 * s.k1z;
         s.status = ST_NORMAL;
     }
-    const double h = reuse_hz ? s.h_at : bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
-    const double zeta = reuse_hz ? s.zeta_at : bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    double h, zeta;
+    if (reuse_hz) {
+        h = s.h_at;
+        zeta = s.zeta_at;
+    } else {
+        hz_at(f, s.yidx, s.xidx, h, zeta);
+    }
     const double Cv = linear(f.C, s.zidx + f.C.o0);
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double dt = sc.dt;
@@ -215,8 +266,8 @@ __device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &
 // ab3_w_advection.pyx:214-229 (post step for one particle)
 template <typename B>
 __device__ __forceinline__ void ab3_post(PState &s, const B &f, const Levels &L, const DScalars &sc) {
-    const double h = bilinear(f.h, s.yidx + f.h.o0, s.xidx + f.h.o1);
-    const double zeta = bilinear(f.zeta, s.yidx + f.zeta.o0, s.xidx + f.zeta.o1);
+    double h, zeta;
+    hz_at(f, s.yidx, s.xidx, h, zeta);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
     s.h_at = h;
     s.zeta_at = zeta;

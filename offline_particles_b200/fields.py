@@ -37,7 +37,7 @@ from .spatial_arrays import BBox, DeviceArray, SpatialArray, Stagger
 # launches).
 pair_observers: list = []
 # elements of the storage dtype per grid element in each pair layout
-PAIR_WIDTH = {"pairs": 2, "quads": 4, "octets": 8}
+PAIR_WIDTH = {"pairs": 2, "quads": 4, "octets": 8, "zeta_h": 8}
 
 FieldData = collections.namedtuple("FieldData", ["array", "offsets"])
 
@@ -174,7 +174,7 @@ class StaticField(Field):
         if data.data.dtype != torch.float64:
             data = DeviceArray(data.data, data.z_stagger, data.y_stagger, data.x_stagger, dtype=torch.float64)
         self._data = data
-        self._neighbours: dict[str, tuple[torch.Tensor, torch.Tensor]] = {}
+        self._neighbours: dict = {}  # neighbour layouts and bundles: (sources kept alive ..., result)
 
     @property
     def data(self) -> DeviceArray:
@@ -222,7 +222,25 @@ class StaticField(Field):
                 out = torch.empty(4 * src.numel(), dtype=torch.float64, device=src.device)
                 _lib.call("opb_neighbour_quads", src.data_ptr(), out.data_ptr(), src.numel(), src.shape[-1], st)
             self._neighbours[kind] = (src, out)  # src kept alive until the build has run
-        return self._neighbours[kind][1]
+        return self._neighbours[kind][-1]
+
+    def bundle(self, other: "StaticField") -> torch.Tensor:
+        """This field bundled with ``other`` of the same shape, each element with its x-neighbour
+        (``{self[i], other[i], self[i+1], other[i+1]}``, shape ``(4 * size,)``; ``opb_bundle_dx_dy``): dx
+        with dy, one 32-byte load per two stencil corners of both.  Built once per partner."""
+        key = ("bundle", other.data.data.data_ptr())  # the partner's buffer, kept alive below
+        if key not in self._neighbours:
+            from . import _lib
+            from ._device import stream_handle
+
+            a = self._data.data.contiguous()
+            b = other.data.data.contiguous()
+            if a.shape != b.shape:
+                raise ValueError("bundled fields must have one shape")
+            out = torch.empty(4 * a.numel(), dtype=torch.float64, device=a.device)
+            _lib.call("opb_bundle_dx_dy", a.data_ptr(), b.data_ptr(), out.data_ptr(), a.numel(), stream_handle(a.device))
+            self._neighbours[key] = (a, b, out)
+        return self._neighbours[key][-1]
 
     @classmethod
     def from_numpy(cls, data, z_stagger: Stagger | str, y_stagger: Stagger | str, x_stagger: Stagger | str,
@@ -556,12 +574,13 @@ class SnapshotRing:
 class _PairCache:
     """Device buffers of one pair layout of a field: the pairs by first snapshot (LRU) and free buffers."""
 
-    __slots__ = ("cache", "store", "free")
+    __slots__ = ("cache", "store", "free", "tag")
 
     def __init__(self) -> None:
         self.cache: collections.OrderedDict[int, torch.Tensor] = collections.OrderedDict()
         self.store: torch.Tensor | None = None
         self.free: list[torch.Tensor] | None = None
+        self.tag = None  # zeta_h: the static field bundled in
 
 
 class TimeDependentField(Field):
@@ -699,14 +718,17 @@ class TimeDependentField(Field):
     def pair_slots(self) -> int:
         return self._pair_slots
 
-    def pair(self, k: int, keep: set[int] | frozenset = frozenset(), *, layout: str = "pairs") -> torch.Tensor:
+    def pair(self, k: int, keep: set[int] | frozenset = frozenset(), *, layout: str = "pairs",
+             static: torch.Tensor | None = None) -> torch.Tensor:
         """Snapshots k and k + 1 interleaved element by element (shape ``(2 * size,)``; element 2i from
         snapshot k, 2i + 1 from k + 1): the layout in which the float64 fused steppers fetch both values
         of a time blend with one load.  ``layout`` (float32 storage for the last two): "pairs"; "quads",
         each element's pair followed by its x-neighbour's (shape ``(4 * size,)``,
         ``opb_interleave_quads``: one 16-byte load per two stencil corners); "octets", the pairs of
         elements i, i + 1, i + R, i + R + 1 with R the x size (shape ``(8 * size,)``,
-        ``opb_interleave_octets``: one 32-byte load per stencil face).  Built on the current stream the
+        ``opb_interleave_octets``: one 32-byte load per stencil face); "zeta_h", the pair bundled with the
+        float64 ``static`` field of the same shape (h beside zeta: 32 bytes per element,
+        ``opb_bundle_zeta_h``).  Built on the current stream the
         first time it is asked for; the ``pair_slots`` most recently used pairs of each layout stay on
         the device, and a buffer is reused for a new one in stream order (after the launches queued
         before it that read the old one).  Pairs in ``keep`` are not evicted."""
@@ -720,6 +742,14 @@ class TimeDependentField(Field):
         if k < 0 or k + 1 >= self._num_timesteps:
             raise IndexError(k)
         pc = self._pair_caches.setdefault(layout, _PairCache())
+        if layout == "zeta_h":
+            if static is None or static.numel() != int(np.prod(self._spatial_shape)):
+                raise ValueError("a zeta_h bundle needs the static field of the same shape")
+            if pc.tag != static.data_ptr():  # bundled with another static field: rebuild every bundle
+                if pc.free is not None:
+                    pc.free.extend(pc.cache.values())
+                pc.cache.clear()
+                pc.tag = static.data_ptr()
         cache = pc.cache
         if k in cache:
             cache.move_to_end(k)
@@ -746,7 +776,10 @@ class TimeDependentField(Field):
         from ._device import stream_handle
 
         st = stream_handle(self._device)
-        if layout == "octets":
+        if layout == "zeta_h":
+            _lib.call("opb_bundle_zeta_h", a.data_ptr(), b.data_ptr(), static.data_ptr(), buf.data_ptr(), a.numel(),
+                      st)
+        elif layout == "octets":
             _lib.call("opb_interleave_octets", a.data_ptr(), b.data_ptr(), buf.data_ptr(), a.numel(),
                       self._spatial_shape[-1], st)
         elif layout == "quads":

@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import abc
 import ctypes
+import dataclasses
 
 import numpy as np
 import numpy.typing as npt
@@ -304,45 +305,86 @@ _PAIR_CODE = {"quads": _lib.F32_QUADS, "octets": _lib.F32_OCTS}
 _STATIC_CODE = {"xpairs": _lib.F64_XPAIRS, "yxpairs": _lib.F64_YXPAIRS}
 
 
+# The 2-D fields h, zeta, dx and dy share one stagger in the ROMS layout: with float32 pairs or quads of
+# u, v, w they are read as two bundles, zeta with h and dx with dy, so one 32-byte load fetches two
+# stencil corners of both fields of a bundle.
+BUNDLE_2D = True
+
+
+@dataclasses.dataclass
+class PairPlan:
+    """How a launch that reads pairs reads its fields: ``layout`` of u, v, w (and zeta when not bundled),
+    ``statics`` read as neighbour layouts beside quads and octets (h, dx, dy), ``bundles`` the static
+    fields of the 2-D bundles (h with zeta, dy with dx) or None."""
+
+    layout: str = "pairs"
+    statics: dict | None = None
+    bundles: dict | None = None
+
+
 def pair_layout(launcher: Launcher, td: dict[str, TimeDependentField], roles: dict[str, str] | None = None,
-                layout: str | None = None) -> tuple[str, dict[str, StaticField] | None]:
-    """The pair layout of a launch that reads pairs ("pairs", "quads" or "octets"; ``layout``, default
-    ``SNAPSHOT_LAYOUT``) and, for the wider two, the static fields read beside them as neighbour
-    layouts.  The wider layouts need float32 storage and static h, dx, dy; otherwise "pairs"."""
+                layout: str | None = None) -> PairPlan:
+    """The pair plan of a launch that reads pairs ("pairs", "quads" or "octets"; ``layout``, default
+    ``SNAPSHOT_LAYOUT``).  The wider layouts and the bundles need float32 storage and static h, dx, dy;
+    otherwise plain pairs."""
     layout = SNAPSHOT_LAYOUT if layout is None else layout
     if layout not in ("pairs", "quads", "octets"):
         raise ValueError(f"unknown pair layout {layout!r}")
-    if layout == "pairs" or not td or not all(f.storage == "float32" for f in td.values()):
-        return "pairs", None
+    if not td or not all(f.storage == "float32" for f in td.values()):
+        return PairPlan()
     fs = launcher.fieldset
     roles = roles or {}
     statics = {n: fs[roles.get(n, n)] for n in NEIGHBOUR_STATICS if roles.get(n, n) in fs}
     if len(statics) != len(NEIGHBOUR_STATICS) or not all(isinstance(f, StaticField) for f in statics.values()):
-        return "pairs", None
-    return layout, statics
+        return PairPlan()
+    plan = PairPlan(layout, statics if layout != "pairs" else None)
+    zeta = td.get("zeta")
+    if (BUNDLE_2D and layout in ("pairs", "quads") and zeta is not None
+            and statics["h"].spatial_shape == zeta.spatial_shape and statics["h"].active_offsets == zeta.active_offsets
+            and statics["dx"].spatial_shape == statics["dy"].spatial_shape
+            and statics["dx"].active_offsets == statics["dy"].active_offsets):
+        plan.statics, plan.bundles = None, statics
+    return plan
 
 
-def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField], layout: str = "pairs",
-                statics: dict[str, StaticField] | None = None) -> dict[int, int]:
-    """Point the time-dependent fields of ``rf`` at snapshot pairs ``its`` (slot q holds pair its[q]) in
-    ``layout`` (``pair_layout``), and for quads and octets the ``statics`` at their neighbour layouts;
-    return pair -> slot."""
+def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField], plan: PairPlan | None = None
+                ) -> dict[int, int]:
+    """Point the time-dependent fields of ``rf`` at snapshot pairs ``its`` (slot q holds pair its[q]) as
+    ``plan`` (``pair_layout``) says: u, v, w (and zeta) in its layout, h, dx, dy at their neighbour layouts
+    beside quads and octets, or zeta with h and dx with dy as bundles; return pair -> slot."""
+    plan = plan or PairPlan()
+    layout = plan.layout
     keep = set(its)
+    bundles = plan.bundles
+    h_data = bundles["h"].data.data.contiguous() if bundles else None
     for name, field in td.items():
         f = getattr(rf, name)
-        if layout in _PAIR_CODE:
+        bundled = bundles is not None and name == "zeta"
+        if bundled:
+            f.dtype = _lib.F32_ZETA_H
+        elif layout in _PAIR_CODE:
             f.dtype = _PAIR_CODE[layout]
         else:
             f.dtype = _lib.F32_PAIRS if field.storage == "float32" else _lib.F64_PAIRS
         for q in range(_lib.MAX_SLOTS):
-            f.data[q] = field.pair(its[q], keep, layout=layout).data_ptr() if q < len(its) else None
+            if q < len(its):
+                buf = (field.pair(its[q], keep, layout="zeta_h", static=h_data) if bundled
+                       else field.pair(its[q], keep, layout=layout))
+                f.data[q] = buf.data_ptr()
+            else:
+                f.data[q] = None
             f.scale[q] = None
         if len(its) == 1:
             f.data[1] = f.data[0]
         f.nslots = max(2, len(its))
-    if layout in _STATIC_KIND:
+    if bundles is not None:
+        rf.h.dtype = _lib.F64_IN_ZETA
+        rf.dx.dtype = _lib.F64_DX_DY
+        rf.dx.data[0] = bundles["dx"].bundle(bundles["dy"]).data_ptr()
+        rf.dy.dtype = _lib.F64_IN_DX
+    elif layout in _STATIC_KIND:
         kind = _STATIC_KIND[layout]
-        for name, field in statics.items():
+        for name, field in plan.statics.items():
             g = getattr(rf, name)
             g.dtype = _STATIC_CODE[kind]
             g.data[0] = field.neighbours(kind).data_ptr()
@@ -355,8 +397,7 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
     rf, dtype = window_fields(launcher, needed, td, roles)
     entries = [t for step in steps for t in step]
     if use_pairs(launcher, td, nparticles):
-        pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td,
-                            *pair_layout(launcher, td, roles))
+        pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td, pair_layout(launcher, td, roles))
         prev_next = lambda It: (pslot[It], pslot[It])  # noqa: E731
     else:
         slot = {k: j for j, k in enumerate(needed)}

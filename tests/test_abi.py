@@ -166,6 +166,29 @@ def test_argument_errors_need_no_gpu():
     assert rc == _lib.EINVAL and b"not 32-byte aligned" in lib.opb_last_error()
     assert lib.opb_interleave_octets(16, 16, 48, 4, 2, None) == _lib.EINVAL
     assert b"32-byte aligned" in lib.opb_last_error()
+    # 2-D bundles: all four codes together, shapes and offsets shared, with float32 pairs or quads
+    for name in ("u", "v", "w"):
+        g = getattr(rf, name)
+        g.dtype, g.data[0], g.data[1] = _lib.F32_PAIRS, 32, 32
+    rf.zeta.dtype, rf.zeta.data[0], rf.zeta.data[1] = _lib.F32_ZETA_H, 32, 32
+    rf.h.dtype = _lib.F64_IN_ZETA
+    rf.dx.dtype, rf.dx.data[0] = _lib.F64_DX_DY, 32
+    rf.dy.dtype = _lib.F64
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"together" in lib.opb_last_error()
+    rf.dy.dtype = _lib.F64_IN_DX
+    rf.dy.offset[0] = 0.5
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"share their shape and offsets" in lib.opb_last_error()
+    rf.dy.offset[0] = 0.0
+    rf.dx.data[0] = 48
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"not 32-byte aligned" in lib.opb_last_error()
+    rf.dx.data[0] = 32
+    for name in ("u", "v", "w"):
+        getattr(rf, name).dtype = _lib.F32_OCTS
+    rc = lib.opb_ab3_w_advection_steps(ctypes.byref(p), ctypes.byref(s), ctypes.byref(rf), 16, 1, 1, None)
+    assert rc == _lib.EINVAL and b"float32 snapshot pairs or quads" in lib.opb_last_error()
     assert lib.opb_interleave_quads(16, 16, 20, 4, None) == _lib.EINVAL
     assert b"16-byte aligned" in lib.opb_last_error()
 
@@ -182,7 +205,8 @@ CONSTANT_PROBE = r"""
 int main(void) {
     C(OPB_ABI_VERSION); C(OPB_MAX_SLOTS); C(OPB_F64); C(OPB_F32); C(OPB_BF16); C(OPB_F16); C(OPB_F64_PAIRS);
     C(OPB_F32_PAIRS); C(OPB_F32_QUADS); C(OPB_F64_XPAIRS); C(OPB_F32_OCTS); C(OPB_F64_YXPAIRS);
-    C(OPB_INLINE_TABLE); C(OPB_EINVAL); C(OPB_ECUDA);
+    C(OPB_INLINE_TABLE); C(OPB_EINVAL); C(OPB_ECUDA); C(OPB_F32_ZETA_H); C(OPB_F64_IN_ZETA); C(OPB_F64_DX_DY);
+    C(OPB_F64_IN_DX);
     return 0;
 }
 """
@@ -199,5 +223,7 @@ def test_header_constants_match_the_binding(tmp_path):
           "OPB_F32": _lib.F32, "OPB_BF16": _lib.BF16, "OPB_F16": _lib.F16, "OPB_F64_PAIRS": _lib.F64_PAIRS,
           "OPB_F32_PAIRS": _lib.F32_PAIRS, "OPB_F32_QUADS": _lib.F32_QUADS, "OPB_F64_XPAIRS": _lib.F64_XPAIRS,
           "OPB_F32_OCTS": _lib.F32_OCTS, "OPB_F64_YXPAIRS": _lib.F64_YXPAIRS,
-          "OPB_INLINE_TABLE": _lib.INLINE_TABLE, "OPB_EINVAL": _lib.EINVAL, "OPB_ECUDA": _lib.ECUDA}
+          "OPB_INLINE_TABLE": _lib.INLINE_TABLE, "OPB_EINVAL": _lib.EINVAL, "OPB_ECUDA": _lib.ECUDA,
+          "OPB_F32_ZETA_H": _lib.F32_ZETA_H, "OPB_F64_IN_ZETA": _lib.F64_IN_ZETA, "OPB_F64_DX_DY": _lib.F64_DX_DY,
+          "OPB_F64_IN_DX": _lib.F64_IN_DX}
     assert c == py

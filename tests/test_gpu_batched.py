@@ -198,7 +198,8 @@ def test_segment_sort_keeps_segments_and_permutes_ids():
 @pytest.mark.parametrize("scheme,dt", [("rk2", 300.0), ("ab3", 120.0)])
 def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
     """The fused float64 steppers read streamed fields as plain snapshots, snapshot pairs, quads (static
-    x-pairs beside them) or octets (static yx-pairs); every layout gives the same bits."""
+    x-pairs beside them) or octets (static yx-pairs), with or without the 2-D bundles (zeta with h, dx
+    with dy); every layout gives the same bits."""
     from b200_runner import b200_fieldset
 
     import offline_particles_b200 as opb
@@ -209,9 +210,12 @@ def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
     z, y, x = g.release(3000, seed=77)
     out = []
     default = timesteppers.SNAPSHOT_LAYOUT
-    for pairs, layout in (("never", "pairs"), ("always", "pairs"), ("always", "quads"), ("always", "octets")):
+    cases = (("never", "pairs", False), ("always", "pairs", False), ("always", "pairs", True),
+             ("always", "quads", False), ("always", "quads", True), ("always", "octets", False))
+    for pairs, layout, bundle in cases:
         timesteppers.SNAPSHOT_PAIRS = pairs
         timesteppers.SNAPSHOT_LAYOUT = layout
+        timesteppers.BUNDLE_2D = bundle
         try:
             f = opb.roms.rk2_w_advection_timestepper if scheme == "rk2" else opb.roms.ab3_w_advection_timestepper
             sim = opb.SimulationBuilder(f(t_arr, np.float64(dt), time=np.float64(1234.5)),
@@ -224,15 +228,17 @@ def test_fused_steppers_same_with_and_without_snapshot_pairs(grid, scheme, dt):
         finally:
             timesteppers.SNAPSHOT_PAIRS = "auto"
             timesteppers.SNAPSHOT_LAYOUT = default
+            timesteppers.BUNDLE_2D = True
     for k in NAMES:
-        for j in (1, 2, 3):
-            assert same_bits(out[0][k], out[j][k]), (k, j)
+        for j in range(1, len(cases)):
+            assert same_bits(out[0][k], out[j][k]), (k, cases[j])
 
 
-@pytest.mark.parametrize("layout", ["pairs", "quads", "octets"])
-def test_batch_same_in_every_pair_layout(grid, alone, layout):
-    """The batched launch reads float32 fields as snapshot pairs, quads or octets; every release ends with
-    the bits of its run alone."""
+@pytest.mark.parametrize("layout,bundle", [("pairs", False), ("pairs", True), ("quads", False), ("quads", True),
+                                           ("octets", False)])
+def test_batch_same_in_every_pair_layout(grid, alone, layout, bundle):
+    """The batched launch reads float32 fields as snapshot pairs, quads or octets, with or without the 2-D
+    bundles; every release ends with the bits of its run alone."""
     from b200_runner import b200_fieldset
 
     from offline_particles_b200 import timesteppers
@@ -242,6 +248,7 @@ def test_batch_same_in_every_pair_layout(grid, alone, layout):
     t_arr = g.time_array[:fields["u"].shape[0]]
     default = timesteppers.BATCH_LAYOUT
     timesteppers.BATCH_LAYOUT = layout
+    timesteppers.BUNDLE_2D = bundle
     try:
         rels = _releases(g, t_arr, SPECS)
         b = ReleaseBatch(b200_fieldset(fields, g.hc, g.spec.nz), rels, buckets=64)
@@ -250,6 +257,7 @@ def test_batch_same_in_every_pair_layout(grid, alone, layout):
         got = [b.result(r) for r in rels]
     finally:
         timesteppers.BATCH_LAYOUT = default
+        timesteppers.BUNDLE_2D = True
     for q, want in enumerate(alone):
         for k in NAMES:
             assert same_bits(got[q][k], want[k]), (q, k, mismatch_report(got[q][k], want[k]))
@@ -373,3 +381,28 @@ def test_host_and_device_step_tables_give_the_same_bits(grid, scheme, dt, monkey
         out.append({k: P[k] for k in NAMES})
     for k in NAMES:
         assert same_bits(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("n,offset", [(786_433, 0), (4096, 1), (3, 0), (1, 0)])
+def test_bundles_match_torch(n, offset):
+    import torch
+
+    from offline_particles_b200 import _lib
+
+    a = torch.randn(n + offset, dtype=torch.float32, device="cuda")[offset:]
+    b = torch.randn(n + offset, dtype=torch.float32, device="cuda")[offset:]
+    h = torch.randn(n + offset, dtype=torch.float64, device="cuda")[offset:]
+    dy = torch.randn(n + offset, dtype=torch.float64, device="cuda")[offset:]
+    zh = torch.full((4 * n,), -1, dtype=torch.int64, device="cuda")
+    dd = torch.full((4 * n,), float("nan"), dtype=torch.float64, device="cuda")
+    _lib.call("opb_bundle_zeta_h", a.data_ptr(), b.data_ptr(), h.data_ptr(), zh.data_ptr(), n, None)
+    _lib.call("opb_bundle_dx_dy", h.data_ptr(), dy.data_ptr(), dd.data_ptr(), n, None)
+    torch.cuda.synchronize()
+    j = torch.cat((torch.arange(1, n, device="cuda"), torch.tensor([n - 1], device="cuda")))
+    words = zh.view(-1, 4)
+    assert torch.equal(words[:, 0].view(torch.float64), h) and torch.equal(words[:, 2].view(torch.float64), h[j])
+    pairs = words[:, 1].view(torch.float32).view(-1, 2)
+    assert torch.equal(pairs[:, 0], a) and torch.equal(pairs[:, 1], b)
+    nxt = words[:, 3].view(torch.float32).view(-1, 2)
+    assert torch.equal(nxt[:, 0], a[j]) and torch.equal(nxt[:, 1], b[j])
+    assert torch.equal(dd.view(-1, 4), torch.stack((h, dy, h[j], dy[j]), dim=1))
