@@ -401,8 +401,8 @@ def test_bundles_match_torch(n, offset):
     j = torch.cat((torch.arange(1, n, device="cuda"), torch.tensor([n - 1], device="cuda")))
     words = zh.view(-1, 4)
     assert torch.equal(words[:, 0].view(torch.float64), h) and torch.equal(words[:, 2].view(torch.float64), h[j])
-    pairs = words[:, 1].view(torch.float32).view(-1, 2)
+    pairs = words[:, 1].contiguous().view(torch.float32).view(-1, 2)
     assert torch.equal(pairs[:, 0], a) and torch.equal(pairs[:, 1], b)
-    nxt = words[:, 3].view(torch.float32).view(-1, 2)
+    nxt = words[:, 3].contiguous().view(torch.float32).view(-1, 2)
     assert torch.equal(nxt[:, 0], a[j]) and torch.equal(nxt[:, 1], b[j])
     assert torch.equal(dd.view(-1, 4), torch.stack((h, dy, h[j], dy[j]), dim=1))
