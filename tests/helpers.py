@@ -127,3 +127,18 @@ def iso_fields():
     del fields["w"]
     fields["rho"] = g.density()
     return g, fields
+
+
+def check_bundles(zh: np.ndarray, dd: np.ndarray, a: np.ndarray, b: np.ndarray, h: np.ndarray, dy: np.ndarray) -> None:
+    """The zeta-with-h bundle ``zh`` (int64 words) of zeta snapshots a, b and h, and the dx-with-dy bundle
+    ``dd`` of dx = h and dy: each element with its x-neighbour (the last element's is itself)."""
+    n = len(a)
+    j = np.minimum(np.arange(n) + 1, n - 1)
+    w = zh.reshape(-1, 4)
+    assert np.array_equal(np.ascontiguousarray(w[:, 0]).view(np.float64), h)
+    assert np.array_equal(np.ascontiguousarray(w[:, 2]).view(np.float64), h[j])
+    pair = np.ascontiguousarray(w[:, 1]).view(np.float32).reshape(-1, 2)
+    nxt = np.ascontiguousarray(w[:, 3]).view(np.float32).reshape(-1, 2)
+    assert np.array_equal(pair[:, 0], a) and np.array_equal(pair[:, 1], b)
+    assert np.array_equal(nxt[:, 0], a[j]) and np.array_equal(nxt[:, 1], b[j])
+    assert np.array_equal(dd.reshape(-1, 4), np.stack((h, dy, h[j], dy[j]), axis=1))

@@ -12,7 +12,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from helpers import same_bits, mismatch_report
+from helpers import check_bundles, mismatch_report, same_bits
 
 pytestmark = pytest.mark.gpu
 
@@ -398,11 +398,5 @@ def test_bundles_match_torch(n, offset):
     _lib.call("opb_bundle_zeta_h", a.data_ptr(), b.data_ptr(), h.data_ptr(), zh.data_ptr(), n, None)
     _lib.call("opb_bundle_dx_dy", h.data_ptr(), dy.data_ptr(), dd.data_ptr(), n, None)
     torch.cuda.synchronize()
-    j = torch.cat((torch.arange(1, n, device="cuda"), torch.tensor([n - 1], device="cuda")))
-    words = zh.view(-1, 4)
-    assert torch.equal(words[:, 0].view(torch.float64), h) and torch.equal(words[:, 2].view(torch.float64), h[j])
-    pairs = words[:, 1].contiguous().view(torch.float32).view(-1, 2)
-    assert torch.equal(pairs[:, 0], a) and torch.equal(pairs[:, 1], b)
-    nxt = words[:, 3].contiguous().view(torch.float32).view(-1, 2)
-    assert torch.equal(nxt[:, 0], a[j]) and torch.equal(nxt[:, 1], b[j])
-    assert torch.equal(dd.view(-1, 4), torch.stack((h, dy, h[j], dy[j]), dim=1))
+    check_bundles(zh.cpu().numpy(), dd.cpu().numpy(), a.cpu().numpy(), b.cpu().numpy(), h.cpu().numpy(),
+                  dy.cpu().numpy())
