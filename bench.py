@@ -395,6 +395,7 @@ def b200_arm(a) -> None:
     barrier(world)
     torch.cuda.synchronize()
     s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0 = torch.cuda.memory_stats(dev)
     w0 = time.perf_counter()
     s3.record()
     sim3.set_indices(hz, hy, hx)
@@ -413,6 +414,10 @@ def b200_arm(a) -> None:
     # means the host blocked there)
     e2e_host_ms = {"set_indices": (w1 - w0) * 1e3, "run": (w2 - w1) * 1e3, "collect": (w3 - w2) * 1e3,
                    "wait": (wall_e2e - (w3 - w0)) * 1e3}
+    m1 = torch.cuda.memory_stats(dev)
+    # device allocations inside the region (cudaMalloc calls, and retries that freed cached blocks first)
+    e2e_alloc = {"cuda_mallocs": m1.get("segment.all.allocated", 0) - m0.get("segment.all.allocated", 0),
+                 "retries": m1.get("num_alloc_retries", 0) - m0.get("num_alloc_retries", 0)}
     sim3.synchronize()
     e2e_ms = dist_max(max(s3.elapsed_time(e3), wall_e2e * 1e3), world)
     h2d = 3 * 8 * n + sum(fs3[k].h2d_bytes for k in TD)
@@ -456,7 +461,7 @@ def b200_arm(a) -> None:
                 "path": "Simulation.set_indices from pinned host + run(K) streaming every snapshot from pinned "
                         "host memory + D2H of zidx/yidx/xidx/status",
                 "h2d_gbs_measured": h2d_gbs, "device_ms": s3.elapsed_time(e3), "wall_ms": wall_e2e * 1e3,
-                "host_ms": e2e_host_ms,
+                "host_ms": e2e_host_ms, "allocator": e2e_alloc,
                 "h2d_bound_value": total / ((h2d + d2h) / (h2d_gbs * 1e9)) if h2d_gbs else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic_per_step * avg_launch_steps if traffic_per_step else None,
