@@ -388,10 +388,10 @@ class SnapshotRing:
         self.last_use: dict[int, torch.cuda.Event | None] = {}
         self.queue = _CopyQueue.of(device)
         self.copy_stream = self.queue.stream
-        # a device-resident or device-generated source is copied device to device: no host staging
-        on_device = (isinstance(source, torch.Tensor) and source.is_cuda) or hasattr(source, "produce")
-        self.staging = [] if on_device else [torch.empty(tuple(spatial_shape), dtype=torch_dtype(np_dtype),
-                                                         pin_memory=True) for _ in range(2)]
+        # pinned host buffers for sources that are neither on the device, generated there, nor already
+        # pinned: allocated on the first upload that needs them
+        self.spatial_shape = tuple(spatial_shape)
+        self.staging: list[torch.Tensor] = []
         self.staging_free = [None, None]  # events: staging buffer's last H2D copy done
         self.staging_next = 0
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=1, thread_name_prefix="opb-snapshots")
@@ -456,6 +456,9 @@ class SnapshotRing:
                 self.h2d_bytes += src[k].numel() * src.element_size()
             return
         host = self._host_snapshot(k)
+        if not self.staging:
+            self.staging = [torch.empty(self.spatial_shape, dtype=torch_dtype(self.np_dtype), pin_memory=True)
+                            for _ in range(2)]
         with torch.cuda.device(self.device):
             b = self.staging_next
             self.staging_next ^= 1
