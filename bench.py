@@ -442,7 +442,7 @@ def b200_arm(a) -> None:
     # physical DRAM bytes per fused step of this kernel on this workload, from one ncu capture of the
     # full-size timed launches (profiles/k_ab3_steps_pairs_config2.md: 3.451 GB and 3.399 GB per 60-step
     # launch, snapshot pairs); traffic per launch scales with the steps it runs
-    traffic_per_step = 57.1e6 if (a.nx, a.ny, a.nz, a.particles) == (1024, 768, 50, 4_194_304) else None
+    traffic_per_step = 59.0e6 if (a.nx, a.ny, a.nz, a.particles) == (1024, 768, 50, 4_194_304) else None
     state_bytes = 2 * (1 + 3 * 8 + 6 * 8)  # status + 3 indices + 6 AB3 history values, float64, read + written
     b_step = n * state_bytes + fb["pair"] + fb["static"]
     tot_steps = sum(launch_steps)
