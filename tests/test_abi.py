@@ -227,3 +227,22 @@ def test_header_constants_match_the_binding(tmp_path):
           "OPB_F32_ZETA_H": _lib.F32_ZETA_H, "OPB_F64_IN_ZETA": _lib.F64_IN_ZETA, "OPB_F64_DX_DY": _lib.F64_DX_DY,
           "OPB_F64_IN_DX": _lib.F64_IN_DX}
     assert c == py
+
+
+def test_integration_stub_matches_the_binding():
+    """The reference-side ctypes stub in INTEGRATION.md declares the structs with the header's layouts."""
+    text = (ROOT / "INTEGRATION.md").read_text()
+    block = re.search(r"```python\n(# offline_particles/kernels/roms/_b200\.py.*?)```", text, flags=re.S).group(1)
+    real_cdll = ctypes.CDLL
+    ns: dict = {}
+    try:
+        ctypes.CDLL = lambda name: real_cdll(str(_lib.LIB_PATH))  # the stub loads the library by name
+        exec(compile(block, "INTEGRATION.md", "exec"), ns)
+    finally:
+        ctypes.CDLL = real_cdll
+    for name in ("opb_field", "opb_roms_fields", "opb_time", "opb_particles", "opb_scalars"):
+        stub, ours = ns[name], getattr(_lib, name)
+        assert ctypes.sizeof(stub) == ctypes.sizeof(ours), name
+        for fname, _ in ours._fields_:
+            assert getattr(stub, fname.lstrip("_") if fname.lstrip("_") in dir(stub) else fname).offset == \
+                getattr(ours, fname).offset, (name, fname)
