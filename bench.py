@@ -468,7 +468,7 @@ def b200_arm(a) -> None:
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic_per_step * avg_launch_steps if traffic_per_step else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the full-size launches, "
-                                       "per launch", "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                                       "per launch", "peak_source": peak_source(),
                      "algorithmic_bytes_per_step": b_step, "bytes_per_particle_step": b_step / n,
                      "steps_per_launch": avg_launch_steps, "launch_ms": avg_launch_ms,
                      "kernel": "k_ab3_steps<float>"},
@@ -561,13 +561,26 @@ def precision_study(a) -> None:
     print(json.dumps(line), flush=True)
 
 
-def measured_peak_gbs() -> float:
-    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json), else the fallback 6650 GB/s."""
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peak_source() -> str:
+    """Where the HBM peak comes from: the measured copy bandwidth, or the fallback figure."""
+    return ("MEASURED_PEAKS.json hbm_gbs (of measured)" if _measured_peaks().get("hbm_gbs")
+            else f"fallback {FALLBACK_HBM_GBS:g} GB/s, an earlier copy measurement on B200 (of fallback; "
+                 "MEASURED_PEAKS.json absent)")
+
+
+def _measured_peaks() -> dict:
     try:
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
     except (OSError, ValueError):
-        peaks = {}
-    return float(peaks.get("hbm_gbs") or 6650.0)
+        return {}
+
+
+def measured_peak_gbs() -> float:
+    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json), else the fallback."""
+    return float(_measured_peaks().get("hbm_gbs") or FALLBACK_HBM_GBS)
 
 
 class EventPairs:
@@ -697,7 +710,7 @@ def batched_study(a) -> None:
                "launch_time_share": kernel_s / batch_s,
                "roofline": {"bound": "hbm", "achieved": alg_bytes / kernel_s / 1e9, "peak": peak, "unit": "GB/s",
                             "frac": alg_bytes / kernel_s / 1e9 / peak,
-                            "algorithmic_bytes": alg_bytes,
+                            "algorithmic_bytes": alg_bytes, "peak_source": peak_source(),
                             "definition": "sum over experiments of particle-steps x state bytes (RK2 50 B, AB3 146 B) "
                                           "+ per interval the snapshot pair and statics x the most steps of one "
                                           "experiment, over the summed launch times"},
