@@ -62,3 +62,38 @@ def test_release_without_waiting_keeps_the_order_moving():
     assert order.issued_below == 2
     order.release(t[2])
     assert order.issued_below == 3 and not order.done
+
+
+class _FakeField:
+    """What _prefetch_after touches on a TimeDependentField, recording the order of prefetches."""
+
+    def __init__(self, name, log, ring_size=8, streamed=True):
+        self.name, self.log, self.ring_size, self.streamed = name, log, ring_size, streamed
+
+    def mark_used(self, ks):
+        pass
+
+    def prefetch(self, k, keep):
+        assert k in keep
+        self.log.append((k, self.name))
+
+
+def test_prefetch_after_a_launch_goes_snapshot_by_snapshot():
+    from offline_particles_b200.timesteppers import _prefetch_after
+
+    log = []
+    td = {n: _FakeField(n, log) for n in ("u", "v", "w", "zeta")}
+    _prefetch_after(td, [0, 1, 2], limit=5)
+    # every field's snapshot 3 before any field's 4, and nothing past the run's horizon
+    assert log == [(k, n) for k in (3, 4, 5) for n in ("u", "v", "w", "zeta")]
+
+
+def test_prefetch_depth_follows_each_ring():
+    from offline_particles_b200.timesteppers import _prefetch_after
+
+    log = []
+    td = {"u": _FakeField("u", log, ring_size=4), "v": _FakeField("v", log, ring_size=6),
+          "zeta": _FakeField("zeta", log, streamed=False)}
+    _prefetch_after(td, [0, 1, 2])
+    # keep {1, 2}: a ring of 4 prefetches 2 ahead, a ring of 6 four ahead, a resident field none
+    assert log == [(3, "u"), (3, "v"), (4, "u"), (4, "v"), (5, "v"), (6, "v")]
