@@ -358,7 +358,9 @@ int opb_trilinear_interpolation(const opb_particles *p, const opb_field *f, cons
  * OPB_INLINE_TABLE entries, which the call copies into the launch's parameters.
  * A host table needs no copy engine, so the launch does not queue behind
  * host-to-device copies issued before it (snapshot uploads); the caller may
- * reuse the array as soon as the call returns. */
+ * reuse the array as soon as the call returns.  Every entry of a host table
+ * is checked (slots within the fields' nslots; OPB_EINVAL otherwise); a device
+ * table is the caller's to get right. */
 #define OPB_INLINE_TABLE 720
 
 /* `nsteps` whole RK2 steps in one launch: per step, the preset's validation

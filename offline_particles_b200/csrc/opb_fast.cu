@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <initializer_list>
 
 #include "opb200.h"
 #include "opb_errors.h"
@@ -786,7 +787,10 @@ int steps_fp32(const char *what, bool rk2, const opb_particles *p, const opb_sca
     if (nsteps > 0 && !table) return fail(OPB_EINVAL, "%s: step table is NULL", what);
     if (fp.n == 0 || nsteps == 0) return OPB_OK;
     static thread_local StepTable tab;  // up to 17 KB: kept off the stack
-    if ((rc = make_step_table(table, (long long)nsteps * (rk2 ? 3 : 2), tab, what))) return rc;
+    int nslots = 0;
+    for (const opb_field *x : {&f->u, &f->v, &f->w, &f->zeta})
+        if (!x->is_static && (nslots == 0 || x->nslots < nslots)) nslots = x->nslots;
+    if ((rc = make_step_table(table, (long long)nsteps * (rk2 ? 3 : 2), tab, what, nslots))) return rc;
     const unsigned g = (unsigned)((fp.n + kBlock - 1) / kBlock);
     cudaStream_t st = (cudaStream_t)stream;
 #define OPB_FAST_LAUNCH(S, SC)                                                                  \

@@ -465,7 +465,10 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     if (rc) return rc;
     if (dp.n == 0 || nsteps == 0) return OPB_OK;
     static thread_local StepTable tab;  // up to 17 KB: kept off the stack
-    if ((rc = make_step_table(table, (long long)nsteps * (rk2 ? 3 : 2), tab, what))) return rc;
+    int nslots = 0;
+    for (const opb_field *x : {&g.u, &g.v, &g.w, &g.zeta})
+        if (!x->is_static && (nslots == 0 || x->nslots < nslots)) nslots = x->nslots;
+    if ((rc = make_step_table(table, (long long)nsteps * (rk2 ? 3 : 2), tab, what, nslots))) return rc;
     const unsigned grid = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
     const bool fixed = roms_layout(dr);

@@ -23,8 +23,10 @@ struct StepTable {
 };
 
 // Fill `out` for a table of `entries` opb_time at `table`: device memory by pointer, host memory
-// (pageable or pinned) by value.
-inline int make_step_table(const opb_time *table, long long entries, StepTable &out, const char *what) {
+// (pageable or pinned) by value, each entry's slots checked against `nslots` (the fewest snapshot slots
+// of the time-dependent fields; 0: every field static, nothing to check).
+inline int make_step_table(const opb_time *table, long long entries, StepTable &out, const char *what,
+                           int nslots) {
     out.dev = nullptr;
     if (entries <= 0) return OPB_OK;
     if (!table) return fail(OPB_EINVAL, "%s: step table is NULL", what);
@@ -41,6 +43,10 @@ inline int make_step_table(const opb_time *table, long long entries, StepTable &
     if (entries > OPB_INLINE_TABLE)
         return fail(OPB_EINVAL, "%s: a host step table holds at most %d entries (got %lld); pass a device table",
                     what, OPB_INLINE_TABLE, entries);
+    for (long long j = 0; j < entries; ++j)
+        if (nslots > 0 && (table[j].prev < 0 || table[j].prev >= nslots || table[j].next < 0 || table[j].next >= nslots))
+            return fail(OPB_EINVAL, "%s: step table entry %lld selects slots (%d, %d) of %d", what, j, table[j].prev,
+                        table[j].next, nslots);
     memcpy(out.inl, table, (size_t)entries * sizeof(opb_time));
     return OPB_OK;
 }

@@ -155,3 +155,31 @@ def test_cancelled_requests_leave_the_others_unchanged(grid):
         sim.run(r.nsteps)
         for k in ("status", "zidx", "yidx", "xidx"):
             assert same_bits(r.result[k], sim.particles[k]), (r.id, k)
+
+
+def test_a_host_step_table_with_a_bad_slot_is_refused(grid, monkeypatch):
+    """A fused launch's host step table is checked entry by entry: a slot outside the fields' slots is an
+    argument error, and nothing is launched."""
+    import offline_particles_b200 as opb
+    from b200_runner import b200_fieldset
+
+    from offline_particles_b200 import timesteppers
+
+    g, fields = grid
+    real = timesteppers._fused_fields
+
+    def corrupt(*args, **kw):
+        rf, table = real(*args, **kw)
+        table[len(table) - 1].next = 7  # no field has 8 slots here
+        return rf, table
+
+    monkeypatch.setattr(timesteppers, "_fused_fields", corrupt)
+    sim = _sim(g, b200_fieldset(fields, g.hc, g.spec.nz), "ab3", n=300)
+    z, y, x = g.release(300, seed=5)
+    sim.set_indices(z, y, x)
+    sim.set_particle_field("status", 10)
+    before = {k: sim.particles[k] for k in NAMES}
+    with pytest.raises(ValueError, match="selects slots"):
+        sim.run(4)
+    for k in NAMES:  # the refused launch changed nothing
+        assert same_bits(sim.particles[k], before[k]), k
