@@ -77,3 +77,53 @@ def test_two_rank_shards_reassemble_the_single_process_run():
         orc.step(p)
     for k in ("status", "zidx", "yidx", "xidx"):
         assert np.array_equal(out[k], p[k], equal_nan=True), k
+
+
+def _ranks_main(rank: int, world: int, port: int, out: dict, fail_rank: int) -> None:
+    """One rank of a product-path job: sharding.Ranks from the launcher's environment, the release shard
+    of this rank, the timed region and the gather that bench.py uses."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    from offline_particles_b200.sharding import Ranks
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    ranks = Ranks(backend="gloo", timeout_s=5.0)
+    try:
+        assert (ranks.rank, ranks.world) == (rank, world) and ranks.device.type == "cpu"
+        g = SyntheticROMS(GridSpec(nx=48, ny=40, nz=8, nt=3, seed=9, dtype="float32"))
+        z, y, x = shard(g.release(1001), rank, world)
+        if rank == fail_rank:
+            raise RuntimeError("rank failed before its first collective")
+        box = {}
+        ms = ranks.timed_ms(lambda: box.update(xz=np.asarray(x) * 2.0 + np.asarray(z)))
+        full = ranks.gather(box["xz"])
+        count = ranks.sum(len(z))
+        slow = ranks.max(float(rank))
+        if rank == 0:
+            out.update(full=full, count=count, slow=slow, ms=ms)
+    except RuntimeError as e:
+        out[f"error{rank}"] = str(e)
+    finally:
+        ranks.close()
+
+
+def test_ranks_product_path_two_gloo_ranks():
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.spawn(_ranks_main, args=(2, _free_port(), out, -1), nprocs=2, join=True)
+    g = SyntheticROMS(GridSpec(nx=48, ny=40, nz=8, nt=3, seed=9, dtype="float32"))
+    z, y, x = g.release(1001)
+    assert np.array_equal(out["full"], x * 2.0 + z)
+    assert out["count"] == 1001.0 and out["slow"] == 1.0 and out["ms"] >= 0.0
+
+
+def test_ranks_failed_rank_ends_the_others_collective_with_an_error():
+    """A rank that raises before the first collective leaves the job; the other rank's barrier ends with an
+    error within the process group's timeout instead of waiting for ever."""
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.spawn(_ranks_main, args=(2, _free_port(), out, 1), nprocs=2, join=True)
+    assert "error1" in out and "first collective" in out["error1"]
+    assert "error0" in out and "full" not in out
