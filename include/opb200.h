@@ -419,9 +419,17 @@ int opb_gather_particles(const opb_particles *src, const opb_particles *dst, con
  *     the library holds it until the process exits.
  *   - At most OPB_NOALLOC_MAX_PARTICLES particles per call; more is rejected
  *     with OPB_EINVAL and a message (use opb_sort_particles then).
- *   - The first call on a device looks up the array's device address (once per
- *     device, with that device current); make that first call before any
- *     stream capture.
+ *   - The first call on a device looks up the array's device address (with
+ *     that device current); make that first call before any stream capture.
+ *     With lazy module loading (the CUDA default) that first call may also
+ *     load this library's device code on that device, which places the array
+ *     in device memory then: a caller that reserves device memory for its own
+ *     pool should make one call (n = 0 is not enough; any n >= 1 is) before
+ *     reserving.  Later calls allocate nothing.
+ *   - Outside stream capture every call looks the address up again, so a
+ *     device reset (cudaDeviceReset) between calls is safe; during capture
+ *     the address found by an earlier call on that device is used, so do not
+ *     capture a call after a reset without an uncaptured call in between.
  *   - Every call on a device shares the one array, which keeps the last call's
  *     contents (nothing in it has to start at zero: each call writes its keys
  *     and ids in full before reading them).  Calls that overlap on the GPU

@@ -521,13 +521,22 @@ void *g_noalloc_ptr[kMaxDevices] = {};
 // Device address of the array on the current device.  In host code the
 // array's name is only a host-side stand-in, never a device address; the
 // runtime maps it the first time, once per device (which may load the module).
-int noalloc_scratch(void **out) {
+// Outside stream capture the address is looked up again on every call (a
+// cheap table lookup once the module is loaded), so a context that was reset
+// and re-created (cudaDeviceReset) never leaves a stale address behind;
+// during capture the address cached by an earlier call is used.
+int noalloc_scratch(void **out, cudaStream_t stream) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fail(OPB_EINVAL, "opb_sort_particles_noalloc: device %d out of range", dev);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) {
+        (void)cudaGetLastError();  // e.g. the legacy stream queried while another stream captures
+        cap = cudaStreamCaptureStatusActive;
+    }
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    if (cap != cudaStreamCaptureStatusActive || !g_noalloc_ptr[dev]) {
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (e != cudaSuccess || !ptr)
@@ -557,7 +566,7 @@ extern "C" int opb_sort_particles_noalloc(const opb_particles *p, const int64_t 
         shape[2] > (1 << 30))
         return fail(OPB_EINVAL, "opb_sort_particles_noalloc: bad grid shape");
     void *base = nullptr;
-    int rc = noalloc_scratch(&base);
+    int rc = noalloc_scratch(&base, (cudaStream_t)stream);
     if (rc) return rc;
     char *ws = (char *)base;
     uint32_t *keys0 = (uint32_t *)ws;

@@ -57,15 +57,21 @@ def test_noalloc_sort_matches_workspace_sort_twice():
 
     lib = _lib.load()
     dims = (ctypes.c_int64 * 3)(50, 768, 1024)
+    side = torch.cuda.Stream()
     for seed, n in ((1, 300_001), (2, _lib.NOALLOC_MAX_PARTICLES)):
         P = _particles(n, seed)
         ref = _reference_perm(lib, P, dims)
-        for call in range(2):  # two calls in a row share (and reuse) the static scratch
+        for call, stream in enumerate((None, side)):  # two calls in a row share (and reuse) the static scratch
             perm = torch.full((n,), -1, dtype=torch.int32, device=P.device)
+            torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
+            handle = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
             rc = lib.opb_sort_particles_noalloc(ctypes.byref(_abi.particles_struct(P)), ctypes.byref(dims),
-                                                perm.data_ptr(), None)
+                                                perm.data_ptr(), handle)
             assert rc == _lib.OK, lib.opb_last_error()
             torch.cuda.synchronize()
+            if call > 0:  # the first call on a device may load the module; later calls allocate nothing
+                assert torch.cuda.mem_get_info()[0] == free0, "the call changed the device's free memory"
             got = perm.cpu().numpy()
             assert np.array_equal(got, ref), f"n={n} call {call}: permutation differs from opb_sort_particles"
 
