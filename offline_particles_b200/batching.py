@@ -529,6 +529,14 @@ class ReleaseBatch:
             It = It.astype(np.int64)
             ft = fr.astype(dtype)
             gt = dtype.type(1) - ft
+            # the device reads these tables unchecked: every pair slot must exist (0, and 1 only when
+            # snapshot j + 2 is in the window) and every experiment's entries must lie in the table
+            npairs = 2 if j + 2 <= min(j + 2, self.num_snapshots - 1) else 1
+            if int((It - j).min()) < 0 or int((It - j).max()) >= npairs:
+                raise RuntimeError(f"interval {j}: a stage reads a snapshot pair outside the window")
+            for e, r, k, first in exps:
+                if first < 0 or first + k * (3 if r.scheme == _lib.SCHEME_RK2 else 2) > len(tidx_all):
+                    raise RuntimeError(f"interval {j}: release {e}'s stage entries run past the table")
             tab = host[self._off_tab:self._off_tab + len(tidx_all) * TIME_DTYPE.itemsize].view(TIME_DTYPE)
             tab["prev"] = It - j  # pair slot: 0 = snapshots j, j+1; 1 = snapshots j+1, j+2
             tab["next"] = It - j
