@@ -25,7 +25,7 @@ template <typename T, typename I, int SCHEME, int LAYOUT, bool B2>
 __device__ __forceinline__ void batched_particle(const DParticles &p, long long i, const opb_experiment &E,
                                                  const DScalars &sc0, const DRoms &r, const opb_time *table,
                                                  const Levels &L) {
-    PState s;
+    PState<I> s;
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
     DScalars sc = sc0;
@@ -51,18 +51,17 @@ __device__ __forceinline__ void batched_particle(const DParticles &p, long long 
         if (s.status & ST_INACTIVE) break;
         if (ab3) {
             const opb_time t1 = tab[2 * k], t2 = tab[2 * k + 1];
-            const bool reuse = k > 0 && same_time(t1, s.at);
-            if (!ab3_step(s, bind_all<T, I, true, LAYOUT, B2>(r, t1), sc, reuse)) {
+            const bool reuse = k > 0 && same_time(t1, tab[2 * k - 1]);  // the last post step's time
+            if (!ab3_step(s, bind_all<T, I, true, LAYOUT, B2>(r, t1), sc, L, reuse, k > 0)) {
                 raise_zero_division(p);
                 break;
             }
             moved = true;
             ab3_post(s, bind_all<T, I, true, LAYOUT, B2>(r, t2), L, sc);
-            s.at = t2;
         } else {
             const opb_time t1 = tab[3 * k], t2 = tab[3 * k + 1], t3 = tab[3 * k + 2];
-            const bool reuse = k > 0 && same_time(t1, s.at);
-            if (!rk2_stage1(s, bind_all<T, I, true, LAYOUT, B2>(r, t1), sc, reuse)) {
+            const bool reuse = k > 0 && same_time(t1, tab[3 * k - 1]);  // the last update's time
+            if (!rk2_stage1(s, bind_all<T, I, true, LAYOUT, B2>(r, t1), sc, L, reuse, k > 0)) {
                 raise_zero_division(p);
                 break;
             }
@@ -72,7 +71,6 @@ __device__ __forceinline__ void batched_particle(const DParticles &p, long long 
                 break;
             }
             rk2_update(s, bind_all<T, I, true, LAYOUT, B2>(r, t3), L, sc);
-            s.at = t3;
         }
     }
     if (s.status != st0) p.status[i] = s.status;
@@ -277,7 +275,7 @@ int opb_batched_steps(const opb_particles *p, opb_batch_header *header, const op
         return fail(OPB_EINVAL, "%s: scheme must be 0, OPB_SCHEME_RK2 or OPB_SCHEME_AB3", what);
     if (!roms_layout(dr))
         return fail(OPB_EINVAL, "%s: fields must have the ROMS layout (u, v, w, zeta time-dependent; h, dx, dy, C "
-                    "static)", what);
+                    "static) and geometry (u, v, w staggered on the Arakawa C grid)", what);
     rc = need_fields(p, what, {{"z", p->z}, {"_dxidx1", p->dxidx1}, {"_dyidx1", p->dyidx1}, {"_dz1", p->dz1},
                                {"_dxidx2", p->dxidx2}, {"_dyidx2", p->dyidx2}, {"_dz2", p->dz2},
                                {"_dxidx0", p->dxidx0}, {"_dyidx0", p->dyidx0}, {"_dz0", p->dz0}});

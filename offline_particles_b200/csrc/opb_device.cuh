@@ -29,8 +29,23 @@ struct DField {
     int is_static;         // 1: data[0] is float64 and time-invariant
 };
 
+// The ROMS field geometry (Arakawa C grid) on nz x ny x nx rho points: u on
+// (nz, ny, nx - 1) at x offset -0.5, v on (nz, ny - 1, nx) at y offset -0.5,
+// w on (nz + 1, ny, nx) at z offset +0.5 (w_centered: the field in the w slot
+// sits on rho points, (nz, ny, nx), as the isopycnal follower's density does),
+// zeta, h, dx, dy on (ny, nx) and C on nz levels, all other offsets 0.  The
+// host sets `roms` when every field of a launch has exactly this geometry;
+// the compiled-layout kernels then share one set of stencil axes per position
+// across all fields.
+struct DGeom {
+    long long nz, ny, nx;
+    int roms;        // 1: the geometry above holds
+    int w_centered;  // 1: the w slot is on rho points (nz, ny, nx), offsets 0
+};
+
 struct DRoms {
     DField u, v, w, dx, dy, h, zeta, C;
+    DGeom geo;
 };
 
 struct DParticles {
@@ -82,25 +97,24 @@ constexpr int KIND_ANY = 0, KIND_STATIC = 1, KIND_TD = 2, KIND_PAIRS = 3, KIND_Q
 // yx-pairs of h, dx, dy.
 constexpr int LAYOUT_PLAIN = 0, LAYOUT_PAIRS = 1, LAYOUT_QUADS = 2, LAYOUT_OCTS = 3;
 
-// 32-byte read-only loads (sm_100: ld.global.nc.v8.f32 / .v4.f64); the
+// 32-byte read-only loads (sm_100: ld.global.nc.v4.f64 / .v4.u64); the
 // address must be 32-byte aligned
-struct alignas(32) F8 {
-    float v[8];
-};
 struct alignas(32) D4 {
     double v[4];
 };
-__device__ __forceinline__ F8 ldg256(const F8 *p) {
-    F8 r;
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]), "=f"(r.v[6]),
-          "=f"(r.v[7])
-        : "l"(p));
-    return r;
-}
 __device__ __forceinline__ D4 ldg256(const D4 *p) {
     D4 r;
     asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3]) : "l"(p));
+    return r;
+}
+
+// four 64-bit words: four float32 snapshot pairs, or h and zeta-pair words (2-D bundles)
+struct alignas(32) U4 {
+    unsigned long long v[4];
+};
+__device__ __forceinline__ U4 ldg256(const U4 *p) {
+    U4 r;
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(r.v[0]), "=l"(r.v[1]), "=l"(r.v[2]), "=l"(r.v[3]) : "l"(p));
     return r;
 }
 
@@ -115,6 +129,21 @@ struct Vec2<double> {
     using type = double2;
 };
 
+// The float32 time blend of one snapshot pair held as one 64-bit word
+// {earlier (low half), later (high half)}, with w = {gt, ft}: both products in
+// one packed multiply (mul.rn.f32x2 rounds each lane to nearest, exactly as
+// two float32 multiplies do), then their float32 sum, widened to float64.
+__device__ __forceinline__ double blend_word(unsigned long long pn, unsigned long long w) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pn), "l"(w));
+    return (double)(__uint_as_float((unsigned)(r & 0xffffffffull)) + __uint_as_float((unsigned)(r >> 32)));
+}
+
+// {gt, ft} as one 64-bit word for blend_word
+__device__ __forceinline__ unsigned long long blend_weights(float ft, float gt) {
+    return (unsigned long long)__float_as_uint(gt) | ((unsigned long long)__float_as_uint(ft) << 32);
+}
+
 template <typename T, typename I, int KIND = KIND_ANY>
 struct View {
     using index_type = I;
@@ -124,6 +153,7 @@ struct View {
     const T *next;
     const double *stat;  // non-null: static float64 field
     T ft, gt;
+    unsigned long long w;  // float32 storage: {gt, ft} for blend_word
     I n0, n1, n2;
     double o0, o1, o2;
 
@@ -140,13 +170,13 @@ struct View {
         if constexpr (KIND == KIND_YXPAIRS) {
             return __ldg(stat + 4 * (long long)i);
         } else if constexpr (KIND == KIND_OCTS) {
-            const float2 v = __ldg((const float2 *)prev + 4 * (long long)i);
-            return blend(v.x, v.y);
+            return blend_word(__ldg((const unsigned long long *)prev + 4 * (long long)i), w);
         } else if constexpr (KIND == KIND_XPAIRS) {
             return __ldg(stat + 2 * (long long)i);
         } else if constexpr (KIND == KIND_QUADS) {
-            const float2 v = __ldg((const float2 *)prev + 2 * (long long)i);
-            return blend(v.x, v.y);
+            return blend_word(__ldg((const unsigned long long *)prev + 2 * (long long)i), w);
+        } else if constexpr (KIND == KIND_PAIRS && sizeof(T) == 4) {
+            return blend_word(__ldg((const unsigned long long *)prev + i), w);
         } else if constexpr (KIND == KIND_PAIRS) {
             const typename Vec2<T>::type v = __ldg((const typename Vec2<T>::type *)prev + i);
             return blend(v.x, v.y);
@@ -164,17 +194,17 @@ struct View {
             lo = v.x;
             hi = v.y;
         } else if constexpr (KIND == KIND_OCTS) {
-            const float4 v = __ldg((const float4 *)prev + 2 * (long long)i);
-            lo = blend(v.x, v.y);
-            hi = blend(v.z, v.w);
+            const ulonglong2 v = __ldg((const ulonglong2 *)prev + 2 * (long long)i);
+            lo = blend_word(v.x, w);
+            hi = blend_word(v.y, w);
         } else if constexpr (KIND == KIND_XPAIRS) {
             const double2 v = __ldg((const double2 *)stat + i);
             lo = v.x;
             hi = v.y;
         } else if constexpr (KIND == KIND_QUADS) {
-            const float4 v = __ldg((const float4 *)prev + i);
-            lo = blend(v.x, v.y);
-            hi = blend(v.z, v.w);
+            const ulonglong2 v = __ldg((const ulonglong2 *)prev + i);
+            lo = blend_word(v.x, w);
+            hi = blend_word(v.y, w);
         } else {
             lo = at(i);
             hi = at(i + 1);
@@ -191,11 +221,11 @@ struct View {
             v10 = v.v[2];
             v11 = v.v[3];
         } else if constexpr (KIND == KIND_OCTS) {
-            const F8 v = ldg256((const F8 *)prev + i);
-            v00 = blend(v.v[0], v.v[1]);
-            v01 = blend(v.v[2], v.v[3]);
-            v10 = blend(v.v[4], v.v[5]);
-            v11 = blend(v.v[6], v.v[7]);
+            const U4 v = ldg256((const U4 *)prev + i);
+            v00 = blend_word(v.v[0], w);
+            v01 = blend_word(v.v[1], w);
+            v10 = blend_word(v.v[2], w);
+            v11 = blend_word(v.v[3], w);
         } else {
             at2(i, v00, v01);
             at2(i + row, v10, v11);
@@ -212,28 +242,17 @@ struct View {
 //     zeta pair[i+1]} as four 64-bit words (a zeta pair: the earlier snapshot's
 //     value in the low half, the later's in the high half);
 //   dx with dy (static): {dx[i], dy[i], dx[i+1], dy[i+1]}.
-struct alignas(32) U4 {
-    unsigned long long v[4];
-};
-__device__ __forceinline__ U4 ldg256(const U4 *p) {
-    U4 r;
-    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(r.v[0]), "=l"(r.v[1]), "=l"(r.v[2]), "=l"(r.v[3]) : "l"(p));
-    return r;
-}
 
 template <typename I>
 struct ZetaHView {
     using index_type = I;
     const U4 *p;
     float ft, gt;
+    unsigned long long w;  // {gt, ft} for blend_word
     I n0, n1;
     double o0, o1;
     // the blend of one zeta pair word, as View::blend in float32
-    __device__ __forceinline__ double zeta(unsigned long long w) const {
-        const float x = __uint_as_float((unsigned)(w & 0xffffffffull)) * gt;
-        const float y = __uint_as_float((unsigned)(w >> 32)) * ft;
-        return (double)(x + y);
-    }
+    __device__ __forceinline__ double zeta(unsigned long long pn) const { return blend_word(pn, w); }
     // h and zeta at i and i + 1
     __device__ __forceinline__ void at2(I i, double &h0, double &z0, double &h1, double &z1) const {
         const U4 w = ldg256(p + i);
@@ -274,6 +293,7 @@ __device__ __forceinline__ View<T, I, KIND> bind(const DField &f, const opb_time
         v.ft = (T)t.ft;  // exact: the host rounded ft, gt to the storage dtype
         v.gt = (T)t.gt;
     }
+    if constexpr (sizeof(T) == 4) v.w = blend_weights((float)v.ft, (float)v.gt);
     v.n0 = (I)f.n0;
     v.n1 = (I)f.n1;
     v.n2 = (I)f.n2;
@@ -367,6 +387,76 @@ __device__ __forceinline__ double trilinear(const F &f, double idx0, double idx1
     const I s1 = f.n2;
     const I s0 = f.n1 * f.n2;
     const I b = I0 * s0 + I1 * s1 + I2;
+    double v000, v001, v010, v011, v100, v101, v110, v111;
+    f.at4(b, s1, v000, v001, v010, v011);
+    f.at4(b + s0, s1, v100, v101, v110, v111);
+    return (g0 * g1 * g2 * v000 +
+            g0 * g1 * f2 * v001 +
+            g0 * f1 * g2 * v010 +
+            g0 * f1 * f2 * v011 +
+            f0 * g1 * g2 * v100 +
+            f0 * g1 * f2 * v101 +
+            f0 * f1 * g2 * v110 +
+            f0 * f1 * f2 * v111);
+}
+
+// ------------------------------------------------------ shared stencil axes
+// One axis of a linear stencil (linear.pxd:3-9 for one dimension): the lower
+// corner I = truncate_index(idx, max_idx), its weight f = idx - I and
+// g = 1 - f.  Every stencil of a field is a product of such axes, so fields
+// that sit on the same points in a dimension share that dimension's axis: the
+// value is the same expression of the same inputs, hence the same bits.
+template <typename I>
+struct Axis {
+    I i;
+    double f, g;
+};
+
+template <typename I>
+__device__ __forceinline__ Axis<I> make_axis(double idx, I max_idx) {
+    Axis<I> a;
+    a.i = trunc_index(idx, max_idx);
+    a.f = idx - (double)a.i;
+    a.g = 1.0 - a.f;
+    return a;
+}
+
+// linear() over an axis of values read from `v` (any readable pointer, e.g. a
+// shared-memory table): g0 * v[I0] + f0 * v[I0 + 1] (linear.pxd:11-17)
+template <typename I>
+__device__ __forceinline__ double linear_ax(const double *v, const Axis<I> &a) {
+    return a.g * v[a.i] + a.f * v[a.i + 1];
+}
+
+// bilinear() over two axes; `row`: the field's x size (linear.pxd:19-33)
+template <typename F, typename I>
+__device__ __forceinline__ double bilinear_ax(const F &f, const Axis<I> &a0, const Axis<I> &a1, I row) {
+    const double g0 = a0.g, f0 = a0.f, g1 = a1.g, f1 = a1.f;
+    double v00, v01, v10, v11;
+    f.at4(a0.i * row + a1.i, row, v00, v01, v10, v11);
+    return g0 * g1 * v00 + g0 * f1 * v01 + f0 * g1 * v10 + f0 * f1 * v11;
+}
+
+// bilinear_pair() over two axes: both fields of a bundle on one stencil
+template <typename F, typename I>
+__device__ __forceinline__ void bilinear_pair_ax(const F &f, const Axis<I> &a0, const Axis<I> &a1, I row, double &a,
+                                                 double &b) {
+    const double g0 = a0.g, f0 = a0.f, g1 = a1.g, f1 = a1.f;
+    const I base = a0.i * row + a1.i;
+    double a00, b00, a01, b01, a10, b10, a11, b11;
+    f.at2(base, a00, b00, a01, b01);
+    f.at2(base + row, a10, b10, a11, b11);
+    a = g0 * g1 * a00 + g0 * f1 * a01 + f0 * g1 * a10 + f0 * f1 * a11;
+    b = g0 * g1 * b00 + g0 * f1 * b01 + f0 * g1 * b10 + f0 * f1 * b11;
+}
+
+// trilinear() over three axes; s0, s1: the field's level and row strides
+// (linear.pxd:35-65)
+template <typename F, typename I>
+__device__ __forceinline__ double trilinear_ax(const F &f, const Axis<I> &a0, const Axis<I> &a1, const Axis<I> &a2,
+                                               I s0, I s1) {
+    const double g0 = a0.g, f0 = a0.f, g1 = a1.g, f1 = a1.f, g2 = a2.g, f2 = a2.f;
+    const I b = a0.i * s0 + a1.i * s1 + a2.i;
     double v000, v001, v010, v011, v100, v101, v110, v111;
     f.at4(b, s1, v000, v001, v010, v011);
     f.at4(b + s0, s1, v100, v101, v110, v111);
@@ -553,8 +643,15 @@ __device__ __forceinline__ double compute_zidx_hint(double z, double h, double z
     constexpr int kMaxWalk = 3;
     int Cidx;
     double S_low, S_high;
+    // S(k) and S(k + 1) are pure functions of the level: evaluated together, their divisions overlap
+    // (the common case, the hint's own level, needs both)
     double lo_v = S_level(L, k, hc, h);
-    if (lo_v > S) {  // walk down
+    const double up_v = S_level(L, k + 1, hc, h);  // k <= top, so k + 1 <= C_size - 1
+    if (lo_v <= S && k < top && up_v > S) {
+        Cidx = k;
+        S_low = lo_v;
+        S_high = up_v;
+    } else if (lo_v > S) {  // walk down
         double hi_v = lo_v;
         int walked = 0;
         while (k > 0 && lo_v > S) {

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <initializer_list>
@@ -36,11 +37,44 @@ void dispatch(int dtype, bool small_index, F &&f) {
 // every field of the launch has fewer than 2^31 elements
 bool fits_int(const DField &f) { return f.n0 * f.n1 * f.n2 < 0x7fffffffLL; }
 
-// u, v, w, zeta time-dependent and h, dx, dy, C static: the layout the ROMS
-// presets use, compiled with the field kinds fixed
-bool roms_layout(const DRoms &r) {
+// An offset of exactly +0.0 (a -0.0 offset changes idx + offset for idx = -0.0)
+bool zero_offset(double o) { return o == 0.0 && !std::signbit(o); }
+
+// Fill r.geo: whether the fields have the ROMS geometry (DGeom) and its sizes.
+void set_geometry(DRoms &r) {
+    DGeom &g = r.geo;
+    g.nz = r.u.n0;
+    g.ny = r.u.n1;
+    g.nx = r.v.n2;
+    g.roms = 0;
+    g.w_centered = 0;
+    const long long nz = g.nz, ny = g.ny, nx = g.nx;
+    auto is3 = [](const DField &f, long long a, long long b, long long c, double oa, double ob, double oc) {
+        return f.n0 == a && f.n1 == b && f.n2 == c && f.o0 == oa && f.o1 == ob && f.o2 == oc &&
+               (oa != 0.0 || zero_offset(f.o0)) && (ob != 0.0 || zero_offset(f.o1)) &&
+               (oc != 0.0 || zero_offset(f.o2));
+    };
+    auto is2 = [&](const DField &f) {
+        return f.n0 == ny && f.n1 == nx && f.n2 == 1 && zero_offset(f.o0) && zero_offset(f.o1);
+    };
+    if (!is3(r.u, nz, ny, nx - 1, 0.0, 0.0, -0.5) || !is3(r.v, nz, ny - 1, nx, 0.0, -0.5, 0.0)) return;
+    if (!is2(r.zeta) || !is2(r.h) || !is2(r.dx) || !is2(r.dy)) return;
+    if (!(r.C.n0 == nz && r.C.n1 == 1 && r.C.n2 == 1 && zero_offset(r.C.o0))) return;
+    if (is3(r.w, nz + 1, ny, nx, 0.5, 0.0, 0.0)) {
+        g.roms = 1;
+    } else if (is3(r.w, nz, ny, nx, 0.0, 0.0, 0.0)) {
+        g.roms = 1;
+        g.w_centered = 1;
+    }
+}
+
+// u, v, w, zeta time-dependent and h, dx, dy, C static, in the ROMS geometry
+// (DGeom; `w_centered`: the w slot on rho points, as the isopycnal follower
+// has it): the layout the ROMS presets use, compiled with the field kinds and
+// the geometry fixed
+bool roms_layout(const DRoms &r, bool w_centered = false) {
     return !r.u.is_static && !r.v.is_static && !r.w.is_static && !r.zeta.is_static && r.h.is_static &&
-           r.dx.is_static && r.dy.is_static && r.C.is_static;
+           r.dx.is_static && r.dy.is_static && r.C.is_static && r.geo.roms && (r.geo.w_centered != 0) == w_centered;
 }
 
 bool fits_int(const DRoms &r) {
@@ -169,6 +203,8 @@ int convert_fields(const opb_roms_fields *in, DRoms &out, const char *what, bool
     if ((rc = convert_field(in->C, out.C, 1, what, "C", dtype))) return rc;
     if (!in->C.is_static) return fail(OPB_EINVAL, "%s: field 'C' must be static", what);
     if (*dtype < 0) *dtype = OPB_F64;  // every field static
+    memset(&out.geo, 0, sizeof(DGeom));
+    if (need_velocity) set_geometry(out);
     return OPB_OK;
 }
 

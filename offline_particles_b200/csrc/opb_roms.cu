@@ -60,11 +60,11 @@ __global__ void __launch_bounds__(kBlock) k_rk2_step_1(const __grid_constant__ D
                                                        const __grid_constant__ DRoms r, opb_time t) {
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
-    PState s;
+    PState<I> s;
     s.zidx = p.zidx[i];
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
-    const bool ok = rk2_stage1(s, bind_all<T, I>(r, t), sc);
+    const bool ok = rk2_stage1(s, bind_all<T, I>(r, t), sc, Levels{});
     p.z[i] = s.z;
     if (!ok) {
         raise_zero_division(p);
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kBlock) k_rk2_step_2(const __grid_constant__ D
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
-    PState s;
+    PState<I> s;
     s.zidx = p.zidx[i];  // hint for the vertical search
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kBlock) k_rk2_update(const __grid_constant__ D
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
-    PState s;
+    PState<I> s;
     s.zidx = p.zidx[i];
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
@@ -125,10 +125,10 @@ __global__ void __launch_bounds__(kBlock) k_rk2_update(const __grid_constant__ D
 }
 
 template <typename T, typename I, bool ISO>
-__device__ __forceinline__ bool ab3_any(PState &s, const Bound<T, I> &f, const DScalars &sc, const DParticles &p,
+__device__ __forceinline__ bool ab3_any(PState<I> &s, const Bound<T, I> &f, const DScalars &sc, const DParticles &p,
                                         long long i) {
-    if constexpr (ISO) return ab3_step(s, f, sc, false, IsoVel{p.rho_t[i], sc.w_max, sc.rho_scale});
-    else return ab3_step(s, f, sc);
+    if constexpr (ISO) return ab3_step(s, f, sc, Levels{}, false, false, IsoVel{p.rho_t[i], sc.w_max, sc.rho_scale});
+    else return ab3_step(s, f, sc, Levels{});
 }
 
 template <typename T, typename I, bool ISO = false>
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3(const __grid_constant__ DParticl
                                                 const __grid_constant__ DRoms r, opb_time t) {
     const long long i = gtid();
     if (i >= p.n) return;
-    PState s;
+    PState<I> s;
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
     s.zidx = p.zidx[i];
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3_post(const __grid_constant__ DPa
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n || (p.status[i] & ST_INACTIVE)) return;
-    PState s;
+    PState<I> s;
     s.zidx = p.zidx[i];  // hint for the vertical search
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
-    PState s;
+    PState<I> s;
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
     s.zidx = p.zidx[i];
@@ -208,8 +208,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table.at(3 * k), t2 = table.at(3 * k + 1), t3 = table.at(3 * k + 2);
-        const bool reuse = k > 0 && same_time(t1, s.at);
-        if (!rk2_stage1(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, reuse)) {
+        // h and zeta of the last update (at the previous step's t + dt, the entry before t1) carry over
+        // when t1 selects the same snapshots and weights
+        const bool reuse = k > 0 && same_time(t1, table.at(3 * k - 1));
+        if (!rk2_stage1(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, L, reuse, k > 0)) {
             raise_zero_division(p);
             break;
         }
@@ -219,7 +221,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
             break;
         }
         rk2_update(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t3), L, sc);
-        s.at = t3;
     }
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;
@@ -246,7 +247,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
-    PState s;
+    PState<I> s;
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
     s.zidx = p.zidx[i];
@@ -265,18 +266,20 @@ __global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table.at(2 * k), t2 = table.at(2 * k + 1);
-        const bool reuse = k > 0 && same_time(t1, s.at);
+        // h and zeta of the last post step (at the previous step's t + dt, the entry before t1) carry over
+        // when t1 selects the same snapshots and weights
+        const bool reuse = k > 0 && same_time(t1, table.at(2 * k - 1));
         bool ok;
-        if constexpr (ISO) ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, reuse, IsoVel{rho_t, sc.w_max,
-                                                                                                     sc.rho_scale});
-        else ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, reuse);
+        if constexpr (ISO)
+            ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, L, reuse, k > 0,
+                          IsoVel{rho_t, sc.w_max, sc.rho_scale});
+        else ok = ab3_step(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t1), sc, L, reuse, k > 0);
         if (!ok) {
             raise_zero_division(p);
             break;
         }
         moved = true;
         ab3_post(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t2), L, sc);
-        s.at = t2;
     }
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;
@@ -450,8 +453,8 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     bool bundled = false;
     if ((rc = unpair_fields(f, g, layout, bundled, what))) return rc;
     if ((rc = convert_fields(&g, dr, what, true, &dtype))) return rc;
-    if (layout != LAYOUT_PLAIN && !roms_layout(dr))
-        return fail(OPB_EINVAL, "%s: snapshot pairs need the ROMS field layout", what);
+    if (layout != LAYOUT_PLAIN && !roms_layout(dr, iso))
+        return fail(OPB_EINVAL, "%s: snapshot pairs need the ROMS field layout and geometry", what);
     if (nsteps < 0) return fail(OPB_EINVAL, "%s: negative step count", what);
     if (nsteps > 0 && !table) return fail(OPB_EINVAL, "%s: step table is NULL", what);
     if (rk2)
@@ -471,7 +474,7 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     if ((rc = make_step_table(table, (long long)nsteps * (rk2 ? 3 : 2), tab, what, nslots))) return rc;
     const unsigned grid = grid_for(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
-    const bool fixed = roms_layout(dr);
+    const bool fixed = roms_layout(dr, iso);
     auto go = [&](auto tv, auto iv, auto lv, auto bv) {
         using T = decltype(tv);
         using I = decltype(iv);

@@ -16,16 +16,19 @@ namespace {
 constexpr int kBlock = 256;
 
 // ------------------------------------------------------------ per particle
+template <typename I = long long>
 struct PState {
     double zidx, yidx, xidx, z;
     double k0x, k0y, k0z;  // AB3 k(n)
     double k1x, k1y, k1z;  // RK2 k1 / AB3 k(n-1)
     double k2x, k2y, k2z;  // RK2 k2 / AB3 k(n-2)
-    // h and zeta at (yidx, xidx) for the time selection `at`, left by the
-    // previous step's last stage; the next step's first stage needs exactly
-    // these values (same position, same time index) and reuses them
+    // h and zeta at (yidx, xidx) for the previous step's last time selection,
+    // left by its last stage; the next step's first stage needs exactly these
+    // values when it selects the same time (same position) and reuses them
     double h_at, zeta_at;
-    opb_time at;
+    // compiled ROMS layout: the rho-point stencil axes at (yidx, xidx), left by
+    // the previous step's last stage (the position has not moved since)
+    Axis<I> ya, xa;
     uint8_t status;
 };
 
@@ -38,14 +41,16 @@ __device__ __forceinline__ void raise_zero_division(const DParticles &p) {
 }
 
 // The fields of one stage.  FIXED: the ROMS layout (u, v, w, zeta
-// time-dependent; h, dx, dy, C static), known at compile time; otherwise each
-// field's kind is read at run time.  LAYOUT (FIXED only): how the
-// time-dependent fields, and with LAYOUT_QUADS / LAYOUT_OCTS the static h, dx,
-// dy, are read.
+// time-dependent; h, dx, dy, C static) and the ROMS geometry (DGeom), known at
+// compile time; otherwise each field's kind, shape and offsets are read at run
+// time.  LAYOUT (FIXED only): how the time-dependent fields, and with
+// LAYOUT_QUADS / LAYOUT_OCTS the static h, dx, dy, are read.
 template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN, bool B2 = false>
 struct Bound {
     static_assert(FIXED || LAYOUT == LAYOUT_PLAIN, "pair layouts need the ROMS field layout");
     static_assert(!B2 || (LAYOUT != LAYOUT_PLAIN && sizeof(T) == 4), "2-D bundles come with float32 pairs");
+    using index_type = I;
+    static constexpr bool kFixed = FIXED;
     static constexpr int KT = LAYOUT == LAYOUT_OCTS ? KIND_OCTS
                               : LAYOUT == LAYOUT_QUADS ? KIND_QUADS
                               : LAYOUT == LAYOUT_PAIRS ? KIND_PAIRS
@@ -60,6 +65,7 @@ struct Bound {
     View<T, I, KC> C;
     ZetaHView<I> zh;  // B2: zeta with h
     DxDyView<I> dd;   // B2: dx with dy
+    I nz, ny, nx;     // FIXED: rho-point sizes (DGeom)
 };
 
 template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN, bool B2 = false>
@@ -70,10 +76,14 @@ __device__ __forceinline__ Bound<T, I, FIXED, LAYOUT, B2> bind_all(const DRoms &
     b.v = bind<T, I, B::KT>(r.v, t);
     b.w = bind<T, I, B::KT>(r.w, t);
     b.C = bind<T, I, B::KC>(r.C, t);  // static float64 (kernels/_core.pyx:5-9)
+    b.nz = (I)r.geo.nz;
+    b.ny = (I)r.geo.ny;
+    b.nx = (I)r.geo.nx;
     if constexpr (B2) {
         b.zh.p = (const U4 *)r.zeta.data[t.prev];
         b.zh.ft = (float)t.ft;  // exact: the host rounded ft, gt to float32
         b.zh.gt = (float)t.gt;
+        b.zh.w = blend_weights(b.zh.ft, b.zh.gt);
         b.zh.n0 = (I)r.zeta.n0;
         b.zh.n1 = (I)r.zeta.n1;
         b.zh.o0 = r.zeta.o0;
@@ -90,6 +100,62 @@ __device__ __forceinline__ Bound<T, I, FIXED, LAYOUT, B2> bind_all(const DRoms &
         b.h = bind<T, I, B::KS>(r.h, t);
     }
     return b;
+}
+
+// ---------------------------------------------- compiled ROMS layout: axes
+// The stencil axes at one position.  In the ROMS geometry each dimension has
+// two kinds of points: rho points (offset 0: u and v in z, u and w in y, v and
+// w in x, the 2-D fields, C) and half a cell off (w in z at +0.5, v in y and u
+// in x at -0.5).  Each axis is make_axis(idx + offset, n - 2) of the fields on
+// those points, exactly what trilinear()/bilinear()/linear() compute for each
+// of them, so one evaluation serves them all.
+template <typename I>
+struct Axes {
+    Axis<I> zc, zs, yc, ys, xc, xs;
+};
+
+template <typename B, typename I = typename B::index_type>
+__device__ __forceinline__ void rho_axes_h(const B &f, double y, double x, Axis<I> &yc, Axis<I> &xc) {
+    yc = make_axis(y + 0.0, (I)(f.ny - 2));
+    xc = make_axis(x + 0.0, (I)(f.nx - 2));
+}
+
+// the remaining axes at (z, y, x) once the rho-point ones in y and x are known;
+// W_CENTERED: the w slot sits on rho points and needs no zs
+template <bool W_CENTERED, typename B, typename I = typename B::index_type>
+__device__ __forceinline__ void other_axes(const B &f, double z, double y, double x, Axes<I> &a) {
+    a.zc = make_axis(z + 0.0, (I)(f.nz - 2));
+    if constexpr (!W_CENTERED) a.zs = make_axis(z + 0.5, (I)(f.nz - 1));
+    a.ys = make_axis(y + -0.5, (I)(f.ny - 3));
+    a.xs = make_axis(x + -0.5, (I)(f.nx - 3));
+}
+
+// u, v and the w-slot field at the axes' position, and dx, dy
+template <bool W_CENTERED, typename B, typename I = typename B::index_type>
+__device__ __forceinline__ void velocity_ax(const B &f, const Axes<I> &a, double &u, double &v, double &w, double &dx,
+                                            double &dy) {
+    const I nx = f.nx, ny = f.ny;
+    u = trilinear_ax(f.u, a.zc, a.yc, a.xs, ny * (nx - 1), nx - 1);
+    if constexpr (B::BUNDLED) {
+        bilinear_pair_ax(f.dd, a.yc, a.xc, nx, dx, dy);
+    } else {
+        dx = bilinear_ax(f.dx, a.yc, a.xc, nx);
+        dy = bilinear_ax(f.dy, a.yc, a.xc, nx);
+    }
+    v = trilinear_ax(f.v, a.zc, a.ys, a.xc, (ny - 1) * nx, nx);
+    if constexpr (W_CENTERED) w = trilinear_ax(f.w, a.zc, a.yc, a.xc, ny * nx, nx);
+    else w = trilinear_ax(f.w, a.zs, a.yc, a.xc, ny * nx, nx);
+}
+
+// h and zeta on the rho-point axes
+template <typename B, typename I = typename B::index_type>
+__device__ __forceinline__ void hz_ax(const B &f, const Axis<I> &yc, const Axis<I> &xc, double &h, double &zeta) {
+    if constexpr (B::BUNDLED) {
+        bilinear_pair_ax(f.zh, yc, xc, f.nx, h, zeta);
+    } else {
+        h = bilinear_ax(f.h, yc, xc, f.nx);
+        zeta = bilinear_ax(f.zeta, yc, xc, f.nx);
+    }
 }
 
 // h and zeta at (y, x): one stencil for both when they are bundled
@@ -114,33 +180,72 @@ __device__ __forceinline__ void dxdy_at(const B &f, double y, double x, double &
     }
 }
 
+// h and zeta at the particle's (yidx, xidx), leaving the rho-point axes there
+// in the state (compiled layout) for the next stage at this position
+template <typename B, typename S>
+__device__ __forceinline__ void hz_here(S &s, const B &f, double &h, double &zeta) {
+    if constexpr (B::kFixed) {
+        rho_axes_h(f, s.yidx, s.xidx, s.ya, s.xa);
+        hz_ax(f, s.ya, s.xa, h, zeta);
+    } else {
+        hz_at(f, s.yidx, s.xidx, h, zeta);
+    }
+}
+
 // Every kernel starts here, before any thread can return: the block's shared
-// tables of the sigma levels (used by compute_zidx).
+// tables of the sigma levels (used by compute_zidx and, in the compiled
+// layout, by the interpolation of C).
 #define OPB_LEVELS(r, sc)                                                                            \
     __shared__ double s_sigma[kMaxLevels];                                                           \
     __shared__ double s_C[kMaxLevels];                                                               \
     const Levels L = load_levels((const double *)(r).C.data[0], (r).C.n0, (r).C.o0, (sc).NZ, s_sigma, s_C); \
     __syncthreads()
 
+// C at z on the rho-point axis (compiled layout: C has nz levels at offset 0)
+template <typename B, typename I = typename B::index_type>
+__device__ __forceinline__ double C_ax(const B &f, const Levels &L, const Axis<I> &zc) {
+    return linear_ax(L.C, zc);
+}
+
 // rk2_w_advection.pyx:97-153 (stage 1 for one particle).  Returns false on a
-// zero grid spacing (the reference raises ZeroDivisionError).
-template <typename B>
-__device__ __forceinline__ bool rk2_stage1(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false) {
-    double h, zeta;
-    if (reuse_hz) {
-        h = s.h_at;
-        zeta = s.zeta_at;
+// zero grid spacing (the reference raises ZeroDivisionError).  `carried`: the
+// state's rho-point axes describe the current position (compiled layout);
+// `reuse_hz`: so do h_at and zeta_at, for this stage's time selection.
+template <typename B, typename S>
+__device__ __forceinline__ bool rk2_stage1(S &s, const B &f, const DScalars &sc, const Levels &L,
+                                           bool reuse_hz = false, bool carried = false) {
+    double h, zeta, u, v, w, dx, dy;
+    if constexpr (B::kFixed) {
+        using I = typename B::index_type;
+        Axes<I> a;
+        if (!carried) rho_axes_h(f, s.yidx, s.xidx, s.ya, s.xa);
+        a.yc = s.ya;
+        a.xc = s.xa;
+        other_axes<false>(f, s.zidx, s.yidx, s.xidx, a);
+        if (reuse_hz) {
+            h = s.h_at;
+            zeta = s.zeta_at;
+        } else {
+            hz_ax(f, a.yc, a.xc, h, zeta);
+        }
+        const double Cv = C_ax(f, L, a.zc);
+        s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
+        velocity_ax<false>(f, a, u, v, w, dx, dy);
     } else {
-        hz_at(f, s.yidx, s.xidx, h, zeta);
+        if (reuse_hz) {
+            h = s.h_at;
+            zeta = s.zeta_at;
+        } else {
+            hz_at(f, s.yidx, s.xidx, h, zeta);
+        }
+        const double Cv = linear(f.C, s.zidx + f.C.o0);
+        s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
+        u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
+        v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
+        dxdy_at(f, s.yidx, s.xidx, dx, dy);
+        // gathered before the check (pure reads): every stencil's loads are in flight together
+        w = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
     }
-    const double Cv = linear(f.C, s.zidx + f.C.o0);
-    s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
-    const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
-    const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
-    double dx, dy;
-    dxdy_at(f, s.yidx, s.xidx, dx, dy);
-    // gathered before the check (pure reads): every stencil's loads are in flight together
-    const double w = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
     if (dx == 0.0 || dy == 0.0) return false;
     s.k1x = u / dx;
     s.k1y = v / dy;
@@ -149,20 +254,29 @@ __device__ __forceinline__ bool rk2_stage1(PState &s, const B &f, const DScalars
 }
 
 // rk2_w_advection.pyx:225-275 (stage 2 for one particle)
-template <typename B>
-__device__ __forceinline__ bool rk2_stage2(PState &s, const B &f, const Levels &L, const DScalars &sc) {
+template <typename B, typename S>
+__device__ __forceinline__ bool rk2_stage2(S &s, const B &f, const Levels &L, const DScalars &sc) {
     const double adt = sc.alpha * sc.dt;
     const double z_int = s.z + adt * s.k1z;
     const double y_int = s.yidx + adt * s.k1y;
     const double x_int = s.xidx + adt * s.k1x;
-    double h, zeta;
-    hz_at(f, y_int, x_int, h, zeta);
-    const double z_idx = compute_zidx_hint(z_int, h, zeta, sc.hc, L, s.zidx);
-    const double u = trilinear(f.u, z_idx + f.u.o0, y_int + f.u.o1, x_int + f.u.o2);
-    const double v = trilinear(f.v, z_idx + f.v.o0, y_int + f.v.o1, x_int + f.v.o2);
-    double dx, dy;
-    dxdy_at(f, y_int, x_int, dx, dy);
-    const double w = trilinear(f.w, z_idx + f.w.o0, y_int + f.w.o1, x_int + f.w.o2);
+    double h, zeta, u, v, w, dx, dy;
+    if constexpr (B::kFixed) {
+        using I = typename B::index_type;
+        Axes<I> a;
+        rho_axes_h(f, y_int, x_int, a.yc, a.xc);
+        hz_ax(f, a.yc, a.xc, h, zeta);
+        const double z_idx = compute_zidx_hint(z_int, h, zeta, sc.hc, L, s.zidx);
+        other_axes<false>(f, z_idx, y_int, x_int, a);
+        velocity_ax<false>(f, a, u, v, w, dx, dy);
+    } else {
+        hz_at(f, y_int, x_int, h, zeta);
+        const double z_idx = compute_zidx_hint(z_int, h, zeta, sc.hc, L, s.zidx);
+        u = trilinear(f.u, z_idx + f.u.o0, y_int + f.u.o1, x_int + f.u.o2);
+        v = trilinear(f.v, z_idx + f.v.o0, y_int + f.v.o1, x_int + f.v.o2);
+        dxdy_at(f, y_int, x_int, dx, dy);
+        w = trilinear(f.w, z_idx + f.w.o0, y_int + f.w.o1, x_int + f.w.o2);
+    }
     if (dx == 0.0 || dy == 0.0) return false;
     s.k2x = u / dx;
     s.k2y = v / dy;
@@ -172,8 +286,8 @@ __device__ __forceinline__ bool rk2_stage2(PState &s, const B &f, const Levels &
 
 // rk2_w_advection.pyx:316-354 (update for one particle); b1 = 1/(2 alpha)
 // weights k1, the reference's own convention (rk2_w_advection.pyx:317-318).
-template <typename B>
-__device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &L, const DScalars &sc) {
+template <typename B, typename S>
+__device__ __forceinline__ void rk2_update(S &s, const B &f, const Levels &L, const DScalars &sc) {
     const double b1 = 1.0 / (2.0 * sc.alpha);
     const double b2 = 1.0 - b1;
     const double b1dt = b1 * sc.dt;
@@ -182,7 +296,7 @@ __device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &
     s.yidx = s.yidx + b1dt * s.k1y + b2dt * s.k2y;
     s.xidx = s.xidx + b1dt * s.k1x + b2dt * s.k2x;
     double h, zeta;
-    hz_at(f, s.yidx, s.xidx, h, zeta);
+    hz_here(s, f, h, zeta);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
     s.h_at = h;
     s.zeta_at = zeta;
@@ -194,7 +308,10 @@ __device__ __forceinline__ void rk2_update(PState &s, const B &f, const Levels &
 // rho(x) - rho_t from the density field in the w slot
 // (ab3_isopycnal_following.pyx:124-132).  False on a zero divisor.
 // finish(g, k): g is the trilinear value of the w-slot field at the particle.
+// kCentered: the w-slot field sits on rho points (density) rather than on w
+// levels.
 struct WVel {
+    static constexpr bool kCentered = false;
     __device__ __forceinline__ bool finish(double g, double &k) const {
         k = g;
         return true;
@@ -202,6 +319,7 @@ struct WVel {
 };
 
 struct IsoVel {
+    static constexpr bool kCentered = true;
     double rho_t, w_max, rho_scale;
     __device__ __forceinline__ bool finish(double rho, double &k) const {
         const double drho = rho - rho_t;
@@ -212,16 +330,33 @@ struct IsoVel {
     }
 };
 
-template <typename B, typename VZ = WVel>
-__device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &sc, bool reuse_hz = false,
-                                         const VZ &vz = VZ{}) {
+template <typename B, typename S, typename VZ = WVel>
+__device__ __forceinline__ bool ab3_step(S &s, const B &f, const DScalars &sc, const Levels &L, bool reuse_hz = false,
+                                         bool carried = false, const VZ &vz = VZ{}) {
     // every gather first (pure reads, so their loads are in flight together), then the divisions and
     // their zero checks in the reference's order: dx, dy, then the vertical velocity's
-    const double u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
-    double dx, dy;
-    dxdy_at(f, s.yidx, s.xidx, dx, dy);
-    const double v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
-    const double wg = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    double u, v, wg, dx, dy, h, zeta, Cv;
+    if constexpr (B::kFixed) {
+        using I = typename B::index_type;
+        Axes<I> a;
+        if (!carried) rho_axes_h(f, s.yidx, s.xidx, s.ya, s.xa);
+        a.yc = s.ya;
+        a.xc = s.xa;
+        other_axes<VZ::kCentered>(f, s.zidx, s.yidx, s.xidx, a);
+        velocity_ax<VZ::kCentered>(f, a, u, v, wg, dx, dy);
+        if (reuse_hz) {
+            h = s.h_at;
+            zeta = s.zeta_at;
+        } else {
+            hz_ax(f, a.yc, a.xc, h, zeta);
+        }
+        Cv = C_ax(f, L, a.zc);
+    } else {
+        u = trilinear(f.u, s.zidx + f.u.o0, s.yidx + f.u.o1, s.xidx + f.u.o2);
+        dxdy_at(f, s.yidx, s.xidx, dx, dy);
+        v = trilinear(f.v, s.zidx + f.v.o0, s.yidx + f.v.o1, s.xidx + f.v.o2);
+        wg = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
+    }
     if (dx == 0.0) return false;
     s.k0x = u / dx;
     if (dy == 0.0) return false;
@@ -241,14 +376,15 @@ __device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &
         s.k2z = -s.k0z + 2.0 * s.k1z;
         s.status = ST_NORMAL;
     }
-    double h, zeta;
-    if (reuse_hz) {
-        h = s.h_at;
-        zeta = s.zeta_at;
-    } else {
-        hz_at(f, s.yidx, s.xidx, h, zeta);
+    if constexpr (!B::kFixed) {
+        if (reuse_hz) {
+            h = s.h_at;
+            zeta = s.zeta_at;
+        } else {
+            hz_at(f, s.yidx, s.xidx, h, zeta);
+        }
+        Cv = linear(f.C, s.zidx + f.C.o0);
     }
-    const double Cv = linear(f.C, s.zidx + f.C.o0);
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double dt = sc.dt;
     s.z = s.z + dt * (23.0 * s.k0z - 16.0 * s.k1z + 5.0 * s.k2z) / 12.0;
@@ -264,10 +400,10 @@ __device__ __forceinline__ bool ab3_step(PState &s, const B &f, const DScalars &
 }
 
 // ab3_w_advection.pyx:214-229 (post step for one particle)
-template <typename B>
-__device__ __forceinline__ void ab3_post(PState &s, const B &f, const Levels &L, const DScalars &sc) {
+template <typename B, typename S>
+__device__ __forceinline__ void ab3_post(S &s, const B &f, const Levels &L, const DScalars &sc) {
     double h, zeta;
-    hz_at(f, s.yidx, s.xidx, h, zeta);
+    hz_here(s, f, h, zeta);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
     s.h_at = h;
     s.zeta_at = zeta;

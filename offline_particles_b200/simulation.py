@@ -152,12 +152,17 @@ class Simulation:
         self._steps_since_sort = 0
 
     def _maybe_sort(self) -> int:
-        """Sort if due; return how many steps may run before the next sort."""
+        """Sort if due; return how many steps may run before the next sort.  A sort falls due
+        ``sort_interval`` steps after the last one and is made at the next snapshot-interval boundary from
+        then on, where a fused launch starts a new snapshot pair anyway: sorting never splits a launch, and
+        the per-interval work (pair builds, sorts) happens at one point."""
         if self._sort_interval <= 0:
             return 1 << 30
-        if self._steps_since_sort is None or self._steps_since_sort >= self._sort_interval:
+        ts = self._timestepper
+        if self._steps_since_sort is None or (self._steps_since_sort >= self._sort_interval
+                                              and ts.at_interval_start):
             self.sort_particles()
-        return self._sort_interval - self._steps_since_sort
+        return ts.steps_to_interval_end(self._sort_interval - self._steps_since_sort)
 
     def step(self) -> None:
         """Advance the simulation by one timestep, then run any scheduled events."""

@@ -15,6 +15,7 @@ from __future__ import annotations
 import abc
 import ctypes
 import dataclasses
+import math
 
 import numpy as np
 import numpy.typing as npt
@@ -138,9 +139,42 @@ class Timestepper(abc.ABC):
 
     def advance_time(self) -> None:
         """timesteppers.py:157-161."""
+        self._last_start_tidx = self._tidx
         self._time += self.dt
         self._tidx = self.get_time_index(self._time)
         self._iteration += 1
+
+    # time index at the start of the last step taken (None before the first)
+    _last_start_tidx = None
+
+    @property
+    def at_interval_start(self) -> bool:
+        """True when the next step starts in a later snapshot interval than the last step did (or no step
+        has run): the point where a fused launch would start a new snapshot pair anyway."""
+        last = self._last_start_tidx
+        return last is None or int(divmod(self._tidx, 1)[0]) != int(divmod(last, 1)[0])
+
+    def steps_to_interval_end(self, at_least: int, limit: int = 1 << 16) -> int:
+        """The fewest steps n >= max(1, at_least) after which the next step starts in a later snapshot
+        interval than step n did: running n steps ends on a snapshot-interval boundary.  Stops early (at
+        least 1) where the time array ends."""
+        t = self._time
+        try:
+            cur = int(divmod(self.get_time_index(t), 1)[0])
+        except (ValueError, IndexError):
+            return max(1, at_least)
+        n = 0
+        while n < limit:
+            t = t + self.dt
+            n += 1
+            try:
+                nxt = int(divmod(self.get_time_index(t), 1)[0])
+            except (ValueError, IndexError):
+                return max(n, 1, min(at_least, limit))
+            if nxt != cur and n >= at_least:
+                return n
+            cur = nxt
+        return max(1, min(at_least, limit))
 
     @property
     @abc.abstractmethod
@@ -194,7 +228,7 @@ class Timestepper(abc.ABC):
         # spanning n intervals would first wait for all n + 2 uploads)
         capacity = min([_lib.MAX_SLOTS] + [min(3, max(2, f.ring_size - 1)) if f.streamed else f.ring_size
                                            for f in td.values()])
-        pairs = use_pairs(launcher, td, len(particles))
+        pairs = use_pairs(launcher, td, len(particles), self.field_roles)
         streamed = any(f.streamed for f in td.values())
         pair_capacity = min([_lib.MAX_SLOTS] + [f.pair_slots for f in td.values()])
         starts: set[int] = set()  # snapshot intervals the launch's stages read (one pair each)
@@ -233,6 +267,7 @@ class Timestepper(abc.ABC):
             return 1
         self._launch_fused(particles, launcher, steps, sorted(needed), td)
         # bookkeeping exactly as advance_time would have left it after each step
+        self._last_start_tidx = steps[-1][0]
         self._time = end_times[-1]
         self._tidx = steps[-1][-1]
         self._iteration += len(steps)
@@ -277,9 +312,38 @@ SNAPSHOT_PAIRS = "auto"
 PAIR_CELLS_PER_PARTICLE = 32
 
 
-def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField], nparticles: int) -> bool:
-    """Snapshot pairs apply to the float64 steppers on the ROMS layout with float32/float64 storage."""
+def roms_geometry(launcher: Launcher, roles: dict[str, str] | None = None) -> bool:
+    """The fields sit on the ROMS Arakawa C grid of the fieldset's nz x ny x nx rho points: u on (nz, ny, nx - 1)
+    at x offset -0.5, v on (nz, ny - 1, nx) at y offset -0.5, w on (nz + 1, ny, nx) at z offset +0.5 (the
+    isopycnal follower's density in the w slot: on rho points), zeta, h, dx, dy on (ny, nx) and C on nz
+    levels, every other offset 0.  The library's compiled-layout kernels (and so the snapshot pairs) need
+    exactly this geometry."""
+    fs = launcher.fieldset
+    roles = roles or {}
+    nz, ny, nx = fs.z_size, fs.y_size, fs.x_size
+    w_rho = roles.get("w", "w") != "w"
+    want = {"u": ((nz, ny, nx - 1), (0.0, 0.0, -0.5)), "v": ((nz, ny - 1, nx), (0.0, -0.5, 0.0)),
+            "w": ((nz, ny, nx), (0.0, 0.0, 0.0)) if w_rho else ((nz + 1, ny, nx), (0.5, 0.0, 0.0)),
+            "C": ((nz,), (0.0,)), **{n: ((ny, nx), (0.0, 0.0)) for n in ("zeta", "h", "dx", "dy")}}
+    for name, (shape, offsets) in want.items():
+        src = roles.get(name, name)
+        if src not in fs:
+            return False
+        f = fs[src]
+        got = tuple(f.active_offsets)
+        if (tuple(f.spatial_shape) != shape or got != offsets
+                or any(o == 0.0 and math.copysign(1.0, o) < 0 for o in got)):
+            return False
+    return True
+
+
+def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField], nparticles: int,
+              roles: dict[str, str] | None = None) -> bool:
+    """Snapshot pairs apply to the float64 steppers on the ROMS layout and geometry with float32/float64
+    storage."""
     if SNAPSHOT_PAIRS == "never" or launcher.arithmetic != "float64" or set(td) != {"u", "v", "w", "zeta"}:
+        return False
+    if not roms_geometry(launcher, roles):
         return False
     if not all(f.storage in ("float32", "float64") for f in td.values()):
         return False
@@ -396,7 +460,7 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
     """opb_roms_fields over the snapshots ``needed`` plus the per-stage opb_time table."""
     rf, dtype = window_fields(launcher, needed, td, roles)
     entries = [t for step in steps for t in step]
-    if use_pairs(launcher, td, nparticles):
+    if use_pairs(launcher, td, nparticles, roles):
         pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td, pair_layout(launcher, td, roles))
         prev_next = lambda It: (pslot[It], pslot[It])  # noqa: E731
     else:
@@ -471,12 +535,18 @@ def _entry(name: str, launcher: Launcher) -> str:
     return name + ("_fp32" if launcher.arithmetic == "float32" else "")
 
 
-def _table_arg(table, device):
+def _table_arg(table, device, rf=None):
     """The step-table argument of a fused launch, and what must stay alive until the call returns: the
     host table itself while it fits the launch's parameters (no copy, so the launch does not queue
-    behind the snapshot uploads already issued), else a device copy."""
+    behind the snapshot uploads already issued), else a device copy.  The library checks a host table's
+    snapshot slots against the fields ``rf``; a device copy it reads unchecked, so its slots are checked
+    here before the copy."""
     if len(table) <= _lib.INLINE_TABLE:
         return ctypes.addressof(table), table
+    if rf is not None:
+        nslots = min(getattr(rf, n).nslots for n in _abi.ROMS_FIELDS if not getattr(rf, n).is_static)
+        if any(not (0 <= e.prev < nslots and 0 <= e.next < nslots) for e in table):
+            raise ValueError(f"step table selects a snapshot slot outside the fields' {nslots} slots")
     raw = torch.frombuffer(bytearray(bytes(table)), dtype=torch.uint8).pin_memory()
     dev = raw.to(device, non_blocking=True)
     return dev.data_ptr(), dev
@@ -585,7 +655,7 @@ class RK2Timestepper(Timestepper):
             "_dt": self._normalised_dt, "_RK2_alpha": self._alpha,
             **{n: launcher.scalar(n, self._tidx) for n in ("zidx_min", "zidx_max", "yidx_min", "yidx_max",
                                                            "xidx_min", "xidx_max")}})
-        table_ptr, _keep = _table_arg(table, particles.device)
+        table_ptr, _keep = _table_arg(table, particles.device, rf)
         _notify("before", len(steps))
         _lib.call(_entry("opb_rk2_w_advection_steps", launcher), ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
                   ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None),
@@ -666,7 +736,7 @@ class ABTimestepper(Timestepper):
         if iso and launcher.arithmetic != "float64":
             raise ValueError("the isopycnal follower has float64 steppers only")
         entry = "opb_ab3_isopycnal_following_steps" if iso else _entry("opb_ab3_w_advection_steps", launcher)
-        table_ptr, _keep = _table_arg(table, particles.device)
+        table_ptr, _keep = _table_arg(table, particles.device, rf)
         _notify("before", len(steps))
         _lib.call(entry, ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
                   ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None),

@@ -72,7 +72,8 @@ def _oracle(g, fields, scheme, dt, steps, z, y, x):
 @pytest.mark.parametrize("scheme,steps", [("ab3", 70), ("rk2", 40)])
 def test_headline_size_matches_oracle(headline, scheme, steps):
     """AB3 (the benchmark's scheme) and RK2 at dt = 120 s across a snapshot boundary (30 steps per
-    interval), Morton re-sorts every 32 steps, the library's default layout decisions."""
+    interval), Morton re-sorts due every 16 steps (made at the interval boundaries), the library's default
+    layout decisions."""
     from b200_runner import build_sim
 
     from offline_particles_b200 import fields as fmod
@@ -85,7 +86,7 @@ def test_headline_size_matches_oracle(headline, scheme, steps):
     fmod.pair_observers.append(lambda: builds.append(1))
     pmod.sort_observers.append(lambda: sorts.append(1))
     try:
-        sim = build_sim(fields, hc=g.hc, nz=g.spec.nz, scheme=scheme, dt=120.0, z=z, y=y, x=x, sort_interval=32)
+        sim = build_sim(fields, hc=g.hc, nz=g.spec.nz, scheme=scheme, dt=120.0, z=z, y=y, x=x, sort_interval=16)
         assert timesteppers.use_pairs(sim.launcher, timesteppers._time_dependent_fields(sim.launcher), N_FULL)
         assert timesteppers.pair_layout(sim.launcher, timesteppers._time_dependent_fields(sim.launcher)).bundles
         sim.run(steps)
