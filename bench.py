@@ -96,10 +96,15 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson request rate (1/s)")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="arrival window (s)")
     ap.add_argument("--serve-count", type=str, default="100,2e6", help="log-uniform particles per request")
-    ap.add_argument("--serve-count-scale", type=float, default=0.15)
+    ap.add_argument("--serve-count-scale", type=float, default=1.0)
     ap.add_argument("--serve-days", type=str, default="1,30", help="request duration range (days)")
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget for particle state")
     ap.add_argument("--serve-plain", type=int, default=64, help="requests of the trace the plain arm runs")
+    ap.add_argument("--serve-plain-budget-s", type=float, default=30.0, help="seconds of plain-arm service")
+    ap.add_argument("--serve-drain", action="store_true",
+                    help="serve every request to its end (only a stream the GPU keeps up with drains)")
+    ap.add_argument("--no-batched", action="store_true", help="default run: skip the config-4 batched block")
+    ap.add_argument("--no-served", action="store_true", help="default run: skip the config-5 served block")
     return ap.parse_args()
 
 
@@ -124,12 +129,17 @@ def workload_config(a, nt: int, pair_bytes: float | None = None) -> dict:
 
 
 # --------------------------------------------------------------- inputs
-def make_inputs(a, rank: int):
+def make_grid(a, nt: int):
     from offline_particles_b200.synth import GridSpec, SyntheticROMS
 
-    span = (a.warmup + a.steps) * a.dt
+    return SyntheticROMS(GridSpec(nx=a.nx, ny=a.ny, nz=a.nz, nt=nt, seed=2, dtype="float32"))
+
+
+def make_inputs(a, rank: int, steps: int | None = None):
+    """Host snapshots for ``steps`` steps from t = 0 (default: warm-up + timed steps), and the release."""
+    span = (a.warmup + a.steps if steps is None else steps) * a.dt
     nt = int(math.floor(span / 3600.0)) + 3
-    grid = SyntheticROMS(GridSpec(nx=a.nx, ny=a.ny, nz=a.nz, nt=nt, seed=2, dtype="float32"))
+    grid = make_grid(a, nt)
     snaps = {name: np.stack([grid.snapshot(k)[name] for k in range(nt)]) for name in TD}
     z, y, x = grid.release(a.particles, seed=1000 + rank)
     return grid, snaps, (z, y, x), nt
@@ -153,6 +163,33 @@ def build_sim(grid, sources: dict, n: int, a, *, ring_size: int = 4):
     fs = opb.Fieldset(nt, a.nz, a.ny, a.nx, constants={"hc": grid.hc, "NZ": a.nz}, **kw)
     ts = opb.roms.ab3_w_advection_timestepper(grid.time_array[:nt], np.float64(a.dt))
     return opb.SimulationBuilder(ts, fs).build_simulation(n), fs
+
+
+def window_plan(a) -> dict:
+    """Where the timed K steps sit in the run.
+
+    The per-interval work (a new snapshot pair for u, v, w and the zeta bundle
+    at every snapshot-interval boundary; a Morton re-sort at the first boundary
+    at least ``sort_interval`` steps after the last) belongs in the timed
+    region.  With P steps per snapshot interval, re-sorts fall every R =
+    ceil(sort_interval / P) * P steps.  The K timed steps straddle the first
+    re-sort boundary B >= W + ceil(K / 2): steps [B - K // 2, B - K // 2 + K),
+    after at least W untimed warm-up steps.  ``amortised`` times the R steps
+    [B, B + R) again on a second simulation: whole intervals with their pair
+    builds and one re-sort, the steady-state rate.
+    """
+    from offline_particles_b200.simulation import DEFAULT_SORT_INTERVAL
+
+    P = 3600.0 / a.dt
+    if abs(P - round(P)) > 1e-9 or P < 1:
+        return {"start": a.warmup, "boundary": None, "resort_every": None, "steps_per_interval": None,
+                "last_step": a.warmup + a.steps}
+    P = int(round(P))
+    R = -(-DEFAULT_SORT_INTERVAL // P) * P
+    B = R * max(1, -(-(a.warmup + (a.steps + 1) // 2) // R))
+    start = B - a.steps // 2
+    return {"start": start, "boundary": B, "resort_every": R, "steps_per_interval": P,
+            "last_step": max(start + a.steps, B + R)}
 
 
 # --------------------------------------------------------------- clocks
@@ -240,29 +277,31 @@ class LaunchTimer:
         return [a.elapsed_time(b) for a, b in self.pairs]
 
 
-def dist_max(value: float, world: int) -> float:
-    from offline_particles_b200.sharding import max_over_ranks
-
-    return max_over_ranks(value) if world > 1 else value
-
-
-def barrier(world: int) -> None:
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-
-
 # --------------------------------------------------------------- CPU path
 def cpu_run(grid, snaps, zyx, a, budget_s: float) -> dict:
-    """The oracle (the reference's algorithm on the CPU: numpy blend + C/OpenMP loops) on this workload."""
-    from oracle import oracle as O
+    """The reference's own code on this host's cores when its compiled form is in oracle/_ref (its Cython/
+    OpenMP kernels and numpy time blend, through its public API), else the oracle (the same algorithm
+    restated: numpy blend + C/OpenMP loops), on this workload."""
+    from oracle import ref_import
 
     fields = dict(snaps)
     fields.update(h=grid.h, dx=grid.dx, dy=grid.dy, C=grid.C)
+    n = zyx[0].size
+    if ref_import.compiled_available():
+        from oracle import ref_run
+
+        r = ref_run.time_ab3(grid.time_array, fields, grid.hc, a.nz, a.dt, zyx, budget_s=budget_s)
+        return {"value": r["particle_steps_per_s"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                "physical_cores": r["physical_cores"], "logical_cpus": r["logical_cpus"],
+                "sample": f"{r['steps']} AB3 steps of all {n:,} particles on the same grid after {r['warmup']} "
+                          f"warm-up step ({r['seconds']:.1f} s): the reference's Simulation.step() with its ROMS "
+                          f"preset, Cython/OpenMP kernels and numpy time blend, {r['threads']} OpenMP threads on "
+                          f"{r['physical_cores']} physical cores"}
+    from oracle import oracle as O
+    from oracle.ref_run import openmp_threads, physical_cores
+
     orc = O.OracleROMS(grid.time_array[: snaps["u"].shape[0]], fields, hc=grid.hc, scheme="ab3",
                        dt=np.float64(a.dt))
-    n = zyx[0].size
     p = O.new_particles(n, "ab3")
     p["zidx"][:], p["yidx"][:], p["xidx"][:] = zyx
     p["status"][:] = O.MULTISTEP_1
@@ -274,18 +313,19 @@ def cpu_run(grid, snaps, zyx, a, budget_s: float) -> dict:
     for _ in range(steps):
         orc.step(p)
     el = time.perf_counter() - t0
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    threads = openmp_threads()
     return {"value": n * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "physical_cores": physical_cores(), "logical_cpus": os.cpu_count(),
             "sample": f"{steps} AB3 steps of all {n:,} particles on the same grid after 1 warm-up step "
-                      f"({el:.1f} s); numpy time blend + C/OpenMP kernels, {threads} threads of "
-                      f"{os.cpu_count()} host CPUs"}
+                      f"({el:.1f} s): the oracle restatement (numpy time blend + C/OpenMP kernels), {threads} "
+                      f"OpenMP threads; the compiled reference was not in oracle/_ref"}
 
 
 def reference_arm(a) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    grid, snaps, zyx, nt = make_inputs(a, 0)
+    grid, snaps, zyx, nt = make_inputs(a, 0, steps=a.warmup + a.steps + 1)
     budget = max(10.0, min(150.0, 3.0 * a.cpu_budget_s))
     cb = cpu_run(grid, snaps, zyx, a, budget)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus,
@@ -297,80 +337,146 @@ def reference_arm(a) -> None:
 
 
 # --------------------------------------------------------------- B200 path
+class Counters:
+    """Observers counting the per-interval work inside a region: Morton re-sorts and snapshot-pair builds."""
+
+    def __init__(self) -> None:
+        from offline_particles_b200 import fields as fmod
+        from offline_particles_b200 import particles as pmod
+
+        self.sorts, self.builds = [], []
+        self._mods = (pmod.sort_observers, fmod.pair_observers)
+
+    def __enter__(self):
+        self._s = lambda: self.sorts.append(1)
+        self._b = lambda: self.builds.append(1)
+        self._mods[0].append(self._s)
+        self._mods[1].append(self._b)
+        return self
+
+    def __exit__(self, *exc):
+        self._mods[0].remove(self._s)
+        self._mods[1].remove(self._b)
+
+
+def resident_sim(grid, dsrc, zyx, a, upto: int):
+    """A simulation on resident snapshots, advanced untimed to step ``upto``."""
+    import offline_particles_b200 as opb
+
+    sim, _ = build_sim(grid, dsrc, a.particles, a)
+    sim.set_indices(*zyx)
+    sim.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+    if upto:
+        sim.run(upto)
+    sim.synchronize()
+    return sim
+
+
+def timed_run(ranks, sim, nsteps: int):
+    """``sim.run(nsteps)`` between barriers (slowest rank's CUDA-event time), with CUDA events around every
+    fused launch and counts of the re-sorts and pair builds it made."""
+    import torch
+
+    from offline_particles_b200 import timesteppers
+
+    timer = LaunchTimer()
+    timesteppers.launch_observers.append(timer)
+    first = {}
+
+    def work():
+        first["t0"] = torch.cuda.Event(enable_timing=True)
+        first["t0"].record()
+        sim.run(nsteps)
+
+    try:
+        with Counters() as cnt:
+            ms = ranks.timed_ms(work)
+    finally:
+        timesteppers.launch_observers.remove(timer)
+    sim.synchronize()
+    # device time before the first launch: host work inside the region (planning, table building, the sort
+    # and pair builds it enqueued first)
+    lead_ms = first["t0"].elapsed_time(timer.pairs[0][0]) if timer.pairs else None
+    return ms, timer, cnt, lead_ms
+
+
+def kernel_counters() -> dict | None:
+    """ncu counters of the headline kernel (profiles/k_ab3_steps_config2_counters.json) when they were taken
+    on the current kernel sources: the file records the SHA-256 of the sources it was measured on."""
+    import hashlib
+
+    path = ROOT / "profiles" / "k_ab3_steps_config2_counters.json"
+    try:
+        rec = json.loads(path.read_text())
+    except (OSError, ValueError):
+        return None
+    h = hashlib.sha256()
+    for rel in rec.get("sources", []):
+        try:
+            h.update((ROOT / rel).read_bytes())
+        except OSError:
+            return None
+    if h.hexdigest() != rec.get("sources_sha256"):
+        return {"stale": True, "path": str(path.relative_to(ROOT))}
+    return rec
+
+
 def b200_arm(a) -> None:
     import torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import offline_particles_b200 as opb
-    from offline_particles_b200 import fields as fmod
-    from offline_particles_b200 import particles as pmod
-    from offline_particles_b200 import timesteppers
+    from offline_particles_b200.sharding import Ranks
 
-    grid, snaps, zyx, nt = make_inputs(a, rank)
-    n = a.particles
-    fb = field_bytes(grid, snaps)
+    ranks = Ranks()
+    rank, world, local = ranks.rank, ranks.world, ranks.local
+    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    n = a.particles
+    plan = window_plan(a)
+    nt_dev = int(math.floor(plan["last_step"] * a.dt / 3600.0)) + 3
+    grid = make_grid(a, nt_dev)
+    zyx = grid.release(n, seed=1000 + rank)
 
-    # ---- device-resident: fused multi-step launches ----------------------------------
-    dsrc = {k: torch.from_numpy(v).to(dev) for k, v in snaps.items()}
-    sim, _ = build_sim(grid, dsrc, n, a)
-    sim.set_indices(*zyx)
-    sim.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
-    sim.run(a.warmup)
-    sim.synchronize()
-    timer = LaunchTimer()
-    sorts = []
-    builds = []
-    timesteppers.launch_observers.append(timer)
-    pmod.sort_observers.append(lambda: sorts.append(1))
-    fmod.pair_observers.append(lambda: builds.append(1))
-    barrier(world)
+    # ---- device-resident: fused multi-step launches -------------------------------------
+    dsrc = grid.device_snapshots(nt_dev)
+    torch.cuda.synchronize()
+    sim = resident_sim(grid, dsrc, zyx, a, plan["start"])
     with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        sim.run(a.steps)
-        e.record()
-        torch.cuda.synchronize()
-    timesteppers.launch_observers.remove(timer)
-    pmod.sort_observers.clear()
-    fmod.pair_observers.clear()
-    sim.synchronize()
-    run_ms = dist_max(s.elapsed_time(e), world)
+        run_ms, timer, cnt, lead_ms = timed_run(ranks, sim, a.steps)
     launch_ms = timer.durations_ms()
     launch_steps = timer.steps
     active = int((sim.particles.tensor("status") & 0x80).eq(0).sum().item())
+    del sim
 
-    # ---- plain path: Simulation.step(), one fused launch per step --------------------
-    sim2, _ = build_sim(grid, dsrc, n, a)
-    sim2.set_indices(*zyx)
-    sim2.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
-    for _ in range(a.warmup):
-        sim2.step()
-    sim2.synchronize()
-    barrier(world)
-    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s2.record()
-    for _ in range(a.steps):
-        sim2.step()
-    e2.record()
-    torch.cuda.synchronize()
-    step_ms = dist_max(s2.elapsed_time(e2), world)
-    del sim2
+    # ---- amortised: whole snapshot intervals with their pair builds and one re-sort ------------
+    amort = None
+    if plan["boundary"] is not None:
+        sim = resident_sim(grid, dsrc, zyx, a, plan["boundary"])
+        am_ms, _, am_cnt, _ = timed_run(ranks, sim, plan["resort_every"])
+        amort = {"value": world * n * plan["resort_every"] / (am_ms * 1e-3), "unit": UNIT,
+                 "steps": plan["resort_every"], "first_step": plan["boundary"],
+                 "ms_per_step": am_ms / plan["resort_every"], "sorts": len(am_cnt.sorts),
+                 "pair_builds": len(am_cnt.builds)}
+        del sim
+
+    # ---- plain path: Simulation.step(), one fused launch per step, same window --------------
+    sim = resident_sim(grid, dsrc, zyx, a, plan["start"])
+
+    def steps_one_by_one():
+        for _ in range(a.steps):
+            sim.step()
+
+    step_ms = ranks.timed_ms(steps_one_by_one)
+    sim.synchronize()
     del sim, dsrc
     torch.cuda.empty_cache()
 
     # ---- end to end from host buffers --------------------------------------------------
-    psrc = {k: torch.from_numpy(v).pin_memory() for k, v in snaps.items()}
+    nt_host = int(math.floor(a.steps * a.dt / 3600.0)) + 3
+    hsrc = grid.device_snapshots(nt_host)
+    psrc = {k: v.cpu().pin_memory() for k, v in hsrc.items()}
+    del hsrc
+    torch.cuda.empty_cache()
     hz, hy, hx = (torch.from_numpy(v).pin_memory() for v in zyx)
     outs = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in ("zidx", "yidx", "xidx")}
     outs["status"] = torch.empty(n, dtype=torch.uint8, pin_memory=True)
@@ -386,99 +492,141 @@ def b200_arm(a) -> None:
     torch.cuda.synchronize()
     h2d_gbs = 3 * probe.numel() * probe.element_size() / (hs.elapsed_time(he) * 1e-3) / 1e9
     del probe
+    gsnap = {k: v.numpy() for k, v in psrc.items()}
+    fb = field_bytes(grid, gsnap)
+    grid_h = grid
     # untimed warm-up of the same path (allocator, ring, copy stream)
-    simw, _ = build_sim(grid, psrc, n, a, ring_size=a.ring_size)
+    simw, _ = build_sim(grid_h, psrc, n, a, ring_size=a.ring_size)
     simw.set_indices(hz, hy, hx)
     simw.run(a.warmup)
     simw.synchronize()
     del simw
     gc.collect()  # the warm-up simulation's teardown (reference cycles) stays out of the timed region
-    sim3, fs3 = build_sim(grid, psrc, n, a, ring_size=a.ring_size)
-    barrier(world)
-    torch.cuda.synchronize()
-    s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sim3, fs3 = build_sim(grid_h, psrc, n, a, ring_size=a.ring_size)
+    host = {}
+
+    def e2e():
+        w0 = time.perf_counter()
+        sim3.set_indices(hz, hy, hx)
+        sim3.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+        w1 = time.perf_counter()
+        sim3.run(a.steps)
+        w2 = time.perf_counter()
+        P = sim3.device_particles
+        for k in outs:
+            outs[k].copy_(P.original(k), non_blocking=True)
+        w3 = time.perf_counter()
+        host.update(set_indices=(w1 - w0) * 1e3, run=(w2 - w1) * 1e3, collect=(w3 - w2) * 1e3)
+
     m0 = torch.cuda.memory_stats(dev)
-    w0 = time.perf_counter()
-    s3.record()
-    sim3.set_indices(hz, hy, hx)
-    sim3.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
-    w1 = time.perf_counter()
-    sim3.run(a.steps)
-    w2 = time.perf_counter()
-    P = sim3.device_particles
-    for k in outs:
-        outs[k].copy_(P.original(k), non_blocking=True)
-    e3.record()
-    w3 = time.perf_counter()
-    torch.cuda.synchronize()
-    wall_e2e = time.perf_counter() - w0
-    # where the host spent the end-to-end region (the calls are asynchronous; a large share in one call
-    # means the host blocked there)
-    e2e_host_ms = {"set_indices": (w1 - w0) * 1e3, "run": (w2 - w1) * 1e3, "collect": (w3 - w2) * 1e3,
-                   "wait": (wall_e2e - (w3 - w0)) * 1e3}
+    wall0 = time.perf_counter()
+    e2e_dev_ms = ranks.timed_ms(e2e)
+    wall_e2e = time.perf_counter() - wall0
     m1 = torch.cuda.memory_stats(dev)
     # device allocations inside the region (cudaMalloc calls, and retries that freed cached blocks first)
     e2e_alloc = {"cuda_mallocs": m1.get("segment.all.allocated", 0) - m0.get("segment.all.allocated", 0),
                  "retries": m1.get("num_alloc_retries", 0) - m0.get("num_alloc_retries", 0)}
     sim3.synchronize()
-    e2e_ms = dist_max(max(s3.elapsed_time(e3), wall_e2e * 1e3), world)
+    e2e_ms = ranks.max(max(e2e_dev_ms, wall_e2e * 1e3))
     h2d = 3 * 8 * n + sum(fs3[k].h2d_bytes for k in TD)
     d2h = sum(t.numel() * t.element_size() for t in outs.values())
+    del sim3, fs3
 
     # ---- CPU baseline (rank 0, one GPU) ------------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_run(grid, snaps, zyx, a, a.cpu_budget_s)
-
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+        cpu = cpu_run(grid_h, gsnap, zyx, a, a.cpu_budget_s)
+    ranks.close()
     if rank != 0:
         return
+    del psrc, gsnap
+    gc.collect()
+    torch.cuda.empty_cache()
+
+    # ---- the batched and served forms (one GPU): config 4 and config 5 ---------------------
+    batched = served = None
+    if world == 1 and not a.no_batched:
+        b = batched_measure(a)
+        batched = {"value": b["value"], "unit": UNIT, "vs_plain": b["vs_plain"],
+                   "plain_value": b["plain"]["value"] if b["plain"] else None,
+                   "identical_to_plain": b["identical_to_plain"], "roofline": b["batched"]["roofline"],
+                   "seconds": b["batched"]["seconds"], "launch_time_share": b["batched"]["launch_time_share"],
+                   "shape": {k: b["batched"][k] for k in ("block", "warps_per_sm", "sort_interval_intervals",
+                                                          "buckets", "split_schemes")},
+                   "autotuned": b["batched"]["autotune"] is not None, "errors": b["batched"]["errors"],
+                   "workload": b["workload"], "clocks": b["batched"]["clocks"]}
+        gc.collect()
+        torch.cuda.empty_cache()
+    if world == 1 and not a.no_served:
+        served = serving_measure(a, a.serve_seconds, a.serve_drain)
+        gc.collect()
+        torch.cuda.empty_cache()
 
     # ---- roofline of the fused kernel -------------------------------------------------
     peak = measured_peak_gbs()
-    # physical DRAM bytes per fused step of this kernel on this workload, from one ncu capture of the
-    # full-size timed launches (profiles/k_ab3_steps_pairs_config2.md: 3.451 GB and 3.399 GB per 60-step
-    # launch, snapshot pairs); traffic per launch scales with the steps it runs
-    traffic_per_step = 59.0e6 if (a.nx, a.ny, a.nz, a.particles) == (1024, 768, 50, 4_194_304) else None
     state_bytes = 2 * (1 + 3 * 8 + 6 * 8)  # status + 3 indices + 6 AB3 history values, float64, read + written
     b_step = n * state_bytes + fb["pair"] + fb["static"]
     tot_steps = sum(launch_steps)
-    avg_launch_ms = sum(launch_ms) / max(1, len(launch_ms))
+    kernel_ms = sum(launch_ms)
+    avg_launch_ms = kernel_ms / max(1, len(launch_ms))
     avg_launch_steps = tot_steps / max(1, len(launch_steps))
-    achieved = b_step * avg_launch_steps / (avg_launch_ms * 1e-3) / 1e9
+    achieved = b_step * tot_steps / (kernel_ms * 1e-3) / 1e9
+    ctr = kernel_counters()
+    fresh = ctr is not None and not ctr.get("stale")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": ctr["dram_bytes_per_step"] * avg_launch_steps if fresh else None,
+            "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, {ctr['traffic_case']}"
+                               if fresh else "no ncu capture of the current kernel sources"),
+            "peak_source": peak_source(), "algorithmic_bytes_per_step": b_step,
+            "bytes_per_particle_step": b_step / n, "steps_per_launch": avg_launch_steps,
+            "launch_ms": avg_launch_ms, "kernel": "k_ab3_steps<float, int, ROMS layout, pairs, 2-D bundles>"}
+    if fresh:
+        # the bound that applies after sorting: instruction issue (4 schedulers per SM, one warp
+        # instruction per cycle each, at the SM clock sampled during the region)
+        mhz = clocks.summary().get("sm_mhz") or 1965
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        issue_peak = sms * 4 * mhz * 1e6
+        ps_rate = n * tot_steps / (kernel_ms * 1e-3)
+        roof["issue"] = {"warp_inst_per_particle_step": ctr["warp_inst_per_particle_step"],
+                         "achieved_warp_inst_per_s": ctr["warp_inst_per_particle_step"] * ps_rate,
+                         "peak_warp_inst_per_s": issue_peak,
+                         "frac": ctr["warp_inst_per_particle_step"] * ps_rate / issue_peak,
+                         "ncu_issue_active": ctr.get("issue_active"), "source": ctr["inst_case"]}
+    elif ctr is not None:
+        roof["counters"] = "stale: recorded on other kernel sources"
 
     total = world * n * a.steps
     line = {
         "metric": METRIC, "value": total / (run_ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": run_ms / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ROMS-like grid; no ROMS output offline)",
-        "config": workload_config(a, nt),
+        "config": workload_config(a, nt_dev),
+        "window": {"first_step": plan["start"], "untimed_steps_before": plan["start"],
+                   "straddles_resort_boundary": plan["boundary"],
+                   "note": "the K timed steps straddle a snapshot-interval boundary at which a new snapshot pair "
+                           "is built and particles are re-sorted"},
+        "amortised": amort,
         "plain_step": {"value": total / (step_ms * 1e-3), "unit": UNIT, "ms_per_step": step_ms / a.steps,
                        "path": "Simulation.step(): one fused launch (validation + AB3 + post) per step"},
         "e2e": {"value": total / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d / a.steps),
                 "d2h_bytes_per_step": int(d2h / a.steps),
                 "path": "Simulation.set_indices from pinned host + run(K) streaming every snapshot from pinned "
                         "host memory + D2H of zidx/yidx/xidx/status",
-                "h2d_gbs_measured": h2d_gbs, "device_ms": s3.elapsed_time(e3), "wall_ms": wall_e2e * 1e3,
-                "host_ms": e2e_host_ms, "allocator": e2e_alloc,
+                "h2d_gbs_measured": h2d_gbs, "device_ms": e2e_dev_ms, "wall_ms": wall_e2e * 1e3,
+                "host_ms": host, "allocator": e2e_alloc,
                 "h2d_bound_value": total / ((h2d + d2h) / (h2d_gbs * 1e9)) if h2d_gbs else None},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic_per_step * avg_launch_steps if traffic_per_step else None,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the full-size launches, "
-                                       "per launch", "peak_source": peak_source(),
-                     "algorithmic_bytes_per_step": b_step, "bytes_per_particle_step": b_step / n,
-                     "steps_per_launch": avg_launch_steps, "launch_ms": avg_launch_ms,
-                     "kernel": "k_ab3_steps<float>"},
-        "gpu_launches": len(launch_ms) + 2 * len(sorts) + len(builds),
-        "sorts_in_timed_region": len(sorts),
-        "pair_builds_in_timed_region": len(builds),
+        "roofline": roof,
+        "gpu_launches": len(launch_ms) + 2 * len(cnt.sorts) + len(cnt.builds),
+        "sorts_in_timed_region": len(cnt.sorts),
+        "pair_builds_in_timed_region": len(cnt.builds),
+        "kernel_ms_in_timed_region": kernel_ms,
+        "lead_ms_before_first_launch": lead_ms,
         "snapshot_layout": a.layout, "bundles_2d": not a.no_bundles,
         "active_particles_end": active,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
+        "batched": batched,
+        "served": served,
     }
     print(json.dumps(line), flush=True)
 
@@ -621,7 +769,7 @@ def batched_workload(a, grid):
             for e in range(E)]
 
 
-def batched_study(a) -> None:
+def batched_measure(a) -> dict:
     """Config-4 batched releases: one ReleaseBatch vs the plain path one release at a time.
 
     Snapshots are generated on the device and stay resident; the plain arm
@@ -761,7 +909,9 @@ def batched_study(a) -> None:
         identical = all(np.array_equal(br[k].view(np.uint8), pr[k].view(np.uint8))
                         for br, pr in zip(batch_res, plain_res) for k in br)
     counts = [s["n"] for s in specs]
-    line = {"study": "batched", "metric": METRIC, "unit": UNIT,
+    del snaps
+    torch.cuda.empty_cache()
+    return {"metric": METRIC, "unit": UNIT,
             "value": batched["value"], "vs_plain": (batched["value"] / plain["value"]) if plain else None,
             "batched": batched, "plain": plain, "identical_to_plain": identical,
             "workload": {"grid": [nz, ny, nx], "field_dtype": "float32", "snapshots": nt,
@@ -773,7 +923,10 @@ def batched_study(a) -> None:
             "snapshot_generation_s": gen_s,
             "data": "synthetic; snapshots generated on the device and resident (plain reads them in place, "
                     "batched copies them into a 4-slot ring)"}
-    print(json.dumps(line), flush=True)
+
+
+def batched_study(a) -> None:
+    print(json.dumps({"study": "batched", **batched_measure(a)}), flush=True)
 
 
 def serving_trace(a, grid):
@@ -800,28 +953,40 @@ def serving_trace(a, grid):
     return reqs
 
 
-def serving_study(a) -> None:
+def serving_measure(a, window_s: float, drain: bool) -> dict:
     """Config-5 serving: a Poisson request stream served with continuous batching (ReleaseServer), and
-    the plain path serving a prefix of the same trace one request at a time.
+    the plain path serving a sample of the same trace one request at a time.
 
     Snapshots of the config-4 grid are generated on the device when a ring
     asks for them (model time runs as long as the service does).  Served arm:
-    requests are submitted at their arrival times (wall clock) and admitted at
-    interval boundaries by the HBM budget; latency = arrival to result in host
-    memory.  Plain arm: the first --serve-plain requests, each alone through
-    Simulation from the start time the server gave it (FIFO from the same
-    arrival times; its results are compared bit for bit with the served ones).
+    requests are submitted at their arrival times (wall clock) over
+    ``window_s`` seconds and admitted at interval boundaries by the HBM budget;
+    latency = arrival to result in host memory.  With ``drain`` the server
+    then runs until every request is done; without, it stops at the end of
+    the window (a stream that offers more than the GPU serves never drains):
+    requests still queued or running are counted, and their age at the end is
+    a lower bound of their latency.  Served throughput counts every
+    particle-step advanced in the run, finished requests or not.  Plain arm:
+    the first --serve-plain finished requests, each alone through Simulation
+    from the start time the server gave it (FIFO from the same arrival times;
+    its results are compared bit for bit with the served ones), within
+    --serve-plain-budget-s seconds.
     """
     import torch
 
     import offline_particles_b200 as opb
-    from offline_particles_b200.serving import ReleaseServer
+    from offline_particles_b200.serving import ReleaseRequest, ReleaseServer
     from offline_particles_b200.synth import GridSpec, SyntheticROMS
 
     torch.cuda.set_device(0)
     nz, ny, nx = (int(v) for v in a.batch_grid.split(","))
     grid = SyntheticROMS(GridSpec(nx=nx, ny=ny, nz=nz, nt=4, seed=4, dtype="float32"))
-    reqs = serving_trace(a, grid)
+    a_window = a.serve_seconds
+    a.serve_seconds = window_s
+    try:
+        reqs = serving_trace(a, grid)
+    finally:
+        a.serve_seconds = a_window
     nt = 400_000  # hourly snapshot indices available to the device source (45 model years)
     t_arr = np.arange(nt, dtype=np.float64) * 3600.0
     statics = {n: opb.StaticField.from_numpy(arr, *STAGGERS[n])
@@ -835,27 +1000,33 @@ def serving_study(a) -> None:
     budget = int(a.serve_budget_gb * 1e9)
     server = ReleaseServer(fieldset(), t_arr, hbm_budget=budget, max_releases=1024, block=256, warps_per_sm=16,
                            buckets=256, sort_interval=4)
-    offered = sum(len(r) * round(r.duration / r.dt) for r in reqs) / a.serve_seconds
+    offered = sum(len(r) * round(r.duration / r.dt) for r in reqs) / window_s
     # warm the kernels (module load, occupancy, graph capture) on a throwaway server
     warm = ReleaseServer(fieldset(), t_arr, hbm_budget=64 * server.per_particle, max_releases=4)
     wz, wy, wx = grid.release(32, seed=1)
-    from offline_particles_b200.serving import ReleaseRequest
     for sch in ("rk2", "ab3"):
         warm.submit(ReleaseRequest(wz, wy, wx, sch, 300.0, 7200.0))
     warm.drain()
     del warm
     torch.cuda.synchronize()
 
+    timeline = []
     with ClockSampler(0) as clocks:
         t0 = time.perf_counter()
         i, n = 0, len(reqs)
         max_running = 0
+        next_sample = 0.0
         while True:
             now = time.perf_counter() - t0
+            if now >= next_sample:
+                timeline.append((round(now, 2), len(server.queue), len(server.running), len(server.done)))
+                next_sample += 1.0
             while i < n and reqs[i].offset <= now:
                 reqs[i].arrival = t0 + reqs[i].offset
                 server.submit(reqs[i])
                 i += 1
+            if not drain and now >= window_s:
+                break
             if not server.queue and not server.running:
                 if i >= n:
                     break
@@ -864,25 +1035,43 @@ def serving_study(a) -> None:
                 continue
             server.tick()
             max_running = max(max_running, len(server.running))
-        server.drain()
-        t_end = max(r.finished for r in server.done)
+        if drain:
+            server.drain()
+        else:
+            torch.cuda.synchronize()
+            server._poll()
+        t_end = time.perf_counter()
     span = t_end - t0
-    served_ps = sum(len(r) * r.nsteps for r in server.done)
+    advanced = server.batch.particle_steps
     lat = server.latencies()
-    served = {"requests": len(server.done), "rejected": len(server.rejected), "value": served_ps / span,
-              "unit": UNIT, "makespan_s": span, "ticks": server.ticks, "launches": server.batch.launches,
-              "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-              "latency_mean_s": float(lat.mean()), "max_running": max_running, "capacity_particles": server.capacity,
-              "bytes_per_particle": server.per_particle, "clocks": clocks.summary()}
+    waiting = [r for r in reqs[:i] if r.finished is None and r.error is None]
+    ages = np.array([t_end - r.arrival for r in waiting])
+    every = np.concatenate([lat, ages]) if ages.size else lat
+    served = {"requests_arrived": i, "requests_done": len(server.done), "rejected": len(server.rejected),
+              "queued_at_end": len(server.queue), "running_at_end": len(server.running),
+              "value": advanced / span, "unit": UNIT, "particle_steps_advanced": int(advanced),
+              "makespan_s": span, "ticks": server.ticks, "launches": server.batch.launches,
+              "latency_p50_s": float(np.percentile(lat, 50)) if lat.size else None,
+              "latency_p99_s": float(np.percentile(lat, 99)) if lat.size else None,
+              "latency_mean_s": float(lat.mean()) if lat.size else None,
+              "latency_p50_lower_bound_s": float(np.percentile(every, 50)) if every.size else None,
+              "latency_p99_lower_bound_s": float(np.percentile(every, 99)) if every.size else None,
+              "max_running": max_running, "capacity_particles": server.capacity,
+              "bytes_per_particle": server.per_particle,
+              "timeline_s_queued_running_done": timeline[:: max(1, len(timeline) // 60)],
+              "clocks": clocks.summary()}
+    done = sorted(server.done, key=lambda r: r.id)
+    del server
+    torch.cuda.empty_cache()
 
     # ---- plain: the same requests one at a time, FIFO ---------------------------
     plain = None
-    if a.serve_plain > 0:
+    if a.serve_plain > 0 and done:
         fs = fieldset()
-        k = min(a.serve_plain, len(server.done))
-        prefix = sorted(server.done, key=lambda r: r.id)[:k]
-        free_at, lat_p, ps, busy, same = 0.0, [], 0, 0.0, 0
-        for r in prefix:
+        free_at, lat_p, ps, busy, same, k = 0.0, [], 0, 0.0, 0, 0
+        for r in done[: a.serve_plain]:
+            if busy > a.serve_plain_budget_s:
+                break
             f = opb.roms.rk2_w_advection_timestepper if r.scheme == "rk2" else opb.roms.ab3_w_advection_timestepper
             torch.cuda.synchronize()
             w0 = time.perf_counter()
@@ -901,24 +1090,28 @@ def serving_study(a) -> None:
             lat_p.append(free_at - r.offset)
             ps += len(r) * r.nsteps
             same += all(np.array_equal(res[key].view(np.uint8), r.result[key].view(np.uint8)) for key in res)
+            k += 1
         lat_p = np.array(lat_p)
         plain = {"requests": k, "value": ps / busy, "unit": UNIT, "busy_s": busy,
                  "latency_p50_s": float(np.percentile(lat_p, 50)), "latency_p99_s": float(np.percentile(lat_p, 99)),
                  "identical_to_served": f"{same}/{k}",
-                 "note": "service times measured one request at a time; FIFO latencies from the same arrival "
-                         "times"}
+                 "note": "service times measured one request at a time (the first finished requests by arrival); "
+                         "FIFO latencies from the same arrival times"}
     sizes = [len(r) for r in reqs]
-    line = {"study": "serving", "metric": "served particle-steps/s and request latency p50/p99", "unit": UNIT,
+    return {"metric": "served particle-steps/s and request latency p50/p99", "unit": UNIT,
             "value": served["value"], "vs_plain": served["value"] / plain["value"] if plain else None,
-            "served": served, "plain": plain,
+            "offered_particle_steps_per_s": offered, "served": served, "plain": plain,
             "workload": {"grid": [nz, ny, nx], "field_dtype": "float32", "rate_per_s": a.serve_rate,
-                         "window_s": a.serve_seconds, "requests": len(reqs),
+                         "window_s": window_s, "drained": drain, "requests": len(reqs),
                          "particles_per_request": [int(min(sizes)), int(np.median(sizes)), int(max(sizes))],
                          "count_range": a.serve_count, "count_scale": a.serve_count_scale,
                          "duration_days": a.serve_days, "dt_s": [60, 120, 300],
-                         "offered_particle_steps_per_s": offered, "hbm_budget_gb": a.serve_budget_gb},
+                         "hbm_budget_gb": a.serve_budget_gb},
             "data": "synthetic; snapshots generated on the device on demand"}
-    print(json.dumps(line), flush=True)
+
+
+def serving_study(a) -> None:
+    print(json.dumps({"study": "serving", **serving_measure(a, a.serve_seconds, a.serve_drain)}), flush=True)
 
 
 def set_layout(layout: str) -> None:

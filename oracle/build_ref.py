@@ -1,17 +1,22 @@
-"""Build recipe for ``oracle/_ref``: the reference's own Cython kernels, compiled here.
+"""Build recipe for ``oracle/_ref``: the reference itself, compiled here.
 
 Test infrastructure only.  The reference (``offline_particles``) keeps its hot
 loops in eight Cython modules (``CMakeLists.txt:14-23``).  This script compiles
 them from the sources where they lie -- nothing is copied into this repository --
 with the flags the reference's CMake build uses (``cython -3 -X
 boundscheck=False``, ``CMakeLists.txt:26``; C at ``-O3 -DNDEBUG`` with OpenMP,
-``CMakeLists.txt:66-68``).  Outputs go only to ``oracle/_ref/`` (git-ignored).
+``CMakeLists.txt:66-68``), in a temporary folder, and keeps only the compiled
+extension modules.  Its pure-Python modules (the fields' time blend, the
+launcher, the steppers, ``Simulation``) are compiled to bytecode (``.pyc``,
+``py_compile``) beside them.  Outputs go only to ``oracle/_ref/``
+(git-ignored, never committed); there the compiled package imports without
+the reference's sources (``oracle/ref_import.py: import_compiled``), which is
+how the CPU baseline runs the reference's own code on a machine that has no
+reference checkout.  It also pins the oracle and generates the committed
+golden fixtures under ``tests/golden/``.
 
-The reference's pure-Python modules are *not* copied: ``oracle/ref_import.py``
-imports them from the reference checkout and takes the compiled extension
-modules from ``oracle/_ref``.  The result therefore exists only on a machine
-that has the reference checkout; it is used to pin the oracle and to generate
-the committed golden fixtures under ``tests/golden/``.
+The sources are read from ``$OFFLINE_PARTICLES_REF_SRC``, else from
+``reference/src`` beside this repository's folder.
 
 Usage: ``python oracle/build_ref.py [--src REF_SRC_DIR]``.
 """
@@ -20,14 +25,16 @@ from __future__ import annotations
 
 import argparse
 import os
+import py_compile
 import subprocess
 import sys
 import sysconfig
+import tempfile
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_SRC = Path(os.environ.get("OFFLINE_PARTICLES_REF_SRC", "/root/reference/src"))
+DEFAULT_SRC = Path(os.environ.get("OFFLINE_PARTICLES_REF_SRC", HERE.parent.parent / "reference" / "src"))
 
 # (module path relative to the package root) -- CMakeLists.txt:14-23
 MODULES = (
@@ -57,22 +64,36 @@ def build(src: Path = DEFAULT_SRC, force: bool = False) -> Path:
         raise FileNotFoundError(f"reference package not found under {src}")
     ext = sysconfig.get_config_var("EXT_SUFFIX")
     inc = sysconfig.get_paths()["include"]
-    cdir = OUT / "csrc"
-    for mod in MODULES:
-        pyx = pkg / f"{mod}.pyx"
-        c_file = cdir / f"{mod}.c"
-        so = OUT / "offline_particles" / f"{mod}{ext}"
-        if so.exists() and not force and so.stat().st_mtime >= pyx.stat().st_mtime:
+    with tempfile.TemporaryDirectory(prefix="opb_ref_") as tmp:
+        for mod in MODULES:
+            pyx = pkg / f"{mod}.pyx"
+            c_file = Path(tmp) / f"{mod}.c"
+            so = OUT / "offline_particles" / f"{mod}{ext}"
+            if so.exists() and not force and so.stat().st_mtime >= pyx.stat().st_mtime:
+                continue
+            c_file.parent.mkdir(parents=True, exist_ok=True)
+            so.parent.mkdir(parents=True, exist_ok=True)
+            # the .pxd files next to the .pyx are found through the include path
+            subprocess.run(
+                [sys.executable, "-m", "cython", "-3", "-X", "boundscheck=False",
+                 "-I", str(src), "-o", str(c_file), str(pyx)],
+                check=True, cwd=str(src),
+            )
+            subprocess.run([_gcc(), *CFLAGS, f"-I{inc}", str(c_file), "-o", str(so)], check=True)
+    # the pure-Python modules as sourceless bytecode (imported from OUT without the sources)
+    for py in sorted(pkg.rglob("*.py")):
+        rel = py.relative_to(pkg)
+        pyc = OUT / "offline_particles" / rel.with_suffix(".pyc")
+        if pyc.exists() and not force and pyc.stat().st_mtime >= py.stat().st_mtime:
             continue
-        c_file.parent.mkdir(parents=True, exist_ok=True)
-        so.parent.mkdir(parents=True, exist_ok=True)
-        # the .pxd files next to the .pyx are found through the include path
-        subprocess.run(
-            [sys.executable, "-m", "cython", "-3", "-X", "boundscheck=False",
-             "-I", str(src), "-o", str(c_file), str(pyx)],
-            check=True, cwd=str(src),
-        )
-        subprocess.run([_gcc(), *CFLAGS, f"-I{inc}", str(c_file), "-o", str(so)], check=True)
+        pyc.parent.mkdir(parents=True, exist_ok=True)
+        py_compile.compile(str(py), cfile=str(pyc), dfile=f"offline_particles/{rel}", doraise=True,
+                           invalidation_mode=py_compile.PycInvalidationMode.UNCHECKED_HASH)
+    stale = OUT / "csrc"  # older builds kept the generated C here
+    if stale.is_dir():
+        import shutil
+
+        shutil.rmtree(stale)
     return OUT
 
 

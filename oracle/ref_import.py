@@ -1,8 +1,12 @@
-"""Import the reference package (``offline_particles``) for pinning the oracle.
+"""Import the reference package (``offline_particles``) for pinning the oracle and timing it.
 
-Test infrastructure only.  The pure-Python modules are read from the reference
-checkout; the eight Cython extension modules come from ``oracle/_ref`` (built by
-``oracle/build_ref.py``).  ``dask`` and ``zarr`` are not installed here, and the
+Test infrastructure only.  ``import_reference``: the pure-Python modules are
+read from the reference checkout, the eight Cython extension modules come from
+``oracle/_ref`` (built by ``oracle/build_ref.py``).  ``import_compiled``: the
+whole package from ``oracle/_ref`` (the extension modules and the bytecode of
+the pure-Python modules), on a machine without the reference's sources -- the
+CPU baseline's way of running the reference's own code.  ``dask`` and ``zarr``
+are not installed here, and the
 reference's numpy path touches them only in annotations and in ``from_dask`` /
 the zarr writer (``fields.py:6,443-458``; ``spatial_arrays.py:9,228-295``;
 ``output/_zarr_writer.py:7-8``), so empty stand-in modules satisfy its imports.
@@ -19,7 +23,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REF_OUT = HERE / "_ref"
-DEFAULT_SRC = Path(os.environ.get("OFFLINE_PARTICLES_REF_SRC", "/root/reference/src"))
+DEFAULT_SRC = Path(os.environ.get("OFFLINE_PARTICLES_REF_SRC", HERE.parent.parent / "reference" / "src"))
 
 
 def available(src: Path = DEFAULT_SRC) -> bool:
@@ -84,4 +88,25 @@ def import_reference(src: Path = DEFAULT_SRC, build: bool = True):
         import offline_particles  # noqa: F401
     finally:
         sys.path.remove(str(src))
+    return sys.modules["offline_particles"]
+
+
+def compiled_available() -> bool:
+    """``oracle/_ref`` holds the whole compiled package (``oracle/build_ref.py`` ran)."""
+    pkg = REF_OUT / "offline_particles"
+    return (pkg / "__init__.pyc").exists() and any((pkg / "kernels" / "roms").glob("ab3_w_advection*.so"))
+
+
+def import_compiled():
+    """Return the reference package imported from ``oracle/_ref`` alone (no sources needed)."""
+    if "offline_particles" in sys.modules:
+        return sys.modules["offline_particles"]
+    if not compiled_available():
+        raise ImportError(f"no compiled reference under {REF_OUT}; run oracle/build_ref.py where the sources are")
+    _stub_missing_deps()
+    sys.path.insert(0, str(REF_OUT))
+    try:
+        import offline_particles  # noqa: F401
+    finally:
+        sys.path.remove(str(REF_OUT))
     return sys.modules["offline_particles"]
