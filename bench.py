@@ -929,11 +929,33 @@ def batched_study(a) -> None:
     print(json.dumps({"study": "batched", **batched_measure(a)}), flush=True)
 
 
+class TracedRequest:
+    """One request of the trace before it arrives: its particles are drawn from its own seed when it is
+    materialised, so a long trace holds only the arrays of requests in the system."""
+
+    def __init__(self, grid, id: int, offset: float, n: int, scheme: str, dt: float, duration: float) -> None:
+        self.grid, self.id, self.offset, self.n = grid, id, offset, n
+        self.scheme, self.dt, self.duration = scheme, dt, duration
+
+    def __len__(self) -> int:
+        return self.n
+
+    @property
+    def nsteps(self) -> int:
+        return round(self.duration / self.dt)
+
+    def materialise(self):
+        from offline_particles_b200.serving import ReleaseRequest
+
+        z, y, x = self.grid.release_in_box(self.n, np.random.default_rng((5, self.id)))
+        r = ReleaseRequest(z, y, x, self.scheme, self.dt, self.duration, id=self.id)
+        r.offset = self.offset  # arrival time after the start of the run
+        return r
+
+
 def serving_trace(a, grid):
     """Poisson arrivals; per request: log-uniform count, random wet rectangle and sigma band, duration,
-    scheme and dt (config-5 construction, seeded)."""
-    from offline_particles_b200.serving import ReleaseRequest
-
+    scheme and dt (config-5 construction, seeded; particles drawn on arrival)."""
     rng = np.random.default_rng(5)
     lo, hi = (float(v) for v in a.serve_count.split(","))
     dlo, dhi = (float(v) for v in a.serve_days.split(","))
@@ -943,13 +965,10 @@ def serving_trace(a, grid):
         if t > a.serve_seconds:
             break
         n = max(1, int(round(np.exp(rng.uniform(np.log(lo), np.log(hi))) * a.serve_count_scale)))
-        z, y, x = grid.release_in_box(n, rng)
         dt = float(rng.choice([60.0, 120.0, 300.0]))
         days = rng.uniform(dlo, dhi)
         scheme = "rk2" if rng.random() < 0.5 else "ab3"
-        r = ReleaseRequest(z, y, x, scheme, dt, round(days * 86400.0 / dt) * dt, id=len(reqs))
-        r.offset = t  # arrival time after the start of the run
-        reqs.append(r)
+        reqs.append(TracedRequest(grid, len(reqs), t, n, scheme, dt, round(days * 86400.0 / dt) * dt))
     return reqs
 
 
@@ -1000,7 +1019,7 @@ def serving_measure(a, window_s: float, drain: bool) -> dict:
     budget = int(a.serve_budget_gb * 1e9)
     server = ReleaseServer(fieldset(), t_arr, hbm_budget=budget, max_releases=1024, block=256, warps_per_sm=16,
                            buckets=256, sort_interval=4)
-    offered = sum(len(r) * round(r.duration / r.dt) for r in reqs) / window_s
+    offered = sum(len(r) * r.nsteps for r in reqs) / window_s
     # warm the kernels (module load, occupancy, graph capture) on a throwaway server
     warm = ReleaseServer(fieldset(), t_arr, hbm_budget=64 * server.per_particle, max_releases=4)
     wz, wy, wx = grid.release(32, seed=1)
@@ -1011,6 +1030,8 @@ def serving_measure(a, window_s: float, drain: bool) -> dict:
     torch.cuda.synchronize()
 
     timeline = []
+    live = []  # every submitted request
+    kept = 0
     with ClockSampler(0) as clocks:
         t0 = time.perf_counter()
         i, n = 0, len(reqs)
@@ -1022,9 +1043,17 @@ def serving_measure(a, window_s: float, drain: bool) -> dict:
                 timeline.append((round(now, 2), len(server.queue), len(server.running), len(server.done)))
                 next_sample += 1.0
             while i < n and reqs[i].offset <= now:
-                reqs[i].arrival = t0 + reqs[i].offset
-                server.submit(reqs[i])
+                r = reqs[i].materialise()
+                r.arrival = t0 + r.offset
+                server.submit(r)
+                live.append(r)
                 i += 1
+            if len(server.done) > kept:  # keep the arrays of the requests the plain arm replays
+                for r in server.done[kept:]:
+                    if r.id >= a.serve_plain:
+                        r.zidx = r.yidx = r.xidx = r.release = None
+                        r.result = {"kept": False} if r.result is not None else None
+                kept = len(server.done)
             if not drain and now >= window_s:
                 break
             if not server.queue and not server.running:
@@ -1044,7 +1073,7 @@ def serving_measure(a, window_s: float, drain: bool) -> dict:
     span = t_end - t0
     advanced = server.batch.particle_steps
     lat = server.latencies()
-    waiting = [r for r in reqs[:i] if r.finished is None and r.error is None]
+    waiting = [r for r in live if r.finished is None and r.error is None]
     ages = np.array([t_end - r.arrival for r in waiting])
     every = np.concatenate([lat, ages]) if ages.size else lat
     served = {"requests_arrived": i, "requests_done": len(server.done), "rejected": len(server.rejected),
@@ -1069,7 +1098,7 @@ def serving_measure(a, window_s: float, drain: bool) -> dict:
     if a.serve_plain > 0 and done:
         fs = fieldset()
         free_at, lat_p, ps, busy, same, k = 0.0, [], 0, 0.0, 0, 0
-        for r in done[: a.serve_plain]:
+        for r in [r for r in done if r.id < a.serve_plain]:
             if busy > a.serve_plain_budget_s:
                 break
             f = opb.roms.rk2_w_advection_timestepper if r.scheme == "rk2" else opb.roms.ab3_w_advection_timestepper

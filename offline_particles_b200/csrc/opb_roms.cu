@@ -23,6 +23,12 @@
 #include "opb_host.cuh"
 #include "opb_stages.cuh"
 
+// Resident CTAs per SM the fused steppers are compiled for (their register
+// budget: 65536 / (256 * OPB_FUSED_MINB) per thread).
+#ifndef OPB_FUSED_MINB
+#define OPB_FUSED_MINB 2
+#endif
+
 namespace opb {
 namespace {
 
@@ -188,7 +194,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3_post(const __grid_constant__ DPa
 // `nsteps` RK2 steps (timesteppers.py:241-257) per launch.  table[3*k + j]
 // selects the fields of step k, stage j (t, t + alpha dt, t + dt).
 template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool B2 = false>
-__global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__ DParticles p,
+__global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_rk2_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
                                                       const __grid_constant__ StepTable table, int nsteps,
@@ -239,7 +245,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_rk2_steps(const __grid_constant__
 // `nsteps` AB3 steps (timesteppers.py:296-305) per launch.  table[2*k + j]
 // selects the fields of step k at t (j = 0) and t + dt (j = 1).
 template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool ISO = false, bool B2 = false>
-__global__ void __launch_bounds__(kBlock, 2) k_ab3_steps(const __grid_constant__ DParticles p,
+__global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_ab3_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
                                                       const __grid_constant__ StepTable table, int nsteps,

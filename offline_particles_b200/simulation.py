@@ -114,8 +114,26 @@ class Simulation:
                 self._launcher.launch_kernel(kernel, self._particles, self.tidx)
             event(self.state)
 
+    def _prefetch_next_step(self) -> None:
+        """Start uploading the snapshots the next step reads (the two around the current time) to every
+        streamed field's device ring, snapshot by snapshot across fields, so that they stream in while the
+        caller's particle arrays are copied in and sorted."""
+        from .timesteppers import _time_dependent_fields
+
+        td = [f for f in _time_dependent_fields(self._launcher, self._timestepper.field_roles).values()
+              if f.streamed]
+        if not td:
+            return
+        it = int(divmod(self._timestepper.tidx, 1)[0])
+        keep = {it, it + 1}
+        for k in (it, it + 1):
+            for f in td:
+                if k < f.num_timesteps:
+                    f.prefetch(k, keep)
+
     def set_indices(self, zidx=None, yidx=None, xidx=None) -> None:
         """Set the particle indices (broadcast to the particle count; validated before any write)."""
+        self._prefetch_next_step()
         vals = {}
         for name, v in (("zidx", zidx), ("yidx", yidx), ("xidx", xidx)):
             if v is not None:

@@ -103,3 +103,47 @@ def test_simulation_from_roms_history_files(tmp_path):
     h.close()
     for k in outs[0]:
         assert same_bits(outs[0][k], outs[1][k]), k
+
+
+def test_mixed_schedules_run_equals_step_and_reference(tmp_path):
+    """An output writer every 1800 s (the reference's fixture) and one every 7 iterations in the same
+    simulation: run() splits its fused launches at both schedules' events, and every row equals the
+    step-by-step run and, for the time schedule, the reference's rows."""
+    from b200_runner import b200_fieldset
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200.output import NpyOutputBuilder, linearly_interpolate_fields
+    from offline_particles_b200.synth import GridSpec, SyntheticROMS
+
+    gold = load("outputs.npz")
+    g = SyntheticROMS(GridSpec(nx=48, ny=40, nz=8, nt=4, seed=41, dtype="float32"))
+    fields = g.oracle_fields()
+    rows = {}
+    for mode in ("step", "run"):
+        fs = b200_fieldset(fields, g.hc, g.spec.nz)
+        t_arr = np.arange(fields["u"].shape[0], dtype=np.float64) * 3600.0
+        sb = opb.SimulationBuilder(opb.roms.rk2_w_advection_timestepper(t_arr, np.float64(300.0)), fs)
+        by_time = NpyOutputBuilder("by_time", tmp_path / mode / "t")
+        by_time.add_output(*linearly_interpolate_fields(fs, "h", "u", "zeta", "w"))
+        sb.add_output_writer(by_time, dt=np.float64(1800.0))
+        by_iter = NpyOutputBuilder("by_iter", tmp_path / mode / "i")
+        by_iter.add_output(*linearly_interpolate_fields(fs, "v", "zeta"))
+        sb.add_output_writer(by_iter, n=7, first=3)
+        sim = sb.build_simulation(512)
+        sim.set_indices(gold["z0"], gold["y0"], gold["x0"])
+        if mode == "step":
+            for _ in range(24):
+                sim.step()
+        else:
+            sim.run(24)
+        sim.synchronize()
+        sim.close_outputs()
+        rows[mode] = {f"{d}/{n}": np.load(tmp_path / mode / d / f"{n}.npy")
+                      for d, names in (("t", ("time", "h", "u", "zeta", "w")), ("i", ("time", "v", "zeta")))
+                      for n in names}
+    assert rows["run"]["i/time"].shape[0] == 4  # iterations 3, 10, 17, 24
+    for key, val in rows["step"].items():
+        assert same_bits(rows["run"][key], val), f"{key}: {mismatch_report(rows['run'][key], val)}"
+    assert same_bits(rows["run"]["t/time"], gold["time"])
+    for name in ("h", "u", "zeta", "w"):
+        assert same_bits(rows["run"][f"t/{name}"], gold[f"out_{name}"]), name
