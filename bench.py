@@ -74,7 +74,7 @@ def parse():
                     help="read h, zeta, dx, dy as separate fields (no 2-D bundles)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=25.0)
-    ap.add_argument("--study", choices=("precision", "batched", "serving"), default=None,
+    ap.add_argument("--study", choices=("precision", "batched", "serving", "launch"), default=None,
                     help="precision: float64 vs float32 arithmetic with float32/float16/bfloat16 storage, "
                          "separation in metres after --days; batched: release experiments in one batch vs "
                          "one after another through the plain path")
@@ -151,7 +151,7 @@ def field_bytes(grid, snaps) -> dict:
     return {"snapshot": per_snap, "pair": 2 * per_snap, "static": static}
 
 
-def build_sim(grid, sources: dict, n: int, a, *, ring_size: int = 4):
+def build_sim(grid, sources: dict, n: int, a, *, ring_size: int = 4, **sim_kw):
     import offline_particles_b200 as opb
 
     kw = {}
@@ -162,7 +162,7 @@ def build_sim(grid, sources: dict, n: int, a, *, ring_size: int = 4):
     nt = sources["u"].shape[0]
     fs = opb.Fieldset(nt, a.nz, a.ny, a.nx, constants={"hc": grid.hc, "NZ": a.nz}, **kw)
     ts = opb.roms.ab3_w_advection_timestepper(grid.time_array[:nt], np.float64(a.dt))
-    return opb.SimulationBuilder(ts, fs).build_simulation(n), fs
+    return opb.SimulationBuilder(ts, fs).build_simulation(n, **sim_kw), fs
 
 
 def window_plan(a) -> dict:
@@ -1143,6 +1143,38 @@ def serving_study(a) -> None:
     print(json.dumps({"study": "serving", **serving_measure(a, a.serve_seconds, a.serve_drain)}), flush=True)
 
 
+def launch_study(a) -> None:
+    """One fused AB3 launch of exactly --steps steps after an explicit Morton sort, inside one snapshot
+    interval (fields resident, no re-sort or pair build inside): the unit an ncu capture of the headline
+    kernel compares between builds.  Runs --warmup steps first (their own launch), then the measured
+    launch; prints its CUDA-event time per step.  Capture it with ``-k regex:k_ab3_steps -s 1 -c 1``."""
+    import torch
+
+    import offline_particles_b200 as opb
+
+    torch.cuda.set_device(0)
+    steps_per_interval = int(round(3600.0 / a.dt))
+    if a.warmup + a.steps > steps_per_interval:
+        raise SystemExit(f"--warmup + --steps must fit one snapshot interval ({steps_per_interval} steps)")
+    grid = make_grid(a, 3)
+    dsrc = grid.device_snapshots(3)
+    sim, _ = build_sim(grid, dsrc, a.particles, a, sort_interval=0)
+    sim.set_indices(*grid.release(a.particles, seed=1000))
+    sim.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+    sim.sort_particles()
+    sim.run(a.warmup)
+    torch.cuda.synchronize()
+    s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_.record()
+    sim.run(a.steps)
+    e_.record()
+    torch.cuda.synchronize()
+    ms = s_.elapsed_time(e_)
+    print(json.dumps({"study": "launch", "steps": a.steps, "particles": a.particles, "grid": [a.nz, a.ny, a.nx],
+                      "ms": ms, "ms_per_step": ms / a.steps,
+                      "particle_steps_per_s": a.particles * a.steps / (ms * 1e-3)}), flush=True)
+
+
 def set_layout(layout: str) -> None:
     """The snapshot layout of every launch in this process (``--layout``)."""
     from offline_particles_b200 import timesteppers
@@ -1167,6 +1199,8 @@ def main() -> None:
         batched_study(a)
     elif a.study == "serving":
         serving_study(a)
+    elif a.study == "launch":
+        launch_study(a)
     elif a.impl == "reference":
         reference_arm(a)
     else:

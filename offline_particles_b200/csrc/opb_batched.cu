@@ -13,6 +13,11 @@
 #include "opb_host.cuh"
 #include "opb_stages.cuh"
 
+// 1: the batched kernels keep the velocity history in shared memory (PState HS)
+#ifndef OPB_BATCH_HIST_SMEM
+#define OPB_BATCH_HIST_SMEM 0
+#endif
+
 namespace opb {
 namespace {
 
@@ -24,8 +29,11 @@ namespace {
 template <typename T, typename I, int SCHEME, int LAYOUT, bool B2>
 __device__ __forceinline__ void batched_particle(const DParticles &p, long long i, const opb_experiment &E,
                                                  const DScalars &sc0, const DRoms &r, const opb_time *table,
-                                                 const Levels &L) {
-    PState<I> s;
+                                                 const Levels &L, double *hs, int hstride) {
+    constexpr bool HS = OPB_BATCH_HIST_SMEM != 0;
+    PState<I, HS> s;
+    s.hs = hs;
+    s.hstride = hstride;
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
     DScalars sc = sc0;
@@ -36,12 +44,8 @@ __device__ __forceinline__ void batched_particle(const DParticles &p, long long 
     s.xidx = p.xidx[i];
     const bool ab3 = SCHEME == OPB_SCHEME_AB3 || (SCHEME == 0 && E.scheme == OPB_SCHEME_AB3);
     if (ab3) {
-        s.k1x = p.dxidx1[i];
-        s.k1y = p.dyidx1[i];
-        s.k1z = p.dz1[i];
-        s.k2x = p.dxidx2[i];
-        s.k2y = p.dyidx2[i];
-        s.k2z = p.dz2[i];
+        s.set_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
+        s.set_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
     }
     const uint8_t st0 = s.status;
     bool moved = false;
@@ -80,16 +84,10 @@ __device__ __forceinline__ void batched_particle(const DParticles &p, long long 
     p.xidx[i] = s.xidx;
     p.z[i] = s.z;
     if (ab3) {
-        p.dxidx0[i] = s.k1x;
-        p.dyidx0[i] = s.k1y;
-        p.dz0[i] = s.k1z;
+        s.get_k1(p.dxidx0[i], p.dyidx0[i], p.dz0[i]);
     }
-    p.dxidx1[i] = s.k1x;
-    p.dyidx1[i] = s.k1y;
-    p.dz1[i] = s.k1z;
-    p.dxidx2[i] = s.k2x;
-    p.dyidx2[i] = s.k2y;
-    p.dz2[i] = s.k2z;
+    s.get_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
+    s.get_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
 }
 
 // Interleaved work order: item t = (bucket t / nexp, experiment t % nexp)
@@ -167,6 +165,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_batched_steps(const __grid_cons
                                                             const int64_t *__restrict__ bounds,
                                                             const int64_t *__restrict__ items) {
     OPB_LEVELS(r, sc);
+    __shared__ double s_hist[OPB_BATCH_HIST_SMEM ? 6 * BLOCK : 1];
     const int nexp = hdr->nexp;
     const int nb = hdr->nbuckets;
     const long long nchunks = hdr->nchunks;
@@ -208,7 +207,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_batched_steps(const __grid_cons
         if (i >= end || i < E.start || i >= E.start + E.count || E.nsteps <= 0) continue;
         if (i < 0 || i >= p.n) continue;
         if (SCHEME != 0 && E.scheme != SCHEME) continue;  // another launch's experiment
-        batched_particle<T, I, SCHEME, LAYOUT, B2>(p, i, E, sc, r, table, L);
+        batched_particle<T, I, SCHEME, LAYOUT, B2>(p, i, E, sc, r, table, L, s_hist + threadIdx.x, BLOCK);
     }
 }
 

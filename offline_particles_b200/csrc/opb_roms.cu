@@ -28,6 +28,10 @@
 #ifndef OPB_FUSED_MINB
 #define OPB_FUSED_MINB 2
 #endif
+// 1: the fused steppers keep the velocity history in shared memory (PState HS)
+#ifndef OPB_FUSED_HIST_SMEM
+#define OPB_FUSED_HIST_SMEM 0
+#endif
 
 namespace opb {
 namespace {
@@ -76,9 +80,7 @@ __global__ void __launch_bounds__(kBlock) k_rk2_step_1(const __grid_constant__ D
         raise_zero_division(p);
         return;
     }
-    p.dxidx1[i] = s.k1x;
-    p.dyidx1[i] = s.k1y;
-    p.dz1[i] = s.k1z;
+    s.get_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
 }
 
 template <typename T, typename I>
@@ -93,16 +95,12 @@ __global__ void __launch_bounds__(kBlock) k_rk2_step_2(const __grid_constant__ D
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
     s.z = p.z[i];
-    s.k1x = p.dxidx1[i];
-    s.k1y = p.dyidx1[i];
-    s.k1z = p.dz1[i];
+    s.set_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
     if (!rk2_stage2(s, bind_all<T, I>(r, t), L, sc)) {
         raise_zero_division(p);
         return;
     }
-    p.dxidx2[i] = s.k2x;
-    p.dyidx2[i] = s.k2y;
-    p.dz2[i] = s.k2z;
+    s.get_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
 }
 
 template <typename T, typename I>
@@ -117,12 +115,8 @@ __global__ void __launch_bounds__(kBlock) k_rk2_update(const __grid_constant__ D
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
     s.z = p.z[i];
-    s.k1x = p.dxidx1[i];
-    s.k1y = p.dyidx1[i];
-    s.k1z = p.dz1[i];
-    s.k2x = p.dxidx2[i];
-    s.k2y = p.dyidx2[i];
-    s.k2z = p.dz2[i];
+    s.set_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
+    s.set_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
     rk2_update(s, bind_all<T, I>(r, t), L, sc);
     p.z[i] = s.z;
     p.yidx[i] = s.yidx;
@@ -149,12 +143,8 @@ __global__ void __launch_bounds__(kBlock) k_ab3(const __grid_constant__ DParticl
     s.zidx = p.zidx[i];
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
-    s.k1x = p.dxidx1[i];
-    s.k1y = p.dyidx1[i];
-    s.k1z = p.dz1[i];
-    s.k2x = p.dxidx2[i];
-    s.k2y = p.dyidx2[i];
-    s.k2z = p.dz2[i];
+    s.set_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
+    s.set_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
     if (!ab3_any<T, I, ISO>(s, bind_all<T, I>(r, t), sc, p, i)) {
         raise_zero_division(p);
         return;
@@ -163,15 +153,9 @@ __global__ void __launch_bounds__(kBlock) k_ab3(const __grid_constant__ DParticl
     p.z[i] = s.z;
     p.yidx[i] = s.yidx;
     p.xidx[i] = s.xidx;
-    p.dxidx0[i] = s.k1x;  // after the history shift k1 == k0
-    p.dyidx0[i] = s.k1y;
-    p.dz0[i] = s.k1z;
-    p.dxidx1[i] = s.k1x;
-    p.dyidx1[i] = s.k1y;
-    p.dz1[i] = s.k1z;
-    p.dxidx2[i] = s.k2x;
-    p.dyidx2[i] = s.k2y;
-    p.dz2[i] = s.k2z;
+    s.get_k1(p.dxidx0[i], p.dyidx0[i], p.dz0[i]);  // after the history shift k1 == k0
+    s.get_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
+    s.get_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
 }
 
 template <typename T, typename I>
@@ -202,7 +186,13 @@ __global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_rk2_steps(const __gr
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
-    PState<I> s;
+    constexpr bool HS = OPB_FUSED_HIST_SMEM != 0;
+    PState<I, HS> s;
+    if constexpr (HS) {
+        __shared__ double s_hist[6 * kBlock];
+        s.hs = s_hist + threadIdx.x;
+        s.hstride = kBlock;
+    }
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
     s.zidx = p.zidx[i];
@@ -234,12 +224,8 @@ __global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_rk2_steps(const __gr
     p.yidx[i] = s.yidx;
     p.xidx[i] = s.xidx;
     p.z[i] = s.z;
-    p.dxidx1[i] = s.k1x;
-    p.dyidx1[i] = s.k1y;
-    p.dz1[i] = s.k1z;
-    p.dxidx2[i] = s.k2x;
-    p.dyidx2[i] = s.k2y;
-    p.dz2[i] = s.k2z;
+    s.get_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
+    s.get_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
 }
 
 // `nsteps` AB3 steps (timesteppers.py:296-305) per launch.  table[2*k + j]
@@ -253,18 +239,20 @@ __global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_ab3_steps(const __gr
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
-    PState<I> s;
+    constexpr bool HS = OPB_FUSED_HIST_SMEM != 0;
+    PState<I, HS> s;
+    if constexpr (HS) {
+        __shared__ double s_hist[6 * kBlock];
+        s.hs = s_hist + threadIdx.x;
+        s.hstride = kBlock;
+    }
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
     s.zidx = p.zidx[i];
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
-    s.k1x = p.dxidx1[i];
-    s.k1y = p.dyidx1[i];
-    s.k1z = p.dz1[i];
-    s.k2x = p.dxidx2[i];
-    s.k2y = p.dyidx2[i];
-    s.k2z = p.dz2[i];
+    s.set_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
+    s.set_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
     const double rho_t = ISO ? p.rho_t[i] : 0.0;
     const uint8_t st0 = s.status;
     bool moved = false;
@@ -293,15 +281,9 @@ __global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_ab3_steps(const __gr
     p.yidx[i] = s.yidx;
     p.xidx[i] = s.xidx;
     p.z[i] = s.z;
-    p.dxidx0[i] = s.k1x;
-    p.dyidx0[i] = s.k1y;
-    p.dz0[i] = s.k1z;
-    p.dxidx1[i] = s.k1x;
-    p.dyidx1[i] = s.k1y;
-    p.dz1[i] = s.k1z;
-    p.dxidx2[i] = s.k2x;
-    p.dyidx2[i] = s.k2y;
-    p.dz2[i] = s.k2z;
+    s.get_k1(p.dxidx0[i], p.dyidx0[i], p.dz0[i]);
+    s.get_k1(p.dxidx1[i], p.dyidx1[i], p.dz1[i]);
+    s.get_k2(p.dxidx2[i], p.dyidx2[i], p.dz2[i]);
 }
 
 // ---------------------------------------------------------- output kernels

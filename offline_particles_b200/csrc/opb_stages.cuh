@@ -16,12 +16,62 @@ namespace {
 constexpr int kBlock = 256;
 
 // ------------------------------------------------------------ per particle
-template <typename I = long long>
+// HS: the velocity history (RK2 k1, k2 / AB3 k(n-1), k(n-2)) lives in this
+// thread's column of a [6][block] shared-memory table instead of registers.
+// It is read and written once per step, after the stencil gathers, so that
+// the registers stay free for the gathers in flight (more resident warps).
+template <typename I = long long, bool HS = false>
 struct PState {
     double zidx, yidx, xidx, z;
     double k0x, k0y, k0z;  // AB3 k(n)
-    double k1x, k1y, k1z;  // RK2 k1 / AB3 k(n-1)
-    double k2x, k2y, k2z;  // RK2 k2 / AB3 k(n-2)
+    double k1x, k1y, k1z;  // RK2 k1 / AB3 k(n-1)  (HS: unused)
+    double k2x, k2y, k2z;  // RK2 k2 / AB3 k(n-2)  (HS: unused)
+    double *hs;            // HS: this thread's column (entry j at hs[j * hstride])
+    int hstride;
+    __device__ __forceinline__ void get_k1(double &x, double &y, double &z_) const {
+        if constexpr (HS) {
+            x = hs[0];
+            y = hs[hstride];
+            z_ = hs[2 * hstride];
+        } else {
+            x = k1x;
+            y = k1y;
+            z_ = k1z;
+        }
+    }
+    __device__ __forceinline__ void get_k2(double &x, double &y, double &z_) const {
+        if constexpr (HS) {
+            x = hs[3 * hstride];
+            y = hs[4 * hstride];
+            z_ = hs[5 * hstride];
+        } else {
+            x = k2x;
+            y = k2y;
+            z_ = k2z;
+        }
+    }
+    __device__ __forceinline__ void set_k1(double x, double y, double z_) {
+        if constexpr (HS) {
+            hs[0] = x;
+            hs[hstride] = y;
+            hs[2 * hstride] = z_;
+        } else {
+            k1x = x;
+            k1y = y;
+            k1z = z_;
+        }
+    }
+    __device__ __forceinline__ void set_k2(double x, double y, double z_) {
+        if constexpr (HS) {
+            hs[3 * hstride] = x;
+            hs[4 * hstride] = y;
+            hs[5 * hstride] = z_;
+        } else {
+            k2x = x;
+            k2y = y;
+            k2z = z_;
+        }
+    }
     // h and zeta at (yidx, xidx) for the previous step's last time selection,
     // left by its last stage; the next step's first stage needs exactly these
     // values when it selects the same time (same position) and reuses them
@@ -247,9 +297,7 @@ __device__ __forceinline__ bool rk2_stage1(S &s, const B &f, const DScalars &sc,
         w = trilinear(f.w, s.zidx + f.w.o0, s.yidx + f.w.o1, s.xidx + f.w.o2);
     }
     if (dx == 0.0 || dy == 0.0) return false;
-    s.k1x = u / dx;
-    s.k1y = v / dy;
-    s.k1z = w;
+    s.set_k1(u / dx, v / dy, w);
     return true;
 }
 
@@ -257,9 +305,11 @@ __device__ __forceinline__ bool rk2_stage1(S &s, const B &f, const DScalars &sc,
 template <typename B, typename S>
 __device__ __forceinline__ bool rk2_stage2(S &s, const B &f, const Levels &L, const DScalars &sc) {
     const double adt = sc.alpha * sc.dt;
-    const double z_int = s.z + adt * s.k1z;
-    const double y_int = s.yidx + adt * s.k1y;
-    const double x_int = s.xidx + adt * s.k1x;
+    double k1x, k1y, k1z;
+    s.get_k1(k1x, k1y, k1z);
+    const double z_int = s.z + adt * k1z;
+    const double y_int = s.yidx + adt * k1y;
+    const double x_int = s.xidx + adt * k1x;
     double h, zeta, u, v, w, dx, dy;
     if constexpr (B::kFixed) {
         using I = typename B::index_type;
@@ -278,9 +328,7 @@ __device__ __forceinline__ bool rk2_stage2(S &s, const B &f, const Levels &L, co
         w = trilinear(f.w, z_idx + f.w.o0, y_int + f.w.o1, x_int + f.w.o2);
     }
     if (dx == 0.0 || dy == 0.0) return false;
-    s.k2x = u / dx;
-    s.k2y = v / dy;
-    s.k2z = w;
+    s.set_k2(u / dx, v / dy, w);
     return true;
 }
 
@@ -292,9 +340,12 @@ __device__ __forceinline__ void rk2_update(S &s, const B &f, const Levels &L, co
     const double b2 = 1.0 - b1;
     const double b1dt = b1 * sc.dt;
     const double b2dt = b2 * sc.dt;
-    s.z = s.z + b1dt * s.k1z + b2dt * s.k2z;
-    s.yidx = s.yidx + b1dt * s.k1y + b2dt * s.k2y;
-    s.xidx = s.xidx + b1dt * s.k1x + b2dt * s.k2x;
+    double k1x, k1y, k1z, k2x, k2y, k2z;
+    s.get_k1(k1x, k1y, k1z);
+    s.get_k2(k2x, k2y, k2z);
+    s.z = s.z + b1dt * k1z + b2dt * k2z;
+    s.yidx = s.yidx + b1dt * k1y + b2dt * k2y;
+    s.xidx = s.xidx + b1dt * k1x + b2dt * k2x;
     double h, zeta;
     hz_here(s, f, h, zeta);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
@@ -362,18 +413,21 @@ __device__ __forceinline__ bool ab3_step(S &s, const B &f, const DScalars &sc, c
     if (dy == 0.0) return false;
     s.k0y = v / dy;
     if (!vz.finish(wg, s.k0z)) return false;
+    double k1x, k1y, k1z, k2x, k2y, k2z;
+    s.get_k1(k1x, k1y, k1z);
+    s.get_k2(k2x, k2y, k2z);
     if (s.status == ST_MULTISTEP_1) {  // ab3_w_advection.pyx:122-131
-        s.k1x = s.k0x;
-        s.k1y = s.k0y;
-        s.k1z = s.k0z;
-        s.k2x = s.k0x;
-        s.k2y = s.k0y;
-        s.k2z = s.k0z;
+        k1x = s.k0x;
+        k1y = s.k0y;
+        k1z = s.k0z;
+        k2x = s.k0x;
+        k2y = s.k0y;
+        k2z = s.k0z;
         s.status = ST_MULTISTEP_2;
     } else if (s.status == ST_MULTISTEP_2) {  // ab3_w_advection.pyx:132-138
-        s.k2x = -s.k0x + 2.0 * s.k1x;
-        s.k2y = -s.k0y + 2.0 * s.k1y;
-        s.k2z = -s.k0z + 2.0 * s.k1z;
+        k2x = -s.k0x + 2.0 * k1x;
+        k2y = -s.k0y + 2.0 * k1y;
+        k2z = -s.k0z + 2.0 * k1z;
         s.status = ST_NORMAL;
     }
     if constexpr (!B::kFixed) {
@@ -387,15 +441,11 @@ __device__ __forceinline__ bool ab3_step(S &s, const B &f, const DScalars &sc, c
     }
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double dt = sc.dt;
-    s.z = s.z + dt * (23.0 * s.k0z - 16.0 * s.k1z + 5.0 * s.k2z) / 12.0;
-    s.yidx = s.yidx + dt * (23.0 * s.k0y - 16.0 * s.k1y + 5.0 * s.k2y) / 12.0;
-    s.xidx = s.xidx + dt * (23.0 * s.k0x - 16.0 * s.k1x + 5.0 * s.k2x) / 12.0;
-    s.k2z = s.k1z;
-    s.k2x = s.k1x;
-    s.k2y = s.k1y;
-    s.k1z = s.k0z;
-    s.k1x = s.k0x;
-    s.k1y = s.k0y;
+    s.z = s.z + dt * (23.0 * s.k0z - 16.0 * k1z + 5.0 * k2z) / 12.0;
+    s.yidx = s.yidx + dt * (23.0 * s.k0y - 16.0 * k1y + 5.0 * k2y) / 12.0;
+    s.xidx = s.xidx + dt * (23.0 * s.k0x - 16.0 * k1x + 5.0 * k2x) / 12.0;
+    s.set_k2(k1x, k1y, k1z);
+    s.set_k1(s.k0x, s.k0y, s.k0z);
     return true;
 }
 

@@ -132,8 +132,9 @@ class Simulation:
                     f.prefetch(k, keep)
 
     def set_indices(self, zidx=None, yidx=None, xidx=None) -> None:
-        """Set the particle indices (broadcast to the particle count; validated before any write)."""
-        self._prefetch_next_step()
+        """Set the particle indices (broadcast to the particle count; validated before any write).  Then
+        the snapshots of the next step start uploading, behind the indices, so that they stream in while
+        the particles are sorted."""
         vals = {}
         for name, v in (("zidx", zidx), ("yidx", yidx), ("xidx", xidx)):
             if v is not None:
@@ -141,6 +142,7 @@ class Simulation:
         for name, t in vals.items():
             self._particles.assign(name, t)
         self._steps_since_sort = None
+        self._prefetch_next_step()
 
     def set_particle_field(self, field_name: str, values) -> None:
         """Set one particle field to ``values`` (cast to the field's dtype, broadcast)."""
@@ -155,6 +157,10 @@ class Simulation:
             from ._device import numpy_dtype
 
             arr = np.asarray(values, dtype=numpy_dtype(target.dtype))
+            if arr.ndim == 0:
+                # one value for every particle: filled on the device, no host-to-device copy (which would
+                # queue behind snapshot uploads already in flight)
+                return torch.full(tuple(target.shape), arr.item(), dtype=target.dtype, device=target.device)
             arr = np.broadcast_to(arr, tuple(target.shape))
             t = torch.from_numpy(np.array(arr, copy=True, order="C")).to(target.device)
         return t.expand(target.shape)

@@ -8,7 +8,7 @@ boundscheck=False``, ``CMakeLists.txt:26``; C at ``-O3 -DNDEBUG`` with OpenMP,
 ``CMakeLists.txt:66-68``), in a temporary folder, and keeps only the compiled
 extension modules.  Its pure-Python modules (the fields' time blend, the
 launcher, the steppers, ``Simulation``) are compiled to bytecode (``.pyc``,
-``py_compile``) beside them.  Outputs go only to ``oracle/_ref/``
+``py_compile``) into one zip beside them (``offline_particles_py.zip``).  Outputs go only to ``oracle/_ref/``
 (git-ignored, never committed); there the compiled package imports without
 the reference's sources (``oracle/ref_import.py: import_compiled``), which is
 how the CPU baseline runs the reference's own code on a machine that has no
@@ -30,10 +30,12 @@ import subprocess
 import sys
 import sysconfig
 import tempfile
+import zipfile
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
+PY_ZIP = OUT / "offline_particles_py.zip"
 DEFAULT_SRC = Path(os.environ.get("OFFLINE_PARTICLES_REF_SRC", HERE.parent.parent / "reference" / "src"))
 
 # (module path relative to the package root) -- CMakeLists.txt:14-23
@@ -58,6 +60,14 @@ def _gcc() -> str:
     return "/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc"
 
 
+def _empty_pyc(path: Path) -> bytes:
+    path.write_text("")
+    out = path.with_suffix(".pyc")
+    py_compile.compile(str(path), cfile=str(out), doraise=True,
+                       invalidation_mode=py_compile.PycInvalidationMode.UNCHECKED_HASH)
+    return out.read_bytes()
+
+
 def build(src: Path = DEFAULT_SRC, force: bool = False) -> Path:
     pkg = src / "offline_particles"
     if not pkg.is_dir():
@@ -80,20 +90,34 @@ def build(src: Path = DEFAULT_SRC, force: bool = False) -> Path:
                 check=True, cwd=str(src),
             )
             subprocess.run([_gcc(), *CFLAGS, f"-I{inc}", str(c_file), "-o", str(so)], check=True)
-    # the pure-Python modules as sourceless bytecode (imported from OUT without the sources)
-    for py in sorted(pkg.rglob("*.py")):
-        rel = py.relative_to(pkg)
-        pyc = OUT / "offline_particles" / rel.with_suffix(".pyc")
-        if pyc.exists() and not force and pyc.stat().st_mtime >= py.stat().st_mtime:
-            continue
-        pyc.parent.mkdir(parents=True, exist_ok=True)
-        py_compile.compile(str(py), cfile=str(pyc), dfile=f"offline_particles/{rel}", doraise=True,
-                           invalidation_mode=py_compile.PycInvalidationMode.UNCHECKED_HASH)
-    stale = OUT / "csrc"  # older builds kept the generated C here
-    if stale.is_dir():
-        import shutil
+    # the pure-Python modules as sourceless bytecode in one zip (zipimport loads .pyc without sources)
+    sources = sorted(pkg.rglob("*.py"))
+    if force or not PY_ZIP.exists() or any(py.stat().st_mtime > PY_ZIP.stat().st_mtime for py in sources):
+        tmp_zip = PY_ZIP.with_suffix(f".{os.getpid()}.tmp")
+        with tempfile.TemporaryDirectory(prefix="opb_ref_pyc_") as tmp, \
+                zipfile.ZipFile(tmp_zip, "w", zipfile.ZIP_DEFLATED) as zf:
+            for py in sources:
+                rel = py.relative_to(pkg)
+                pyc = Path(tmp) / rel.with_suffix(".pyc")
+                pyc.parent.mkdir(parents=True, exist_ok=True)
+                py_compile.compile(str(py), cfile=str(pyc), dfile=f"offline_particles/{rel}", doraise=True,
+                                   invalidation_mode=py_compile.PycInvalidationMode.UNCHECKED_HASH)
+                zf.write(pyc, f"offline_particles/{rel.with_suffix('.pyc')}")
+            # folders the reference leaves as namespace packages (no __init__.py, e.g. models/) get an
+            # empty package module: zipimport does not resolve namespace packages
+            dirs = {py.parent for py in sources} | {d for py in sources for d in py.parents if pkg in d.parents}
+            for d in sorted(dirs):
+                if d != pkg and pkg in d.parents and not (d / "__init__.py").exists():
+                    zf.writestr(f"offline_particles/{d.relative_to(pkg)}/__init__.pyc",
+                                _empty_pyc(Path(tmp) / "empty.py"))
+        os.replace(tmp_zip, PY_ZIP)
+    import shutil
 
-        shutil.rmtree(stale)
+    for stale in [OUT / "csrc", *(p for p in (OUT / "offline_particles").rglob("*.pyc"))]:
+        if stale.is_dir():  # older builds kept the generated C here
+            shutil.rmtree(stale)
+        elif stale.exists():  # older builds kept loose bytecode
+            stale.unlink()
     return OUT
 
 

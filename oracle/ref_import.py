@@ -91,22 +91,28 @@ def import_reference(src: Path = DEFAULT_SRC, build: bool = True):
     return sys.modules["offline_particles"]
 
 
+PY_ZIP = REF_OUT / "offline_particles_py.zip"
+
+
 def compiled_available() -> bool:
-    """``oracle/_ref`` holds the whole compiled package (``oracle/build_ref.py`` ran)."""
+    """``oracle/_ref`` holds the whole compiled package (``oracle/build_ref.py`` ran): the bytecode zip of
+    the pure-Python modules and the extension modules."""
     pkg = REF_OUT / "offline_particles"
-    return (pkg / "__init__.pyc").exists() and any((pkg / "kernels" / "roms").glob("ab3_w_advection*.so"))
+    return PY_ZIP.exists() and any((pkg / "kernels" / "roms").glob("ab3_w_advection*.so"))
 
 
 def import_compiled():
-    """Return the reference package imported from ``oracle/_ref`` alone (no sources needed)."""
+    """Return the reference package imported from ``oracle/_ref`` alone (no sources needed): its
+    pure-Python modules from the bytecode zip, its extension modules from ``oracle/_ref``."""
     if "offline_particles" in sys.modules:
         return sys.modules["offline_particles"]
     if not compiled_available():
         raise ImportError(f"no compiled reference under {REF_OUT}; run oracle/build_ref.py where the sources are")
     _stub_missing_deps()
-    sys.path.insert(0, str(REF_OUT))
+    sys.meta_path.insert(0, _ExtFinder(REF_OUT))
+    sys.path.insert(0, str(PY_ZIP))
     try:
         import offline_particles  # noqa: F401
     finally:
-        sys.path.remove(str(REF_OUT))
+        sys.path.remove(str(PY_ZIP))
     return sys.modules["offline_particles"]

@@ -29,6 +29,11 @@ edge_cases.npz     NaN land, inactive / out-of-domain / non-finite particles,
 zero_division.json the reference's error for a zero grid spacing.
 outputs.npz        rows of the reference's output events: linearly_interpolate_fields
                    (h, u, zeta, w) every 1800 s of an RK2 run, time and values.
+outputs_mixed.npz  the same run with a second writer (v, zeta) every 7 iterations from
+                   iteration 3: both writers' rows.  Output kernels skip inactive
+                   particles and every output of one dtype shares a particle field, so
+                   an inactive particle's row holds the value the previous output left
+                   there; the second writer changes those values in the first's rows.
 iso_f32.npz        the AB3 isopycnal follower (ab3_isopycnal_following.pyx) on a
                    96x80x16 float32 grid with a synthetic density field,
                    4096 particles with target densities, dt=120 s, 149 steps.
@@ -356,6 +361,81 @@ OUTPUT_CASE = dict(grid=GridSpec(nx=48, ny=40, nz=8, nt=4, seed=41, dtype="float
                    every=1800.0, variables=("h", "u", "zeta", "w"))
 
 
+def _memory_writer_classes():
+    from offline_particles.output import AbstractOutputWriter, AbstractOutputWriterBuilder
+
+    class MemoryWriter(AbstractOutputWriter):
+        def __init__(self, name, outputs):
+            self._name = name
+            self._outputs = outputs
+            self.times, self.rows = [], {k: [] for k in outputs}
+
+        name = property(lambda self: self._name)
+        outputs = property(lambda self: self._outputs)
+
+        def write_time(self, state):
+            self.times.append(state.time)
+
+        def write_output(self, name, state):
+            self.rows[name].append(np.array(state.particles[self._outputs[name].particle_field]))
+
+        def finalise_write_round(self, state):
+            pass
+
+    class MemoryBuilder(AbstractOutputWriterBuilder):
+        def __init__(self, name):
+            self._name = name
+            self._outputs = {}
+            self.writer = None
+
+        name = property(lambda self: self._name)
+        outputs = property(lambda self: self._outputs)
+
+        def add_output(self, *outputs, **kwargs):
+            for o in outputs:
+                self._outputs[o.name] = o
+
+        def remove_output(self, name):
+            del self._outputs[name]
+
+        def build(self, nparticles, time_type=np.dtype(np.float64)):
+            self.writer = MemoryWriter(self._name, dict(self._outputs))
+            return self.writer
+
+    return MemoryBuilder
+
+
+def make_outputs_mixed(op) -> None:
+    """OUTPUT_CASE with a second writer of (v, zeta) every 7 iterations from iteration 3: the rows of
+    both writers when an iteration schedule and a time schedule share one simulation."""
+    from offline_particles.models.roms import rk2_w_advection_timestepper
+    from offline_particles.output import linearly_interpolate_fields
+
+    MemoryBuilder = _memory_writer_classes()
+    c = OUTPUT_CASE
+    g = SyntheticROMS(c["grid"])
+    fields = g.oracle_fields()
+    fs = ref_fieldset(op, fields, g.hc, g.spec.nz)
+    t_arr = np.arange(fields["u"].shape[0], dtype=np.float64) * 3600.0
+    sb = op.SimulationBuilder(rk2_w_advection_timestepper(t_arr, np.float64(c["dt"])), fs)
+    by_time = MemoryBuilder("by_time")
+    by_time.add_output(*linearly_interpolate_fields(fs, *c["variables"]))
+    sb.add_output_writer(by_time, dt=np.float64(c["every"]))
+    by_iter = MemoryBuilder("by_iter")
+    by_iter.add_output(*linearly_interpolate_fields(fs, "v", "zeta"))
+    sb.add_output_writer(by_iter, n=7, first=3)
+    z, y, x = g.release(c["n"], seed=3)
+    sim = sb.build_simulation(c["n"])
+    sim.set_indices(z, y, x)
+    for _ in range(c["steps"]):
+        sim.step()
+    rows = {f"t_{k}": np.stack(v) for k, v in by_time.writer.rows.items()}
+    rows.update({f"i_{k}": np.stack(v) for k, v in by_iter.writer.rows.items()})
+    np.savez_compressed(HERE / "outputs_mixed.npz", fingerprint=fingerprint(fields), z0=z, y0=y, x0=x,
+                        t_time=np.array(by_time.writer.times), i_time=np.array(by_iter.writer.times), **rows)
+    print("outputs_mixed rows", {k: v.shape for k, v in rows.items()})
+
+
 def make_outputs(op) -> None:
     """Rows the reference's output events produce: linearly_interpolate_fields outputs written every
     `every` seconds by an in-memory writer on the reference's own AbstractOutputWriter interface (the
@@ -422,6 +502,10 @@ def make_outputs(op) -> None:
 
 def main() -> None:
     op = import_reference()
+    if len(sys.argv) > 1:  # only the named fixtures, e.g. outputs_mixed
+        for name in sys.argv[1:]:
+            globals()[f"make_{name}"](op)
+        return
     make_interp_kat(op)
     make_vertical_kat(op)
     make_workloads(op)
@@ -429,6 +513,7 @@ def main() -> None:
     make_zero_division(op)
     make_isopycnal(op)
     make_outputs(op)
+    make_outputs_mixed(op)
     for p in sorted(HERE.glob("*.npz")) + sorted(HERE.glob("*.json")):
         print(p.name, p.stat().st_size)
 
