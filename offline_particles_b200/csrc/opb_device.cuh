@@ -39,6 +39,7 @@ struct DField {
 // across all fields.
 struct DGeom {
     long long nz, ny, nx;
+    long long su0, sv0, sw0;  // level strides of u (ny (nx - 1)), v ((ny - 1) nx) and w (ny nx)
     int roms;        // 1: the geometry above holds
     int w_centered;  // 1: the w slot is on rho points (nz, ny, nx), offsets 0
 };
@@ -166,6 +167,16 @@ struct View {
         return (double)(x + y);
     }
 
+    // an L1 prefetch of the element that holds the value at i (pair and wider layouts)
+    __device__ __forceinline__ void prefetch(I i) const {
+        const void *q;
+        if constexpr (KIND == KIND_OCTS) q = (const char *)prev + 32 * (long long)i;
+        else if constexpr (KIND == KIND_QUADS) q = (const char *)prev + 16 * (long long)i;
+        else if constexpr (KIND == KIND_PAIRS) q = (const char *)prev + 2 * sizeof(T) * (long long)i;
+        else q = prev + i;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+    }
+
     __device__ __forceinline__ double at(I i) const {
         if constexpr (KIND == KIND_YXPAIRS) {
             return __ldg(stat + 4 * (long long)i);
@@ -269,6 +280,7 @@ struct DxDyView {
     const D4 *p;
     I n0, n1;
     double o0, o1;
+    __device__ __forceinline__ void prefetch(I i) const { asm volatile("prefetch.global.L1 [%0];" ::"l"(p + i)); }
     // dx and dy at i and i + 1
     __device__ __forceinline__ void at2(I i, double &a0, double &b0, double &a1, double &b1) const {
         const D4 w = ldg256(p + i);
@@ -318,10 +330,15 @@ __device__ __forceinline__ long long trunc_index(double idx, long long max_idx) 
 // The same map in 32-bit arithmetic, for max_idx < 2^31: anything that is not
 // in [1, 2^63) (NaN, negatives, -inf, +huge) gives 0, [max_idx, 2^63) gives
 // max_idx, and the rest truncates exactly as the 64-bit conversion does.
+//
+// Without branches: the saturating conversion (cvt.rzi.s32: toward zero,
+// values past INT_MAX give INT_MAX) then min with max_idx gives (int)idx below
+// max_idx and max_idx from there on (idx >= max_idx implies trunc(idx) >=
+// max_idx, an integer); the range test selects 0 outside [1, 2^63).
 __device__ __forceinline__ int trunc_index(double idx, int max_idx) {
-    if (!(idx >= 1.0 && idx < 9.223372036854775808e18)) return 0;
-    if (idx >= (double)max_idx) return max_idx;
-    return (int)idx;
+    const bool in = idx >= 1.0 && idx < 9.223372036854775808e18;
+    const int t = min(__double2int_rz(idx), max_idx);
+    return in ? t : 0;
 }
 
 // linear.pxd:11-17

@@ -49,6 +49,9 @@ void set_geometry(DRoms &r) {
     g.roms = 0;
     g.w_centered = 0;
     const long long nz = g.nz, ny = g.ny, nx = g.nx;
+    g.su0 = ny * (nx - 1);
+    g.sv0 = (ny - 1) * nx;
+    g.sw0 = ny * nx;
     auto is3 = [](const DField &f, long long a, long long b, long long c, double oa, double ob, double oc) {
         return f.n0 == a && f.n1 == b && f.n2 == c && f.o0 == oa && f.o1 == ob && f.o2 == oc &&
                (oa != 0.0 || zero_offset(f.o0)) && (ob != 0.0 || zero_offset(f.o1)) &&

@@ -116,6 +116,7 @@ struct Bound {
     ZetaHView<I> zh;  // B2: zeta with h
     DxDyView<I> dd;   // B2: dx with dy
     I nz, ny, nx;     // FIXED: rho-point sizes (DGeom)
+    I su0, sv0, sw0;  // FIXED: level strides of u, v and w (DGeom)
 };
 
 template <typename T, typename I, bool FIXED = false, int LAYOUT = LAYOUT_PLAIN, bool B2 = false>
@@ -129,6 +130,9 @@ __device__ __forceinline__ Bound<T, I, FIXED, LAYOUT, B2> bind_all(const DRoms &
     b.nz = (I)r.geo.nz;
     b.ny = (I)r.geo.ny;
     b.nx = (I)r.geo.nx;
+    b.su0 = (I)r.geo.su0;
+    b.sv0 = (I)r.geo.sv0;
+    b.sw0 = (I)r.geo.sw0;
     if constexpr (B2) {
         b.zh.p = (const U4 *)r.zeta.data[t.prev];
         b.zh.ft = (float)t.ft;  // exact: the host rounded ft, gt to float32
@@ -184,17 +188,17 @@ __device__ __forceinline__ void other_axes(const B &f, double z, double y, doubl
 template <bool W_CENTERED, typename B, typename I = typename B::index_type>
 __device__ __forceinline__ void velocity_ax(const B &f, const Axes<I> &a, double &u, double &v, double &w, double &dx,
                                             double &dy) {
-    const I nx = f.nx, ny = f.ny;
-    u = trilinear_ax(f.u, a.zc, a.yc, a.xs, ny * (nx - 1), nx - 1);
+    const I nx = f.nx;
+    u = trilinear_ax(f.u, a.zc, a.yc, a.xs, f.su0, nx - 1);
     if constexpr (B::BUNDLED) {
         bilinear_pair_ax(f.dd, a.yc, a.xc, nx, dx, dy);
     } else {
         dx = bilinear_ax(f.dx, a.yc, a.xc, nx);
         dy = bilinear_ax(f.dy, a.yc, a.xc, nx);
     }
-    v = trilinear_ax(f.v, a.zc, a.ys, a.xc, (ny - 1) * nx, nx);
-    if constexpr (W_CENTERED) w = trilinear_ax(f.w, a.zc, a.yc, a.xc, ny * nx, nx);
-    else w = trilinear_ax(f.w, a.zs, a.yc, a.xc, ny * nx, nx);
+    v = trilinear_ax(f.v, a.zc, a.ys, a.xc, f.sv0, nx);
+    if constexpr (W_CENTERED) w = trilinear_ax(f.w, a.zc, a.yc, a.xc, f.sw0, nx);
+    else w = trilinear_ax(f.w, a.zs, a.yc, a.xc, f.sw0, nx);
 }
 
 // h and zeta on the rho-point axes
@@ -255,6 +259,46 @@ __device__ __forceinline__ void hz_here(S &s, const B &f, double &h, double &zet
 template <typename B, typename I = typename B::index_type>
 __device__ __forceinline__ double C_ax(const B &f, const Levels &L, const Axis<I> &zc) {
     return linear_ax(L.C, zc);
+}
+
+// Compiled layout, OPB_PREFETCH_NEXT: before the vertical search of a step's
+// last stage, prefetch into L1 the stencil rows the next step's first stage
+// will gather, predicting its vertical cell from the current level (a particle
+// changes level rarely in one step).  A prefetch moves no value into a
+// register and changes no result; a wrong prediction only wastes it.
+#ifndef OPB_PREFETCH_NEXT
+#define OPB_PREFETCH_NEXT 0
+#endif
+
+template <bool W_CENTERED, typename B, typename S>
+__device__ __forceinline__ void prefetch_next(const S &s, const B &f) {
+    if constexpr (B::kFixed && OPB_PREFETCH_NEXT && B::KT != KIND_TD) {
+        using I = typename B::index_type;
+        const I nz = f.nz, ny = f.ny, nx = f.nx;
+        const I zc = trunc_index(s.zidx + 0.0, (I)(nz - 2));
+        const I zw = W_CENTERED ? zc : trunc_index(s.zidx + 0.5, (I)(nz - 1));
+        const I ys = trunc_index(s.yidx + -0.5, (I)(ny - 3));
+        const I xs = trunc_index(s.xidx + -0.5, (I)(nx - 3));
+        const I yc = s.ya.i, xc = s.xa.i;
+        const I su1 = nx - 1, su0 = f.su0, sv0 = f.sv0, sw0 = f.sw0;
+        const I bu = zc * su0 + yc * su1 + xs, bv = zc * sv0 + ys * nx + xc, bw = zw * sw0 + yc * nx + xc;
+        f.u.prefetch(bu);
+        f.u.prefetch(bu + su1);
+        f.u.prefetch(bu + su0);
+        f.u.prefetch(bu + su0 + su1);
+        f.v.prefetch(bv);
+        f.v.prefetch(bv + nx);
+        f.v.prefetch(bv + sv0);
+        f.v.prefetch(bv + sv0 + nx);
+        f.w.prefetch(bw);
+        f.w.prefetch(bw + nx);
+        f.w.prefetch(bw + sw0);
+        f.w.prefetch(bw + sw0 + nx);
+        if constexpr (B::BUNDLED) {
+            f.dd.prefetch(yc * nx + xc);
+            f.dd.prefetch(yc * nx + xc + nx);
+        }
+    }
 }
 
 // rk2_w_advection.pyx:97-153 (stage 1 for one particle).  Returns false on a
@@ -348,6 +392,7 @@ __device__ __forceinline__ void rk2_update(S &s, const B &f, const Levels &L, co
     s.xidx = s.xidx + b1dt * k1x + b2dt * k2x;
     double h, zeta;
     hz_here(s, f, h, zeta);
+    prefetch_next<false>(s, f);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
     s.h_at = h;
     s.zeta_at = zeta;
@@ -449,11 +494,13 @@ __device__ __forceinline__ bool ab3_step(S &s, const B &f, const DScalars &sc, c
     return true;
 }
 
-// ab3_w_advection.pyx:214-229 (post step for one particle)
-template <typename B, typename S>
+// ab3_w_advection.pyx:214-229 (post step for one particle); W_CENTERED: the
+// w slot holds a field on rho points (the isopycnal follower's density)
+template <bool W_CENTERED = false, typename B, typename S>
 __device__ __forceinline__ void ab3_post(S &s, const B &f, const Levels &L, const DScalars &sc) {
     double h, zeta;
     hz_here(s, f, h, zeta);
+    prefetch_next<W_CENTERED>(s, f);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
     s.h_at = h;
     s.zeta_at = zeta;

@@ -806,9 +806,12 @@ class TimeDependentField(Field):
     @property
     def storage(self) -> str:
         """Device storage dtype of the snapshots: "float64", "float32", "bfloat16" or "float16"."""
-        if self._storage is None:
-            return str(self._data_dtype)
-        return {torch.bfloat16: "bfloat16", torch.float16: "float16"}[self._storage]
+        name = self.__dict__.get("_storage_name")
+        if name is None:
+            name = (str(self._data_dtype) if self._storage is None
+                    else {torch.bfloat16: "bfloat16", torch.float16: "float16"}[self._storage])
+            self.__dict__["_storage_name"] = name
+        return name
 
     @property
     def storage_bytes_per_snapshot(self) -> int:

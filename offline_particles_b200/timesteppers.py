@@ -13,6 +13,7 @@ identical to the stage-by-stage sequence.
 from __future__ import annotations
 
 import abc
+import bisect
 import ctypes
 import dataclasses
 import math
@@ -75,6 +76,16 @@ class Timestepper(abc.ABC):
 
     def get_time_index(self, time: T) -> np.float64:
         """timesteppers.py:64-85: searchsorted plus the fraction within the interval."""
+        fast = self._float_times()
+        if fast is not None and isinstance(time, (float, np.float64)):
+            # the same arithmetic on Python floats (IEEE doubles, as numpy's float64 scalars): bisect_right
+            # is searchsorted(side="right"), and int + float equals numpy's int64 + float64 for these sizes
+            if time < fast[0] or time > fast[-1]:
+                raise ValueError("Time is out of bounds of the time array.")
+            idx = bisect.bisect_right(fast, time) - 1
+            t0 = fast[idx]
+            t1 = fast[idx + 1]  # IndexError at the last time, as the numpy path raises
+            return np.float64(idx + (float(time) - t0) / (t1 - t0))
         time_array = self._time_array
         if time < time_array[0] or time > time_array[-1]:
             raise ValueError("Time is out of bounds of the time array.")
@@ -83,6 +94,16 @@ class Timestepper(abc.ABC):
         t1 = time_array[idx + 1]
         fraction = (time - t0) / (t1 - t0)
         return idx + fraction
+
+    def _float_times(self) -> list | None:
+        """The time array as Python floats when it is float64 (cached), else None."""
+        arr = self._time_array
+        cached = self.__dict__.get("_float_times_cache")
+        if cached is None or cached[0] is not arr:
+            fast = arr.tolist() if isinstance(arr, np.ndarray) and arr.dtype == np.float64 and arr.ndim == 1 else None
+            cached = (arr, fast)
+            self.__dict__["_float_times_cache"] = cached
+        return cached[1]
 
     def set_dt(self, dt: D) -> None:
         try:
@@ -320,6 +341,15 @@ def roms_geometry(launcher: Launcher, roles: dict[str, str] | None = None) -> bo
     exactly this geometry."""
     fs = launcher.fieldset
     roles = roles or {}
+    key = (tuple(sorted(roles.items())),
+           tuple((n, id(fs[roles.get(n, n)]) if roles.get(n, n) in fs else None) for n in _abi.ROMS_FIELDS))
+    cache = launcher.__dict__.setdefault("_roms_geometry_cache", {})
+    if key not in cache:
+        cache[key] = _roms_geometry(fs, roles)
+    return cache[key]
+
+
+def _roms_geometry(fs, roles: dict[str, str]) -> bool:
     nz, ny, nx = fs.z_size, fs.y_size, fs.x_size
     w_rho = roles.get("w", "w") != "w"
     want = {"u": ((nz, ny, nx - 1), (0.0, 0.0, -0.5)), "v": ((nz, ny - 1, nx), (0.0, -0.5, 0.0)),

@@ -43,7 +43,8 @@ def test_a_stuck_ticket_is_passed_over_once_then_ignored():
     order = TicketOrder(limit=5.0)
     stuck, a, b = order.ticket(), order.ticket(), order.ticket()
     t0 = time.perf_counter()
-    issued, results = _run(order, [(a, 0.0), (b, 0.0)], limit=0.2)
+    # b starts waiting later, so a's wait is the first to run out (both waits are 0.2 s)
+    issued, results = _run(order, [(a, 0.0), (b, 0.05)], limit=0.2)
     took = time.perf_counter() - t0
     assert issued == [a, b]
     assert results[a] is False and results[b] is True  # only the first waiter waits for the stuck one

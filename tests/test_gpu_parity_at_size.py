@@ -142,7 +142,7 @@ def test_batched_grid_releases_match_oracle():
     batch = ReleaseBatch(fs, rels, sort_interval=1, buckets=256)
     batch.run()
     batch.synchronize()
-    assert batch.graphs and batch.sorts > len(rels)
+    assert batch.graphs and batch.sorts >= 2 and batch.launches >= 3  # re-sorts between graph replays
     from oracle import oracle as O
 
     for q, (r, (scheme, t0, nsteps, n)) in enumerate(zip(rels, BATCH_SPECS)):
