@@ -425,6 +425,8 @@ def b200_arm(a) -> None:
     import torch
 
     import offline_particles_b200 as opb
+    from offline_particles_b200 import fields as fmod
+    from offline_particles_b200 import timesteppers
     from offline_particles_b200.sharding import Ranks
 
     ranks = Ranks()
@@ -504,24 +506,56 @@ def b200_arm(a) -> None:
     gc.collect()  # the warm-up simulation's teardown (reference cycles) stays out of the timed region
     sim3, fs3 = build_sim(grid_h, psrc, n, a, ring_size=a.ring_size)
     host = {}
+    # timeline of the region on the device: events on the compute stream, around every fused launch and
+    # after every snapshot upload (on the copy stream)
+    marks, uploads = {}, []
+    e2e_timer = LaunchTimer()
+
+    def on_upload(k, stream):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(stream)
+        uploads.append(ev)
+
+    def mark(name):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        marks[name] = ev
 
     def e2e():
+        mark("start")
         w0 = time.perf_counter()
         sim3.set_indices(hz, hy, hx)
         sim3.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+        mark("indices_in")
         w1 = time.perf_counter()
         sim3.run(a.steps)
+        mark("steps_done")
         w2 = time.perf_counter()
         P = sim3.device_particles
         for k in outs:
             outs[k].copy_(P.original(k), non_blocking=True)
+        mark("results_out")
         w3 = time.perf_counter()
         host.update(set_indices=(w1 - w0) * 1e3, run=(w2 - w1) * 1e3, collect=(w3 - w2) * 1e3)
+
+    fmod.upload_observers.append(on_upload)
+    timesteppers.launch_observers.append(e2e_timer)
 
     m0 = torch.cuda.memory_stats(dev)
     wall0 = time.perf_counter()
     e2e_dev_ms = ranks.timed_ms(e2e)
     wall_e2e = time.perf_counter() - wall0
+    fmod.upload_observers.remove(on_upload)
+    timesteppers.launch_observers.remove(e2e_timer)
+    t0 = marks["start"]
+    timeline = {k: t0.elapsed_time(v) for k, v in marks.items() if k != "start"}
+    if uploads:
+        timeline["uploads_done"] = max(t0.elapsed_time(u) for u in uploads)
+        timeline["uploads"] = len(uploads)
+    if e2e_timer.pairs:
+        timeline["first_launch_start"] = t0.elapsed_time(e2e_timer.pairs[0][0])
+        timeline["last_launch_end"] = t0.elapsed_time(e2e_timer.pairs[-1][1])
+        timeline["launches"] = len(e2e_timer.pairs)
     m1 = torch.cuda.memory_stats(dev)
     # device allocations inside the region (cudaMalloc calls, and retries that freed cached blocks first)
     e2e_alloc = {"cuda_mallocs": m1.get("segment.all.allocated", 0) - m0.get("segment.all.allocated", 0),
@@ -613,7 +647,7 @@ def b200_arm(a) -> None:
                 "path": "Simulation.set_indices from pinned host + run(K) streaming every snapshot from pinned "
                         "host memory + D2H of zidx/yidx/xidx/status",
                 "h2d_gbs_measured": h2d_gbs, "device_ms": e2e_dev_ms, "wall_ms": wall_e2e * 1e3,
-                "host_ms": host, "allocator": e2e_alloc,
+                "host_ms": host, "allocator": e2e_alloc, "timeline_ms": timeline,
                 "h2d_bound_value": total / ((h2d + d2h) / (h2d_gbs * 1e9)) if h2d_gbs else None},
         "roofline": roof,
         "gpu_launches": len(launch_ms) + 2 * len(cnt.sorts) + len(cnt.builds),

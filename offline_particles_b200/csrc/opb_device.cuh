@@ -167,16 +167,6 @@ struct View {
         return (double)(x + y);
     }
 
-    // an L1 prefetch of the element that holds the value at i (pair and wider layouts)
-    __device__ __forceinline__ void prefetch(I i) const {
-        const void *q;
-        if constexpr (KIND == KIND_OCTS) q = (const char *)prev + 32 * (long long)i;
-        else if constexpr (KIND == KIND_QUADS) q = (const char *)prev + 16 * (long long)i;
-        else if constexpr (KIND == KIND_PAIRS) q = (const char *)prev + 2 * sizeof(T) * (long long)i;
-        else q = prev + i;
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
-    }
-
     __device__ __forceinline__ double at(I i) const {
         if constexpr (KIND == KIND_YXPAIRS) {
             return __ldg(stat + 4 * (long long)i);
@@ -280,7 +270,6 @@ struct DxDyView {
     const D4 *p;
     I n0, n1;
     double o0, o1;
-    __device__ __forceinline__ void prefetch(I i) const { asm volatile("prefetch.global.L1 [%0];" ::"l"(p + i)); }
     // dx and dy at i and i + 1
     __device__ __forceinline__ void at2(I i, double &a0, double &b0, double &a1, double &b1) const {
         const D4 w = ldg256(p + i);

@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_ab3_steps(const __gr
             break;
         }
         moved = true;
-        ab3_post<ISO>(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t2), L, sc);
+        ab3_post(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t2), L, sc);
     }
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;

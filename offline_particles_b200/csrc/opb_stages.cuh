@@ -261,46 +261,6 @@ __device__ __forceinline__ double C_ax(const B &f, const Levels &L, const Axis<I
     return linear_ax(L.C, zc);
 }
 
-// Compiled layout, OPB_PREFETCH_NEXT: before the vertical search of a step's
-// last stage, prefetch into L1 the stencil rows the next step's first stage
-// will gather, predicting its vertical cell from the current level (a particle
-// changes level rarely in one step).  A prefetch moves no value into a
-// register and changes no result; a wrong prediction only wastes it.
-#ifndef OPB_PREFETCH_NEXT
-#define OPB_PREFETCH_NEXT 0
-#endif
-
-template <bool W_CENTERED, typename B, typename S>
-__device__ __forceinline__ void prefetch_next(const S &s, const B &f) {
-    if constexpr (B::kFixed && OPB_PREFETCH_NEXT && B::KT != KIND_TD) {
-        using I = typename B::index_type;
-        const I nz = f.nz, ny = f.ny, nx = f.nx;
-        const I zc = trunc_index(s.zidx + 0.0, (I)(nz - 2));
-        const I zw = W_CENTERED ? zc : trunc_index(s.zidx + 0.5, (I)(nz - 1));
-        const I ys = trunc_index(s.yidx + -0.5, (I)(ny - 3));
-        const I xs = trunc_index(s.xidx + -0.5, (I)(nx - 3));
-        const I yc = s.ya.i, xc = s.xa.i;
-        const I su1 = nx - 1, su0 = f.su0, sv0 = f.sv0, sw0 = f.sw0;
-        const I bu = zc * su0 + yc * su1 + xs, bv = zc * sv0 + ys * nx + xc, bw = zw * sw0 + yc * nx + xc;
-        f.u.prefetch(bu);
-        f.u.prefetch(bu + su1);
-        f.u.prefetch(bu + su0);
-        f.u.prefetch(bu + su0 + su1);
-        f.v.prefetch(bv);
-        f.v.prefetch(bv + nx);
-        f.v.prefetch(bv + sv0);
-        f.v.prefetch(bv + sv0 + nx);
-        f.w.prefetch(bw);
-        f.w.prefetch(bw + nx);
-        f.w.prefetch(bw + sw0);
-        f.w.prefetch(bw + sw0 + nx);
-        if constexpr (B::BUNDLED) {
-            f.dd.prefetch(yc * nx + xc);
-            f.dd.prefetch(yc * nx + xc + nx);
-        }
-    }
-}
-
 // rk2_w_advection.pyx:97-153 (stage 1 for one particle).  Returns false on a
 // zero grid spacing (the reference raises ZeroDivisionError).  `carried`: the
 // state's rho-point axes describe the current position (compiled layout);
@@ -392,7 +352,6 @@ __device__ __forceinline__ void rk2_update(S &s, const B &f, const Levels &L, co
     s.xidx = s.xidx + b1dt * k1x + b2dt * k2x;
     double h, zeta;
     hz_here(s, f, h, zeta);
-    prefetch_next<false>(s, f);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
     s.h_at = h;
     s.zeta_at = zeta;
@@ -494,13 +453,11 @@ __device__ __forceinline__ bool ab3_step(S &s, const B &f, const DScalars &sc, c
     return true;
 }
 
-// ab3_w_advection.pyx:214-229 (post step for one particle); W_CENTERED: the
-// w slot holds a field on rho points (the isopycnal follower's density)
-template <bool W_CENTERED = false, typename B, typename S>
+// ab3_w_advection.pyx:214-229 (post step for one particle)
+template <typename B, typename S>
 __device__ __forceinline__ void ab3_post(S &s, const B &f, const Levels &L, const DScalars &sc) {
     double h, zeta;
     hz_here(s, f, h, zeta);
-    prefetch_next<W_CENTERED>(s, f);
     s.zidx = compute_zidx_hint(s.z, h, zeta, sc.hc, L, s.zidx);
     s.h_at = h;
     s.zeta_at = zeta;

@@ -36,6 +36,9 @@ from .spatial_arrays import BBox, DeviceArray, SpatialArray, Stagger
 # Observers of snapshot pair/quad/octet builds: callables run after each build launch (used for counting
 # launches).
 pair_observers: list = []
+# Observers of snapshot uploads: callables obs(k, copy_stream) run right after a snapshot's copy is queued
+# on the copy stream (for timelines; they may record an event on that stream)
+upload_observers: list = []
 # elements of the storage dtype per grid element in each pair layout
 PAIR_WIDTH = {"pairs": 2, "quads": 4, "octets": 8, "zeta_h": 8}
 
@@ -397,6 +400,13 @@ class SnapshotRing:
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=1, thread_name_prefix="opb-snapshots")
         self.lock = threading.Lock()
         self.h2d_bytes = 0
+        # start the worker now and bind it to the device, so that the first upload does not pay for a
+        # thread start and a first CUDA call
+        self.pool.submit(self._bind_worker).result()
+
+    def _bind_worker(self) -> None:
+        torch.cuda.set_device(self.device)
+        torch.cuda.Event().record(self.copy_stream)
 
     def _host_snapshot(self, k: int) -> np.ndarray:
         src = self.source
@@ -451,6 +461,8 @@ class SnapshotRing:
                 self._to_slot(slot, src[k])
                 ev = torch.cuda.Event()
                 ev.record(self.copy_stream)
+                for obs in upload_observers:
+                    obs(k, self.copy_stream)
             self.ready[k] = ev
             if not src.is_cuda:
                 self.h2d_bytes += src[k].numel() * src.element_size()
@@ -473,6 +485,8 @@ class SnapshotRing:
                 self._to_slot(slot, stage)
                 ev = torch.cuda.Event()
                 ev.record(self.copy_stream)
+                for obs in upload_observers:
+                    obs(k, self.copy_stream)
             self.staging_free[b] = ev
             self.ready[k] = ev
             self.h2d_bytes += stage.numel() * stage.element_size()
