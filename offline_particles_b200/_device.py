@@ -19,8 +19,17 @@ def cuda_device(device=None) -> torch.device:
     return dev
 
 
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def stream_handle(device: torch.device | None = None) -> int:
-    """cudaStream_t of the current torch stream on ``device``."""
+    """cudaStream_t of the current torch stream on ``device`` (the raw-handle query where torch offers
+    it: the launch path asks for it several times per launch)."""
+    if _raw_stream is not None:
+        index = device.index if isinstance(device, torch.device) and device.index is not None else (
+            torch.cuda.current_device() if device is None else torch.device(device).index)
+        if index is not None:
+            return _raw_stream(index)
     return torch.cuda.current_stream(device).cuda_stream
 
 

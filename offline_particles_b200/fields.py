@@ -636,6 +636,7 @@ class TimeDependentField(Field):
         self._output_dtype = output_dtype
         self._num_timesteps = int(data.shape[0])
         self._spatial_shape = tuple(int(s) for s in data.shape[1:])
+        self._elements = int(np.prod(self._spatial_shape))
         self._device = cuda_device(device)
         self._prefetch = max(0, int(prefetch))
         if storage not in STORAGE:
@@ -760,7 +761,7 @@ class TimeDependentField(Field):
             raise IndexError(k)
         pc = self._pair_caches.setdefault(layout, _PairCache())
         if layout == "zeta_h":
-            if static is None or static.numel() != int(np.prod(self._spatial_shape)):
+            if static is None or static.numel() != self._elements:
                 raise ValueError("a zeta_h bundle needs the static field of the same shape")
             if pc.tag != static.data_ptr():  # bundled with another static field: rebuild every bundle
                 if pc.free is not None:
@@ -773,7 +774,7 @@ class TimeDependentField(Field):
             return cache[k]
         if pc.free is None:
             # every buffer at once, on first use: a large allocation later could synchronise the device
-            n = int(np.prod(self._spatial_shape))
+            n = self._elements
             pc.store = torch.empty((self._pair_slots, width * n), dtype=torch_dtype(self._data_dtype),
                                    device=self._device)
             pc.free = list(pc.store.unbind(0))

@@ -127,14 +127,19 @@ class Particles(_FrozenArrayMapping):
             raise RuntimeError(f"device error word 0x{value:x}")
 
     # ---------------------------------------------------------- original order
-    def original(self, name: str) -> torch.Tensor:
-        """A device copy of field ``name`` in the particles' original order."""
+    def original(self, name: str, out: torch.Tensor | None = None) -> torch.Tensor:
+        """A device copy of field ``name`` in the particles' original order (into ``out`` when given: a
+        device tensor of the field's shape and dtype, so that repeated reads allocate nothing)."""
         t = self.arrays[name]
+        if out is None:
+            out = torch.empty_like(t)
+        elif out.shape != t.shape or out.dtype != t.dtype or out.device != t.device:
+            raise ValueError(f"out must be a {t.dtype} tensor of shape {tuple(t.shape)} on {t.device}")
         order = self.order
         if order is None:
-            return t.clone()
-        out = torch.empty_like(t)
-        out.index_copy_(0, order, t)
+            out.copy_(t)
+        else:
+            out.index_copy_(0, order, t)
         return out
 
     def assign(self, name: str, values: torch.Tensor) -> None:
@@ -145,6 +150,20 @@ class Particles(_FrozenArrayMapping):
         t.copy_(values if order is None else values.index_select(0, order))
 
     # ------------------------------------------------------------- reordering
+    def reserve_sort(self) -> None:
+        """Allocate the sort's scratch now (key workspace, permutation, a second copy of every field), so
+        that the first ``sort`` allocates nothing."""
+        from . import _lib
+
+        n = len(self)
+        if n == 0 or object.__getattribute__(self, "_workspace") is not None:
+            return
+        lib = _lib.load()
+        ws = torch.empty(int(lib.opb_sort_workspace_bytes(n)), dtype=torch.uint8, device=self.device)
+        object.__setattr__(self, "_workspace", ws)
+        object.__setattr__(self, "_perm", torch.empty(n, dtype=torch.int32, device=self.device))
+        object.__setattr__(self, "_spare", {k: torch.empty_like(v) for k, v in self.arrays.items()})
+
     def sort(self, shape: tuple[int, int, int]) -> None:
         """Reorder storage by the Morton code of each particle's cell on the centred ``(z, y, x)`` grid."""
         from . import _lib
@@ -153,12 +172,7 @@ class Particles(_FrozenArrayMapping):
         n = len(self)
         if n == 0:
             return
-        lib = _lib.load()
-        if object.__getattribute__(self, "_workspace") is None:
-            ws = torch.empty(int(lib.opb_sort_workspace_bytes(n)), dtype=torch.uint8, device=self.device)
-            object.__setattr__(self, "_workspace", ws)
-            object.__setattr__(self, "_perm", torch.empty(n, dtype=torch.int32, device=self.device))
-            object.__setattr__(self, "_spare", {k: torch.empty_like(v) for k, v in self.arrays.items()})
+        self.reserve_sort()
         ws = object.__getattribute__(self, "_workspace")
         perm = object.__getattribute__(self, "_perm")
         spare = object.__getattribute__(self, "_spare")

@@ -56,6 +56,8 @@ class Simulation:
         self._particles_view = ParticlesView(self._particles)
         self._sort_interval = int(sort_interval)
         self._steps_since_sort: int | None = None  # None: never sorted
+        if self._sort_interval > 0:
+            self._particles.reserve_sort()  # the sort's scratch now, not inside the first run
         self._invoke_events()
 
     @property

@@ -496,18 +496,37 @@ def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: 
     else:
         slot = {k: j for j, k in enumerate(needed)}
         prev_next = lambda It: (slot[It], slot[It + 1])  # noqa: E731
-    table = (_lib.opb_time * len(entries))()
-    for j, tidx in enumerate(entries):
-        It, ft = divmod(tidx, 1)
-        It = int(It)
-        ft = dtype.type(ft)
-        gt = dtype.type(1 - ft)
-        table[j] = _lib.opb_time(*prev_next(It), float(ft), float(gt))
-    # move the field windows the way the stage launches would have
+    table, its = step_table(entries, dtype, prev_next)
+    # move the field windows the way the stage launches would have (each distinct index in order)
+    seq = [i for j, i in enumerate(its) if j == 0 or i != its[j - 1]]
     for field in td.values():
-        for tidx in entries:
-            field.set_time_index(int(divmod(tidx, 1)[0]))
+        for i in seq:
+            field.set_time_index(i)
     return rf, table
+
+
+def step_table(entries, dtype, prev_next):
+    """The opb_time table of a fused launch and the snapshot index of each entry.  Per entry (a time index
+    tidx): It, ft = divmod(tidx, 1); ft and gt = 1 - ft rounded to the storage ``dtype``
+    (fields.py:423-424); (prev, next) = prev_next(It).  The numpy operations of that scalar form, applied
+    to the whole table at once."""
+    It_f, fr = np.divmod(np.asarray(entries, dtype=np.float64), 1.0)
+    ft = fr.astype(dtype)
+    gt = dtype.type(1) - ft
+    its = It_f.astype(np.int64).tolist()
+    rec = np.empty(len(its), dtype=_TIME_DTYPE)
+    if its:
+        rec["prev"], rec["next"] = zip(*(prev_next(i) for i in its))
+    rec["ft"] = ft.astype(np.float64)
+    rec["gt"] = gt.astype(np.float64)
+    table = (_lib.opb_time * len(its))()
+    ctypes.memmove(table, rec.ctypes.data, rec.nbytes)
+    return table, its
+
+
+# opb_time as a numpy record (int32 prev, int32 next, float64 ft, float64 gt: 24 bytes, no padding)
+_TIME_DTYPE = np.dtype([("prev", np.int32), ("next", np.int32), ("ft", np.float64), ("gt", np.float64)])
+assert _TIME_DTYPE.itemsize == ctypes.sizeof(_lib.opb_time)
 
 
 def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDependentField],
@@ -552,9 +571,19 @@ def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDepen
                 f.shape[d] = shape[d]
                 f.offset[d] = offsets[d]
         else:
-            f = _abi.field_struct(field.get_field_data(0.0), _abi.ROMS_NDIM[name], name)
+            f = _static_struct(field, name)
         setattr(rf, name, f)
     return rf, dtype
+
+
+def _static_struct(field, name: str):
+    """opb_field of a static field (built once per field and slot name; ctypes copies it into each
+    launch's struct)."""
+    cache = field.__dict__.setdefault("_opb_structs", {})
+    f = cache.get(name)
+    if f is None:
+        f = cache[name] = _abi.field_struct(field.get_field_data(0.0), _abi.ROMS_NDIM[name], name)
+    return f
 
 
 _STORAGE_CODE = {"float64": _lib.F64, "float32": _lib.F32, "bfloat16": _lib.BF16, "float16": _lib.F16}

@@ -102,3 +102,30 @@ def test_dt_longer_than_the_snapshot_spacing_stops_the_release():
     planner = IntervalPlanner(t_arr, 10)
     exps, _ = planner.plan([r], 0)
     assert not exps and r.done == 0 and isinstance(r.error, IndexError)
+
+
+def test_step_table_equals_the_scalar_form():
+    """The vectorised step table of the fused launches equals, bit for bit, the table built entry by entry
+    as the stage launches' blend weights are (fields.py:423-424)."""
+    import ctypes
+
+    import numpy as np
+
+    from offline_particles_b200 import _lib
+    from offline_particles_b200.timesteppers import step_table
+
+    rng = np.random.default_rng(3)
+    for dtype in (np.dtype(np.float32), np.dtype(np.float64)):
+        entries = [np.float64(v) for v in np.concatenate([rng.uniform(0, 40, 500), np.arange(0, 12, 0.25),
+                                                           [3.0 - 2 ** -40, 7.0, 1e-18]])]
+        slot = {k: k % 8 for k in range(64)}
+        table, its = step_table(entries, dtype, lambda It: (slot[It], slot[It + 1]))
+        for j, tidx in enumerate(entries):
+            It, ft = divmod(tidx, 1)
+            It = int(It)
+            ft = dtype.type(ft)
+            gt = dtype.type(1 - ft)
+            want = _lib.opb_time(slot[It], slot[It + 1], float(ft), float(gt))
+            assert its[j] == It
+            assert bytes(table[j]) == bytes(want), (j, tidx)
+        assert ctypes.sizeof(table) == len(entries) * ctypes.sizeof(_lib.opb_time)
