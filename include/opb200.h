@@ -399,6 +399,19 @@ size_t opb_sort_workspace_bytes(int64_t n);
  * of at least opb_sort_workspace_bytes(n) bytes, used as scratch. */
 int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *perm, void *workspace,
                        size_t workspace_bytes, void *stream);
+/* As opb_sort_particles, within id ranges: the particle in slot i has id
+ * ids[i] (int64, DEVICE; NULL: id = i), and the particles with ids in
+ * [bounds[r], bounds[r + 1]) are ordered among themselves into the positions
+ * [bounds[r], bounds[r + 1]).  bounds: HOST array of nranges + 1 increasing
+ * values from 0 to n, nranges 1 to 4 (the range index takes the top two bits
+ * of the cell key).  With ids a permutation of 0..n-1 whose range r occupies
+ * those slots already (an earlier call with the same bounds, or the identity),
+ * every particle stays in its range: a caller can then read back the particles
+ * of one range as soon as the launches over its slots are done.  Same
+ * workspace as opb_sort_particles. */
+int opb_sort_particles_ranges(const opb_particles *p, const int64_t shape[3], const int64_t *ids,
+                              const int64_t *bounds, int32_t nranges, int32_t *perm, void *workspace,
+                              size_t workspace_bytes, void *stream);
 /* dst.f[j] = src.f[perm[j]] for status and every float64 field present in
  * both (src and dst must not alias), and dst_ids[j] = src_ids[perm[j]] when
  * id arrays are given. */

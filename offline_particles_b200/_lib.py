@@ -125,6 +125,8 @@ SIGNATURES = {
 
 SIGNATURES_OTHER = {
     "opb_sort_particles": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
+    "opb_sort_particles_ranges": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP, ctypes.c_int32, _VP,
+                                   _VP, ctypes.c_size_t, _VP], ctypes.c_int),
     "opb_gather_particles": ([_P(opb_particles), _P(opb_particles), _VP, _VP, _VP, _VP], ctypes.c_int),
     "opb_sort_workspace_bytes": ([ctypes.c_int64], ctypes.c_size_t),
     "opb_sort_particles_noalloc": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP], ctypes.c_int),

@@ -21,6 +21,8 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr uint32_t kInactiveKey = 0xFFFFFFFFu;
+constexpr uint32_t kRangeKeyMask = 0x3FFFFFFFu;  // the cell key below the two range bits
+constexpr int kMaxRanges = 4;
 
 // spread the low 10 bits of v to every third bit
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {
@@ -45,6 +47,12 @@ struct KeyArgs {
     long long n;
     int nz, ny, nx;
     int sz, sy, sx;  // right shifts that bring each dimension under 2^10 (x additionally by 2)
+    // id ranges kept in place (opb_sort_particles_ranges): with nbounds > 0 the particle whose id
+    // (range_ids[i], or i without ids) is in [bound[r - 1], bound[r]) (bound[-1] = 0, bound[nbounds] =
+    // n) sorts into the storage slots of that range
+    const int64_t *range_ids;
+    long long bound[kMaxRanges - 1];
+    int nbounds;
 };
 
 __global__ void __launch_bounds__(kBlock) k_cell_keys(KeyArgs a, uint32_t *keys, int32_t *ids) {
@@ -58,6 +66,14 @@ __global__ void __launch_bounds__(kBlock) k_cell_keys(KeyArgs a, uint32_t *keys,
         // x in the lowest bit of each triple: boxes of a Morton range are elongated along x,
         // the contiguous dimension of every field
         key = (spread3(z) << 2) | (spread3(y) << 1) | spread3(x);
+    }
+    if (a.nbounds > 0) {
+        // the cell key fits 30 bits (three spread 10-bit values); the range index takes the top two, and
+        // an inactive particle sorts last within its range
+        const long long id = a.range_ids ? a.range_ids[i] : i;
+        uint32_t r = 0;
+        for (int j = 0; j < a.nbounds; ++j) r += id >= a.bound[j] ? 1u : 0u;
+        key = (r << 30) | (key & kRangeKeyMask);
     }
     keys[i] = key;
     ids[i] = (int32_t)i;
@@ -298,19 +314,32 @@ size_t opb_sort_workspace_bytes(int64_t n) {
     return 3 * align256((size_t)n * 4) + align256(cub_temp_bytes(n));
 }
 
-int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *perm, void *workspace,
-                       size_t workspace_bytes, void *stream) {
-    if (!p) return fail(OPB_EINVAL, "opb_sort_particles: particles is NULL");
-    if (p->n < 0 || p->n > 0x7fffffffLL) return fail(OPB_EINVAL, "opb_sort_particles: particle count out of range");
+}  // extern "C"
+
+namespace {
+
+// opb_sort_particles, and with nranges > 1 opb_sort_particles_ranges (bounds: nranges + 1 host values)
+int sort_particles(const char *what, const opb_particles *p, const int64_t shape[3], const int64_t *range_ids,
+                   const int64_t *bounds, int nranges, int32_t *perm, void *workspace, size_t workspace_bytes,
+                   void *stream) {
+    if (!p) return fail(OPB_EINVAL, "%s: particles is NULL", what);
+    if (p->n < 0 || p->n > 0x7fffffffLL) return fail(OPB_EINVAL, "%s: particle count out of range", what);
     if (p->n == 0) return OPB_OK;
     if (!p->status || !p->zidx || !p->yidx || !p->xidx || !perm || !shape)
-        return fail(OPB_EINVAL, "opb_sort_particles: NULL argument");
+        return fail(OPB_EINVAL, "%s: NULL argument", what);
     if (shape[0] < 1 || shape[1] < 1 || shape[2] < 1 || shape[0] > (1 << 30) || shape[1] > (1 << 30) ||
         shape[2] > (1 << 30))
-        return fail(OPB_EINVAL, "opb_sort_particles: bad grid shape");
+        return fail(OPB_EINVAL, "%s: bad grid shape", what);
+    if (nranges > 1) {
+        if (!bounds || nranges > kMaxRanges) return fail(OPB_EINVAL, "%s: 1 to %d ranges", what, kMaxRanges);
+        if (bounds[0] != 0 || bounds[nranges] != p->n)
+            return fail(OPB_EINVAL, "%s: the range bounds must run from 0 to the particle count", what);
+        for (int r = 0; r < nranges; ++r)
+            if (bounds[r + 1] <= bounds[r]) return fail(OPB_EINVAL, "%s: the range bounds must increase", what);
+    }
     const size_t need = opb_sort_workspace_bytes(p->n);
     if (!workspace || workspace_bytes < need)
-        return fail(OPB_EINVAL, "opb_sort_particles: workspace of %zu bytes is smaller than the %zu needed",
+        return fail(OPB_EINVAL, "%s: workspace of %zu bytes is smaller than the %zu needed", what,
                     workspace_bytes, need);
     const size_t a = align256((size_t)p->n * 4);
     char *ws = (char *)workspace;
@@ -319,7 +348,7 @@ int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *
     int32_t *ids_in = (int32_t *)(ws + 2 * a);
     void *temp = ws + 3 * a;
     size_t temp_bytes = workspace_bytes - 3 * a;
-    KeyArgs k;
+    KeyArgs k{};
     k.status = p->status;
     k.zidx = p->zidx;
     k.yidx = p->yidx;
@@ -331,15 +360,39 @@ int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *
     k.sz = shift_for(k.nz, 0);
     k.sy = shift_for(k.ny, 0);
     k.sx = shift_for(k.nx, 2);
+    k.range_ids = range_ids;
+    k.nbounds = nranges > 1 ? nranges - 1 : 0;
+    for (int j = 0; j < k.nbounds; ++j) k.bound[j] = bounds[j + 1];
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned grid = (unsigned)((p->n + kBlock - 1) / kBlock);
     k_cell_keys<<<grid, kBlock, 0, st>>>(k, keys_in, ids_in);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
     e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, ids_in, perm, (int)p->n, 0, 32, st);
-    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles: radix sort: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: radix sort: %s", what, cudaGetErrorString(e));
     opb::clear_error();
     return OPB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *perm, void *workspace,
+                       size_t workspace_bytes, void *stream) {
+    return sort_particles("opb_sort_particles", p, shape, nullptr, nullptr, 1, perm, workspace, workspace_bytes,
+                          stream);
+}
+
+int opb_sort_particles_ranges(const opb_particles *p, const int64_t shape[3], const int64_t *ids,
+                              const int64_t *bounds, int32_t nranges, int32_t *perm, void *workspace,
+                              size_t workspace_bytes, void *stream) {
+    if (nranges < 1 || nranges > kMaxRanges || !bounds)
+        return fail(OPB_EINVAL, "opb_sort_particles_ranges: 1 to %d ranges and their bounds", kMaxRanges);
+    if (p && p->n > 0 && nranges == 1 && (bounds[0] != 0 || bounds[1] != p->n))
+        return fail(OPB_EINVAL, "opb_sort_particles_ranges: the range bounds must run from 0 to the particle count");
+    return sort_particles("opb_sort_particles_ranges", p, shape, ids, bounds, nranges, perm, workspace,
+                          workspace_bytes, stream);
 }
 
 int opb_gather_particles(const opb_particles *src, const opb_particles *dst, const int32_t *perm,
@@ -426,7 +479,7 @@ int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int6
     }
     cudaError_t e = stage_to_device(ws + L.seg, seg.data(), seg.size() * 8, st);
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
-    SegArgs a;
+    SegArgs a{};
     a.k.status = p->status;
     a.k.zidx = p->zidx;
     a.k.yidx = p->yidx;
@@ -584,7 +637,7 @@ extern "C" int opb_sort_particles_noalloc(const opb_particles *p, const int64_t 
     if (temp_bytes > OPB_NOALLOC_CUB_TEMP_BYTES)
         return fail(OPB_EINVAL, "opb_sort_particles_noalloc: radix sort needs %zu temporary bytes, the static "
                     "scratch reserves %zu", temp_bytes, (size_t)OPB_NOALLOC_CUB_TEMP_BYTES);
-    KeyArgs k;
+    KeyArgs k{};
     k.status = p->status;
     k.zidx = p->zidx;
     k.yidx = p->yidx;

@@ -759,7 +759,7 @@ class TimeDependentField(Field):
             raise ValueError("snapshot quads and octets hold float32 storage only")
         if k < 0 or k + 1 >= self._num_timesteps:
             raise IndexError(k)
-        pc = self._pair_caches.setdefault(layout, _PairCache())
+        pc = self._reserve_pair_buffers(layout)
         if layout == "zeta_h":
             if static is None or static.numel() != self._elements:
                 raise ValueError("a zeta_h bundle needs the static field of the same shape")
@@ -772,12 +772,6 @@ class TimeDependentField(Field):
         if k in cache:
             cache.move_to_end(k)
             return cache[k]
-        if pc.free is None:
-            # every buffer at once, on first use: a large allocation later could synchronise the device
-            n = self._elements
-            pc.store = torch.empty((self._pair_slots, width * n), dtype=torch_dtype(self._data_dtype),
-                                   device=self._device)
-            pc.free = list(pc.store.unbind(0))
         if pc.free:
             buf = pc.free.pop()
         else:
@@ -809,6 +803,26 @@ class TimeDependentField(Field):
             obs()
         cache[k] = buf
         return buf
+
+    def _reserve_pair_buffers(self, layout: str) -> _PairCache:
+        """The pair cache of ``layout`` with all ``pair_slots`` buffers allocated: every buffer at once,
+        since a large allocation between launches can synchronise the device."""
+        pc = self._pair_caches.setdefault(layout, _PairCache())
+        if pc.free is None:
+            width = PAIR_WIDTH[layout]
+            pc.store = torch.empty((self._pair_slots, width * self._elements), dtype=torch_dtype(self._data_dtype),
+                                   device=self._device)
+            pc.free = list(pc.store.unbind(0))
+        return pc
+
+    def reserve_pairs(self, layout: str = "pairs") -> None:
+        """Allocate the device buffers of ``pair(..., layout=layout)`` now (``pair_slots`` of them), so
+        that the first pair build allocates nothing."""
+        if PAIR_WIDTH.get(layout) is None:
+            raise ValueError(f"unknown pair layout {layout!r}")
+        if self._storage is not None:
+            raise ValueError("snapshot pairs hold float32/float64 storage only")
+        self._reserve_pair_buffers(layout)
 
     def snapshot_scales(self, k: int) -> torch.Tensor | None:
         """Per-level scales of resident snapshot ``k`` (None for unscaled storage)."""

@@ -60,6 +60,20 @@ def particles_struct(particles) -> _lib.opb_particles:
     return s
 
 
+def particles_struct_range(particles, lo: int, hi: int) -> _lib.opb_particles:
+    """opb_particles over storage slots ``[lo, hi)`` of a Particles object (the same arrays, offset; the
+    error word is shared)."""
+    full = particles_struct(particles)
+    if not 0 <= lo <= hi <= full.n:
+        raise ValueError(f"slots [{lo}, {hi}) outside 0..{full.n}")
+    s = _lib.opb_particles(n=hi - lo, err=full.err)
+    s.status = None if full.status is None else full.status + lo
+    for name in ("rho_t", *(p.lstrip("_") for p in _lib.PARTICLE_POINTERS)):
+        ptr = getattr(full, name)
+        setattr(s, name, None if ptr is None else ptr + 8 * lo)
+    return s
+
+
 def scalars_struct(scalars: Mapping[str, object]) -> _lib.opb_scalars:
     s = _lib.opb_scalars()
     s.hc = float(scalars.get("hc", 0.0))

@@ -82,7 +82,7 @@ class _FrozenArrayMapping:
 class Particles(_FrozenArrayMapping):
     """``nparticles`` particles with the given ``field=dtype`` arrays, zero-initialised on the device."""
 
-    __slots__ = ("_length", "_device", "_err", "_abi_cache", "_order", "_spare", "_perm", "_workspace")
+    __slots__ = ("_length", "_device", "_err", "_abi_cache", "_order", "_spare", "_perm", "_workspace", "_range")
 
     def __init__(self, nparticles: int, *, device=None, **fields) -> None:
         dev = cuda_device(device)
@@ -97,6 +97,7 @@ class Particles(_FrozenArrayMapping):
         object.__setattr__(self, "_spare", None)
         object.__setattr__(self, "_perm", None)
         object.__setattr__(self, "_workspace", None)
+        object.__setattr__(self, "_range", None)  # id bounds kept by the last sort (None: none)
 
     def __len__(self) -> int:
         return object.__getattribute__(self, "_length")
@@ -164,14 +165,34 @@ class Particles(_FrozenArrayMapping):
         object.__setattr__(self, "_perm", torch.empty(n, dtype=torch.int32, device=self.device))
         object.__setattr__(self, "_spare", {k: torch.empty_like(v) for k, v in self.arrays.items()})
 
-    def sort(self, shape: tuple[int, int, int]) -> None:
-        """Reorder storage by the Morton code of each particle's cell on the centred ``(z, y, x)`` grid."""
+    @property
+    def sort_bounds(self) -> tuple[int, ...] | None:
+        """The id ranges the storage order keeps (``sort(shape, id_bounds=...)``): the particles with
+        original ids in ``[b[r], b[r + 1])`` occupy those storage slots.  None after a sort without
+        ranges; () while storage order is the original order (any ranges hold)."""
+        if self.order is None:
+            return ()
+        return object.__getattribute__(self, "_range")
+
+    def sort(self, shape: tuple[int, int, int], id_bounds: tuple[int, ...] | None = None) -> None:
+        """Reorder storage by the Morton code of each particle's cell on the centred ``(z, y, x)`` grid.
+        ``id_bounds``: 0 = b0 < b1 < ... < bR = n, R at most 4: order within the id ranges
+        ``[b[r], b[r + 1])`` (``opb_sort_particles_ranges``), each kept in those storage slots, so that
+        each range's results can be read back on their own."""
         from . import _lib
         from .kernels import _abi
 
         n = len(self)
         if n == 0:
             return
+        if id_bounds is not None:
+            id_bounds = tuple(int(b) for b in id_bounds)
+            R = len(id_bounds) - 1
+            if not 1 <= R <= 4 or id_bounds[0] != 0 or id_bounds[-1] != n or any(
+                    b >= c for b, c in zip(id_bounds, id_bounds[1:])):
+                raise ValueError(f"id_bounds must rise from 0 to {n} in 1 to 4 steps, got {id_bounds}")
+            if self.sort_bounds not in ((), id_bounds):
+                raise ValueError("storage order keeps other id ranges; sort without ranges first")
         self.reserve_sort()
         ws = object.__getattribute__(self, "_workspace")
         perm = object.__getattribute__(self, "_perm")
@@ -179,9 +200,15 @@ class Particles(_FrozenArrayMapping):
         src = _abi.particles_struct(self)
         dims = (ctypes.c_int64 * 3)(*[int(s) for s in shape])
         stream = stream_handle(self.device)
-        _lib.call("opb_sort_particles", ctypes.byref(src), ctypes.byref(dims), perm.data_ptr(), ws.data_ptr(),
-                  ws.numel(), stream)
         order = self.order
+        if id_bounds is None:
+            _lib.call("opb_sort_particles", ctypes.byref(src), ctypes.byref(dims), perm.data_ptr(), ws.data_ptr(),
+                      ws.numel(), stream)
+        else:
+            bounds = (ctypes.c_int64 * len(id_bounds))(*id_bounds)
+            _lib.call("opb_sort_particles_ranges", ctypes.byref(src), ctypes.byref(dims),
+                      None if order is None else order.data_ptr(), bounds, len(id_bounds) - 1, perm.data_ptr(),
+                      ws.data_ptr(), ws.numel(), stream)
         if order is None:
             order = torch.arange(n, dtype=torch.int64, device=self.device)
         new_order = torch.empty_like(order)
@@ -200,6 +227,7 @@ class Particles(_FrozenArrayMapping):
         object.__setattr__(self, "_arrays", types.MappingProxyType(dict(spare)))
         object.__setattr__(self, "_spare", old)
         object.__setattr__(self, "_order", new_order)
+        object.__setattr__(self, "_range", id_bounds)
         object.__setattr__(self, "_abi_cache", None)
         for obs in sort_observers:
             obs()

@@ -231,18 +231,42 @@ class Timestepper(abc.ABC):
         except (ValueError, IndexError):
             return None
 
-    def timestep_particles_many(self, particles, launcher: Launcher, nsteps: int) -> None:
-        """Advance ``nsteps`` steps; fused launches where possible, else step by step."""
+    def reserve_launch_buffers(self, launcher: Launcher, nparticles: int) -> None:
+        """Allocate what the fused launches over ``nparticles`` particles will read besides the snapshots
+        (the snapshot-pair buffers; the static bundles or neighbour layouts, built once), so that no
+        launch allocates device memory."""
+        if not self.fused():
+            return
+        roles = self.field_roles
+        td = _time_dependent_fields(launcher, roles)
+        if not use_pairs(launcher, td, nparticles, roles):
+            return
+        plan = pair_layout(launcher, td, roles)
+        for name, field in td.items():
+            field.reserve_pairs("zeta_h" if plan.bundles is not None and name == "zeta" else plan.layout)
+        if plan.bundles is not None:
+            plan.bundles["dx"].bundle(plan.bundles["dy"])
+        elif plan.layout in _STATIC_KIND:
+            for field in plan.statics.values():
+                field.neighbours(_STATIC_KIND[plan.layout])
+
+    def timestep_particles_many(self, particles, launcher: Launcher, nsteps: int,
+                                split: "RangeLaunches | None" = None) -> None:
+        """Advance ``nsteps`` steps; fused launches where possible, else step by step.  ``split``: run the
+        fused launch that takes the last of these steps range by range over particle storage (one launch
+        per range, ``split.after(i)`` once range i's launch is queued)."""
         if not self.fused():
             for _ in range(nsteps):
                 self.timestep_particles(particles, launcher)
             return
         done = 0
         while done < nsteps:
-            done += self._fused_chunk(particles, launcher, nsteps - done)
+            done += self._fused_chunk(particles, launcher, nsteps - done, split)
 
-    def _fused_chunk(self, particles, launcher: Launcher, max_steps: int) -> int:
-        """Plan and launch as many steps as fit in one fused launch; return the number taken."""
+    def _fused_chunk(self, particles, launcher: Launcher, max_steps: int,
+                     split: "RangeLaunches | None" = None) -> int:
+        """Plan and launch as many steps as fit in one fused launch; return the number taken.  ``split``
+        applies when the launch takes all ``max_steps``."""
         td = _time_dependent_fields(launcher, self.field_roles)
         # streamed fields: a launch spans at most one snapshot interval (3 snapshots) and a slot stays free,
         # so each launch waits for at most one new upload and the next ones stream in while it runs (a launch
@@ -286,7 +310,10 @@ class Timestepper(abc.ABC):
             # the next step raises or cannot be fused: run it the reference way (raises where it raises)
             self._unfused_step(particles, launcher)
             return 1
-        self._launch_fused(particles, launcher, steps, sorted(needed), td)
+        last = split if split is not None and len(steps) == max_steps else None
+        self._launch_fused(particles, launcher, steps, sorted(needed), td, last)
+        if last is not None:
+            last.used = True
         # bookkeeping exactly as advance_time would have left it after each step
         self._last_start_tidx = steps[-1][0]
         self._time = end_times[-1]
@@ -298,8 +325,31 @@ class Timestepper(abc.ABC):
         raise NotImplementedError
 
     def _launch_fused(self, particles, launcher: Launcher, steps: list[list], needed: list[int],
-                      td: dict[str, TimeDependentField]) -> None:
+                      td: dict[str, TimeDependentField], split: "RangeLaunches | None" = None) -> None:
         raise NotImplementedError
+
+
+class RangeLaunches:
+    """One fused launch issued as one launch per range of particle storage: ``ranges`` are ``(lo, hi)``
+    slot ranges covering the particles in order, and ``after(i)`` is called once range i's launch is
+    queued (the caller starts reading that range back while the next range computes).  Particles are
+    independent, so the split changes no result.  ``used`` is set once a launch was split."""
+
+    def __init__(self, ranges: list[tuple[int, int]], after) -> None:
+        self.ranges = list(ranges)
+        self.after = after
+        self.used = False
+
+
+def _fused_call(entry: str, particles, split: RangeLaunches | None, *args) -> None:
+    """Call a fused entry point over all particles, or range by range (``split``)."""
+    if split is None:
+        _lib.call(entry, ctypes.byref(_abi.particles_struct(particles)), *args)
+        return
+    for i, (lo, hi) in enumerate(split.ranges):
+        if hi > lo:
+            _lib.call(entry, ctypes.byref(_abi.particles_struct_range(particles, lo, hi)), *args)
+        split.after(i)
 
 
 def _require_float64(launcher: Launcher) -> None:
@@ -487,10 +537,13 @@ def pair_fields(rf, its: list[int], td: dict[str, TimeDependentField], plan: Pai
 
 def _fused_fields(launcher: Launcher, steps: list[list], needed: list[int], td: dict[str, TimeDependentField],
                   nparticles: int, roles: dict[str, str] | None = None):
-    """opb_roms_fields over the snapshots ``needed`` plus the per-stage opb_time table."""
-    rf, dtype = window_fields(launcher, needed, td, roles)
+    """opb_roms_fields over the snapshots ``needed`` plus the per-stage opb_time table.  With snapshot
+    pairs the launch reads pairs only: the single snapshots are not acquired (a pair build waits for the
+    uploads of its own two snapshots, not for those of every field)."""
+    pairs = use_pairs(launcher, td, nparticles, roles)
+    rf, dtype = window_fields(launcher, needed, td, roles, acquire=not pairs)
     entries = [t for step in steps for t in step]
-    if use_pairs(launcher, td, nparticles, roles):
+    if pairs:
         pslot = pair_fields(rf, sorted({int(divmod(t, 1)[0]) for t in entries}), td, pair_layout(launcher, td, roles))
         prev_next = lambda It: (pslot[It], pslot[It])  # noqa: E731
     else:
@@ -530,9 +583,10 @@ assert _TIME_DTYPE.itemsize == ctypes.sizeof(_lib.opb_time)
 
 
 def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDependentField],
-                  roles: dict[str, str] | None = None):
+                  roles: dict[str, str] | None = None, acquire: bool = True):
     """opb_roms_fields whose slot j of every time-dependent field holds snapshot ``needed[j]``, and the
-    storage dtype of the time-dependent fields (numpy float64 or float32)."""
+    storage dtype of the time-dependent fields (numpy float64 or float32).  ``acquire=False`` leaves the
+    time-dependent slots empty (the caller points them at snapshot pairs)."""
     fs = launcher.fieldset
     roles = roles or {}
     for name in _abi.ROMS_FIELDS:
@@ -555,7 +609,7 @@ def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDepen
             f = _lib.opb_field()
             f.is_static = 0
             f.dtype = _STORAGE_CODE[field.storage]
-            for k in needed:
+            for k in needed if acquire else ():
                 f.data[slot[k]] = _abi._ptr(field.snapshot(k, keep))
                 sc = field.snapshot_scales(k)
                 if sc is not None:
@@ -707,7 +761,7 @@ class RK2Timestepper(Timestepper):
         if self._post_step_kernel is not None:
             launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
 
-    def _launch_fused(self, particles, launcher, steps, needed, td) -> None:
+    def _launch_fused(self, particles, launcher, steps, needed, td, split=None) -> None:
         rf, table = _fused_fields(launcher, steps, needed, td, len(particles))
         sc = _abi.scalars_struct({
             "hc": launcher.scalar("hc", self._tidx), "NZ": launcher.scalar("NZ", self._tidx),
@@ -716,9 +770,9 @@ class RK2Timestepper(Timestepper):
                                                            "xidx_min", "xidx_max")}})
         table_ptr, _keep = _table_arg(table, particles.device, rf)
         _notify("before", len(steps))
-        _lib.call(_entry("opb_rk2_w_advection_steps", launcher), ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
-                  ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None),
-                  _abi.stream(particles))
+        _fused_call(_entry("opb_rk2_w_advection_steps", launcher), particles, split, ctypes.byref(sc),
+                    ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None),
+                    _abi.stream(particles))
         _notify("after", len(steps))
         _prefetch_after(td, needed, self._prefetch_limit)
 
@@ -783,7 +837,7 @@ class ABTimestepper(Timestepper):
         if self._post_step_kernel is not None:
             launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
 
-    def _launch_fused(self, particles, launcher, steps, needed, td) -> None:
+    def _launch_fused(self, particles, launcher, steps, needed, td, split=None) -> None:
         rf, table = _fused_fields(launcher, steps, needed, td, len(particles), self.field_roles)
         iso = self.isopycnal
         sc = _abi.scalars_struct({
@@ -797,8 +851,7 @@ class ABTimestepper(Timestepper):
         entry = "opb_ab3_isopycnal_following_steps" if iso else _entry("opb_ab3_w_advection_steps", launcher)
         table_ptr, _keep = _table_arg(table, particles.device, rf)
         _notify("before", len(steps))
-        _lib.call(entry, ctypes.byref(_abi.particles_struct(particles)), ctypes.byref(sc),
-                  ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None),
-                  _abi.stream(particles))
+        _fused_call(entry, particles, split, ctypes.byref(sc), ctypes.byref(rf), table_ptr, len(steps),
+                    int(self._pre_step_kernel is not None), _abi.stream(particles))
         _notify("after", len(steps))
         _prefetch_after(td, needed, self._prefetch_limit)

@@ -33,7 +33,7 @@ def b200_fieldset(fields: dict, hc: float, nz: int, ring_size: int = 4, storage:
 
 
 def build_sim(fields, *, hc, nz, scheme, dt, z, y, x, status=None, unfused=False, ring_size=4, time=None,
-              sort_interval=None, arithmetic="float64", storage=None):
+              sort_interval=None, arithmetic="float64", storage=None, result_ranges=1):
     import offline_particles_b200 as opb
     from offline_particles_b200.kernels import ParticleKernel
     from offline_particles_b200.kernels.validation import domain_bounds_kernel, finite_indices_kernel
@@ -51,7 +51,8 @@ def build_sim(fields, *, hc, nz, scheme, dt, z, y, x, status=None, unfused=False
     else:
         assert ts.fused()
     kw = {} if sort_interval is None else {"sort_interval": sort_interval}
-    sim = opb.SimulationBuilder(ts, fs).build_simulation(len(z), arithmetic=arithmetic, **kw)
+    sim = opb.SimulationBuilder(ts, fs).build_simulation(len(z), arithmetic=arithmetic, result_ranges=result_ranges,
+                                                         **kw)
     sim.set_indices(z, y, x)
     if status is not None:
         sim.set_particle_field("status", status)
