@@ -110,6 +110,8 @@ def parse():
                     help="serve every request to its end (only a stream the GPU keeps up with drains)")
     ap.add_argument("--no-batched", action="store_true", help="default run: skip the config-4 batched block")
     ap.add_argument("--no-served", action="store_true", help="default run: skip the config-5 served block")
+    ap.add_argument("--no-streamed", action="store_true", help="default run: skip the streamed-week block")
+    ap.add_argument("--stream-days", type=float, default=7.0, help="model days of the streamed-week block")
     return ap.parse_args()
 
 
@@ -599,6 +601,9 @@ def b200_arm(a) -> None:
         served = serving_measure(a, a.serve_seconds, a.serve_drain)
         gc.collect()
         torch.cuda.empty_cache()
+    streamed = None
+    if world == 1 and not a.no_streamed:
+        streamed = streamed_measure(a, h2d_gbs)
 
     # ---- roofline of the fused kernel -------------------------------------------------
     peak = measured_peak_gbs()
@@ -666,6 +671,7 @@ def b200_arm(a) -> None:
         "cpu_baseline": cpu,
         "batched": batched,
         "served": served,
+        "streamed_week": streamed,
     }
     print(json.dumps(line), flush=True)
 
@@ -1009,6 +1015,95 @@ def serving_trace(a, grid):
         scheme = "rk2" if rng.random() < 0.5 else "ab3"
         reqs.append(TracedRequest(grid, len(reqs), t, n, scheme, dt, round(days * 86400.0 / dt) * dt))
     return reqs
+
+
+# distinct snapshots the streamed week cycles through (pinned host memory: 8 x 478 MB on the 1024x768x50 grid)
+STREAM_DISTINCT = 8
+
+
+def streamed_measure(a, h2d_gbs: float | None) -> dict:
+    """The headline workload over a whole model week: hourly snapshots (``--stream-days`` x 24 + 2 of
+    them) streamed from pinned host memory through the fields' device rings while the particles advance,
+    from ``set_indices`` to the results in pinned host memory (``run(..., results=...)``), timed on the
+    device.  The series repeats ``STREAM_DISTINCT`` distinct snapshots (``synth.CyclicSnapshots``): a week
+    of distinct snapshots is 81 GB of pinned memory, more than a host should be asked to pin, and the
+    upload of each snapshot costs the same whatever its values.  The same run on the same snapshots
+    uploaded from device memory (no PCIe) gives the compute-bound time and must match bit for bit."""
+    import torch
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200.synth import CyclicSnapshots
+
+    n = a.particles
+    steps = int(round(a.stream_days * 86400.0 / a.dt))
+    nt = int(math.floor(steps * a.dt / 3600.0)) + 2
+    grid = make_grid(a, nt)
+    host_src = grid.pinned_cycle(STREAM_DISTINCT, nt)
+    z, y, x = grid.release(n, seed=1000)
+    hz, hy, hx = (torch.from_numpy(v).pin_memory() for v in (z, y, x))
+    names = ("zidx", "yidx", "xidx", "status")
+
+    def outs():
+        o = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in names[:3]}
+        o["status"] = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        return o
+
+    def build(src):
+        kw = {name: opb.TimeDependentField(src[name], *STAGGERS[name], ring_size=a.ring_size) for name in TD}
+        for name, arr in (("h", grid.h), ("dx", grid.dx), ("dy", grid.dy), ("C", grid.C)):
+            kw[name] = opb.StaticField.from_numpy(arr, *STAGGERS[name])
+        fs = opb.Fieldset(nt, a.nz, a.ny, a.nx, constants={"hc": grid.hc, "NZ": a.nz}, **kw)
+        ts = opb.roms.ab3_w_advection_timestepper(grid.time_array[:nt], np.float64(a.dt))
+        return opb.SimulationBuilder(ts, fs).build_simulation(n, result_ranges=a.e2e_ranges), fs
+
+    def week(src, res):
+        w, _ = build(src)  # untimed warm-up of the same path
+        w.set_indices(hz, hy, hx)
+        w.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+        w.run(a.warmup, results=res)
+        w.synchronize()
+        del w
+        gc.collect()
+        sim, fs = build(src)
+        sim.reserve_results(res)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        t0.record()
+        sim.set_indices(hz, hy, hx)
+        sim.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+        sim.run(steps, results=res)
+        t1.record()
+        torch.cuda.synchronize()
+        ms = max(t0.elapsed_time(t1), (time.perf_counter() - w0) * 1e3)
+        sim.synchronize()
+        h2d = 3 * 8 * n + sum(fs[k].h2d_bytes for k in TD)
+        del sim, fs
+        gc.collect()
+        return ms, h2d
+
+    streamed = outs()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        ms, h2d = week(host_src, streamed)
+    dev_src = {k: CyclicSnapshots(v.base.cuda(), nt) for k, v in host_src.items()}
+    resident = outs()
+    ms_dev, _ = week(dev_src, resident)
+    identical = all(torch.equal(streamed[k], resident[k]) for k in names)
+    d2h = sum(t.numel() * t.element_size() for t in streamed.values())
+    del dev_src, host_src
+    gc.collect()
+    torch.cuda.empty_cache()
+    total = n * steps
+    bound_ms = (h2d + d2h) / (h2d_gbs * 1e9) * 1e3 if h2d_gbs else None
+    return {"value": total / (ms * 1e-3), "unit": UNIT, "steps": steps, "days": a.stream_days, "snapshots": nt,
+            "distinct_snapshots": STREAM_DISTINCT, "ms": ms, "h2d_bytes": h2d, "d2h_bytes": d2h,
+            "pcie_bound_value": total / (bound_ms * 1e-3) if bound_ms else None,
+            "from_device_value": total / (ms_dev * 1e-3), "from_device_ms": ms_dev,
+            "identical_to_from_device": identical,
+            "path": "Simulation.set_indices from pinned host + run(steps, results=...): every snapshot uploaded "
+                    "from pinned host memory through the rings while the particles advance, results copied "
+                    "back in original order",
+            "clocks": clocks.summary()}
 
 
 def serving_measure(a, window_s: float, drain: bool) -> dict:

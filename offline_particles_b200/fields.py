@@ -453,21 +453,20 @@ class SnapshotRing:
             self.ready[k] = ev
             return
         if isinstance(src, torch.Tensor) and (src.is_pinned() or src.is_cuda):
-            # already in pinned host memory (or on the device): one async copy, no staging
-            self._wait_turn(ticket)
-            with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
-                if slot_free is not None:
-                    self.copy_stream.wait_event(slot_free)
-                self._to_slot(slot, src[k])
-                ev = torch.cuda.Event()
-                ev.record(self.copy_stream)
-                for obs in upload_observers:
-                    obs(k, self.copy_stream)
-            self.ready[k] = ev
-            if not src.is_cuda:
-                self.h2d_bytes += src[k].numel() * src.element_size()
+            self._copy_direct(k, slot, slot_free, ticket, src[k])
             return
-        host = self._host_snapshot(k)
+        item = None if isinstance(src, torch.Tensor) else src[k]
+        if (isinstance(item, torch.Tensor) and (item.is_pinned() or item.is_cuda)
+                and item.dtype == torch_dtype(self.np_dtype)):
+            # a source whose snapshots are pinned host (or device) tensors: no staging either
+            self._copy_direct(k, slot, slot_free, ticket, item)
+            return
+        if item is None:
+            host = self._host_snapshot(k)
+        elif isinstance(item, torch.Tensor):
+            host = np.ascontiguousarray(item.detach().cpu().numpy(), dtype=self.np_dtype)
+        else:
+            host = np.ascontiguousarray(np.asarray(item), dtype=self.np_dtype)
         if not self.staging:
             self.staging = [torch.empty(self.spatial_shape, dtype=torch_dtype(self.np_dtype), pin_memory=True)
                             for _ in range(2)]
@@ -490,6 +489,23 @@ class SnapshotRing:
             self.staging_free[b] = ev
             self.ready[k] = ev
             self.h2d_bytes += stage.numel() * stage.element_size()
+
+    def _copy_direct(self, k: int, slot: int, slot_free, ticket: int, snap: torch.Tensor) -> None:
+        """Snapshot ``k`` already in pinned host memory (or on the device): one async copy, no staging."""
+        if tuple(snap.shape) != self.spatial_shape:
+            raise ValueError(f"snapshot {k} has shape {tuple(snap.shape)}, expected {self.spatial_shape}")
+        self._wait_turn(ticket)
+        with torch.cuda.device(self.device), torch.cuda.stream(self.copy_stream):
+            if slot_free is not None:
+                self.copy_stream.wait_event(slot_free)
+            self._to_slot(slot, snap)
+            ev = torch.cuda.Event()
+            ev.record(self.copy_stream)
+            for obs in upload_observers:
+                obs(k, self.copy_stream)
+        self.ready[k] = ev
+        if not snap.is_cuda:
+            self.h2d_bytes += snap.numel() * snap.element_size()
 
     def _free_slot(self, keep: set[int]) -> int | None:
         used = set(self.slot_of.values())

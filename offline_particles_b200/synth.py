@@ -368,6 +368,19 @@ class SyntheticROMS:
             self._device_snapshot(it, c, td, {k: v[it] for k, v in out.items()})
         return out
 
+    def pinned_cycle(self, distinct: int, nt: int, device=None) -> dict:
+        """u, v, w, zeta as ``CyclicSnapshots`` of ``nt`` snapshots repeating the first ``distinct`` ones,
+        generated on the device and held in pinned host memory."""
+        import torch
+
+        snaps = self.device_snapshots(distinct, device)
+        out = {}
+        for name, t in snaps.items():
+            host = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+            host.copy_(t)
+            out[name] = CyclicSnapshots(host, nt)
+        return out
+
     def device_source(self, nt: int, device=None, dtype=None, cache: int = 6) -> "DeviceSnapshotSource":
         """Snapshots 0..nt-1 generated on the device when a field's ring asks for them (no storage for
         the whole series: serving runs whose model time has no fixed end)."""
@@ -440,6 +453,32 @@ class SyntheticROMS:
         out = {name: self.dense(name) for name in ("u", "v", "w", "zeta")}
         out.update(h=self.h, dx=self.dx, dy=self.dy, C=self.C)
         return out
+
+
+class CyclicSnapshots:
+    """An array-like ``(nt, ...)`` for ``TimeDependentField`` whose snapshot k is ``base[k % len(base)]``:
+    a long series (a week of hourly snapshots) from a few distinct snapshots held in pinned host memory,
+    which the field's ring uploads with one asynchronous copy each (no staging), as it would uploads from
+    a reader that fills pinned buffers."""
+
+    def __init__(self, base, nt: int) -> None:
+        import torch
+
+        if not isinstance(base, torch.Tensor) or base.ndim < 2 or base.shape[0] < 1:
+            raise ValueError("base must be a tensor of at least one snapshot")
+        self.base = base
+        self.shape = (int(nt),) + tuple(base.shape[1:])
+        self.ndim = len(self.shape)
+        self.dtype = np.dtype(str(base.dtype).replace("torch.", ""))
+
+    def __len__(self) -> int:
+        return self.shape[0]
+
+    def __getitem__(self, k):
+        k = int(k)
+        if not 0 <= k < self.shape[0]:
+            raise IndexError(k)
+        return self.base[k % self.base.shape[0]]
 
 
 def _torch_dtype(dtype):
