@@ -457,6 +457,12 @@ int opb_sort_particles_noalloc(const opb_particles *p, const int64_t shape[3], i
 
 /* Message of the last failed call on this host thread ("" if none). */
 const char *opb_last_error(void);
+/* Self-check of the AB3 update's division by 12 (three floating-point
+ * operations instead of the IEEE division; the same bits by Markstein's
+ * theorem): adds to *mismatches (DEVICE, uint64) the number of x[i] (DEVICE)
+ * for which the two quotients differ in any bit.  No reference counterpart. */
+int opb_check_div12(const double *x, int64_t n, uint64_t *mismatches, void *stream);
+
 /* OPB_ABI_VERSION of the loaded library. */
 int opb_abi_version(void);
 

@@ -121,6 +121,7 @@ SIGNATURES = {
     "opb_bundle_zeta_h": [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP],
     "opb_bundle_dx_dy": [_VP, _VP, _VP, ctypes.c_int64, _VP],
     "opb_quantize_levels": [_VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP, _VP, _VP],
+    "opb_check_div12": [_VP, ctypes.c_int64, _VP, _VP],
 }
 
 SIGNATURES_OTHER = {

@@ -707,6 +707,25 @@ __device__ __forceinline__ double compute_zidx_hint(double z, double h, double z
     return ((double)Cidx - L.C_offset) + f;
 }
 
+// x / 12.0 rounded to nearest, as the IEEE division gives it, in three
+// floating-point operations: Markstein's correction step (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990; the final step of FMA-based
+// division).  Theorem: if r is within half an ulp of 1/y and q within one ulp
+// of x/y, then RN(q + RN(x - q y) r), with the remainder x - q y exact in an
+// FMA, is RN(x/y).  Here y = 12 and r = RN(1/12) = (1/12)(1 - 2^-54) (RN(1/3)
+// = (2^54 - 1) / (3 * 2^54)), so |x r - x/12| = |x/12| 2^-54 < ulp(x/12) / 2
+// and q = RN(x r) is within one ulp.  Zeros (the sign of a zero quotient),
+// infinities, NaN and magnitudes below 2^-960 (where the remainder could
+// underflow) take the division itself.
+__device__ __forceinline__ double div12(double x) {
+    constexpr double kR = 0x1.5555555555555p-4;  // RN(1/12)
+    if (!(fabs(x) >= 0x1p-960) || isinf(x)) return x / 12.0;
+    const double q = x * kR;
+    const double e = fma(-q, 12.0, x);
+    return fma(e, kR, q);
+}
+
 // ----------------------------------------------------------------- status
 __device__ __forceinline__ bool is_finite(double x) { return isfinite(x); }
 

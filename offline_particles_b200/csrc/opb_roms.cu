@@ -12,6 +12,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <initializer_list>
 #include <string>
 #include <type_traits>
@@ -23,8 +24,12 @@
 #include "opb_host.cuh"
 #include "opb_stages.cuh"
 
-// Resident CTAs per SM the fused steppers are compiled for (their register
-// budget: 65536 / (256 * OPB_FUSED_MINB) per thread).
+// Threads per CTA of the fused steppers, and the resident CTAs per SM they are
+// compiled for (their register budget: 65536 / (OPB_FUSED_BLOCK *
+// OPB_FUSED_MINB) per thread).
+#ifndef OPB_FUSED_BLOCK
+#define OPB_FUSED_BLOCK 256
+#endif
 #ifndef OPB_FUSED_MINB
 #define OPB_FUSED_MINB 2
 #endif
@@ -35,6 +40,9 @@
 
 namespace opb {
 namespace {
+
+constexpr int kFusedBlock = OPB_FUSED_BLOCK;
+unsigned fused_grid(long long n) { return (unsigned)((n + kFusedBlock - 1) / kFusedBlock); }
 
 // ------------------------------------------------------------ stage kernels
 __global__ void __launch_bounds__(kBlock) k_validation(const __grid_constant__ DParticles p,
@@ -178,7 +186,7 @@ __global__ void __launch_bounds__(kBlock) k_ab3_post(const __grid_constant__ DPa
 // `nsteps` RK2 steps (timesteppers.py:241-257) per launch.  table[3*k + j]
 // selects the fields of step k, stage j (t, t + alpha dt, t + dt).
 template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool B2 = false>
-__global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_rk2_steps(const __grid_constant__ DParticles p,
+__global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_rk2_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
                                                       const __grid_constant__ StepTable table, int nsteps,
@@ -189,9 +197,9 @@ __global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_rk2_steps(const __gr
     constexpr bool HS = OPB_FUSED_HIST_SMEM != 0;
     PState<I, HS> s;
     if constexpr (HS) {
-        __shared__ double s_hist[6 * kBlock];
+        __shared__ double s_hist[6 * kFusedBlock];
         s.hs = s_hist + threadIdx.x;
-        s.hstride = kBlock;
+        s.hstride = kFusedBlock;
     }
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
@@ -231,7 +239,7 @@ __global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_rk2_steps(const __gr
 // `nsteps` AB3 steps (timesteppers.py:296-305) per launch.  table[2*k + j]
 // selects the fields of step k at t (j = 0) and t + dt (j = 1).
 template <typename T, typename I, bool FIXED, int LAYOUT = LAYOUT_PLAIN, bool ISO = false, bool B2 = false>
-__global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_ab3_steps(const __grid_constant__ DParticles p,
+__global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_ab3_steps(const __grid_constant__ DParticles p,
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
                                                       const __grid_constant__ StepTable table, int nsteps,
@@ -242,9 +250,9 @@ __global__ void __launch_bounds__(kBlock, OPB_FUSED_MINB) k_ab3_steps(const __gr
     constexpr bool HS = OPB_FUSED_HIST_SMEM != 0;
     PState<I, HS> s;
     if constexpr (HS) {
-        __shared__ double s_hist[6 * kBlock];
+        __shared__ double s_hist[6 * kFusedBlock];
         s.hs = s_hist + threadIdx.x;
-        s.hstride = kBlock;
+        s.hstride = kFusedBlock;
     }
     s.status = p.status[i];
     if (s.status & ST_INACTIVE) return;
@@ -303,6 +311,19 @@ __global__ void __launch_bounds__(kBlock) k_interpolate(const __grid_constant__ 
     else out[i] = trilinear(v, i0[i] + v.o0, i1[i] + v.o1, i2[i] + v.o2);
 }
 
+// div12 against the IEEE division of the same build: counts the x[i] whose two
+// quotients differ in any bit (two NaNs agree)
+__global__ void __launch_bounds__(kBlock) k_check_div12(const double *__restrict__ x, long long n,
+                                                        unsigned long long *bad) {
+    unsigned long long mine = 0;
+    for (long long i = gtid(); i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double a = div12(x[i]);
+        const double b = x[i] / 12.0;
+        if (__double_as_longlong(a) != __double_as_longlong(b) && !(isnan(a) && isnan(b))) ++mine;
+    }
+    if (mine) atomicAdd(bad, mine);
+}
+
 }  // namespace
 }  // namespace opb
 
@@ -312,6 +333,14 @@ using namespace opb;
 extern "C" {
 
 int opb_abi_version(void) { return OPB_ABI_VERSION; }
+
+int opb_check_div12(const double *x, int64_t n, uint64_t *mismatches, void *stream) {
+    if (n < 0 || (n > 0 && (!x || !mismatches))) return fail(OPB_EINVAL, "opb_check_div12: bad arguments");
+    if (n == 0) return OPB_OK;
+    const long long blocks = std::min<long long>((n + kBlock - 1) / kBlock, 148LL * 8);
+    k_check_div12<<<(unsigned)blocks, kBlock, 0, (cudaStream_t)stream>>>(x, n, (unsigned long long *)mismatches);
+    return check_launch("opb_check_div12");
+}
 
 static int validation_impl(const opb_particles *p, const opb_scalars *s, void *stream, int finite, int bounds,
                            const char *what) {
@@ -460,7 +489,7 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     for (const opb_field *x : {&g.u, &g.v, &g.w, &g.zeta})
         if (!x->is_static && (nslots == 0 || x->nslots < nslots)) nslots = x->nslots;
     if ((rc = make_step_table(table, (long long)nsteps * (rk2 ? 3 : 2), tab, what, nslots))) return rc;
-    const unsigned grid = grid_for(dp.n);
+    const unsigned grid = fused_grid(dp.n);
     cudaStream_t st = (cudaStream_t)stream;
     const bool fixed = roms_layout(dr, iso);
     auto go = [&](auto tv, auto iv, auto lv, auto bv) {
@@ -468,10 +497,10 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
         using I = decltype(iv);
         constexpr int LAYOUT = decltype(lv)::value;
         constexpr bool B2 = decltype(bv)::value;
-        if (rk2) k_rk2_steps<T, I, true, LAYOUT, B2><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        if (rk2) k_rk2_steps<T, I, true, LAYOUT, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
         else if (iso)
-            k_ab3_steps<T, I, true, LAYOUT, true, B2><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
-        else k_ab3_steps<T, I, true, LAYOUT, false, B2><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+            k_ab3_steps<T, I, true, LAYOUT, true, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        else k_ab3_steps<T, I, true, LAYOUT, false, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
     };
     using NoB = std::false_type;
     using Bun = std::true_type;
@@ -499,11 +528,11 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
         using I = decltype(iv);
         if (layout == LAYOUT_PAIRS) go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{}, NoB{});
         else if (fixed) go(tv, iv, std::integral_constant<int, LAYOUT_PLAIN>{}, NoB{});
-        else if (rk2) k_rk2_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        else if (rk2) k_rk2_steps<T, I, false><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
         else if (iso)
-            k_ab3_steps<T, I, false, LAYOUT_PLAIN, true><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps,
+            k_ab3_steps<T, I, false, LAYOUT_PLAIN, true><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps,
                                                                                  validate_pre);
-        else k_ab3_steps<T, I, false><<<grid, kBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        else k_ab3_steps<T, I, false><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
     });
     return check_launch(what);
 }

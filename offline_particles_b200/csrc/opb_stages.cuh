@@ -445,9 +445,10 @@ __device__ __forceinline__ bool ab3_step(S &s, const B &f, const DScalars &sc, c
     }
     s.z = compute_z(s.zidx, sc.NZ, sc.hc, h, Cv, zeta);
     const double dt = sc.dt;
-    s.z = s.z + dt * (23.0 * s.k0z - 16.0 * k1z + 5.0 * k2z) / 12.0;
-    s.yidx = s.yidx + dt * (23.0 * s.k0y - 16.0 * k1y + 5.0 * k2y) / 12.0;
-    s.xidx = s.xidx + dt * (23.0 * s.k0x - 16.0 * k1x + 5.0 * k2x) / 12.0;
+    // ab3_w_advection.pyx:168-170: (dt * (...)) / 12.0, the quotient through div12 (the same bits)
+    s.z = s.z + div12(dt * (23.0 * s.k0z - 16.0 * k1z + 5.0 * k2z));
+    s.yidx = s.yidx + div12(dt * (23.0 * s.k0y - 16.0 * k1y + 5.0 * k2y));
+    s.xidx = s.xidx + div12(dt * (23.0 * s.k0x - 16.0 * k1x + 5.0 * k2x));
     s.set_k2(k1x, k1y, k1z);
     s.set_k1(s.k0x, s.k0y, s.k0z);
     return true;
