@@ -378,6 +378,34 @@ int opb_rk2_w_advection_steps(const opb_particles *p, const opb_scalars *s, cons
 int opb_ab3_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                               const opb_time *table, int32_t nsteps, int32_t validate, void *stream);
 
+/* Particle state recorded after chosen steps of one fused launch, for the
+ * events that fall inside it (output events: Simulation._invoke_events,
+ * simulation.py:169-176, fires them between steps; here they replay after the
+ * launch on the recorded state, so they no longer end the launch).  Bit k of
+ * mask[k / 64] asks for the state after step k (k < nsteps <= 256); the r-th
+ * recorded step (in step order) of particle i goes to index r * stride + i of
+ * each array (stride >= n; DEVICE pointers).  The state is what the particle
+ * arrays would hold at that point: status, zidx, yidx, xidx and z (a particle
+ * that stopped, or was inactive from the start, records its unchanged state).
+ * No reference counterpart. */
+typedef struct {
+    uint64_t mask[4];
+    int64_t stride;
+    double *zidx, *yidx, *xidx, *z;
+    uint8_t *status;
+} opb_records;
+
+/* The three fused entry points above, with `rec` (NULL: none) recorded. */
+int opb_rk2_w_advection_steps_rec(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                  const opb_time *table, int32_t nsteps, int32_t validate, const opb_records *rec,
+                                  void *stream);
+int opb_ab3_w_advection_steps_rec(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                  const opb_time *table, int32_t nsteps, int32_t validate, const opb_records *rec,
+                                  void *stream);
+int opb_ab3_isopycnal_following_steps_rec(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                          const opb_time *table, int32_t nsteps, int32_t validate,
+                                          const opb_records *rec, void *stream);
+
 /* ABTimestepper.timestep_particles with ab3_isopycnal_following_timestepper's
  * kernels (models/roms/__init__.py:109-141): nsteps fused steps, as
  * opb_ab3_w_advection_steps with the isopycnal follower's vertical velocity. */

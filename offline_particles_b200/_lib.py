@@ -54,6 +54,12 @@ class opb_particles(ctypes.Structure):
     ] + [("err", ctypes.c_void_p), ("rho_t", ctypes.c_void_p)]
 
 
+class opb_records(ctypes.Structure):
+    _fields_ = [("mask", ctypes.c_uint64 * 4), ("stride", ctypes.c_int64), ("zidx", ctypes.c_void_p),
+                ("yidx", ctypes.c_void_p), ("xidx", ctypes.c_void_p), ("z", ctypes.c_void_p),
+                ("status", ctypes.c_void_p)]
+
+
 class opb_scalars(ctypes.Structure):
     _fields_ = [
         ("hc", ctypes.c_double),
@@ -107,6 +113,12 @@ SIGNATURES = {
                                   ctypes.c_int32, _VP],
     "opb_ab3_w_advection_steps": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP, ctypes.c_int32,
                                   ctypes.c_int32, _VP],
+    "opb_rk2_w_advection_steps_rec": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP, ctypes.c_int32,
+                                      ctypes.c_int32, _VP, _VP],
+    "opb_ab3_w_advection_steps_rec": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP, ctypes.c_int32,
+                                      ctypes.c_int32, _VP, _VP],
+    "opb_ab3_isopycnal_following_steps_rec": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP,
+                                              ctypes.c_int32, ctypes.c_int32, _VP, _VP],
     "opb_rk2_w_advection_steps_fp32": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP,
                                        ctypes.c_int32, ctypes.c_int32, _VP],
     "opb_ab3_w_advection_steps_fp32": [_P(opb_particles), _P(opb_scalars), _P(opb_roms_fields), _VP,

@@ -44,6 +44,40 @@ namespace {
 constexpr int kFusedBlock = OPB_FUSED_BLOCK;
 unsigned fused_grid(long long n) { return (unsigned)((n + kFusedBlock - 1) / kFusedBlock); }
 
+// opb_records: the particle state after chosen steps of a fused launch
+struct DRecords {
+    unsigned long long mask[4];
+    long long stride;
+    double *zidx, *yidx, *xidx, *z;
+    uint8_t *status;
+    bool any;
+
+    __device__ __forceinline__ bool at(int k) const { return any && ((mask[k >> 6] >> (k & 63)) & 1ull); }
+    // records before step k: the slot of step k's record
+    __device__ __forceinline__ long long slot(int k) const {
+        int c = 0;
+        for (int w = 0; w < (k >> 6); ++w) c += __popcll(mask[w]);
+        const int b = k & 63;
+        return c + (b ? __popcll(mask[k >> 6] & ((1ull << b) - 1ull)) : 0);
+    }
+    __device__ __forceinline__ void put(int k, long long i, uint8_t st, double zi, double yi, double xi,
+                                        double zz) const {
+        const long long o = slot(k) * stride + i;
+        status[o] = st;
+        zidx[o] = zi;
+        yidx[o] = yi;
+        xidx[o] = xi;
+        z[o] = zz;
+    }
+    // steps [from, to) of a particle whose state no longer changes
+    __device__ __forceinline__ void hold(int from, int to, long long i, uint8_t st, double zi, double yi, double xi,
+                                         double zz) const {
+        if (!any) return;
+        for (int k = from; k < to; ++k)
+            if (at(k)) put(k, i, st, zi, yi, xi, zz);
+    }
+};
+
 // ------------------------------------------------------------ stage kernels
 __global__ void __launch_bounds__(kBlock) k_validation(const __grid_constant__ DParticles p,
                                                        const __grid_constant__ DScalars sc, int finite, int bounds) {
@@ -190,7 +224,7 @@ __global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_rk2_steps(const
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
                                                       const __grid_constant__ StepTable table, int nsteps,
-                                                      int validate_pre) {
+                                                      int validate_pre, const __grid_constant__ DRecords rec) {
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
@@ -202,13 +236,17 @@ __global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_rk2_steps(const
         s.hstride = kFusedBlock;
     }
     s.status = p.status[i];
-    if (s.status & ST_INACTIVE) return;
+    if (s.status & ST_INACTIVE) {
+        rec.hold(0, nsteps, i, s.status, p.zidx[i], p.yidx[i], p.xidx[i], p.z[i]);
+        return;
+    }
     s.zidx = p.zidx[i];
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
     const uint8_t st0 = s.status;
     bool moved = false;
-    for (int k = 0; k < nsteps; ++k) {
+    int k = 0;
+    for (; k < nsteps; ++k) {
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table.at(3 * k), t2 = table.at(3 * k + 1), t3 = table.at(3 * k + 2);
@@ -225,7 +263,9 @@ __global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_rk2_steps(const
             break;
         }
         rk2_update(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t3), L, sc);
+        if (rec.at(k)) rec.put(k, i, s.status, s.zidx, s.yidx, s.xidx, s.z);
     }
+    rec.hold(k, nsteps, i, s.status, s.zidx, s.yidx, s.xidx, moved ? s.z : p.z[i]);
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;
     p.zidx[i] = s.zidx;
@@ -243,7 +283,7 @@ __global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_ab3_steps(const
                                                       const __grid_constant__ DScalars sc,
                                                       const __grid_constant__ DRoms r,
                                                       const __grid_constant__ StepTable table, int nsteps,
-                                                      int validate_pre) {
+                                                      int validate_pre, const __grid_constant__ DRecords rec) {
     OPB_LEVELS(r, sc);
     const long long i = gtid();
     if (i >= p.n) return;
@@ -255,7 +295,10 @@ __global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_ab3_steps(const
         s.hstride = kFusedBlock;
     }
     s.status = p.status[i];
-    if (s.status & ST_INACTIVE) return;
+    if (s.status & ST_INACTIVE) {
+        rec.hold(0, nsteps, i, s.status, p.zidx[i], p.yidx[i], p.xidx[i], p.z[i]);
+        return;
+    }
     s.zidx = p.zidx[i];
     s.yidx = p.yidx[i];
     s.xidx = p.xidx[i];
@@ -264,7 +307,8 @@ __global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_ab3_steps(const
     const double rho_t = ISO ? p.rho_t[i] : 0.0;
     const uint8_t st0 = s.status;
     bool moved = false;
-    for (int k = 0; k < nsteps; ++k) {
+    int k = 0;
+    for (; k < nsteps; ++k) {
         if (validate_pre) s.status = validate(s.status, s.zidx, s.yidx, s.xidx, sc.bounds);
         if (s.status & ST_INACTIVE) break;
         const opb_time t1 = table.at(2 * k), t2 = table.at(2 * k + 1);
@@ -282,7 +326,9 @@ __global__ void __launch_bounds__(kFusedBlock, OPB_FUSED_MINB) k_ab3_steps(const
         }
         moved = true;
         ab3_post(s, bind_all<T, I, FIXED, LAYOUT, B2>(r, t2), L, sc);
+        if (rec.at(k)) rec.put(k, i, s.status, s.zidx, s.yidx, s.xidx, s.z);
     }
+    rec.hold(k, nsteps, i, s.status, s.zidx, s.yidx, s.xidx, moved ? s.z : p.z[i]);
     if (s.status != st0) p.status[i] = s.status;
     if (!moved) return;
     p.zidx[i] = s.zidx;
@@ -455,9 +501,37 @@ int opb_ab3_post_w_advection(const opb_particles *p, const opb_scalars *s, const
     return stage_launch("opb_ab3_post_w_advection", 4, p, s, f, t, stream);
 }
 
+// opb_records -> DRecords, checked against the launch
+static int convert_records(const opb_records *rec, long long n, int32_t nsteps, DRecords &d, const char *what) {
+    d = DRecords{};
+    if (!rec) return OPB_OK;
+    int count = 0;
+    for (int w = 0; w < 4; ++w) {
+        d.mask[w] = rec->mask[w];
+        for (int b = 0; b < 64; ++b)
+            if ((rec->mask[w] >> b) & 1ull) {
+                if (w * 64 + b >= nsteps) return fail(OPB_EINVAL, "%s: a record after step %d of %d", what, w * 64 + b, nsteps);
+                ++count;
+            }
+    }
+    if (count == 0) return OPB_OK;
+    if (rec->stride < n) return fail(OPB_EINVAL, "%s: record stride %lld below the particle count", what,
+                                     (long long)rec->stride);
+    if (!rec->zidx || !rec->yidx || !rec->xidx || !rec->z || !rec->status)
+        return fail(OPB_EINVAL, "%s: a record array is NULL", what);
+    d.stride = rec->stride;
+    d.zidx = rec->zidx;
+    d.yidx = rec->yidx;
+    d.xidx = rec->xidx;
+    d.z = rec->z;
+    d.status = rec->status;
+    d.any = true;
+    return OPB_OK;
+}
+
 static int steps_launch(const char *what, bool rk2, const opb_particles *p, const opb_scalars *s,
                         const opb_roms_fields *f, const opb_time *table, int32_t nsteps, int32_t validate_pre,
-                        void *stream, bool iso = false) {
+                        void *stream, bool iso = false, const opb_records *records = nullptr) {
     DParticles dp;
     DScalars ds;
     DRoms dr;
@@ -473,6 +547,8 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
     if (layout != LAYOUT_PLAIN && !roms_layout(dr, iso))
         return fail(OPB_EINVAL, "%s: snapshot pairs need the ROMS field layout and geometry", what);
     if (nsteps < 0) return fail(OPB_EINVAL, "%s: negative step count", what);
+    DRecords rec;
+    if ((rc = convert_records(records, dp.n, nsteps, rec, what))) return rc;
     if (nsteps > 0 && !table) return fail(OPB_EINVAL, "%s: step table is NULL", what);
     if (rk2)
         rc = need_fields(p, what, {{"z", p->z}, {"_dxidx1", p->dxidx1}, {"_dyidx1", p->dyidx1}, {"_dz1", p->dz1},
@@ -497,10 +573,10 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
         using I = decltype(iv);
         constexpr int LAYOUT = decltype(lv)::value;
         constexpr bool B2 = decltype(bv)::value;
-        if (rk2) k_rk2_steps<T, I, true, LAYOUT, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        if (rk2) k_rk2_steps<T, I, true, LAYOUT, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre, rec);
         else if (iso)
-            k_ab3_steps<T, I, true, LAYOUT, true, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
-        else k_ab3_steps<T, I, true, LAYOUT, false, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+            k_ab3_steps<T, I, true, LAYOUT, true, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre, rec);
+        else k_ab3_steps<T, I, true, LAYOUT, false, B2><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre, rec);
     };
     using NoB = std::false_type;
     using Bun = std::true_type;
@@ -528,11 +604,11 @@ static int steps_launch(const char *what, bool rk2, const opb_particles *p, cons
         using I = decltype(iv);
         if (layout == LAYOUT_PAIRS) go(tv, iv, std::integral_constant<int, LAYOUT_PAIRS>{}, NoB{});
         else if (fixed) go(tv, iv, std::integral_constant<int, LAYOUT_PLAIN>{}, NoB{});
-        else if (rk2) k_rk2_steps<T, I, false><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+        else if (rk2) k_rk2_steps<T, I, false><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre, rec);
         else if (iso)
             k_ab3_steps<T, I, false, LAYOUT_PLAIN, true><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps,
-                                                                                 validate_pre);
-        else k_ab3_steps<T, I, false><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre);
+                                                                                 validate_pre, rec);
+        else k_ab3_steps<T, I, false><<<grid, kFusedBlock, 0, st>>>(dp, ds, dr, tab, nsteps, validate_pre, rec);
     });
     return check_launch(what);
 }
@@ -555,6 +631,26 @@ int opb_rk2_w_advection_steps(const opb_particles *p, const opb_scalars *s, cons
 int opb_ab3_w_advection_steps(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
                               const opb_time *table, int32_t nsteps, int32_t validate, void *stream) {
     return steps_launch("opb_ab3_w_advection_steps", false, p, s, f, table, nsteps, validate, stream);
+}
+
+int opb_rk2_w_advection_steps_rec(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                  const opb_time *table, int32_t nsteps, int32_t validate, const opb_records *rec,
+                                  void *stream) {
+    return steps_launch("opb_rk2_w_advection_steps_rec", true, p, s, f, table, nsteps, validate, stream, false, rec);
+}
+
+int opb_ab3_w_advection_steps_rec(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                  const opb_time *table, int32_t nsteps, int32_t validate, const opb_records *rec,
+                                  void *stream) {
+    return steps_launch("opb_ab3_w_advection_steps_rec", false, p, s, f, table, nsteps, validate, stream, false,
+                        rec);
+}
+
+int opb_ab3_isopycnal_following_steps_rec(const opb_particles *p, const opb_scalars *s, const opb_roms_fields *f,
+                                          const opb_time *table, int32_t nsteps, int32_t validate,
+                                          const opb_records *rec, void *stream) {
+    return steps_launch("opb_ab3_isopycnal_following_steps_rec", false, p, s, f, table, nsteps, validate, stream,
+                        true, rec);
 }
 
 static int interpolate_impl(const char *what, int nd, const opb_particles *p, const double *i0, const double *i1,

@@ -27,10 +27,16 @@ type EventFunction = Callable[[SimulationState], None]
 
 
 class Event:
-    def __init__(self, name: str, func: EventFunction, *kernels) -> None:
+    """``Event(name, func, *kernels)`` (events/_events.py:26-52).  ``deferrable=True`` declares that the
+    event's kernels read only the particles' status and indices and write only fields of their own, and
+    that ``func`` reads only those fields and the state's time: such an event may fire after a fused
+    launch on the particle state recorded at its step instead of ending the launch there."""
+
+    def __init__(self, name: str, func: EventFunction, *kernels, deferrable: bool = False) -> None:
         self._name = name
         self._func = func
         self._kernels = kernels
+        self.deferrable = bool(deferrable)
 
     def __call__(self, state: SimulationState) -> None:
         self._func(state)
@@ -67,6 +73,13 @@ class IterationScheduler:
     def register_event(self, first: int, n: int, event: Event) -> None:
         self._schedule_event(first, n, event)
         self.set_next()
+
+    def copy(self) -> "IterationScheduler":
+        """A scheduler in the same state (the same events), to look ahead without firing."""
+        c = IterationScheduler()
+        c._events = {k: list(v) for k, v in self._events.items()}
+        c._next = self._next
+        return c
 
     def set_next(self) -> None:
         self._next = min(self._events) if self._events else None
@@ -105,6 +118,13 @@ class TimeScheduler:
     def register_event(self, first, dt, event: Event) -> None:
         self._schedule_event(first, dt, event)
         self.set_next()
+
+    def copy(self) -> "TimeScheduler":
+        """A scheduler in the same state (the same events), to look ahead without firing."""
+        c = TimeScheduler(forward=self._forward)
+        c._events = {k: list(v) for k, v in self._events.items()}
+        c._next_time = self._next_time
+        return c
 
     def set_next(self) -> None:
         if not self._events:

@@ -87,6 +87,21 @@ def trilinear_interpolation_kernel(field: str, output_name: str | None = None) -
                           scalars={}, simulation_fields=[field])
 
 
+_SAMPLERS = (linear_interpolation_kernel_function, bilinear_interpolation_kernel_function,
+             trilinear_interpolation_kernel_function)
+
+
+def samples_only(kernel: ParticleKernel, protected) -> bool:
+    """True when every function of ``kernel`` samples a field at the particles into a particle field that is
+    not in ``protected`` (such a kernel reads only the status and indices and writes only its output)."""
+    for fn in kernel.functions:
+        if not (isinstance(fn, partial) and fn.func in _SAMPLERS):
+            return False
+        if fn.keywords.get("particle_name") in protected:
+            return False
+    return True
+
+
 def vertical_interpolation_kernel(field: str, output_name: str | None = None) -> ParticleKernel:
     return linear_interpolation_kernel(field, output_name, dimension="z")
 

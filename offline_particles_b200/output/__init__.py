@@ -81,11 +81,19 @@ class AbstractOutputWriter(abc.ABC):
         return f"{self.name}:{output_name}"
 
     def create_events(self) -> list[Event]:
-        """Events in firing order: the time, each output (after its kernels), the round check."""
-        events = [Event(self.event_name("time"), self.write_time)]
+        """Events in firing order: the time, each output (after its kernels), the round check.  The events
+        are deferrable (they may fire after a fused launch on the state recorded at their step) when every
+        output's kernels only sample fields into fields of their own."""
+        from .. import _lib
+        from ..kernels.output.linear_interpolation import samples_only
+
+        step_fields = {"status", "rho_t", *_lib.PARTICLE_POINTERS}
+        defer = all(samples_only(k, step_fields) for o in self.outputs.values() for k in o.kernels)
+        events = [Event(self.event_name("time"), self.write_time, deferrable=defer)]
         for name, output in self.outputs.items():
-            events.append(Event(self.event_name(name), functools.partial(self.write_output, name), *output.kernels))
-        events.append(Event(self.event_name("finalise"), self.finalise_write_round))
+            events.append(Event(self.event_name(name), functools.partial(self.write_output, name), *output.kernels,
+                                deferrable=defer))
+        events.append(Event(self.event_name("finalise"), self.finalise_write_round, deferrable=defer))
         return events
 
 

@@ -99,6 +99,18 @@ class Particles(_FrozenArrayMapping):
         object.__setattr__(self, "_workspace", None)
         object.__setattr__(self, "_range", None)  # id bounds kept by the last sort (None: none)
 
+    @classmethod
+    def view(cls, arrays: dict[str, torch.Tensor], base: "Particles") -> "Particles":
+        """Particles over existing device arrays (no copy), in the storage order of ``base`` and with its
+        error word: e.g. a recorded state whose other fields are ``base``'s own."""
+        obj = object.__new__(cls)
+        _FrozenArrayMapping.__init__(obj, **arrays)
+        for slot in ("_length", "_device", "_err", "_order", "_range"):
+            object.__setattr__(obj, slot, object.__getattribute__(base, slot))
+        for slot in ("_abi_cache", "_spare", "_perm", "_workspace"):
+            object.__setattr__(obj, slot, None)
+        return obj
+
     def __len__(self) -> int:
         return object.__getattribute__(self, "_length")
 

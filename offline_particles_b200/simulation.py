@@ -65,6 +65,7 @@ class Simulation:
         self._id_bounds = result_bounds(n, int(result_ranges))
         self._readback: dict[str, torch.Tensor] = {}  # device buffers of run(results=...), by field
         self._readback_stream: torch.cuda.Stream | None = None
+        self._records: dict[str, torch.Tensor] | None = None  # states recorded inside fused launches
         self._steps_since_sort: int | None = None  # None: never sorted
         if self._sort_interval > 0:
             self._particles.reserve_sort()  # the sort's scratch now, not inside the first run
@@ -265,6 +266,18 @@ class Simulation:
         if reader is not None:
             reader.finish()
 
+    def _record_buffers(self, count: int) -> dict[str, torch.Tensor]:
+        """Device buffers for ``count`` recorded states (grown on demand, reused by later launches in stream
+        order)."""
+        bufs = self._records
+        n = len(self._particles)
+        if bufs is None or bufs["zidx"].shape[0] < count:
+            dev = self._particles.device
+            bufs = {name: torch.empty((count, n), dtype=torch.uint8 if name == "status" else torch.float64, device=dev)
+                    for name in _RECORDED}
+            self._records = bufs
+        return bufs
+
     def reserve_results(self, names) -> None:
         """Allocate what ``run(results=...)`` uses for the fields ``names`` (device buffers in original
         order, a copy stream) now, so that such a run allocates nothing."""
@@ -278,12 +291,36 @@ class Simulation:
                 if buf is None or buf.shape != t.shape or buf.dtype != t.dtype:
                     self._readback[name] = torch.empty_like(t)
 
+    def _recordable(self) -> bool:
+        """Events may fire after a fused launch on the state it recorded (float64 fused steppers)."""
+        return self._timestepper.fused() and self._launcher.arithmetic == "float64"
+
+    def plan_events(self, limit: int) -> tuple[int, set[int]]:
+        """How many steps (at most ``limit``) can run before an event that must fire between launches, and
+        the iterations before that whose events are all deferrable (recorded inside the launches and fired
+        after them, in step order).  The schedulers are looked ahead on copies."""
+        if not self._recordable():
+            return self.steps_to_next_event(limit), set()
+        its, tms = self._iteration_scheduler.copy(), self._time_scheduler.copy()
+        it, t = self.iteration, self.time
+        deferred: set[int] = set()
+        for k in range(1, limit + 1):
+            t = t + self.dt
+            fired = its(it + k) + tms(t)
+            if not fired:
+                continue
+            if k == limit or not all(e.deferrable for e in fired):
+                return k, deferred
+            deferred.add(it + k)
+        return limit, deferred
+
     def _run(self, nsteps: int, reader: "_ResultReader | None" = None) -> None:
         done = 0
         while done < nsteps:
-            k = min(self.steps_to_next_event(nsteps - done), self._maybe_sort())
+            k, deferred = self.plan_events(min(nsteps - done, self._maybe_sort()))
             split = reader.split() if reader is not None and done + k == nsteps else None
-            self._timestepper.timestep_particles_many(self._particles, self._launcher, k, split)
+            recorder = _EventRecorder(self, deferred) if deferred else None
+            self._timestepper.timestep_particles_many(self._particles, self._launcher, k, split, recorder)
             done += k
             if self._steps_since_sort is not None:
                 self._steps_since_sort += k
@@ -325,6 +362,87 @@ class Simulation:
             close = getattr(w, "close", None)
             if close is not None:
                 close()
+
+
+# bytes of device memory the recorded states of one fused launch may take (status, zidx, yidx, xidx and z:
+# 33 bytes per particle and recorded step); at least one step is recorded
+RECORD_BUDGET_BYTES = 2 << 30
+_RECORDED = ("zidx", "yidx", "xidx", "z", "status")
+
+
+class _RecordPlan:
+    """The records of one fused launch (``opb_records``) and the events they replay."""
+
+    def __init__(self, sim: Simulation, steps: list[tuple[int, object, object, int]]) -> None:
+        from . import _lib
+
+        self.sim = sim
+        self.steps = steps  # (iteration, time, tidx, step index in the launch)
+        P = sim._particles
+        n = len(P)
+        self.bufs = sim._record_buffers(len(steps))
+        st = _lib.opb_records()
+        for *_, j in steps:
+            st.mask[j >> 6] |= 1 << (j & 63)
+        st.stride = n
+        for name in _RECORDED:
+            setattr(st, name, self.bufs[name].data_ptr())
+        self.struct = st
+
+    def at(self, lo: int):
+        """The records of a launch over storage slots from ``lo`` on (the same records, offset)."""
+        from . import _lib
+
+        st = _lib.opb_records()
+        st.mask[:] = self.struct.mask[:]
+        st.stride = self.struct.stride
+        for name in _RECORDED:
+            setattr(st, name, getattr(self.struct, name) + lo * (1 if name == "status" else 8))
+        return st
+
+    def replay(self, td) -> None:
+        """Fire the recorded steps' events in step order, each on the state recorded at its step (the other
+        particle fields, the events' outputs among them, are the simulation's own)."""
+        sim = self.sim
+        P = sim._particles
+        for slot, (it, t, tidx, _) in enumerate(self.steps):
+            arrays = dict(P.arrays)
+            for name in _RECORDED:
+                arrays[name] = self.bufs[name][slot]
+            V = Particles.view(arrays, P)
+            state = SimulationState(time=t, dt=sim.dt, tidx=tidx, iteration=it, particles=ParticlesView(V))
+            for event in itertools.chain(sim._iteration_scheduler(it), sim._time_scheduler(t)):
+                if not event.deferrable:
+                    raise RuntimeError(f"event {event.name!r} fired inside a fused launch")
+                for kernel in event.kernels:
+                    sim._launcher.launch_kernel(kernel, V, tidx)
+                event(state)
+
+
+class _EventRecorder:
+    """Events inside the fused launches of one stretch of steps (``Simulation.plan_events``): a launch
+    records the particle state after the steps whose events are deferred (``opb_records``), and the events
+    fire after the launch, in step order, on those states."""
+
+    def __init__(self, sim: Simulation, deferred: set[int]) -> None:
+        self.sim = sim
+        self.deferred = deferred
+        n = max(1, len(sim._particles))
+        self.max_records = max(1, min(256, RECORD_BUDGET_BYTES // (33 * n)))
+
+    def full(self, iteration0: int, nsteps: int) -> bool:
+        """A launch of ``nsteps`` steps from ``iteration0`` would record more states than the budget."""
+        return sum(1 for k in range(iteration0 + 1, iteration0 + nsteps + 1) if k in self.deferred) > self.max_records
+
+    def plan(self, iteration0: int, end_times: list, end_tidxs: list) -> _RecordPlan | None:
+        steps = [(iteration0 + j + 1, end_times[j], end_tidxs[j], j) for j in range(len(end_times))
+                 if iteration0 + j + 1 in self.deferred]
+        return _RecordPlan(self.sim, steps) if steps else None
+
+    def after_step(self, iteration: int) -> None:
+        """A step run on its own: its deferred events fire now, on the live state."""
+        if iteration in self.deferred:
+            self.sim._invoke_events()
 
 
 def result_bounds(n: int, ranges: int) -> tuple[int, ...] | None:

@@ -251,20 +251,24 @@ class Timestepper(abc.ABC):
                 field.neighbours(_STATIC_KIND[plan.layout])
 
     def timestep_particles_many(self, particles, launcher: Launcher, nsteps: int,
-                                split: "RangeLaunches | None" = None) -> None:
+                                split: "RangeLaunches | None" = None, recorder=None) -> None:
         """Advance ``nsteps`` steps; fused launches where possible, else step by step.  ``split``: run the
         fused launch that takes the last of these steps range by range over particle storage (one launch
-        per range, ``split.after(i)`` once range i's launch is queued)."""
+        per range, ``split.after(i)`` once range i's launch is queued).  ``recorder``: events that fall
+        inside the launches (``recorder.plan`` gives a launch its records, ``after_step`` follows a step
+        run on its own)."""
         if not self.fused():
             for _ in range(nsteps):
                 self.timestep_particles(particles, launcher)
+                if recorder is not None:
+                    recorder.after_step(self._iteration)
             return
         done = 0
         while done < nsteps:
-            done += self._fused_chunk(particles, launcher, nsteps - done, split)
+            done += self._fused_chunk(particles, launcher, nsteps - done, split, recorder)
 
     def _fused_chunk(self, particles, launcher: Launcher, max_steps: int,
-                     split: "RangeLaunches | None" = None) -> int:
+                     split: "RangeLaunches | None" = None, recorder=None) -> int:
         """Plan and launch as many steps as fit in one fused launch; return the number taken.  ``split``
         applies when the launch takes all ``max_steps``."""
         td = _time_dependent_fields(launcher, self.field_roles)
@@ -282,6 +286,8 @@ class Timestepper(abc.ABC):
         needed: set[int] = set()
         end_times = []
         while len(steps) < min(max_steps, MAX_FUSED_STEPS):
+            if recorder is not None and steps and recorder.full(self._iteration, len(steps) + 1):
+                break  # the launch's recorded states would pass their memory budget
             try:
                 tidxs, nxt = self._stage_times(time)
             except (ValueError, IndexError):
@@ -309,9 +315,14 @@ class Timestepper(abc.ABC):
         if not steps:
             # the next step raises or cannot be fused: run it the reference way (raises where it raises)
             self._unfused_step(particles, launcher)
+            if recorder is not None:
+                recorder.after_step(self._iteration)
             return 1
         last = split if split is not None and len(steps) == max_steps else None
-        self._launch_fused(particles, launcher, steps, sorted(needed), td, last)
+        rec = None
+        if recorder is not None:
+            rec = recorder.plan(self._iteration, end_times, [st[-1] for st in steps])
+        self._launch_fused(particles, launcher, steps, sorted(needed), td, last, rec)
         if last is not None:
             last.used = True
         # bookkeeping exactly as advance_time would have left it after each step
@@ -325,7 +336,7 @@ class Timestepper(abc.ABC):
         raise NotImplementedError
 
     def _launch_fused(self, particles, launcher: Launcher, steps: list[list], needed: list[int],
-                      td: dict[str, TimeDependentField], split: "RangeLaunches | None" = None) -> None:
+                      td: dict[str, TimeDependentField], split: "RangeLaunches | None" = None, rec=None) -> None:
         raise NotImplementedError
 
 
@@ -341,14 +352,22 @@ class RangeLaunches:
         self.used = False
 
 
-def _fused_call(entry: str, particles, split: RangeLaunches | None, *args) -> None:
-    """Call a fused entry point over all particles, or range by range (``split``)."""
+def _fused_call(entry: str, particles, split: RangeLaunches | None, args: tuple, stream, rec=None) -> None:
+    """Call a fused entry point over all particles, or range by range (``split``); with ``rec`` (a record
+    plan: ``struct``, ``at(lo)``) its ``_rec`` form, recording the state after the planned steps."""
+
+    def call(ps, r) -> None:
+        if r is None:
+            _lib.call(entry, ctypes.byref(ps), *args, stream)
+        else:
+            _lib.call(entry + "_rec", ctypes.byref(ps), *args, ctypes.byref(r), stream)
+
     if split is None:
-        _lib.call(entry, ctypes.byref(_abi.particles_struct(particles)), *args)
+        call(_abi.particles_struct(particles), None if rec is None else rec.struct)
         return
     for i, (lo, hi) in enumerate(split.ranges):
         if hi > lo:
-            _lib.call(entry, ctypes.byref(_abi.particles_struct_range(particles, lo, hi)), *args)
+            call(_abi.particles_struct_range(particles, lo, hi), None if rec is None else rec.at(lo))
         split.after(i)
 
 
@@ -761,7 +780,7 @@ class RK2Timestepper(Timestepper):
         if self._post_step_kernel is not None:
             launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
 
-    def _launch_fused(self, particles, launcher, steps, needed, td, split=None) -> None:
+    def _launch_fused(self, particles, launcher, steps, needed, td, split=None, rec=None) -> None:
         rf, table = _fused_fields(launcher, steps, needed, td, len(particles))
         sc = _abi.scalars_struct({
             "hc": launcher.scalar("hc", self._tidx), "NZ": launcher.scalar("NZ", self._tidx),
@@ -770,10 +789,12 @@ class RK2Timestepper(Timestepper):
                                                            "xidx_min", "xidx_max")}})
         table_ptr, _keep = _table_arg(table, particles.device, rf)
         _notify("before", len(steps))
-        _fused_call(_entry("opb_rk2_w_advection_steps", launcher), particles, split, ctypes.byref(sc),
-                    ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None),
-                    _abi.stream(particles))
+        _fused_call(_entry("opb_rk2_w_advection_steps", launcher), particles, split,
+                    (ctypes.byref(sc), ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None)),
+                    _abi.stream(particles), rec)
         _notify("after", len(steps))
+        if rec is not None:
+            rec.replay(td)
         _prefetch_after(td, needed, self._prefetch_limit)
 
 
@@ -837,7 +858,7 @@ class ABTimestepper(Timestepper):
         if self._post_step_kernel is not None:
             launcher.launch_kernel(self._post_step_kernel, particles, self._tidx)
 
-    def _launch_fused(self, particles, launcher, steps, needed, td, split=None) -> None:
+    def _launch_fused(self, particles, launcher, steps, needed, td, split=None, rec=None) -> None:
         rf, table = _fused_fields(launcher, steps, needed, td, len(particles), self.field_roles)
         iso = self.isopycnal
         sc = _abi.scalars_struct({
@@ -851,7 +872,10 @@ class ABTimestepper(Timestepper):
         entry = "opb_ab3_isopycnal_following_steps" if iso else _entry("opb_ab3_w_advection_steps", launcher)
         table_ptr, _keep = _table_arg(table, particles.device, rf)
         _notify("before", len(steps))
-        _fused_call(entry, particles, split, ctypes.byref(sc), ctypes.byref(rf), table_ptr, len(steps),
-                    int(self._pre_step_kernel is not None), _abi.stream(particles))
+        _fused_call(entry, particles, split,
+                    (ctypes.byref(sc), ctypes.byref(rf), table_ptr, len(steps), int(self._pre_step_kernel is not None)),
+                    _abi.stream(particles), rec)
         _notify("after", len(steps))
+        if rec is not None:
+            rec.replay(td)
         _prefetch_after(td, needed, self._prefetch_limit)
