@@ -84,6 +84,8 @@ def parse():
                          "separation in metres after --days; batched: release experiments in one batch vs "
                          "one after another through the plain path")
     ap.add_argument("--days", type=str, default="1,3,7")
+    ap.add_argument("--release-box", type=str, default=None,
+                    help="--study launch: release in a box of nz,ny,nx cells at the middle of the grid")
     # batched releases (--study batched)
     ap.add_argument("--batch-grid", type=str, default="40,512,512", help="nz,ny,nx of the batched workload")
     ap.add_argument("--experiments", type=int, default=256)
@@ -1281,7 +1283,10 @@ def launch_study(a) -> None:
     """One fused AB3 launch of exactly --steps steps after an explicit Morton sort, inside one snapshot
     interval (fields resident, no re-sort or pair build inside): the unit an ncu capture of the headline
     kernel compares between builds.  Runs --warmup steps first (their own launch), then the measured
-    launch; prints its CUDA-event time per step.  Capture it with ``-k regex:k_ab3_steps -s 1 -c 1``."""
+    launch; prints its CUDA-event time per step.  Capture it with ``-k regex:k_ab3_steps -s 1 -c 1``.
+    ``--release-box nz,ny,nx``: release every particle uniformly in a box of that many cells at the middle
+    of the grid instead of over all wet cells, so that every gather hits the caches: the kernel's time
+    without memory latency."""
     import torch
 
     import offline_particles_b200 as opb
@@ -1293,7 +1298,14 @@ def launch_study(a) -> None:
     grid = make_grid(a, 3)
     dsrc = grid.device_snapshots(3)
     sim, _ = build_sim(grid, dsrc, a.particles, a, sort_interval=0)
-    sim.set_indices(*grid.release(a.particles, seed=1000))
+    if a.release_box:
+        bz, by, bx = (float(v) for v in a.release_box.split(","))
+        rng = np.random.default_rng(5)
+        n = a.particles
+        zyx = (20.0 + rng.uniform(0, bz, n), a.ny / 2 + rng.uniform(0, by, n), a.nx / 2 + rng.uniform(0, bx, n))
+    else:
+        zyx = grid.release(a.particles, seed=1000)
+    sim.set_indices(*zyx)
     sim.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
     sim.sort_particles()
     sim.run(a.warmup)
@@ -1305,6 +1317,7 @@ def launch_study(a) -> None:
     torch.cuda.synchronize()
     ms = s_.elapsed_time(e_)
     print(json.dumps({"study": "launch", "steps": a.steps, "particles": a.particles, "grid": [a.nz, a.ny, a.nx],
+                      "release_box": a.release_box,
                       "ms": ms, "ms_per_step": ms / a.steps,
                       "particle_steps_per_s": a.particles * a.steps / (ms * 1e-3)}), flush=True)
 
