@@ -301,12 +301,20 @@ class Simulation:
         after them, in step order).  The schedulers are looked ahead on copies."""
         if not self._recordable():
             return self.steps_to_next_event(limit), set()
+        if self._iteration_scheduler.next is None and self._time_scheduler.next_time is None:
+            return limit, set()
         its, tms = self._iteration_scheduler.copy(), self._time_scheduler.copy()
-        it, t = self.iteration, self.time
+        forward = tms._forward
+        it, t, dt = self.iteration, self.time, self.dt
         deferred: set[int] = set()
+        nit, nt = its.next, tms.next_time
         for k in range(1, limit + 1):
-            t = t + self.dt
+            t = t + dt
+            # the schedulers are asked only where one of them is due (what they would fire is then the same)
+            if not ((nit is not None and it + k >= nit) or (nt is not None and (t >= nt if forward else t <= nt))):
+                continue
             fired = its(it + k) + tms(t)
+            nit, nt = its.next, tms.next_time
             if not fired:
                 continue
             if k == limit or not all(e.deferrable for e in fired):

@@ -34,14 +34,24 @@ def _run(mode: str, ring_size: int = 4):
         assert not ts.fused()
     else:
         assert ts.fused()
-    sim = opb.SimulationBuilder(ts, fs).build_simulation(c["n"])
-    sim.set_indices(gold["z0"], gold["y0"], gold["x0"])
-    sim.set_particle_field("status", 10)
-    sim.set_particle_field("rho_t", gold["rho_t0"])
+    sb = opb.SimulationBuilder(ts, fs)
     ridx = gold["record_idx"]
     rec = []
     every = c["record_every"]
-    if mode == "run":
+    if mode == "run_events":
+        # the positions read by a deferrable event: recorded inside the fused launches, read after them
+        def sample(state):
+            P = state.particles
+            rec.append(np.stack([P[n][ridx] for n in ("zidx", "yidx", "xidx")]))
+
+        sb.add_event(opb.events.Event("sample", sample, deferrable=True), n=every, first=every)
+    sim = sb.build_simulation(c["n"])
+    sim.set_indices(gold["z0"], gold["y0"], gold["x0"])
+    sim.set_particle_field("status", 10)
+    sim.set_particle_field("rho_t", gold["rho_t0"])
+    if mode == "run_events":
+        sim.run(c["steps"])
+    elif mode == "run":
         for _ in range(c["steps"] // every):
             sim.run(every)
             P = sim.particles
@@ -57,7 +67,7 @@ def _run(mode: str, ring_size: int = 4):
     return gold, np.stack(rec), sim.particles
 
 
-@pytest.mark.parametrize("mode,ring", [("run", 4), ("step", 4), ("stages", 4), ("run", 2)])
+@pytest.mark.parametrize("mode,ring", [("run", 4), ("step", 4), ("stages", 4), ("run", 2), ("run_events", 4)])
 def test_isopycnal_follower_matches_reference(mode, ring):
     gold, rec, P = _run(mode, ring)
     assert same_bits(rec, gold["record"]), mismatch_report(rec, gold["record"])
