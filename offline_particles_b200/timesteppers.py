@@ -180,22 +180,47 @@ class Timestepper(abc.ABC):
         interval than step n did: running n steps ends on a snapshot-interval boundary.  Stops early (at
         least 1) where the time array ends."""
         t = self._time
+        fast = self._float_times()
+        if fast is not None and isinstance(t, (float, np.float64)):
+            interval = self._fast_interval(fast)
+            t = float(t)
+            dt = float(self.dt)  # the same double as self.dt, added as the stepping adds it
+        else:
+            def interval(x):
+                return int(divmod(self.get_time_index(x), 1)[0])
+
+            dt = self.dt
         try:
-            cur = int(divmod(self.get_time_index(t), 1)[0])
+            cur = interval(t)
         except (ValueError, IndexError):
             return max(1, at_least)
         n = 0
         while n < limit:
-            t = t + self.dt
+            t = t + dt
             n += 1
             try:
-                nxt = int(divmod(self.get_time_index(t), 1)[0])
+                nxt = interval(t)
             except (ValueError, IndexError):
                 return max(n, 1, min(at_least, limit))
             if nxt != cur and n >= at_least:
                 return n
             cur = nxt
         return max(1, min(at_least, limit))
+
+    @staticmethod
+    def _fast_interval(fast: list):
+        """int(divmod(get_time_index(x), 1)[0]) for a Python float x: get_time_index's fast path inlined
+        (the same operations on the same doubles), without the numpy scalar around the result."""
+        lo, hi = fast[0], fast[-1]
+
+        def interval(x: float) -> int:
+            if x < lo or x > hi:
+                raise ValueError("Time is out of bounds of the time array.")
+            idx = bisect.bisect_right(fast, x) - 1
+            t0 = fast[idx]
+            return int(divmod(idx + (x - t0) / (fast[idx + 1] - t0), 1)[0])
+
+        return interval
 
     @property
     @abc.abstractmethod
@@ -223,9 +248,11 @@ class Timestepper(abc.ABC):
 
     def snapshot_horizon(self, nsteps: int) -> int | None:
         """The last snapshot index the next ``nsteps`` steps read (None when past the time array)."""
-        t = self._time
+        t, dt = self._time, self.dt
+        if isinstance(t, (float, np.float64)) and isinstance(dt, (float, np.float64)):
+            t, dt = float(t), float(dt)  # the same doubles, added without numpy scalars
         for _ in range(nsteps):
-            t = t + self.dt
+            t = t + dt
         try:
             return int(divmod(self.get_time_index(t), 1)[0]) + 1
         except (ValueError, IndexError):

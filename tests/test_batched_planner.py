@@ -129,3 +129,22 @@ def test_step_table_equals_the_scalar_form():
             assert its[j] == It
             assert bytes(table[j]) == bytes(want), (j, tidx)
         assert ctypes.sizeof(table) == len(entries) * ctypes.sizeof(_lib.opb_time)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_steps_to_interval_end_fast_path_equals_the_generic_one(seed):
+    """steps_to_interval_end on Python floats (get_time_index's fast path inlined) gives the step counts
+    of the path through get_time_index, for odd time arrays, dt that do not divide the spacing, and starts
+    next to snapshot times."""
+    rng = np.random.default_rng(seed)
+    for _ in range(20):
+        nt = int(rng.integers(3, 30))
+        t_arr = np.cumsum(np.concatenate([[rng.uniform(-5e4, 5e4)], rng.choice([3600.0, 1800.0, 977.3], nt - 1)]))
+        dt = np.float64(rng.choice([120.0, 300.0, 61.7, 3600.0]))
+        start = t_arr[int(rng.integers(0, nt - 1))] + rng.choice([0.0, 1e-9, dt / 3])
+        for maker in (ab3_w_advection_timestepper, rk2_w_advection_timestepper):
+            ts = maker(t_arr, dt, time=np.float64(start))
+            fast = [ts.steps_to_interval_end(k) for k in (0, 1, 5, 64, 200)]
+            ts.__dict__["_float_times_cache"] = (ts.time_array, None)  # force the generic path
+            slow = [ts.steps_to_interval_end(k) for k in (0, 1, 5, 64, 200)]
+            assert fast == slow, (t_arr, dt, start)
