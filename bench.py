@@ -203,7 +203,7 @@ def window_plan(a) -> dict:
 
 # --------------------------------------------------------------- clocks
 class ClockSampler:
-    """NVML samples of the SM clock and clock-event reasons every 10 ms while running (reads only)."""
+    """NVML samples of the SM clock and clock-event reasons every ``period_s`` while running (reads only)."""
 
     REASONS = (("nvmlClocksEventReasonHwSlowdown", "hw_slowdown"),
                ("nvmlClocksEventReasonHwThermalSlowdown", "hw_thermal_slowdown"),
@@ -211,8 +211,9 @@ class ClockSampler:
                ("nvmlClocksEventReasonSwPowerCap", "sw_power_cap"),
                ("nvmlClocksEventReasonHwPowerBrakeSlowdown", "hw_power_brake"))
 
-    def __init__(self, index: int) -> None:
+    def __init__(self, index: int, period_s: float = 0.01) -> None:
         self.index = index
+        self.period_s = period_s
         self.samples: list[tuple[float, int]] = []
         self.max_mhz = None
         self.stop = threading.Event()
@@ -240,7 +241,7 @@ class ClockSampler:
                                      nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
             except Exception:
                 pass
-            self.stop.wait(0.01)
+            self.stop.wait(self.period_s)
 
     def __exit__(self, *exc):
         if self.nv is not None:
@@ -257,7 +258,8 @@ class ClockSampler:
                 if mask and bits & mask:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(reasons), "samples": len(self.samples), "source": "NVML, 10 ms"}
+                "reasons": sorted(reasons), "samples": len(self.samples),
+                "source": f"NVML, every {self.period_s * 1e3:g} ms"}
 
 
 # --------------------------------------------------------------- timing helpers
@@ -452,7 +454,7 @@ def b200_arm(a) -> None:
     dsrc = grid.device_snapshots(nt_dev)
     torch.cuda.synchronize()
     sim = resident_sim(grid, dsrc, zyx, a, plan["start"])
-    with ClockSampler(local) as clocks:
+    with ClockSampler(local, period_s=0.001) as clocks:  # a few ms of timed region: sample every ms
         run_ms, timer, cnt, lead_ms = timed_run(ranks, sim, a.steps)
     launch_ms = timer.durations_ms()
     launch_steps = timer.steps
