@@ -240,7 +240,7 @@ def test_integration_stub_matches_the_binding():
         exec(compile(block, "INTEGRATION.md", "exec"), ns)
     finally:
         ctypes.CDLL = real_cdll
-    for name in ("opb_field", "opb_roms_fields", "opb_time", "opb_particles", "opb_scalars"):
+    for name in ("opb_field", "opb_roms_fields", "opb_time", "opb_particles", "opb_scalars", "opb_records"):
         stub, ours = ns[name], getattr(_lib, name)
         assert ctypes.sizeof(stub) == ctypes.sizeof(ours), name
         for fname, _ in ours._fields_:
