@@ -74,8 +74,21 @@ class Timestepper(abc.ABC):
         self._index_padding = 0
         self.set_index_padding(index_padding)
 
+    # the last time asked for and its index (the planner asks for each step's end time twice: as the end
+    # of one step and the start of the next)
+    _time_index_memo: tuple | None = None
+
     def get_time_index(self, time: T) -> np.float64:
         """timesteppers.py:64-85: searchsorted plus the fraction within the interval."""
+        memo = self._time_index_memo
+        if memo is not None and memo[0] is self._time_array and type(time) is memo[1] and time == memo[2]:
+            return memo[3]
+        r = self._get_time_index(time)
+        if isinstance(time, (float, np.float64)):
+            self._time_index_memo = (self._time_array, type(time), time, r)
+        return r
+
+    def _get_time_index(self, time: T) -> np.float64:
         fast = self._float_times()
         if fast is not None and isinstance(time, (float, np.float64)):
             # the same arithmetic on Python floats (IEEE doubles, as numpy's float64 scalars): bisect_right
@@ -312,6 +325,7 @@ class Timestepper(abc.ABC):
         steps: list[list] = []
         needed: set[int] = set()
         end_times = []
+        last_snapshot = min(f.num_timesteps for f in td.values()) - 1 if td else None
         while len(steps) < min(max_steps, MAX_FUSED_STEPS):
             if recorder is not None and steps and recorder.full(self._iteration, len(steps) + 1):
                 break  # the launch's recorded states would pass their memory budget
@@ -321,7 +335,7 @@ class Timestepper(abc.ABC):
                 break
             its = {int(divmod(t, 1)[0]) for t in tidxs}
             more = needed | its | {i + 1 for i in its}
-            if len(more) > capacity or any(i + 1 >= f.num_timesteps for f in td.values() for i in its):
+            if len(more) > capacity or (last_snapshot is not None and max(its) + 1 > last_snapshot):
                 break
             if pairs and len(starts | its) > pair_capacity:
                 break
