@@ -480,7 +480,18 @@ def _roms_geometry(fs, roles: dict[str, str]) -> bool:
 def use_pairs(launcher: Launcher, td: dict[str, TimeDependentField], nparticles: int,
               roles: dict[str, str] | None = None) -> bool:
     """Snapshot pairs apply to the float64 steppers on the ROMS layout and geometry with float32/float64
-    storage."""
+    storage (the answer is kept per launcher for the same fields, count and module settings)."""
+    key = (SNAPSHOT_PAIRS, PAIR_CELLS_PER_PARTICLE, launcher.arithmetic, nparticles,
+           tuple(sorted((roles or {}).items())), tuple((n, id(f)) for n, f in td.items()))
+    cache = launcher.__dict__.setdefault("_use_pairs_cache", {})
+    hit = cache.get(key)
+    if hit is None:
+        hit = cache[key] = _use_pairs(launcher, td, nparticles, roles)
+    return hit
+
+
+def _use_pairs(launcher: Launcher, td: dict[str, TimeDependentField], nparticles: int,
+               roles: dict[str, str] | None = None) -> bool:
     if SNAPSHOT_PAIRS == "never" or launcher.arithmetic != "float64" or set(td) != {"u", "v", "w", "zeta"}:
         return False
     if not roms_geometry(launcher, roles):
@@ -534,6 +545,16 @@ def pair_layout(launcher: Launcher, td: dict[str, TimeDependentField], roles: di
     layout = SNAPSHOT_LAYOUT if layout is None else layout
     if layout not in ("pairs", "quads", "octets"):
         raise ValueError(f"unknown pair layout {layout!r}")
+    key = (layout, BUNDLE_2D, tuple(sorted((roles or {}).items())), tuple((n, id(f)) for n, f in td.items()))
+    cache = launcher.__dict__.setdefault("_pair_layout_cache", {})
+    plan = cache.get(key)
+    if plan is None:
+        plan = cache[key] = _pair_layout(launcher, td, roles, layout)
+    return plan
+
+
+def _pair_layout(launcher: Launcher, td: dict[str, TimeDependentField], roles: dict[str, str] | None,
+                 layout: str) -> PairPlan:
     if not td or not all(f.storage == "float32" for f in td.values()):
         return PairPlan()
     fs = launcher.fieldset
@@ -666,28 +687,39 @@ def window_fields(launcher: Launcher, needed: list[int], td: dict[str, TimeDepen
     for name in _abi.ROMS_FIELDS:
         field = fs[roles.get(name, name)]
         if name in td:
-            f = _lib.opb_field()
-            f.is_static = 0
-            f.dtype = _STORAGE_CODE[field.storage]
+            f = _lib.opb_field.from_buffer_copy(_td_skeleton(field, name))
             for k in needed if acquire else ():
                 f.data[slot[k]] = _abi._ptr(field.snapshot(k, keep))
                 sc = field.snapshot_scales(k)
                 if sc is not None:
                     f.scale[slot[k]] = _abi._ptr(sc)
             f.nslots = len(needed)
-            shape = field.spatial_shape
-            offsets = field.active_offsets
-            nd = _abi.ROMS_NDIM[name]
-            if len(shape) != nd:
-                raise ValueError(f"field '{name}' must have {nd} active dimensions")
-            f.ndim = nd
-            for d in range(nd):
-                f.shape[d] = shape[d]
-                f.offset[d] = offsets[d]
         else:
             f = _static_struct(field, name)
         setattr(rf, name, f)
     return rf, dtype
+
+
+def _td_skeleton(field, name: str):
+    """opb_field of a time-dependent field without its snapshot pointers (storage dtype, shape, offsets;
+    built once per field and slot name)."""
+    cache = field.__dict__.setdefault("_opb_skeletons", {})
+    f = cache.get(name)
+    if f is None:
+        f = _lib.opb_field()
+        f.is_static = 0
+        f.dtype = _STORAGE_CODE[field.storage]
+        shape = field.spatial_shape
+        offsets = field.active_offsets
+        nd = _abi.ROMS_NDIM[name]
+        if len(shape) != nd:
+            raise ValueError(f"field '{name}' must have {nd} active dimensions")
+        f.ndim = nd
+        for d in range(nd):
+            f.shape[d] = shape[d]
+            f.offset[d] = offsets[d]
+        cache[name] = f
+    return f
 
 
 def _static_struct(field, name: str):
