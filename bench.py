@@ -220,6 +220,8 @@ class ClockSampler:
         self.nv = None
 
     def __enter__(self):
+        """Start sampling (again: the samples of every ``with`` block add up)."""
+        self.stop.clear()
         try:
             import pynvml as nv
 
@@ -454,7 +456,10 @@ def b200_arm(a) -> None:
     dsrc = grid.device_snapshots(nt_dev)
     torch.cuda.synchronize()
     sim = resident_sim(grid, dsrc, zyx, a, plan["start"])
-    with ClockSampler(local, period_s=0.001) as clocks:  # a few ms of timed region: sample every ms
+    # clocks during the three timed regions of the resident arm (the window, the amortised steps and
+    # the plain steps): a few ms each, sampled every ms
+    clocks = ClockSampler(local, period_s=0.001)
+    with clocks:
         run_ms, timer, cnt, lead_ms = timed_run(ranks, sim, a.steps)
     launch_ms = timer.durations_ms()
     launch_steps = timer.steps
@@ -465,7 +470,8 @@ def b200_arm(a) -> None:
     amort = None
     if plan["boundary"] is not None:
         sim = resident_sim(grid, dsrc, zyx, a, plan["boundary"])
-        am_ms, _, am_cnt, _ = timed_run(ranks, sim, plan["resort_every"])
+        with clocks:
+            am_ms, _, am_cnt, _ = timed_run(ranks, sim, plan["resort_every"])
         amort = {"value": world * n * plan["resort_every"] / (am_ms * 1e-3), "unit": UNIT,
                  "steps": plan["resort_every"], "first_step": plan["boundary"],
                  "ms_per_step": am_ms / plan["resort_every"], "sorts": len(am_cnt.sorts),
@@ -479,7 +485,8 @@ def b200_arm(a) -> None:
         for _ in range(a.steps):
             sim.step()
 
-    step_ms = ranks.timed_ms(steps_one_by_one)
+    with clocks:
+        step_ms = ranks.timed_ms(steps_one_by_one)
     sim.synchronize()
     del sim, dsrc
     torch.cuda.empty_cache()
