@@ -51,7 +51,7 @@ def time_ab3(time_array, fields: dict, hc: float, nz: int, dt: float, zyx, *, bu
              max_steps: int = 30, warmup: int = 1) -> dict:
     """AB3 steps of the reference's ROMS preset on ``fields`` (u, v, w, zeta with a leading time axis;
     h, dx, dy, C) from the release ``zyx``: ``warmup`` untimed steps, then as many timed steps as fit
-    ``budget_s`` (at most ``max_steps``, at least 1), judged by the warm-up's duration."""
+    ``budget_s`` (at most ``max_steps``, at least 1), estimated from the warm-up's duration."""
     from oracle.ref_import import import_compiled
 
     op = import_compiled()
