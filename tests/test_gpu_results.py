@@ -233,3 +233,57 @@ def test_sort_in_id_ranges_is_the_global_order_within_each_range():
     rc = lib.opb_sort_particles_ranges(ctypes.byref(_abi.particles_struct(Q)), ctypes.byref(dims), None, None, 2,
                                        perm.data_ptr(), ws.data_ptr(), ws.numel(), None)
     assert rc == _lib.EINVAL
+
+
+@pytest.mark.parametrize("n", [1, 3, 5])
+def test_results_with_fewer_particles_than_ranges(n):
+    """result_ranges=4 with fewer particles than ranges: as many ranges as particles, one launch each."""
+    c = CASES["ab3_f32"]
+    gold = load("ab3_f32.npz")
+    grid = SyntheticROMS(c["grid"])
+    z, y, x = grid.release(c["n"])
+    sim = build_sim(grid.oracle_fields(), hc=grid.hc, nz=grid.spec.nz, scheme="ab3", dt=c["dt"], z=z[:n], y=y[:n],
+                    x=x[:n], result_ranges=4)
+    out = _host_buffers(sim)
+    sim.run(c["steps"], results=out)
+    sim.synchronize()
+    for name in NAMES:
+        assert same_bits(out[name].numpy(), gold[name][:n]), name
+
+
+def test_record_budget_shortens_launches_not_results(tmp_path, monkeypatch):
+    """Events at every step with a record budget of two states per launch: the launches stop at the budget,
+    the rows equal step mode's."""
+    from b200_runner import b200_fieldset
+
+    import offline_particles_b200 as opb
+    from offline_particles_b200 import simulation as simmod
+    from offline_particles_b200.output import NpyOutputBuilder, linearly_interpolate_fields
+
+    c = CASES["ab3_f32"]
+    grid = SyntheticROMS(c["grid"])
+    fields = grid.oracle_fields()
+    z, y, x = grid.release(c["n"])
+    rows = {}
+    for mode in ("step", "run"):
+        if mode == "run":
+            monkeypatch.setattr(simmod, "RECORD_BUDGET_BYTES", 33 * c["n"] * 2)
+        fs = b200_fieldset(fields, grid.hc, grid.spec.nz)
+        t_arr = np.arange(fields["u"].shape[0], dtype=np.float64) * 3600.0
+        sb = opb.SimulationBuilder(opb.roms.ab3_w_advection_timestepper(t_arr, np.float64(c["dt"])), fs)
+        ob = NpyOutputBuilder("o", tmp_path / mode)
+        ob.add_output(*linearly_interpolate_fields(fs, "h", "u"))
+        sb.add_output_writer(ob, n=1)
+        sim = sb.build_simulation(c["n"])
+        sim.set_indices(z, y, x)
+        sim.set_particle_field("status", 10)
+        if mode == "step":
+            for _ in range(40):
+                sim.step()
+        else:
+            sim.run(40)
+        sim.synchronize()
+        sim.close_outputs()
+        rows[mode] = {k: np.load(tmp_path / mode / f"{k}.npy") for k in ("time", "h", "u")}
+    for k, v in rows["step"].items():
+        assert v.shape[0] == 41 and same_bits(rows["run"][k], v), k
