@@ -259,12 +259,14 @@ class Simulation:
         reader = _ResultReader(self, results) if results is not None else None
         ts = self._timestepper
         ts._prefetch_limit = ts.snapshot_horizon(nsteps)
+        ok = False
         try:
             self._run(nsteps, reader)
+            ok = True
         finally:
             ts._prefetch_limit = None
-        if reader is not None:
-            reader.finish()
+            if reader is not None:
+                reader.finish(read=ok)
 
     def _record_buffers(self, count: int) -> dict[str, torch.Tensor]:
         """Device buffers for ``count`` recorded states (grown on demand, reused by later launches in stream
@@ -531,10 +533,10 @@ class _ResultReader:
     def discard(self) -> None:
         self.read.clear()
 
-    def finish(self) -> None:
-        """Read what the ranges did not (all of it when the last launch was not split), then let the
-        current stream wait for the copies."""
-        if not self.ranges or len(self.read) < len(self.ranges):
+    def finish(self, read: bool = True) -> None:
+        """Read what the ranges did not (all of it when the last launch was not split; nothing after a
+        failed run), then let the current stream wait for the copies already queued."""
+        if read and (not self.ranges or len(self.read) < len(self.ranges)):
             self._read(0, len(self.sim._particles))
         if self.began:
             torch.cuda.current_stream(self.sim._particles.device).wait_stream(self.stream)
