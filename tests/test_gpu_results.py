@@ -287,3 +287,19 @@ def test_record_budget_shortens_launches_not_results(tmp_path, monkeypatch):
         rows[mode] = {k: np.load(tmp_path / mode / f"{k}.npy") for k in ("time", "h", "u")}
     for k, v in rows["step"].items():
         assert v.shape[0] == 41 and same_bits(rows["run"][k], v), k
+
+
+def test_results_of_a_run_that_raises():
+    """A run that steps onto the last snapshot time raises as the reference does; the copies already queued
+    are joined, and the simulation stays usable."""
+    from offline_particles_b200.synth import GridSpec
+
+    g = SyntheticROMS(GridSpec(nx=16, ny=12, nz=4, nt=2, seed=3, dtype="float32"))
+    z, y, x = g.release(8)
+    sim = build_sim(g.oracle_fields(), hc=g.hc, nz=g.spec.nz, scheme="ab3", dt=1800.0, z=z, y=y, x=x,
+                    result_ranges=2)
+    out = _host_buffers(sim)
+    with pytest.raises((IndexError, ValueError)):
+        sim.run(3, results=out)
+    sim.synchronize()
+    assert np.asarray(sim.particles["zidx"]).shape == (8,)
