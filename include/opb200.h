@@ -440,16 +440,6 @@ int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *
 int opb_sort_particles_ranges(const opb_particles *p, const int64_t shape[3], const int64_t *ids,
                               const int64_t *bounds, int32_t nranges, int32_t *perm, void *workspace,
                               size_t workspace_bytes, void *stream);
-/* A re-sort of particles that moved little since a full sort: as
- * opb_sort_particles_ranges (nranges 1 to 4; bounds may be NULL for one range),
- * but every run of `block` consecutive storage slots (block must be 2048) is
- * ordered only among itself, by (cell key, slot): a bitonic sort in shared
- * memory instead of a radix sort over all particles.  No particle leaves its
- * run, so id ranges whose bounds the runs straddle keep their slots (the range
- * index is part of the key).  Same workspace as opb_sort_particles. */
-int opb_sort_particles_blocks(const opb_particles *p, const int64_t shape[3], const int64_t *ids,
-                              const int64_t *bounds, int32_t nranges, int32_t block, int32_t *perm,
-                              void *workspace, size_t workspace_bytes, void *stream);
 /* dst.f[j] = src.f[perm[j]] for status and every float64 field present in
  * both (src and dst must not alias), and dst_ids[j] = src_ids[perm[j]] when
  * id arrays are given. */

@@ -140,8 +140,6 @@ SIGNATURES_OTHER = {
     "opb_sort_particles": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
     "opb_sort_particles_ranges": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP, ctypes.c_int32, _VP,
                                    _VP, ctypes.c_size_t, _VP], ctypes.c_int),
-    "opb_sort_particles_blocks": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP, ctypes.c_int32,
-                                   ctypes.c_int32, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
     "opb_gather_particles": ([_P(opb_particles), _P(opb_particles), _VP, _VP, _VP, _VP], ctypes.c_int),
     "opb_sort_workspace_bytes": ([ctypes.c_int64], ctypes.c_size_t),
     "opb_sort_particles_noalloc": ([_P(opb_particles), _P(ctypes.c_int64 * 3), _VP, _VP], ctypes.c_int),
@@ -150,7 +148,6 @@ SIGNATURES_OTHER = {
                            ctypes.c_int32, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
 }
 NOALLOC_MAX_PARTICLES = 1 << 20
-LOCAL_SORT_BLOCK = 2048  # storage slots a block-local re-sort orders among themselves
 
 _lock = threading.Lock()
 _lib: ctypes.CDLL | None = None

@@ -107,44 +107,6 @@ int shift_for(int n, int extra) {
     return s;
 }
 
-// Block-local ordering: each run of kLocalBlock consecutive storage slots is
-// sorted among itself by (cell key, slot), a bitonic sort in shared memory.
-// Particles that moved little since the last full sort are almost in place:
-// this restores the order inside each run at a fraction of a full radix sort,
-// and nobody crosses a run boundary.
-constexpr int kLocalBlock = 2048;
-constexpr int kLocalThreads = kLocalBlock / 2;
-
-__global__ void __launch_bounds__(kLocalThreads) k_block_sort(const uint32_t *__restrict__ keys, long long n,
-                                                              int32_t *__restrict__ perm) {
-    __shared__ unsigned long long s[kLocalBlock];
-    const long long base = (long long)blockIdx.x * kLocalBlock;
-    for (int t = threadIdx.x; t < kLocalBlock; t += kLocalThreads) {
-        const long long i = base + t;
-        // the slot in the low bits: ties keep storage order, so the result is the same every time
-        s[t] = i < n ? ((unsigned long long)keys[i] << 32) | (unsigned long long)t : ~0ull;
-    }
-    __syncthreads();
-    for (int size = 2; size <= kLocalBlock; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            const int t = threadIdx.x;  // one compare-exchange per thread: kLocalBlock / 2 pairs
-            const int lo = 2 * t - (t & (stride - 1));
-            const int hi = lo + stride;
-            const bool up = (lo & size) == 0;
-            const unsigned long long a = s[lo], b = s[hi];
-            if ((a > b) == up) {
-                s[lo] = b;
-                s[hi] = a;
-            }
-            __syncthreads();
-        }
-    }
-    for (int t = threadIdx.x; t < kLocalBlock; t += kLocalThreads) {
-        const long long j = base + t;
-        if (j < n) perm[j] = (int32_t)(base + (long long)(s[t] & 0xffffffffull));
-    }
-}
-
 size_t cub_temp_bytes(long long n) {
     size_t bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
@@ -359,7 +321,7 @@ namespace {
 // opb_sort_particles, and with nranges > 1 opb_sort_particles_ranges (bounds: nranges + 1 host values)
 int sort_particles(const char *what, const opb_particles *p, const int64_t shape[3], const int64_t *range_ids,
                    const int64_t *bounds, int nranges, int32_t *perm, void *workspace, size_t workspace_bytes,
-                   void *stream, bool local = false) {
+                   void *stream) {
     if (!p) return fail(OPB_EINVAL, "%s: particles is NULL", what);
     if (p->n < 0 || p->n > 0x7fffffffLL) return fail(OPB_EINVAL, "%s: particle count out of range", what);
     if (p->n == 0) return OPB_OK;
@@ -406,14 +368,6 @@ int sort_particles(const char *what, const opb_particles *p, const int64_t shape
     k_cell_keys<<<grid, kBlock, 0, st>>>(k, keys_in, ids_in);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
-    if (local) {
-        const unsigned blocks = (unsigned)((p->n + kLocalBlock - 1) / kLocalBlock);
-        k_block_sort<<<blocks, kLocalThreads, 0, st>>>(keys_in, p->n, perm);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
-        opb::clear_error();
-        return OPB_OK;
-    }
     e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, ids_in, perm, (int)p->n, 0, 32, st);
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: radix sort: %s", what, cudaGetErrorString(e));
     opb::clear_error();
@@ -428,16 +382,6 @@ int opb_sort_particles(const opb_particles *p, const int64_t shape[3], int32_t *
                        size_t workspace_bytes, void *stream) {
     return sort_particles("opb_sort_particles", p, shape, nullptr, nullptr, 1, perm, workspace, workspace_bytes,
                           stream);
-}
-
-int opb_sort_particles_blocks(const opb_particles *p, const int64_t shape[3], const int64_t *ids,
-                              const int64_t *bounds, int32_t nranges, int32_t block, int32_t *perm,
-                              void *workspace, size_t workspace_bytes, void *stream) {
-    const char *what = "opb_sort_particles_blocks";
-    if (block != kLocalBlock) return fail(OPB_EINVAL, "%s: block must be %d", what, kLocalBlock);
-    if (nranges < 1 || nranges > kMaxRanges) return fail(OPB_EINVAL, "%s: 1 to %d ranges", what, kMaxRanges);
-    if (nranges > 1 && !bounds) return fail(OPB_EINVAL, "%s: the range bounds are NULL", what);
-    return sort_particles(what, p, shape, ids, bounds, nranges, perm, workspace, workspace_bytes, stream, true);
 }
 
 int opb_sort_particles_ranges(const opb_particles *p, const int64_t shape[3], const int64_t *ids,

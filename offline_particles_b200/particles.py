@@ -186,14 +186,11 @@ class Particles(_FrozenArrayMapping):
             return ()
         return object.__getattribute__(self, "_range")
 
-    def sort(self, shape: tuple[int, int, int], id_bounds: tuple[int, ...] | None = None,
-             local: bool = False) -> None:
+    def sort(self, shape: tuple[int, int, int], id_bounds: tuple[int, ...] | None = None) -> None:
         """Reorder storage by the Morton code of each particle's cell on the centred ``(z, y, x)`` grid.
         ``id_bounds``: 0 = b0 < b1 < ... < bR = n, R at most 4: order within the id ranges
         ``[b[r], b[r + 1])`` (``opb_sort_particles_ranges``), each kept in those storage slots, so that
-        each range's results can be read back on their own.  ``local``: order each run of
-        ``LOCAL_SORT_BLOCK`` storage slots among itself only (``opb_sort_particles_blocks``), a re-sort
-        for particles that moved little since a full sort."""
+        each range's results can be read back on their own."""
         from . import _lib
         from .kernels import _abi
 
@@ -216,13 +213,7 @@ class Particles(_FrozenArrayMapping):
         dims = (ctypes.c_int64 * 3)(*[int(s) for s in shape])
         stream = stream_handle(self.device)
         order = self.order
-        if local:
-            bounds = None if id_bounds is None else (ctypes.c_int64 * len(id_bounds))(*id_bounds)
-            _lib.call("opb_sort_particles_blocks", ctypes.byref(src), ctypes.byref(dims),
-                      None if order is None or id_bounds is None else order.data_ptr(), bounds,
-                      1 if id_bounds is None else len(id_bounds) - 1, _lib.LOCAL_SORT_BLOCK, perm.data_ptr(),
-                      ws.data_ptr(), ws.numel(), stream)
-        elif id_bounds is None:
+        if id_bounds is None:
             _lib.call("opb_sort_particles", ctypes.byref(src), ctypes.byref(dims), perm.data_ptr(), ws.data_ptr(),
                       ws.numel(), stream)
         else:

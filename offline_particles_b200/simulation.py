@@ -26,9 +26,6 @@ from .timesteppers import Timestepper
 # steps between spatial re-sorts of particle storage (particles drift ~0.03 cells per step at
 # 0.5 m/s, dx = 2 km, dt = 120 s, so locality decays slowly)
 DEFAULT_SORT_INTERVAL = 64
-# every this many re-sorts is a full radix sort; the ones between order each run of 2048 storage slots
-# among itself (particles moved only a few cells since the last full sort); 1: always full
-FULL_SORT_EVERY = 4
 
 
 class Simulation:
@@ -70,7 +67,6 @@ class Simulation:
         self._readback_stream: torch.cuda.Stream | None = None
         self._records: dict[str, torch.Tensor] | None = None  # states recorded inside fused launches
         self._steps_since_sort: int | None = None  # None: never sorted
-        self._sorts_since_full = 0  # re-sorts since the last full sort (a full sort counts 1)
         if self._sort_interval > 0:
             self._particles.reserve_sort()  # the sort's scratch now, not inside the first run
         self._timestepper.reserve_launch_buffers(self._launcher, len(self._particles))
@@ -207,13 +203,9 @@ class Simulation:
         return self._sort_interval
 
     def sort_particles(self) -> None:
-        """Reorder particle storage by cell now, a full sort (results are unchanged; locality improves)."""
-        self._sort(local=False)
-
-    def _sort(self, local: bool) -> None:
+        """Reorder particle storage by cell now (results are unchanged; locality improves)."""
         fs = self._fieldset
-        self._particles.sort((fs.z_size, fs.y_size, fs.x_size), id_bounds=self._id_bounds, local=local)
-        self._sorts_since_full = self._sorts_since_full + 1 if local else 1
+        self._particles.sort((fs.z_size, fs.y_size, fs.x_size), id_bounds=self._id_bounds)
         self._steps_since_sort = 0
 
     def _maybe_sort(self) -> int:
@@ -226,9 +218,7 @@ class Simulation:
         ts = self._timestepper
         if self._steps_since_sort is None or (self._steps_since_sort >= self._sort_interval
                                               and ts.at_interval_start):
-            # a full sort first and every FULL_SORT_EVERY-th time; block-local re-sorts between
-            local = self._steps_since_sort is not None and self._sorts_since_full % max(1, FULL_SORT_EVERY) != 0
-            self._sort(local)
+            self.sort_particles()
         return ts.steps_to_interval_end(self._sort_interval - self._steps_since_sort)
 
     def step(self) -> None:

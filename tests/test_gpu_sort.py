@@ -102,51 +102,3 @@ def test_results_do_not_depend_on_sorting(sort_interval, mode):
     for name in gold:
         if name in final:
             assert same_bits(final[name], gold[name]), f"{name}: {mismatch_report(final[name], gold[name])}"
-
-
-def test_block_local_resort():
-    """opb_sort_particles_blocks: each run of 2048 storage slots ordered among itself by (cell key, slot),
-    nobody leaves its run; with id ranges the range index leads the key."""
-    import torch
-
-    from offline_particles_b200 import _lib
-    from offline_particles_b200.kernels import _abi
-    from offline_particles_b200.particles import Particles
-
-    rng = np.random.default_rng(21)
-    n, shape, B = 2048 * 7 + 333, (50, 768, 1024), _lib.LOCAL_SORT_BLOCK
-    z = rng.uniform(-1, 50, n)
-    y = rng.uniform(-3, 770, n)
-    x = rng.uniform(-3, 1030, n)
-    z[:3] = [np.nan, np.inf, -1e300]
-    st = np.zeros(n, np.uint8)
-    st[rng.integers(0, n, 700)] = 0x82
-    P = Particles(n, status=np.uint8, zidx=np.float64, yidx=np.float64, xidx=np.float64, z=np.float64)
-    for name, v in (("zidx", z), ("yidx", y), ("xidx", x), ("status", st)):
-        P[name].copy_(torch.from_numpy(v))
-    lib = _lib.load()
-    ws = torch.empty(lib.opb_sort_workspace_bytes(n), dtype=torch.uint8, device="cuda")
-    perm = torch.empty(n, dtype=torch.int32, device="cuda")
-    dims = (ctypes.c_int64 * 3)(*shape)
-    keys = host_keys(st, z, y, x, shape).astype(np.int64)
-    for bounds in (None, (0, 5000, n)):
-        arr = None if bounds is None else (ctypes.c_int64 * len(bounds))(*bounds)
-        _lib.call("opb_sort_particles_blocks", ctypes.byref(_abi.particles_struct(P)), ctypes.byref(dims), None,
-                  arr, 1 if bounds is None else len(bounds) - 1, B, perm.data_ptr(), ws.data_ptr(), ws.numel(),
-                  None)
-        p = perm.cpu().numpy().astype(np.int64)
-        r = np.zeros(n, np.int64) if bounds is None else np.searchsorted(np.asarray(bounds[1:-1]), np.arange(n),
-                                                                          side="right")
-        full = r * (1 << 32) + keys
-        for lo in range(0, n, B):
-            hi = min(lo + B, n)
-            blk = p[lo:hi]
-            assert np.array_equal(np.sort(blk), np.arange(lo, hi)), "a particle left its run"
-            k = full[blk]
-            assert np.all(np.diff(k) >= 0), "a run not in key order"
-            assert np.all(np.diff(blk)[np.diff(k) == 0] > 0), "ties not in slot order"
-        if bounds is not None:
-            assert np.all(p[:5000] < 5000) and np.all(p[5000:] >= 5000), "an id range lost its slots"
-    bad = lib.opb_sort_particles_blocks(ctypes.byref(_abi.particles_struct(P)), ctypes.byref(dims), None, None, 1,
-                                        1024, perm.data_ptr(), ws.data_ptr(), ws.numel(), None)
-    assert bad == _lib.EINVAL
