@@ -213,3 +213,37 @@ def test_streamed_week_matches_oracle():
     for name, got in out.items():
         got = got.numpy()[idx]
         assert same_bits(got, p[name]), f"{name}: {mismatch_report(got, p[name])}"
+
+
+def test_end_to_end_path_at_size_matches_oracle(headline):
+    """The end-to-end configuration the benchmark times: the 4,194,304-particle release from pinned host
+    arrays, every snapshot uploaded from pinned host tensors through 8-slot rings, 20 AB3 steps, the results
+    read back in original order over two id ranges (the last launch split): every 64th particle against the
+    oracle, bit for bit."""
+    import torch
+    from b200_runner import STAGGERS
+
+    import offline_particles_b200 as opb
+
+    g, fields = headline
+    nt = fields["u"].shape[0]
+    kw = {k: opb.TimeDependentField(torch.from_numpy(fields[k]).pin_memory(), *STAGGERS[k], ring_size=8)
+          for k in ("u", "v", "w", "zeta")}
+    kw.update({k: opb.StaticField.from_numpy(fields[k], *STAGGERS[k]) for k in ("h", "dx", "dy", "C")})
+    fs = opb.Fieldset(nt, g.spec.nz, g.spec.ny, g.spec.nx, constants={"hc": g.hc, "NZ": g.spec.nz}, **kw)
+    ts = opb.roms.ab3_w_advection_timestepper(g.time_array[:nt], np.float64(120.0))
+    sim = opb.SimulationBuilder(ts, fs).build_simulation(N_FULL, result_ranges=2)
+    z, y, x = g.release(N_FULL, seed=1000)
+    hz, hy, hx = (torch.from_numpy(v).pin_memory() for v in (z, y, x))
+    names = ("zidx", "yidx", "xidx", "status", "z")
+    out = {k: torch.empty(N_FULL, dtype=sim.device_particles[k].dtype, pin_memory=True) for k in names}
+    sim.reserve_results(out)
+    sim.set_indices(hz, hy, hx)
+    sim.set_particle_field("status", opb.kernels.ParticleStatus.MULTISTEP_1)
+    sim.run(20, results=out)
+    sim.synchronize()
+    idx = np.arange(0, N_FULL, SUBSET)
+    ref = _oracle(g, fields, "ab3", 120.0, 20, z[idx], y[idx], x[idx])
+    for name in names:
+        got = out[name].numpy()[idx]
+        assert same_bits(got, ref[name]), f"{name}: {mismatch_report(got, ref[name])}"
