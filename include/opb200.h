@@ -456,7 +456,7 @@ int opb_gather_particles(const opb_particles *src, const opb_particles *dst, con
  * opb_sort_particles but takes its scratch from a static device array inside
  * this library instead of a caller workspace, and calls no allocating routine.
  *
- *   - The array is OPB_NOALLOC_SCRATCH_BYTES (17 MiB).  Every GPU that loads
+ *   - The array is OPB_NOALLOC_SCRATCH_BYTES (13 MiB).  Every GPU that loads
  *     the library holds it until the process exits.
  *   - At most OPB_NOALLOC_MAX_PARTICLES particles per call; more is rejected
  *     with OPB_EINVAL and a message (use opb_sort_particles then).
@@ -476,8 +476,8 @@ int opb_gather_particles(const opb_particles *src, const opb_particles *dst, con
  *     and ids in full before reading them).  Calls that overlap on the GPU
  *     race on it: issue them on one stream, or wait for one before the next. */
 #define OPB_NOALLOC_MAX_PARTICLES (1 << 20)
-#define OPB_NOALLOC_CUB_TEMP_BYTES (1u << 20)
-#define OPB_NOALLOC_SCRATCH_BYTES ((size_t)16 * OPB_NOALLOC_MAX_PARTICLES + OPB_NOALLOC_CUB_TEMP_BYTES)
+#define OPB_NOALLOC_SORT_TEMP_BYTES (1u << 20)
+#define OPB_NOALLOC_SCRATCH_BYTES ((size_t)12 * OPB_NOALLOC_MAX_PARTICLES + OPB_NOALLOC_SORT_TEMP_BYTES)
 
 int opb_sort_particles_noalloc(const opb_particles *p, const int64_t shape[3], int32_t *perm, void *stream);
 

@@ -7,7 +7,6 @@
 // no result -- only where each particle's state is stored.
 #include <cuda_runtime.h>
 
-#include <cub/device/device_radix_sort.cuh>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -15,6 +14,7 @@
 
 #include "opb200.h"
 #include "opb_errors.h"
+#include "opb_radix.cuh"
 
 namespace opb_sort {
 namespace {
@@ -55,7 +55,7 @@ struct KeyArgs {
     int nbounds;
 };
 
-__global__ void __launch_bounds__(kBlock) k_cell_keys(KeyArgs a, uint32_t *keys, int32_t *ids) {
+__global__ void __launch_bounds__(kBlock) k_cell_keys(KeyArgs a, uint32_t *keys) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     uint32_t key = kInactiveKey;
@@ -76,7 +76,6 @@ __global__ void __launch_bounds__(kBlock) k_cell_keys(KeyArgs a, uint32_t *keys,
         key = (r << 30) | (key & kRangeKeyMask);
     }
     keys[i] = key;
-    ids[i] = (int32_t)i;
 }
 
 struct GatherArgs {
@@ -107,14 +106,7 @@ int shift_for(int n, int extra) {
     return s;
 }
 
-size_t cub_temp_bytes(long long n) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
-                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, 32);
-    return bytes;
-}
-
-size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+using opb_radix::align256;
 
 // ------------------------------------------------------------ segment sort
 // Compact position q enumerates the segments' particles in storage order;
@@ -137,7 +129,7 @@ __device__ __forceinline__ int segment_of(const int64_t *cstart, int nseg, long 
     return lo;
 }
 
-__global__ void __launch_bounds__(kBlock) k_segment_keys(SegArgs a, uint64_t *keys, int32_t *ids, int32_t *slot) {
+__global__ void __launch_bounds__(kBlock) k_segment_keys(SegArgs a, uint64_t *keys, int32_t *slot) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= a.m) return;
     const int s = segment_of(a.seg_cstart, a.nseg, q);
@@ -150,7 +142,6 @@ __global__ void __launch_bounds__(kBlock) k_segment_keys(SegArgs a, uint64_t *ke
         key = (spread3(z) << 2) | (spread3(y) << 1) | spread3(x);
     }
     keys[q] = ((uint64_t)s << 32) | key;
-    ids[q] = (int32_t)q;
     slot[q] = (int32_t)i;
 }
 
@@ -261,13 +252,6 @@ cudaError_t stage_to_device(void *dst, const void *src, size_t bytes, cudaStream
     return cudaSuccess;
 }
 
-size_t cub_temp_bytes64(long long n, int end_bit) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
-                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, end_bit);
-    return bytes;
-}
-
 int key_end_bit(int nseg) {
     int bits = 0;
     while ((1LL << bits) < (long long)nseg) ++bits;
@@ -296,7 +280,7 @@ SegLayout seg_layout(long long m, int nseg) {
     L.status = take((size_t)m);
     L.fields = take((size_t)m * 8 * 13);
     L.ids = take((size_t)m * 8);
-    L.temp = take(cub_temp_bytes64(m, key_end_bit(nseg)));
+    L.temp = take(opb_radix::temp_bytes<uint64_t>(m));
     L.total = o;
     return L;
 }
@@ -311,7 +295,7 @@ extern "C" {
 
 size_t opb_sort_workspace_bytes(int64_t n) {
     if (n <= 0) return 0;
-    return 3 * align256((size_t)n * 4) + align256(cub_temp_bytes(n));
+    return 3 * align256((size_t)n * 4) + opb_radix::temp_bytes<uint32_t>(n);
 }
 
 }  // extern "C"
@@ -347,7 +331,6 @@ int sort_particles(const char *what, const opb_particles *p, const int64_t shape
     uint32_t *keys_out = (uint32_t *)(ws + a);
     int32_t *ids_in = (int32_t *)(ws + 2 * a);
     void *temp = ws + 3 * a;
-    size_t temp_bytes = workspace_bytes - 3 * a;
     KeyArgs k{};
     k.status = p->status;
     k.zidx = p->zidx;
@@ -365,10 +348,10 @@ int sort_particles(const char *what, const opb_particles *p, const int64_t shape
     for (int j = 0; j < k.nbounds; ++j) k.bound[j] = bounds[j + 1];
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned grid = (unsigned)((p->n + kBlock - 1) / kBlock);
-    k_cell_keys<<<grid, kBlock, 0, st>>>(k, keys_in, ids_in);
+    k_cell_keys<<<grid, kBlock, 0, st>>>(k, keys_in);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
-    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, ids_in, perm, (int)p->n, 0, 32, st);
+    e = opb_radix::radix_sort_index<uint32_t>(keys_in, keys_out, perm, ids_in, p->n, 32, temp, st, nullptr);
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: radix sort: %s", what, cudaGetErrorString(e));
     opb::clear_error();
     return OPB_OK;
@@ -501,12 +484,12 @@ int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int6
     int32_t *perm = (int32_t *)(ws + L.perm);
     int32_t *slot = (int32_t *)(ws + L.slot);
     const unsigned grid = (unsigned)((m + kBlock - 1) / kBlock);
-    k_segment_keys<<<grid, kBlock, 0, st>>>(a, keys_in, ids_in, slot);
+    k_segment_keys<<<grid, kBlock, 0, st>>>(a, keys_in, slot);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
-    size_t temp_bytes = workspace_bytes - L.temp;
-    e = cub::DeviceRadixSort::SortPairs(ws + L.temp, temp_bytes, keys_in, keys_out, ids_in, perm, (int)m, 0,
-                                        key_end_bit(nseg), st);
+    uint64_t *keys_sorted = nullptr;
+    e = opb_radix::radix_sort_index<uint64_t>(keys_in, keys_out, perm, ids_in, m, key_end_bit(nseg), ws + L.temp, st,
+                                              &keys_sorted);
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: radix sort: %s", what, cudaGetErrorString(e));
     // arena -> scratch in sorted order -> arena
     const double *arena[13] = {p->zidx, p->yidx, p->xidx, p->z, p->dxidx0, p->dyidx0, p->dz0,
@@ -539,7 +522,7 @@ int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int6
     if (bucket_bounds) {
         const long long nt = (long long)nseg * (nbuckets + 1);
         k_bucket_bounds<<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-            keys_out, a.seg_start, a.seg_cstart, m, nseg, nbuckets, bucket_shift(a.k, nbuckets), bucket_bounds);
+            keys_sorted, a.seg_start, a.seg_cstart, m, nseg, nbuckets, bucket_shift(a.k, nbuckets), bucket_bounds);
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(OPB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -554,15 +537,16 @@ int opb_sort_segments(const opb_particles *p, const int64_t shape[3], const int6
 // device array, for callers that cannot allocate device memory when they
 // sort.  Sizes are stated in include/opb200.h (OPB_NOALLOC_*).
 //
-// Layout of the array: two key buffers and two id buffers of
-// OPB_NOALLOC_MAX_PARTICLES entries each (the double buffers of the radix
-// sort), then OPB_NOALLOC_CUB_TEMP_BYTES of CUB temporary storage.
+// Layout of the array: two key buffers and one id buffer of
+// OPB_NOALLOC_MAX_PARTICLES entries each (the radix sort's double buffers; the
+// caller's perm is the other id buffer), then OPB_NOALLOC_SORT_TEMP_BYTES for
+// the radix sort's tile counts.
 namespace opb_sort {
 namespace {
 
 constexpr size_t kNoAllocBuf = (size_t)OPB_NOALLOC_MAX_PARTICLES * 4;
-constexpr size_t kNoAllocCubOffset = 4 * kNoAllocBuf;
-static_assert(kNoAllocCubOffset + OPB_NOALLOC_CUB_TEMP_BYTES == OPB_NOALLOC_SCRATCH_BYTES, "scratch layout");
+constexpr size_t kNoAllocTempOffset = 3 * kNoAllocBuf;
+static_assert(kNoAllocTempOffset + OPB_NOALLOC_SORT_TEMP_BYTES == OPB_NOALLOC_SCRATCH_BYTES, "scratch layout");
 
 // Every GPU that loads this library holds this array until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[OPB_NOALLOC_SCRATCH_BYTES];
@@ -624,19 +608,13 @@ extern "C" int opb_sort_particles_noalloc(const opb_particles *p, const int64_t 
     char *ws = (char *)base;
     uint32_t *keys0 = (uint32_t *)ws;
     uint32_t *keys1 = (uint32_t *)(ws + kNoAllocBuf);
-    int32_t *ids0 = (int32_t *)(ws + 2 * kNoAllocBuf);
-    int32_t *ids1 = (int32_t *)(ws + 3 * kNoAllocBuf);
-    void *temp = ws + kNoAllocCubOffset;
-    const int n = (int)p->n;
-    cub::DoubleBuffer<uint32_t> keys(keys0, keys1);
-    cub::DoubleBuffer<int32_t> ids(ids0, ids1);
-    size_t temp_bytes = 0;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys, ids, n, 0, 32);
-    if (e != cudaSuccess)
-        return fail(OPB_ECUDA, "opb_sort_particles_noalloc: radix sort sizing: %s", cudaGetErrorString(e));
-    if (temp_bytes > OPB_NOALLOC_CUB_TEMP_BYTES)
+    int32_t *ids = (int32_t *)(ws + 2 * kNoAllocBuf);
+    void *temp = ws + kNoAllocTempOffset;
+    const long long n = p->n;
+    const size_t temp_bytes = opb_radix::temp_bytes<uint32_t>(n);
+    if (temp_bytes > OPB_NOALLOC_SORT_TEMP_BYTES)
         return fail(OPB_EINVAL, "opb_sort_particles_noalloc: radix sort needs %zu temporary bytes, the static "
-                    "scratch reserves %zu", temp_bytes, (size_t)OPB_NOALLOC_CUB_TEMP_BYTES);
+                    "scratch reserves %zu", temp_bytes, (size_t)OPB_NOALLOC_SORT_TEMP_BYTES);
     KeyArgs k{};
     k.status = p->status;
     k.zidx = p->zidx;
@@ -650,15 +628,13 @@ extern "C" int opb_sort_particles_noalloc(const opb_particles *p, const int64_t 
     k.sy = shift_for(k.ny, 0);
     k.sx = shift_for(k.nx, 2);
     cudaStream_t st = (cudaStream_t)stream;
-    // keys0 and ids0 are written in full before the sort reads them; the sort
-    // itself needs no initial contents in the other buffers or in its temp storage
-    k_cell_keys<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(k, keys0, ids0);
-    e = cudaGetLastError();
+    // keys0 is written in full before the sort reads it; every pass of the sort writes its outputs and its
+    // tile counts in full before reading them, so no buffer of the array needs initial contents
+    k_cell_keys<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(k, keys0);
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles_noalloc: %s", cudaGetErrorString(e));
-    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, ids, n, 0, 32, st);
+    e = opb_radix::radix_sort_index<uint32_t>(keys0, keys1, perm, ids, n, 32, temp, st, nullptr);
     if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles_noalloc: radix sort: %s", cudaGetErrorString(e));
-    e = cudaMemcpyAsync(perm, ids.Current(), (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, st);
-    if (e != cudaSuccess) return fail(OPB_ECUDA, "opb_sort_particles_noalloc: copy: %s", cudaGetErrorString(e));
     opb::clear_error();
     return OPB_OK;
 }

@@ -102,3 +102,97 @@ def test_results_do_not_depend_on_sorting(sort_interval, mode):
     for name in gold:
         if name in final:
             assert same_bits(final[name], gold[name]), f"{name}: {mismatch_report(final[name], gold[name])}"
+
+
+def _particles_with_keys(n, shape, seed):
+    """Particles spread over the grid, a third of them packed into a few cells (long runs of equal keys), some
+    outside it, some inactive; their Morton keys computed on the host."""
+    import torch
+
+    from offline_particles_b200.particles import Particles
+
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    z = rng.uniform(-1, nz + 1, n)
+    y = rng.uniform(-2, ny + 2, n)
+    x = rng.uniform(-2, nx + 2, n)
+    packed = rng.random(n) < 1 / 3
+    z[packed], y[packed], x[packed] = 2.5, rng.integers(3, 5, packed.sum()) + 0.5, 7.5
+    st = np.zeros(n, np.uint8)
+    st[rng.random(n) < 0.05] = 0x82
+    P = Particles(n, status=np.uint8, zidx=np.float64, yidx=np.float64, xidx=np.float64)
+    for name, v in (("zidx", z), ("yidx", y), ("xidx", x), ("status", st)):
+        P[name].copy_(torch.from_numpy(v))
+    return P, host_keys(st, z, y, x, shape)
+
+
+@pytest.mark.parametrize("n", [1, 2, 4095, 4096, 4097, 100_003, 4_194_304 + 17])
+def test_sort_permutation_is_the_stable_key_order(n):
+    """The radix sort's permutation is exactly the stable order of the keys (numpy's stable argsort of the
+    host keys), for counts below, at and across the 4096-key tiles of its passes."""
+    import torch
+
+    from offline_particles_b200 import _lib
+    from offline_particles_b200.kernels import _abi
+
+    shape = (50, 768, 1024)
+    P, keys = _particles_with_keys(n, shape, seed=n)
+    lib = _lib.load()
+    ws = torch.empty(lib.opb_sort_workspace_bytes(n), dtype=torch.uint8, device="cuda")
+    perm = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    _lib.call("opb_sort_particles", ctypes.byref(_abi.particles_struct(P)), ctypes.byref((ctypes.c_int64 * 3)(*shape)),
+              perm.data_ptr(), ws.data_ptr(), ws.numel(), None)
+    assert np.array_equal(perm.cpu().numpy(), np.argsort(keys, kind="stable"))
+
+
+def test_ranged_sort_permutation_is_the_stable_key_order():
+    """Within id ranges: the stable order of (range index, cell key), the range index in the key's top bits."""
+    import torch
+
+    from offline_particles_b200 import _lib
+    from offline_particles_b200.kernels import _abi
+
+    n, shape = 250_001, (40, 512, 512)
+    P, keys = _particles_with_keys(n, shape, seed=11)
+    ids = np.random.default_rng(12).permutation(n).astype(np.int64)
+    bounds = (0, 60_000, 61_000, n)
+    rng_of = np.searchsorted(np.array(bounds[1:-1]), ids, side="right").astype(np.uint64)
+    expect = np.argsort((rng_of << np.uint64(30)) | (keys & np.uint64(0x3FFFFFFF)), kind="stable")
+    lib = _lib.load()
+    ws = torch.empty(lib.opb_sort_workspace_bytes(n), dtype=torch.uint8, device="cuda")
+    perm = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    dev_ids = torch.from_numpy(ids).cuda()
+    _lib.call("opb_sort_particles_ranges", ctypes.byref(_abi.particles_struct(P)),
+              ctypes.byref((ctypes.c_int64 * 3)(*shape)), dev_ids.data_ptr(), (ctypes.c_int64 * 4)(*bounds), 3,
+              perm.data_ptr(), ws.data_ptr(), ws.numel(), None)
+    assert np.array_equal(perm.cpu().numpy(), expect)
+
+
+def test_segment_sort_is_the_stable_key_order_in_each_segment():
+    """The segment sort (64-bit keys: segment above the cell key, five digit passes) leaves in each segment
+    exactly the stable key order of its particles."""
+    import torch
+
+    from offline_particles_b200 import _lib
+    from offline_particles_b200.batching import ARENA_FIELDS
+    from offline_particles_b200.kernels import _abi
+    from offline_particles_b200.particles import Particles
+
+    n, shape = 400_000, (12, 80, 96)
+    Q, keys = _particles_with_keys(n, shape, seed=21)
+    P = Particles(n, **ARENA_FIELDS)
+    for k in ("status", "zidx", "yidx", "xidx"):
+        P[k].copy_(Q[k])
+    ids = torch.arange(n, dtype=torch.int64, device="cuda")
+    starts, counts = [0, 5000, 5001, 70_000, 399_000], [4000, 1, 60_000, 300_000, 1000]
+    lib = _lib.load()
+    ws = torch.empty(int(lib.opb_sort_segments_workspace_bytes(sum(counts), len(starts))), dtype=torch.uint8,
+                     device="cuda")
+    _lib.call("opb_sort_segments", ctypes.byref(_abi.particles_struct(P)), ctypes.byref((ctypes.c_int64 * 3)(*shape)),
+              (ctypes.c_int64 * 5)(*starts), (ctypes.c_int64 * 5)(*counts), 5, ids.data_ptr(), 0, None,
+              ws.data_ptr(), ws.numel(), None)
+    got = ids.cpu().numpy()
+    expect = np.arange(n)
+    for s, c in zip(starts, counts):
+        expect[s:s + c] = s + np.argsort(keys[s:s + c], kind="stable")
+    assert np.array_equal(got, expect)
