@@ -30,11 +30,18 @@ constexpr int kDigits = 256;
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
 
-// keys per thread of a tile: 16 for 32-bit keys (tiles of 4096), 8 for 64-bit keys (2048); the staged
-// tile (keys and values) then takes 32 or 24 KB of shared memory
+// keys per thread of a tile (build knobs): by default 8 for 32-bit and 64-bit keys (tiles of 2048); the staged
+// tile (keys and values) then takes 16 or 24 KB of shared memory.  Measured on 4,194,304 32-bit keys: 8 keys
+// per thread 0.294 ms per sort with the keys, 12 keys 0.295 ms, 16 keys 0.310 ms.
+#ifndef OPB_RADIX_ITEMS32
+#define OPB_RADIX_ITEMS32 8
+#endif
+#ifndef OPB_RADIX_ITEMS64
+#define OPB_RADIX_ITEMS64 8
+#endif
 template <class K>
 __host__ __device__ constexpr int items_per_thread() {
-    return sizeof(K) == 4 ? 16 : 8;
+    return sizeof(K) == 4 ? OPB_RADIX_ITEMS32 : OPB_RADIX_ITEMS64;
 }
 
 template <class K>

@@ -89,13 +89,26 @@ struct GatherArgs {
     long long n;
 };
 
+// d[j] = s[i] for every field of one particle.  All loads are issued before the first store: as far as the
+// compiler knows the arrays may alias, so a loop of load-store pairs would wait out each load's latency in turn.
+__device__ __forceinline__ void move_particle(const GatherArgs &a, long long i, long long j) {
+    double v[13];
+#pragma unroll
+    for (int f = 0; f < 13; ++f)
+        if (f < a.nf) v[f] = a.s[f][i];
+    const uint8_t st = a.s_status[i];
+    const int64_t id = a.d_ids ? a.s_ids[i] : 0;
+#pragma unroll
+    for (int f = 0; f < 13; ++f)
+        if (f < a.nf) a.d[f][j] = v[f];
+    a.d_status[j] = st;
+    if (a.d_ids) a.d_ids[j] = id;
+}
+
 __global__ void __launch_bounds__(kBlock) k_gather(const __grid_constant__ GatherArgs a, const int32_t *perm) {
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= a.n) return;
-    const int32_t i = perm[j];
-    a.d_status[j] = a.s_status[i];
-    for (int f = 0; f < a.nf; ++f) a.d[f][j] = a.s[f][i];
-    if (a.d_ids) a.d_ids[j] = a.s_ids[i];
+    move_particle(a, perm[j], j);
 }
 
 int shift_for(int n, int extra) {
@@ -150,20 +163,14 @@ __global__ void __launch_bounds__(kBlock) k_segment_take(const __grid_constant__
                                                          const int32_t *slot) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= a.n) return;
-    const int32_t i = slot[perm[q]];
-    a.d_status[q] = a.s_status[i];
-    for (int f = 0; f < a.nf; ++f) a.d[f][q] = a.s[f][i];
-    if (a.d_ids) a.d_ids[q] = a.s_ids[i];
+    move_particle(a, slot[perm[q]], q);
 }
 
 // arena[slot[q]] <- scratch[q]
 __global__ void __launch_bounds__(kBlock) k_segment_put(const __grid_constant__ GatherArgs a, const int32_t *slot) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= a.n) return;
-    const int32_t i = slot[q];
-    a.d_status[i] = a.s_status[q];
-    for (int f = 0; f < a.nf; ++f) a.d[f][i] = a.s[f][q];
-    if (a.d_ids) a.d_ids[i] = a.s_ids[q];
+    move_particle(a, q, slot[q]);
 }
 
 // bucket_bounds[s * (nb + 1) + b]: storage index of segment s's first particle

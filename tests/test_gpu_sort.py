@@ -126,10 +126,11 @@ def _particles_with_keys(n, shape, seed):
     return P, host_keys(st, z, y, x, shape)
 
 
-@pytest.mark.parametrize("n", [1, 2, 4095, 4096, 4097, 100_003, 4_194_304 + 17])
+@pytest.mark.parametrize("n", [1, 2, 2047, 2048, 2049, 4095, 4096, 4097, 100_003, 4_194_304 + 17])
 def test_sort_permutation_is_the_stable_key_order(n):
     """The radix sort's permutation is exactly the stable order of the keys (numpy's stable argsort of the
-    host keys), for counts below, at and across the 4096-key tiles of its passes."""
+    host keys), for counts below, at and across the 2048-key tiles of its passes, and with more tiles than
+    one chunk of its per-digit scan (1024 tiles)."""
     import torch
 
     from offline_particles_b200 import _lib
