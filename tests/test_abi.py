@@ -206,7 +206,7 @@ int main(void) {
     C(OPB_ABI_VERSION); C(OPB_MAX_SLOTS); C(OPB_F64); C(OPB_F32); C(OPB_BF16); C(OPB_F16); C(OPB_F64_PAIRS);
     C(OPB_F32_PAIRS); C(OPB_F32_QUADS); C(OPB_F64_XPAIRS); C(OPB_F32_OCTS); C(OPB_F64_YXPAIRS);
     C(OPB_INLINE_TABLE); C(OPB_EINVAL); C(OPB_ECUDA); C(OPB_F32_ZETA_H); C(OPB_F64_IN_ZETA); C(OPB_F64_DX_DY);
-    C(OPB_F64_IN_DX);
+    C(OPB_F64_IN_DX); C(OPB_NOALLOC_MAX_PARTICLES); C(OPB_NOALLOC_SORT_TEMP_BYTES); C(OPB_NOALLOC_SCRATCH_BYTES);
     return 0;
 }
 """
@@ -226,7 +226,39 @@ def test_header_constants_match_the_binding(tmp_path):
           "OPB_INLINE_TABLE": _lib.INLINE_TABLE, "OPB_EINVAL": _lib.EINVAL, "OPB_ECUDA": _lib.ECUDA,
           "OPB_F32_ZETA_H": _lib.F32_ZETA_H, "OPB_F64_IN_ZETA": _lib.F64_IN_ZETA, "OPB_F64_DX_DY": _lib.F64_DX_DY,
           "OPB_F64_IN_DX": _lib.F64_IN_DX}
+    noalloc = {k: c.pop(k) for k in ("OPB_NOALLOC_MAX_PARTICLES", "OPB_NOALLOC_SORT_TEMP_BYTES",
+                                     "OPB_NOALLOC_SCRATCH_BYTES")}
     assert c == py
+    # the static scratch of opb_sort_particles_noalloc: two key buffers and one id buffer of the maximum count,
+    # then the radix passes' tile counts, which fit its temporary part at the maximum count
+    assert noalloc["OPB_NOALLOC_MAX_PARTICLES"] == _lib.NOALLOC_MAX_PARTICLES
+    assert noalloc["OPB_NOALLOC_SCRATCH_BYTES"] == 12 * _lib.NOALLOC_MAX_PARTICLES + noalloc["OPB_NOALLOC_SORT_TEMP_BYTES"]
+    assert _radix_temp(_lib.NOALLOC_MAX_PARTICLES, 2048) <= noalloc["OPB_NOALLOC_SORT_TEMP_BYTES"]
+
+
+def _a256(b: int) -> int:
+    return (b + 255) // 256 * 256
+
+
+def _radix_temp(n: int, tile: int) -> int:
+    """Scratch of the radix sort for n keys: 256 tile counts per tile of `tile` keys and 256 digit totals."""
+    return _a256(256 * -(-n // tile) * 4) + _a256(256 * 4)
+
+
+def test_sort_workspace_sizes_need_no_gpu():
+    """The sort workspaces are sized on the host, with no device query: for opb_sort_particles three 4-byte
+    arrays of n entries (keys in and out, the intermediate ids) and the radix scratch of 2048-key tiles; for
+    opb_sort_segments the 64-bit keys, ids, slots, segment table, staged particle state and the radix scratch.
+    Every piece starts on a 256-byte boundary."""
+    lib = _lib.load()
+    assert lib.opb_sort_workspace_bytes(0) == 0
+    for n in (1, 2047, 2048, 2049, 1 << 20, 4_194_304, 45_728_029):
+        assert lib.opb_sort_workspace_bytes(n) == 3 * _a256(4 * n) + _radix_temp(n, 2048), n
+    assert lib.opb_sort_segments_workspace_bytes(0, 3) == 0
+    for m, nseg in ((1, 1), (50_000, 3), (45_728_029, 256)):
+        want = (2 * _a256(8 * m) + 3 * _a256(4 * m) + _a256(16 * nseg) + _a256(m) + _a256(8 * 13 * m) + _a256(8 * m)
+                + _radix_temp(m, 2048))
+        assert lib.opb_sort_segments_workspace_bytes(m, nseg) == want, (m, nseg)
 
 
 def test_integration_stub_matches_the_binding():
